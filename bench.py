@@ -1,0 +1,334 @@
+#!/usr/bin/env python
+"""Benchmark of the B200 p-dit QAP solver: swap proposals per second.
+
+Workload (one instance per GPU, weak scaling over GPUs): n = 256, flow a symmetric
+Bernoulli(0.36) 0/1 matrix, distance the squared Euclidean distance on a 16 x 16 integer grid
+plus a symmetric uniform [0, 3] perturbation (seeded synthetic stand-in for the published
+single-instance workload), 64 replicas on one geometric beta ladder, replica exchange every
+4 sweeps (the reference's NUMITERA default), 10^4 sweeps = 100 steps of 100 sweeps.
+
+A "step" is 25 mega-iterations = 100 sweeps of all 64 replicas.  Proposals are counted as
+the published metric defines them: n (n - 1) / 2 per sweep per replica.
+
+  value       device-timed throughput with the instance resident in HBM (CUDA events on
+              the solver's stream, L2 flushed between steps, max over ranks)
+  e2e         the same work through the C ABI (pimqap_solve) from pinned host buffers:
+              upload, set-up, all sweeps and the read-back of the result, host wall clock
+  roofline    the sweep kernel against shared-memory read-modify-write bandwidth measured on
+              this GPU (the force matrices are resident in shared memory), plus its HBM traffic
+  cpu_baseline  the reference's own CPU_PIM.cpp (built from its source, oracle/_ref) on the
+              host cores, one parallel-tempering group per thread
+
+--impl reference times the reference's CPU implementation alone (rank 0 only).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import re
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+PKG = os.path.join(ROOT, "p-dit-probabilistic-ising-machine-for-solving-the-quadratic-assignment-problem_b200")
+sys.path.insert(0, PKG)
+
+import instances  # noqa: E402
+
+N = 256
+REPLICAS = 64
+GROUPS = 1
+SWEEPS_PER_EXCHANGE = 4
+MEGAITERS_PER_STEP = 25
+# Geometric ladder: beta_max in the reference's -b units (natural), ratio between neighbours.
+BETA_MAX = 0.05
+BETA_RATIO = 1.104
+METRIC = "swap proposals/sec"
+UNIT = "proposals/s"
+L2_FLUSH_BYTES = 256 << 20
+
+
+def proposals(replicas: int, sweeps: int, n: int = N) -> float:
+    return float(replicas) * sweeps * n * (n - 1) / 2.0
+
+
+# ------------------------------------------------------------------ clocks
+
+REASON_BITS = {0x1: "gpu_idle", 0x2: "applications_clocks_setting", 0x4: "sw_power_cap",
+               0x8: "hw_slowdown", 0x10: "sync_boost", 0x20: "sw_thermal_slowdown",
+               0x40: "hw_thermal_slowdown", 0x80: "hw_power_brake_slowdown",
+               0x100: "display_clock_setting"}
+
+
+class ClockSampler:
+    """nvidia-smi samples of SM clock and throttle reasons during the timed region."""
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        cmd = ["nvidia-smi", "-i", str(self.device),
+               "--query-gpu=clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active",
+               "--format=csv,noheader,nounits", "-lms", "200"]
+        try:
+            self.proc = subprocess.Popen(cmd, stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        sm, smax, reasons = [], [], set()
+        for line in self.lines:
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 4:
+                continue
+            try:
+                sm.append(float(parts[0]))
+                smax.append(float(parts[1]))
+                bits = int(parts[3], 16)
+            except ValueError:
+                continue
+            for b, name in REASON_BITS.items():
+                if bits & b and name != "gpu_idle":
+                    reasons.add(name)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(smax), "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+# ------------------------------------------------------------------ reference CPU timing
+
+def ref_cpu_throughput(F, D, budget_s: float, replicas: int = REPLICAS):
+    """The reference's threadToRun on one thread per host core for ~budget_s seconds.
+    Returns (proposals/s, cores, kind, sample description) or None."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    from oracle import RefHarness, ref_available
+    if not ref_available("big_mt"):
+        return None
+    ref = RefHarness("big_mt")
+    cores = max(1, min(os.cpu_count() or 1, ref.maxt))
+    ref.load(F, D)
+    ref.setup_replicated(cores, replicas, SWEEPS_PER_EXCHANGE, BETA_MAX * 1.44269504089, BETA_RATIO, 1)
+    t1 = ref.run(1)
+    m = max(1, int(budget_s / max(t1, 1e-3)))
+    el = ref.run(m)
+    sweeps = m * SWEEPS_PER_EXCHANGE
+    val = proposals(cores * replicas, sweeps) / el
+    sample = (f"{cores} threads x {replicas} replicas of the n=256 instance, {sweeps} sweeps each "
+              f"({m} mega-iterations of 4 sweeps), {el:.1f} s")
+    return val, cores, "reference", sample
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    from oracle import RefHarness, ref_available
+    cfg = {"workload": "grid256 n=256, 64 replicas, exchange every 4 sweeps", "n": N,
+           "replicas": REPLICAS, "sweeps_per_exchange": SWEEPS_PER_EXCHANGE}
+    if not ref_available("big_mt"):
+        print(json.dumps({"impl": "reference", "unavailable": "reference CPU_PIM.cpp not built (oracle/_ref missing)"}))
+        return
+    inst = instances.grid256(1000)
+    ref = RefHarness("big_mt")
+    cores = max(1, min(os.cpu_count() or 1, ref.maxt))
+    ref.load(inst.F, inst.D)
+    ref.setup_replicated(cores, REPLICAS, SWEEPS_PER_EXCHANGE, BETA_MAX * 1.44269504089, BETA_RATIO, 1)
+    t1 = ref.run(1)
+    # each step a bounded sample: the whole run stays within ~3 minutes
+    per_step = min(2.0, 180.0 / max(1, args.steps + args.warmup))
+    m = max(1, int(per_step / max(t1, 1e-3)))
+    for _ in range(args.warmup):
+        ref.run(m)
+    total = 0.0
+    for _ in range(args.steps):
+        total += ref.run(m)
+    sweeps = args.steps * m * SWEEPS_PER_EXCHANGE
+    val = proposals(cores * REPLICAS, sweeps) / total
+    sample = (f"each step {m} mega-iterations (4 sweeps each) of {cores} groups x {REPLICAS} replicas "
+              f"of the n=256 instance; one group per host thread")
+    line = {"impl": "reference", "metric": METRIC, "value": val, "unit": UNIT, "n_gpus": 0,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * total / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int32",
+            "data": "synthetic (seeded grid256 instance)", "config": cfg,
+            "cpu_baseline": {"value": val, "unit": UNIT, "cores": cores, "kind": "reference", "sample": sample},
+            "e2e": {"value": val, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+
+
+# ------------------------------------------------------------------ our arm
+
+def read_traffic():
+    """dram bytes per launch of the sweep kernel from the committed ncu summary, or None."""
+    path = os.path.join(ROOT, "profiles", "epoch_kernel_grid256.md")
+    if not os.path.exists(path):
+        return None
+    m = re.search(r"dram_bytes_per_launch:\s*([0-9.eE+]+)", open(path).read())
+    return float(m.group(1)) if m else None
+
+
+def run_ours(args):
+    import torch
+    import torch.distributed as dist
+    import pimqap
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world != args.gpus and "WORLD_SIZE" in os.environ:
+        raise SystemExit(f"--gpus {args.gpus} but WORLD_SIZE={world}")
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+
+    inst = instances.grid256(1000 + rank)
+    params = pimqap.default_params(replicas=REPLICAS, groups=GROUPS, sweeps_per_exchange=SWEEPS_PER_EXCHANGE,
+                                   beta_max=BETA_MAX, beta_ratio=BETA_RATIO, seed=1 + rank,
+                                   device=local, megaiters_per_launch=MEGAITERS_PER_STEP,
+                                   max_megaiters=2 ** 31 - 1)
+    flush = torch.empty(L2_FLUSH_BYTES, dtype=torch.uint8, device=f"cuda:{local}")
+    solver = pimqap.Solver(inst.F, inst.D, params)
+    for _ in range(args.warmup):
+        solver.run(MEGAITERS_PER_STEP)
+    r0 = solver.result()
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    ms_total = 0.0
+    with ClockSampler(local) as clocks:
+        barrier()
+        torch.cuda.synchronize()
+        w0 = time.perf_counter()
+        for _ in range(args.steps):
+            flush.zero_()
+            torch.cuda.synchronize()
+            ms_total += solver.run(MEGAITERS_PER_STEP)
+        torch.cuda.synchronize()
+        barrier()
+        wall = time.perf_counter() - w0
+    r1 = solver.result()
+    solver.close()
+    t = torch.tensor([ms_total], dtype=torch.float64, device=f"cuda:{local}")
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    ms_max = float(t.item())
+    sweeps = args.steps * MEGAITERS_PER_STEP * SWEEPS_PER_EXCHANGE
+    reps = REPLICAS * GROUPS
+    value = proposals(reps, sweeps) * world / (ms_max * 1e-3)
+
+    # roofline of the sweep kernel (every timed launch is that kernel)
+    accepts = r1["accepts"] - r0["accepts"]
+    cand = float(reps) * sweeps * N * N
+    s = r1["force_bits"] // 8
+    alg_bytes = (3 * s + 20) * cand + (2 * N * N * s + 32 * N) * float(accepts)
+    launches = args.steps * MEGAITERS_PER_STEP
+    achieved = alg_bytes / (ms_total * 1e-3) / 1e9
+    smem_peak = pimqap.probe_smem_bandwidth(local)
+    traffic = read_traffic()
+
+    # e2e through the C ABI from pinned host buffers
+    Fp = torch.from_numpy(inst.F).pin_memory()
+    Dp = torch.from_numpy(inst.D).pin_memory()
+    p2 = pimqap.default_params(replicas=REPLICAS, groups=GROUPS, sweeps_per_exchange=SWEEPS_PER_EXCHANGE,
+                               beta_max=BETA_MAX, beta_ratio=BETA_RATIO, seed=1 + rank, device=local,
+                               megaiters_per_launch=MEGAITERS_PER_STEP,
+                               max_megaiters=args.steps * MEGAITERS_PER_STEP)
+    barrier()
+    e0 = time.perf_counter()
+    res = pimqap.solve(Fp.numpy(), Dp.numpy(), p2)
+    e_wall = time.perf_counter() - e0
+    te = torch.tensor([e_wall], dtype=torch.float64, device=f"cuda:{local}")
+    if world > 1:
+        dist.all_reduce(te, op=dist.ReduceOp.MAX)
+    e2e_value = proposals(reps, sweeps) * world / float(te.item())
+
+    line = None
+    if rank == 0:
+        cpu = None
+        if world == 1 and not args.no_cpu_baseline:
+            got = ref_cpu_throughput(inst.F, inst.D, budget_s=12.0)
+            if got:
+                v, cores, kind, sample = got
+                cpu = {"value": v, "unit": UNIT, "cores": cores, "kind": kind, "sample": sample}
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": f"int{8 * s}",
+            "data": "synthetic (seeded grid256 instance per GPU)",
+            "config": {"workload": "grid256: n=256 Bernoulli(0.36) flow, 16x16 grid sq. distance + U[0,3]; "
+                                   "64 replicas, geometric beta ladder, exchange every 4 sweeps, "
+                                   "10^4 sweeps = 100 steps",
+                       "n": N, "replicas": reps, "sweeps_per_step": MEGAITERS_PER_STEP * SWEEPS_PER_EXCHANGE,
+                       "beta_max": BETA_MAX, "beta_ratio": BETA_RATIO, "parallelism": f"instances x{world}",
+                       "cluster_size": r1["cluster_size"], "force_bits": r1["force_bits"],
+                       "l2": "flushed between steps (256 MiB write)"},
+            "candidate_deltas_per_s": cand * world / (ms_max * 1e-3),
+            "accept_rate": accepts / (reps * sweeps * N),
+            "best_energy": r1["best_energy"],
+            "gpu_launches": launches,
+            "wall_s_timed_region": wall,
+            "roofline": {"bound": "smem", "achieved": achieved, "peak": smem_peak, "unit": "GB/s",
+                         "frac": achieved / smem_peak,
+                         "peak_source": "measured on this GPU by pimqap_probe_smem_bandwidth (shared-memory "
+                                        "read-modify-write, 128-bit, 2 CTAs/SM)",
+                         "traffic": traffic,
+                         "alg_bytes_per_launch": alg_bytes / launches,
+                         "bytes_model": f"({3 * s}+20) B per candidate delta + (2 n^2 {s} + 32 n) B per accept"},
+            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": res["h2d_bytes"],
+                    "d2h_bytes_per_step": res["d2h_bytes"], "wall_s": e_wall,
+                    "note": "one step = one pimqap_solve of the whole workload (upload, set-up, sweeps, result)"},
+            "clocks": clocks.summary(),
+            "cpu_baseline": cpu,
+        }
+        print(json.dumps(line))
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    return line
+
+
+def main():
+    ap = argparse.ArgumentParser(description=__doc__.split("\n")[0])
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=100)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        ap.error("--warmup must be >= 3")
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

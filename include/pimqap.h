@@ -1,0 +1,173 @@
+/*
+ * pimqap.h - C ABI of the B200 parallel-tempering p-dit QAP solver.
+ *
+ * The solver is a drop-in for the reference's CPU_PIM path (CPU-PIM/CPU_PIM.cpp): the same
+ * instance file, the same replica / temperature / sweep parameters and the same outputs.
+ * The reference has no library interface: its path is the CLI main() over global arrays
+ * with compile-time capacities.  Each entry point below names the reference function or
+ * block it replaces.
+ *
+ * Conventions
+ *   - Every function returns a pimqap_status (0 = OK).  No exception crosses the ABI.
+ *     pimqap_last_error() gives the message of the calling thread's last failure.
+ *   - All pointers are caller-owned host memory unless stated otherwise; the solver copies
+ *     what it needs.  Device memory is owned by the solver / server handles.
+ *   - A solver handle is used by one host thread at a time.  A server handle is locked
+ *     internally and may be used from several threads.
+ *   - Energies and costs are exact int64.  The force matrix is int32 when a bound computed
+ *     from the instance proves every value fits, else int64 (or as forced by params).
+ *   - Random words come from a counter-based Philox4x32-10 stream keyed by params.seed, so a
+ *     run is a pure function of (instance, params) and does not depend on what else runs on
+ *     the GPU.
+ */
+#ifndef PIMQAP_H
+#define PIMQAP_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define PIMQAP_MAX_N 256          /* reference: MAXN = 160 (CPU_PIM.cpp:16) */
+#define PIMQAP_MAX_REPLICAS 64    /* reference: MAXNUMREPLICAS = 10 (CPU_PIM.cpp:23) */
+#define PIMQAP_MAX_GROUPS 1024    /* reference: MAXNUMTHREADS = 20 (CPU_PIM.cpp:26) */
+/* "No best energy yet": the reference's INT_MAX sentinel (CPU_PIM.cpp:123, :129). */
+#define PIMQAP_NO_BEST ((int64_t)2147483647)
+
+typedef enum pimqap_status {
+    PIMQAP_OK = 0,
+    PIMQAP_ERR_ARG = 1,        /* invalid argument (n, replicas, groups, beta, ...) */
+    PIMQAP_ERR_IO = 2,         /* instance file missing or malformed */
+    PIMQAP_ERR_CUDA = 3,       /* CUDA runtime failure (message has the CUDA error) */
+    PIMQAP_ERR_NO_DEVICE = 4,  /* no sm_100 device, or the kernels are not loadable */
+    PIMQAP_ERR_RANGE = 5,      /* instance values overflow the int64 bound */
+    PIMQAP_ERR_DEVICE = 6,     /* a device-side check failed (error word set) */
+    PIMQAP_ERR_BUSY = 7,       /* server queue full / memory budget exhausted */
+    PIMQAP_ERR_NOT_READY = 8,  /* server ticket not finished yet */
+} pimqap_status;
+
+/* One QAP instance.  flow is F (n x n, facility x facility) and dist is D (n x n, location
+   x location), both row-major int32, in the order the reference's file lists them
+   (CPU_PIM.cpp:94-103). */
+typedef struct pimqap_instance {
+    int32_t n;
+    const int32_t *flow;
+    const int32_t *dist;
+} pimqap_instance;
+
+/* Solve parameters; the CLI flag of the reference is given for each field
+   (CPU_PIM.cpp:478-610). */
+typedef struct pimqap_params {
+    int32_t replicas;            /* -r  replicas per group (NUMREPLICAS) */
+    int32_t groups;              /* -t  independent parallel-tempering groups (NUMTHREADS) */
+    int32_t sweeps_per_exchange; /* -i  sweeps between replica exchanges (NUMITERA, default 4) */
+    int32_t rank_slots;          /* the reference's compiled MAXNUMREPLICAS, which places the
+                                    forced extreme swap (CPU_PIM.cpp:340); 0 = max(replicas, 10) */
+    int64_t max_megaiters;       /* -w  mega-iterations (exchange + sweeps_per_exchange sweeps) */
+    double beta_max;             /* -b  largest beta in natural units (stored x 1/ln2, :528) */
+    double beta_ratio;           /* -m  divisive step between adjacent betas (deltaBeta) */
+    int64_t goal;                /* -g  stop once the best energy is <= goal */
+    double timeout_s;            /* -s  stop after this many seconds (0 = none) */
+    uint64_t seed;               /* Philox key */
+    int32_t force_bits;          /* 0 = choose from the instance bound, 32 or 64 = force */
+    int32_t device;              /* CUDA device ordinal */
+    int32_t megaiters_per_launch;/* mega-iterations per CUDA-graph launch (0 = automatic) */
+    int32_t threads_per_block;   /* 0 = automatic, else 64, 128 or 256 */
+} pimqap_params;
+
+/* Fills p with the reference's defaults: 10 replicas, 20 groups, 4 sweeps per exchange,
+   beta_ratio 1.2 (CPU_PIM.cpp:19-31), no goal, no timeout, seed 1, automatic shapes. */
+void pimqap_default_params(pimqap_params *p);
+
+typedef struct pimqap_result {
+    int64_t best_energy;        /* best energy of any visited state (PIMQAP_NO_BEST if none) */
+    int32_t *best_perm;         /* caller-provided, n entries (may be NULL): facility at each
+                                   location for best_energy */
+    int64_t target_megaiter;    /* mega-iteration whose tracking first saw best <= goal, or -1 */
+    double time_to_target_ms;   /* device time from the first sweep to that tracking, or -1 */
+    int64_t megaiters_done;     /* mega-iterations completed */
+    int64_t updates;            /* p-dit updates over all replicas */
+    int64_t accepts;            /* accepted swaps over all replicas */
+    double device_ms;           /* device time of the sweep launches */
+    double wall_ms;             /* host wall time of the whole call */
+    int32_t force_bits;         /* 32 or 64: the force-matrix width used */
+    int32_t cluster_size;       /* CTAs per replica (1, 2 or 4) */
+    int32_t stopped_by;         /* 0 = max_megaiters, 1 = goal, 2 = timeout */
+    int64_t h2d_bytes;          /* host-to-device bytes copied by the solver so far */
+    int64_t d2h_bytes;          /* device-to-host bytes copied by the solver so far */
+} pimqap_result;
+
+/* ---------------------------------------------------------------- instance I/O */
+
+/* Reads a reference instance file (replaces readProblem, CPU_PIM.cpp:79-107): n, then F,
+   then D, whitespace separated.  Call with flow = dist = NULL to get n; then with arrays
+   of n*n entries.  n > max_n is rejected like the reference's MAXN check (:88-92). */
+pimqap_status pimqap_read_problem(const char *path, int32_t max_n, int32_t *n,
+                                  int32_t *flow, int32_t *dist);
+
+/* ---------------------------------------------------------------- one-shot solve */
+
+/* The whole CPU_PIM run with fixed beta parameters (replaces setup() + the threadToRun
+   loop, CPU_PIM.cpp:109-364 and :636-684): uploads the instance, builds the replicas,
+   runs max_megaiters mega-iterations (or until goal / timeout) on the GPU and returns the
+   best energy and permutation. */
+pimqap_status pimqap_solve(const pimqap_instance *inst, const pimqap_params *params,
+                           pimqap_result *result);
+
+/* ---------------------------------------------------------------- solver handle */
+
+typedef struct pimqap_solver pimqap_solver;
+
+/* setup() on the device (CPU_PIM.cpp:109-193): beta ladder, initial shuffle, force
+   matrices, energies, and the tracking/exchange step of mega-iteration 0. */
+pimqap_status pimqap_solver_create(const pimqap_instance *inst, const pimqap_params *params,
+                                   pimqap_solver **out);
+
+/* Runs megaiters more mega-iterations (threadToRun's loop body, CPU_PIM.cpp:293-362):
+   sweeps_per_exchange sweeps of every replica (doMegaItera, :195-290), then each group's
+   best tracking and replica exchange.  Stops early when the goal is reached.  If device_ms
+   is not NULL it receives the device time measured with CUDA events on the solver's stream.
+   Returns after the work completes. */
+pimqap_status pimqap_solver_run(pimqap_solver *s, int64_t megaiters, double *device_ms);
+
+/* Best energy, permutation and counters so far. */
+pimqap_status pimqap_solver_result(pimqap_solver *s, pimqap_result *result);
+
+/* Full state of replica l of group t, for parity checks against the reference's globals
+   facilityOfLocation / locationOfFacility / I / currentE / bestE / beta (CPU_PIM.cpp:44-62).
+   I (n*n, row-major) is returned widened to int64.  Any output pointer may be NULL. */
+pimqap_status pimqap_solver_replica(pimqap_solver *s, int32_t t, int32_t l, int32_t *phi,
+                                    int64_t *force, int64_t *energy, int64_t *best_energy,
+                                    double *beta);
+
+/* Exchange state of group t: indexOfBetaOrder (rank_slots entries), timeSinceSwap and
+   threadBestE (CPU_PIM.cpp:44, :52, :69). */
+pimqap_status pimqap_solver_group(pimqap_solver *s, int32_t t, int32_t *order,
+                                  int32_t *time_since_swap, int64_t *group_best);
+
+void pimqap_solver_destroy(pimqap_solver *s);
+
+/* ---------------------------------------------------------------- batched solve */
+
+/* Many independent instances of uneven n, each with its own replica set and parameters,
+   in one persistent launch (no reference counterpart: the reference solves one instance
+   per process).  results[k].best_perm must hold insts[k].n entries or be NULL.
+   Each result equals what pimqap_solve returns for that instance alone. */
+pimqap_status pimqap_batch_solve(const pimqap_instance *insts, const pimqap_params *params,
+                                 int32_t count, pimqap_result *results);
+
+/* ---------------------------------------------------------------- misc */
+
+/* Diagnostic with no reference counterpart: measures the shared-memory read-modify-write
+   bandwidth of the device (GB/s, reads + writes), the ceiling of the resident sweep. */
+pimqap_status pimqap_probe_smem_bandwidth(int32_t device, double *gbs);
+
+const char *pimqap_last_error(void);
+const char *pimqap_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,67 @@
+#!/usr/bin/env bash
+# Builds the reference CPU_PIM solver, from the reference's own source file where it lies,
+# into oracle/_ref/ (git-ignored).  TEST INFRASTRUCTURE ONLY: the outputs pin the oracle
+# restatement and time the reference's CPU code; the solver never links them.
+#
+# No copy of the reference source is written anywhere: the source is streamed through
+# sed (capacity constants only) into g++ together with ref_harness.cpp.
+#
+# Outputs:
+#   _ref/libref_stock.so   capacity constants unchanged (MAXN 160, 10 replicas, 20 threads),
+#                          Philox engine shim (ref_prelude.h)
+#   _ref/libref_big.so     MAXN 256, 64 replicas, 64 threads, Philox engine shim
+#   _ref/libref_big_mt.so  MAXN 256, 64 replicas, 256 threads, the reference's own
+#                          std::mt19937 (no shim): the timed CPU baseline
+#   _ref/cpu_pim_stock     the unmodified reference CLI (for output-format checks)
+#
+# The reference source path is $PIMQAP_REF_ROOT (default /root/reference).  When it is
+# absent the script does nothing and exits 0.
+set -euo pipefail
+
+REF_ROOT="${PIMQAP_REF_ROOT:-/root/reference}"
+SRC="$REF_ROOT/CPU-PIM/CPU_PIM.cpp"
+HERE="$(cd "$(dirname "$0")" && pwd)"
+OUT="$HERE/_ref"
+# The system g++ (libstdc++ linked dynamically, shared with the host process); $CXX may name
+# a wrapper that links libstdc++ statically, which breaks iostream facets under Python.
+CXX="${PIMQAP_REF_CXX:-/usr/bin/g++}"
+# x86-64-v3 (AVX2/FMA/BMI2): runs on the GPU hosts as well as on the build container.
+# Hidden visibility + -Bsymbolic: the reference's globals (N, I, D, F, beta, setup, ...) must
+# bind inside the library, not to same-named symbols of the host process.
+CXXFLAGS="-std=c++17 -O3 -march=x86-64-v3 -pthread -fPIC -w"
+LIBFLAGS="-fvisibility=hidden -Wl,-Bsymbolic"
+
+if [ ! -f "$SRC" ]; then
+    echo "build_ref.sh: $SRC not found, reference harness not built"
+    exit 0
+fi
+mkdir -p "$OUT"
+
+# Exactly one line must match each capacity constant, or the recipe fails.
+for pat in '^const int MAXN = 160;' '^const int MAXNUMREPLICAS = 10;' '^const int MAXNUMTHREADS = 20;'; do
+    c=$(grep -c "$pat" "$SRC" || true)
+    if [ "$c" != "1" ]; then
+        echo "build_ref.sh: pattern '$pat' matched $c lines in $SRC" >&2
+        exit 1
+    fi
+done
+
+patched() {  # maxn maxr maxt
+    sed -e "s/^const int MAXN = 160;/const int MAXN = $1;/" \
+        -e "s/^const int MAXNUMREPLICAS = 10;/const int MAXNUMREPLICAS = $2;/" \
+        -e "s/^const int MAXNUMTHREADS = 20;/const int MAXNUMTHREADS = $3;/" "$SRC"
+}
+
+build_lib() {  # out maxn maxr maxt extra-flags
+    local out="$1"; shift
+    local maxn="$1" maxr="$2" maxt="$3"; shift 3
+    { patched "$maxn" "$maxr" "$maxt"; cat "$HERE/ref_harness.cpp"; } |
+        $CXX $CXXFLAGS $LIBFLAGS "$@" -shared -include "$HERE/ref_prelude.h" -x c++ - -o "$OUT/$out.tmp"
+    mv "$OUT/$out.tmp" "$OUT/$out"
+}
+
+build_lib libref_stock.so 160 10 20
+build_lib libref_big.so 256 64 64
+build_lib libref_big_mt.so 256 64 256 -DPIMQAP_REF_NO_SHIM -mcmodel=medium
+$CXX $CXXFLAGS "$SRC" -o "$OUT/cpu_pim_stock.tmp" && mv "$OUT/cpu_pim_stock.tmp" "$OUT/cpu_pim_stock"
+echo "build_ref.sh: built $(ls "$OUT" | tr '\n' ' ')"

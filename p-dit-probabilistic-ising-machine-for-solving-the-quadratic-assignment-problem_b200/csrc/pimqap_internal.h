@@ -1,0 +1,67 @@
+// pimqap_internal.h - device-side layout of a solve, shared by the kernels and the host
+// runtime.  Not part of the C ABI.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstddef>
+#include <cstdint>
+
+namespace pimqap {
+
+constexpr int kMaxN = 256;
+constexpr int kMaxWarps = 8;           // kernels run with 64, 128 or 256 threads
+constexpr int32_t kNoStop = 0x7fffffff;
+constexpr int64_t kNoBest = 2147483647;  // the reference's INT_MAX sentinel
+
+// Device-side error word bits (SolveDev::error).
+enum : int32_t {
+    kErrBadPerm = 1,      // a permutation loaded from global memory is not a bijection
+    kErrShape = 2,        // launch shape does not match the solve
+};
+
+// Everything one solve (one instance, T groups x R replicas) keeps in device memory.
+// Arrays are indexed by replica slot rep = t * R + l or by group t.
+struct SolveDev {
+    int n, R, T, cap, spe;     // size, replicas/group, groups, rank slots, sweeps per epoch
+    int ldg;                   // row stride of I in global memory (elements, 16-byte rows)
+    int lds;                   // row stride of I in shared memory (elements)
+    int rpc;                   // rows of I per CTA (= ceil(n / cluster size))
+    int64_t goal;
+    uint64_t seed;
+    const int32_t *D, *DT, *F, *FT;  // n*n each, row-major (DT = D transposed)
+    const int32_t *Ddiag, *Fdiag;    // n each
+    void *I;                   // [T*R][n][ldg] of int32 or int64
+    int32_t *phi;              // [T*R][n]  facility at location
+    int32_t *best_phi;         // [T*R][n]  phi of the replica's best state
+    int64_t *E, *bestE;        // [T*R]
+    double *beta;              // [T*R]     by replica slot, swapped by the exchange
+    unsigned long long *accepts;   // [T*R]
+    int32_t *order;            // [T][cap]  indexOfBetaOrder
+    int32_t *tss;              // [T]       timeSinceSwap
+    int64_t *group_best;       // [T]       threadBestE
+    unsigned int *finish;      // [T]       replicas of the group done with this epoch
+    int32_t *epoch;            // [T]       mega-iterations completed by the group
+    int64_t *single_best;      // [1]       best over all groups (at tracking points)
+    int32_t *stop_epoch;       // [1]       first epoch that must not run (goal reached)
+    int64_t *target_epoch;     // [1]       mega-iteration whose tracking reached the goal
+    unsigned long long *target_ns;  // [1]  %globaltimer at that tracking
+    unsigned long long *start_ns;   // [1]  %globaltimer when sweeping started
+    int32_t *error;            // [1]       kErr* bits
+};
+
+// Shared memory of one CTA of the epoch kernel.
+size_t epoch_smem_bytes(int n, int rpc, int lds, int cluster, int bits);
+
+// One-time kernel attributes (dynamic shared memory, non-portable cluster size).
+cudaError_t prepare_kernels();
+
+// setup(): force matrices + energies of every replica from its phi, then the tracking /
+// exchange step of mega-iteration 0 (which also records start_ns).
+cudaError_t launch_setup(const SolveDev &s, int bits, cudaStream_t st);
+
+// One epoch: spe sweeps of every replica, then each group's tracking + exchange.
+cudaError_t launch_epoch(const SolveDev &s, int bits, int cluster, bool sym, int threads,
+                         size_t smem, cudaStream_t st);
+
+}  // namespace pimqap

@@ -1,0 +1,233 @@
+"""Python binding of the solver's C ABI (``include/pimqap.h``) over ctypes.
+
+The solver itself is ``csrc/libpimqap.so`` (host runtime + sm_100a kernels).  This module
+only marshals arguments; it has no compute path of its own, and every call fails loudly
+when the library is missing or has no usable GPU.
+
+Reference mapping (``CPU-PIM/CPU_PIM.cpp``): ``read_problem`` is readProblem() (:79-107),
+``Solver`` is setup() + the threadToRun() loop (:109-364), ``solve`` is main() (:612-684).
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from typing import List, Optional, Sequence
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "csrc", "libpimqap.so")
+
+OK = 0
+STATUS = {0: "OK", 1: "ERR_ARG", 2: "ERR_IO", 3: "ERR_CUDA", 4: "ERR_NO_DEVICE", 5: "ERR_RANGE",
+          6: "ERR_DEVICE", 7: "ERR_BUSY", 8: "ERR_NOT_READY"}
+NO_BEST = 2147483647
+MAX_N = 256
+MAX_REPLICAS = 64
+LN2_INV = 1.44269504089  # the reference's -b scaling (CPU_PIM.cpp:528)
+
+
+class PimqapError(RuntimeError):
+    def __init__(self, status: int, msg: str):
+        super().__init__(f"{STATUS.get(status, status)}: {msg}")
+        self.status = status
+
+
+class Instance(C.Structure):
+    _fields_ = [("n", C.c_int32), ("flow", C.POINTER(C.c_int32)), ("dist", C.POINTER(C.c_int32))]
+
+
+class Params(C.Structure):
+    _fields_ = [
+        ("replicas", C.c_int32), ("groups", C.c_int32), ("sweeps_per_exchange", C.c_int32),
+        ("rank_slots", C.c_int32), ("max_megaiters", C.c_int64), ("beta_max", C.c_double),
+        ("beta_ratio", C.c_double), ("goal", C.c_int64), ("timeout_s", C.c_double),
+        ("seed", C.c_uint64), ("force_bits", C.c_int32), ("device", C.c_int32),
+        ("megaiters_per_launch", C.c_int32), ("threads_per_block", C.c_int32),
+    ]
+
+
+class Result(C.Structure):
+    _fields_ = [
+        ("best_energy", C.c_int64), ("best_perm", C.POINTER(C.c_int32)),
+        ("target_megaiter", C.c_int64), ("time_to_target_ms", C.c_double),
+        ("megaiters_done", C.c_int64), ("updates", C.c_int64), ("accepts", C.c_int64),
+        ("device_ms", C.c_double), ("wall_ms", C.c_double), ("force_bits", C.c_int32),
+        ("cluster_size", C.c_int32), ("stopped_by", C.c_int32),
+        ("h2d_bytes", C.c_int64), ("d2h_bytes", C.c_int64),
+    ]
+
+
+_lib = None
+
+
+def lib() -> C.CDLL:
+    """Loads csrc/libpimqap.so (raises if it has not been built)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise FileNotFoundError(f"{LIB_PATH} is not built (run make -C csrc or __graft_entry__.build())")
+    L = C.CDLL(LIB_PATH)
+    st = C.c_int
+    L.pimqap_default_params.argtypes = [C.POINTER(Params)]
+    L.pimqap_default_params.restype = None
+    L.pimqap_last_error.restype = C.c_char_p
+    L.pimqap_version.restype = C.c_char_p
+    L.pimqap_read_problem.argtypes = [C.c_char_p, C.c_int32, C.POINTER(C.c_int32), C.c_void_p, C.c_void_p]
+    L.pimqap_read_problem.restype = st
+    L.pimqap_solve.argtypes = [C.POINTER(Instance), C.POINTER(Params), C.POINTER(Result)]
+    L.pimqap_solve.restype = st
+    L.pimqap_solver_create.argtypes = [C.POINTER(Instance), C.POINTER(Params), C.POINTER(C.c_void_p)]
+    L.pimqap_solver_create.restype = st
+    L.pimqap_solver_run.argtypes = [C.c_void_p, C.c_int64, C.POINTER(C.c_double)]
+    L.pimqap_solver_run.restype = st
+    L.pimqap_solver_result.argtypes = [C.c_void_p, C.POINTER(Result)]
+    L.pimqap_solver_result.restype = st
+    L.pimqap_solver_replica.argtypes = [C.c_void_p, C.c_int32, C.c_int32, C.c_void_p, C.c_void_p,
+                                        C.c_void_p, C.c_void_p, C.c_void_p]
+    L.pimqap_solver_replica.restype = st
+    L.pimqap_solver_group.argtypes = [C.c_void_p, C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p]
+    L.pimqap_solver_group.restype = st
+    L.pimqap_solver_destroy.argtypes = [C.c_void_p]
+    L.pimqap_solver_destroy.restype = None
+    L.pimqap_batch_solve.argtypes = [C.POINTER(Instance), C.POINTER(Params), C.c_int32, C.POINTER(Result)]
+    L.pimqap_batch_solve.restype = st
+    L.pimqap_probe_smem_bandwidth.argtypes = [C.c_int32, C.POINTER(C.c_double)]
+    L.pimqap_probe_smem_bandwidth.restype = st
+    _lib = L
+    return L
+
+
+def _check(status: int) -> None:
+    if status != OK:
+        raise PimqapError(status, lib().pimqap_last_error().decode(errors="replace"))
+
+
+def default_params(**kw) -> Params:
+    p = Params()
+    lib().pimqap_default_params(C.byref(p))
+    for k, v in kw.items():
+        if not hasattr(p, k):
+            raise AttributeError(k)
+        setattr(p, k, v)
+    return p
+
+
+class _Inst:
+    """Keeps the numpy buffers of a pimqap_instance alive."""
+
+    def __init__(self, F: np.ndarray, D: np.ndarray):
+        self.F = np.ascontiguousarray(F, dtype=np.int32)
+        self.D = np.ascontiguousarray(D, dtype=np.int32)
+        n = self.F.shape[0]
+        if self.F.shape != (n, n) or self.D.shape != (n, n):
+            raise ValueError("flow and dist must be n x n")
+        self.c = Instance(n, self.F.ctypes.data_as(C.POINTER(C.c_int32)),
+                          self.D.ctypes.data_as(C.POINTER(C.c_int32)))
+
+
+def read_problem(path: str, max_n: int = MAX_N):
+    """The reference's file reader: returns (F, D) as int32 arrays."""
+    n = C.c_int32(0)
+    _check(lib().pimqap_read_problem(path.encode(), max_n, C.byref(n), None, None))
+    F = np.zeros((n.value, n.value), np.int32)
+    D = np.zeros((n.value, n.value), np.int32)
+    _check(lib().pimqap_read_problem(path.encode(), max_n, C.byref(n), F.ctypes.data, D.ctypes.data))
+    return F, D
+
+
+def _result_dict(r: Result, perm: Optional[np.ndarray]) -> dict:
+    d = {k: getattr(r, k) for k, _ in Result._fields_ if k != "best_perm"}
+    d["best_perm"] = perm
+    return d
+
+
+def solve(F: np.ndarray, D: np.ndarray, params: Params) -> dict:
+    inst = _Inst(F, D)
+    perm = np.zeros(inst.F.shape[0], np.int32)
+    r = Result()
+    r.best_perm = perm.ctypes.data_as(C.POINTER(C.c_int32))
+    _check(lib().pimqap_solve(C.byref(inst.c), C.byref(params), C.byref(r)))
+    return _result_dict(r, perm)
+
+
+def batch_solve(instances: Sequence, params: Sequence[Params]) -> List[dict]:
+    """instances: sequence of (F, D); params: one Params per instance."""
+    keep = [_Inst(F, D) for F, D in instances]
+    count = len(keep)
+    insts = (Instance * count)(*[k.c for k in keep])
+    ps = (Params * count)(*params)
+    perms = [np.zeros(k.F.shape[0], np.int32) for k in keep]
+    rs = (Result * count)()
+    for r, p in zip(rs, perms):
+        r.best_perm = p.ctypes.data_as(C.POINTER(C.c_int32))
+    _check(lib().pimqap_batch_solve(insts, ps, count, rs))
+    return [_result_dict(r, p) for r, p in zip(rs, perms)]
+
+
+def probe_smem_bandwidth(device: int = 0) -> float:
+    """Measured shared-memory read-modify-write bandwidth of the device, GB/s."""
+    v = C.c_double(0)
+    _check(lib().pimqap_probe_smem_bandwidth(device, C.byref(v)))
+    return v.value
+
+
+class Solver:
+    """A solver handle: setup() on construction, then run() mega-iterations at a time."""
+
+    def __init__(self, F: np.ndarray, D: np.ndarray, params: Params):
+        self._inst = _Inst(F, D)
+        self.params = params
+        self.n = self._inst.F.shape[0]
+        h = C.c_void_p()
+        _check(lib().pimqap_solver_create(C.byref(self._inst.c), C.byref(params), C.byref(h)))
+        self.h = h
+
+    def run(self, megaiters: int) -> float:
+        """Runs megaiters mega-iterations; returns their device time in ms."""
+        ms = C.c_double(0)
+        _check(lib().pimqap_solver_run(self.h, megaiters, C.byref(ms)))
+        return ms.value
+
+    def result(self) -> dict:
+        perm = np.zeros(self.n, np.int32)
+        r = Result()
+        r.best_perm = perm.ctypes.data_as(C.POINTER(C.c_int32))
+        _check(lib().pimqap_solver_result(self.h, C.byref(r)))
+        return _result_dict(r, perm)
+
+    def replica(self, t: int, l: int) -> dict:
+        n = self.n
+        phi = np.zeros(n, np.int32)
+        I = np.zeros((n, n), np.int64)
+        E = np.zeros(1, np.int64)
+        bE = np.zeros(1, np.int64)
+        b = np.zeros(1, np.float64)
+        _check(lib().pimqap_solver_replica(self.h, t, l, phi.ctypes.data, I.ctypes.data,
+                                           E.ctypes.data, bE.ctypes.data, b.ctypes.data))
+        return dict(phi=phi, I=I, E=int(E[0]), bestE=int(bE[0]), beta=float(b[0]))
+
+    def group(self, t: int, rank_slots: int) -> dict:
+        order = np.zeros(rank_slots, np.int32)
+        tss = np.zeros(1, np.int32)
+        gb = np.zeros(1, np.int64)
+        _check(lib().pimqap_solver_group(self.h, t, order.ctypes.data, tss.ctypes.data, gb.ctypes.data))
+        return dict(order=order, time_since_swap=int(tss[0]), group_best=int(gb[0]))
+
+    def close(self) -> None:
+        if getattr(self, "h", None):
+            lib().pimqap_solver_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()

@@ -1,0 +1,85 @@
+"""The C ABI library loads, exports every declared entry point, and validates arguments and
+files without touching a GPU (CPU only)."""
+import ctypes as C
+import os
+import re
+import subprocess
+
+import numpy as np
+import pytest
+
+import instances
+import pimqap
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+HEADER = os.path.join(ROOT, "include", "pimqap.h")
+
+
+def declared_functions():
+    text = open(HEADER).read()
+    return sorted(set(re.findall(r"^[A-Za-z_][\w ]*?\**\s*\**(pimqap_\w+)\(", text, re.M)))
+
+
+def test_library_exports_every_declared_symbol():
+    names = declared_functions()
+    assert "pimqap_solve" in names and "pimqap_read_problem" in names
+    out = subprocess.run(["nm", "-D", "--defined-only", pimqap.LIB_PATH], capture_output=True,
+                         text=True, check=True).stdout
+    exported = set(re.findall(r" T (pimqap_\w+)", out))
+    missing = [n for n in names if n not in exported]
+    assert not missing, f"declared but not exported: {missing}"
+    L = pimqap.lib()
+    for n in names:
+        assert hasattr(L, n)
+
+
+def test_default_params_mirror_reference_defaults():
+    p = pimqap.default_params()
+    assert (p.replicas, p.groups, p.sweeps_per_exchange) == (10, 20, 4)
+    assert p.beta_ratio == 1.2 and p.goal == 0
+    assert abs(p.beta_max * pimqap.LN2_INV - 2.0 ** -12) < 1e-15
+
+
+def test_read_problem_round_trip(tmp_path):
+    inst = instances.heavy(41, 3)
+    path = str(tmp_path / "h41.dat")
+    instances.write_instance(path, inst)
+    F, D = pimqap.read_problem(path)
+    assert np.array_equal(F, inst.F) and np.array_equal(D, inst.D)
+
+
+def test_read_problem_errors(tmp_path):
+    with pytest.raises(pimqap.PimqapError) as e:
+        pimqap.read_problem(str(tmp_path / "missing.dat"))
+    assert e.value.status == 2
+    big = instances.uniform(30, 1)
+    path = str(tmp_path / "u30.dat")
+    instances.write_instance(path, big)
+    with pytest.raises(pimqap.PimqapError) as e:      # the reference's MAXN check
+        pimqap.read_problem(path, max_n=20)
+    assert e.value.status == 1 and "MAXN" in str(e.value)
+    trunc = tmp_path / "trunc.dat"
+    trunc.write_text("3\n1 2 3\n4 5 6\n")
+    with pytest.raises(pimqap.PimqapError) as e:
+        pimqap.read_problem(str(trunc))
+    assert e.value.status == 2
+
+
+@pytest.mark.parametrize("field,value", [("replicas", 0), ("replicas", 65), ("groups", 0),
+                                         ("sweeps_per_exchange", 0), ("beta_max", 0.0),
+                                         ("beta_ratio", -1.0), ("force_bits", 16),
+                                         ("threads_per_block", 96), ("rank_slots", 2)])
+def test_invalid_params_rejected_before_device(field, value):
+    inst = instances.uniform(8, 1)
+    p = pimqap.default_params(replicas=4, groups=1, max_megaiters=1)
+    setattr(p, field, value)
+    with pytest.raises(pimqap.PimqapError) as e:
+        pimqap.Solver(inst.F, inst.D, p)
+    assert e.value.status == 1
+
+
+def test_n_out_of_range_rejected():
+    F = np.zeros((257, 257), np.int32)
+    with pytest.raises(pimqap.PimqapError) as e:
+        pimqap.Solver(F, F, pimqap.default_params())
+    assert e.value.status == 1

@@ -1,0 +1,147 @@
+"""GPU parity: the CUDA solver, called through its C ABI, against the oracle restatement.
+
+Integer state (permutations, force matrices, energies, bests) must be bit-exact; the
+replica-exchange state (betas, rank slots, timeSinceSwap) must be identical; and the
+trajectory, driven by the same Philox stream, must take the same decision at every update.
+The heat-bath weights are float64 on the GPU and x87 long double in the reference; a
+decision can only differ when r * total lands within a few ulps of a prefix-sum boundary,
+which these tests would show as a state mismatch (tolerance: zero mismatches).
+"""
+import numpy as np
+import pytest
+
+import instances
+from helpers import compare_solver_to_oracle, oracle_after
+
+pytestmark = pytest.mark.gpu
+
+
+def asym(n, seed):
+    rng = np.random.default_rng(seed)
+    return instances.Instance(n, rng.integers(-5, 40, (n, n)), rng.integers(-3, 60, (n, n)))
+
+
+def heavy_small(n, seed):
+    inst = instances.heavy(n, seed)
+    return instances.Instance(n, np.minimum(inst.F, 60), inst.D // 4)
+
+
+# name: (instance factory, T, R, spe, beta_max (natural), beta_ratio, megaiters, extra params)
+CASES = {
+    "plain_n32_R16": (lambda: instances.uniform(32, 11), 1, 16, 1, 10.0, 1.5849, 25, {}),
+    "groups_T3_R5_i4": (lambda: instances.uniform(20, 12), 3, 5, 4, 0.4, 1.3, 8, {}),
+    "asym_signed_n18": (lambda: asym(18, 13), 2, 3, 3, 0.015, 1.5, 10, {}),
+    "int64_forced_n24": (lambda: instances.uniform(24, 14), 1, 4, 2, 0.01, 1.4, 10, {"force_bits": 64}),
+    "heavy_n60": (lambda: heavy_small(60, 15), 1, 3, 1, 0.0005, 2.0, 4, {}),
+    "heavy_int64_n48": (lambda: instances.heavy(48, 16), 1, 3, 1, 1e-5, 2.0, 4, {}),
+    "grid_n256_cluster": (lambda: instances.grid256(17), 1, 2, 1, 0.0015, 1.5, 2, {}),
+    "grid_n256_int64_cluster4": (lambda: instances.grid256(18), 1, 1, 1, 0.0015, 1.5, 1, {"force_bits": 64}),
+    "n200_single_cta": (lambda: instances.uniform(200, 19), 1, 2, 1, 0.0005, 1.5, 1, {}),
+    "cold_forced_swaps": (lambda: instances.uniform(12, 20), 2, 10, 1, 40.0, 1.2, 150, {}),
+    "junk_rank_slot": (lambda: instances.uniform(14, 21), 1, 4, 1, 3.0 / 1.4427, 1.4, 140, {}),
+    "hot_cutoff_min": (lambda: instances.uniform(16, 22), 1, 5, 2, 1e-6, 1.1, 10, {}),
+    "threads64_n40": (lambda: instances.uniform(40, 23), 1, 4, 2, 0.02, 1.3, 6, {"threads_per_block": 64}),
+    "threads256_n40": (lambda: instances.uniform(40, 23), 1, 4, 2, 0.02, 1.3, 6, {"threads_per_block": 256}),
+    "n1_trivial": (lambda: instances.uniform(1, 24), 1, 2, 1, 1.0, 1.2, 3, {}),
+    "n5_tiny": (lambda: instances.uniform(5, 25), 2, 3, 2, 0.05, 1.3, 6, {}),
+}
+
+
+def run_case(gpu, oracle, name, seed=7):
+    make, T, R, spe, bmax, ratio, M, extra = CASES[name]
+    inst = make()
+    cap = max(R, 10)
+    p = gpu.default_params(replicas=R, groups=T, sweeps_per_exchange=spe, beta_max=bmax,
+                           beta_ratio=ratio, seed=seed, max_megaiters=M, megaiters_per_launch=7,
+                           **extra)
+    with gpu.Solver(inst.F, inst.D, p) as s:
+        s.run(M)
+        st = oracle_after(oracle, inst.F, inst.D, T=T, R=R, spe=spe, beta_max=bmax,
+                          beta_ratio=ratio, seed=seed, cap=cap, megaiters=M)
+        bad = compare_solver_to_oracle(s, st, cap)
+        res = s.result()
+    return inst, st, bad, res
+
+
+@pytest.mark.parametrize("name", list(CASES))
+def test_trajectory_matches_oracle(gpu, oracle, name):
+    inst, st, bad, res = run_case(gpu, oracle, name)
+    assert not bad, bad[:10]
+    assert res["megaiters_done"] == CASES[name][6]
+    assert res["accepts"] == st.accepts
+    assert res["best_energy"] == min(int(st.bestE.min()), st.single_best)
+
+
+def test_force_width_and_cluster_choice(gpu, oracle):
+    _, _, _, r = run_case(gpu, oracle, "grid_n256_cluster")
+    assert (r["force_bits"], r["cluster_size"]) == (32, 2)
+    _, _, _, r = run_case(gpu, oracle, "grid_n256_int64_cluster4")
+    assert (r["force_bits"], r["cluster_size"]) == (64, 4)
+    _, _, _, r = run_case(gpu, oracle, "heavy_int64_n48")
+    assert r["force_bits"] == 64
+
+
+def test_setup_matches_oracle(gpu, oracle):
+    inst = instances.uniform(50, 31)
+    p = gpu.default_params(replicas=6, groups=3, sweeps_per_exchange=2, beta_max=0.01,
+                           beta_ratio=1.3, seed=123)
+    with gpu.Solver(inst.F, inst.D, p) as s:
+        st = oracle_after(oracle, inst.F, inst.D, T=3, R=6, spe=2, beta_max=0.01, beta_ratio=1.3,
+                          seed=123, cap=10, megaiters=0)
+        assert not compare_solver_to_oracle(s, st, 10)
+
+
+def test_best_permutation_has_best_energy(gpu):
+    inst = instances.uniform(30, 41)
+    p = gpu.default_params(replicas=8, groups=2, sweeps_per_exchange=2, beta_max=0.05,
+                           beta_ratio=1.4, seed=5, max_megaiters=40)
+    r = gpu.solve(inst.F, inst.D, p)
+    perm = r["best_perm"]
+    assert sorted(perm.tolist()) == list(range(30))
+    e = int((inst.D.astype(np.int64) * inst.F[np.ix_(perm, perm)]).sum())
+    assert e == r["best_energy"]
+
+
+def test_goal_stops_at_the_oracle_megaiter(gpu, oracle):
+    inst = instances.uniform(24, 51)
+    kw = dict(T=2, R=6, spe=1, beta_max=0.05, beta_ratio=1.3, seed=9, cap=10)
+    st = oracle_after(oracle, inst.F, inst.D, megaiters=30, **kw)
+    goal = int(st.single_best) + 500       # reachable within the 30 mega-iterations
+    st2 = oracle.setup(inst.D, inst.F, 2, 6, 1, 0.05 * 1.44269504089, 1.3, 9, cap=10)
+    stopped = oracle.run(st2, inst.D, inst.F, 100, goal)
+    assert stopped == 1
+    p = gpu.default_params(replicas=6, groups=2, sweeps_per_exchange=1, beta_max=0.05,
+                           beta_ratio=1.3, seed=9, max_megaiters=100, goal=goal,
+                           megaiters_per_launch=4)
+    r = gpu.solve(inst.F, inst.D, p)
+    assert r["stopped_by"] == 1
+    assert r["target_megaiter"] == st2.target_megaiter
+    assert r["megaiters_done"] == st2.megaiters_done
+    assert r["best_energy"] <= goal
+    assert r["time_to_target_ms"] >= 0
+
+
+def test_same_seed_same_result_other_seed_differs(gpu):
+    inst = instances.uniform(28, 61)
+    p = gpu.default_params(replicas=4, groups=1, sweeps_per_exchange=2, beta_max=0.05,
+                           beta_ratio=1.3, seed=77, max_megaiters=20)
+    a = gpu.solve(inst.F, inst.D, p)
+    b = gpu.solve(inst.F, inst.D, p)
+    assert a["best_energy"] == b["best_energy"] and np.array_equal(a["best_perm"], b["best_perm"])
+    assert a["accepts"] == b["accepts"]
+    p.seed = 78
+    c = gpu.solve(inst.F, inst.D, p)
+    assert c["accepts"] != a["accepts"] or not np.array_equal(c["best_perm"], a["best_perm"])
+
+
+def test_chunking_does_not_change_the_trajectory(gpu):
+    inst = instances.uniform(36, 71)
+    out = []
+    for per in (1, 5, 50):
+        p = gpu.default_params(replicas=5, groups=2, sweeps_per_exchange=1, beta_max=0.03,
+                               beta_ratio=1.3, seed=3, max_megaiters=17, megaiters_per_launch=per)
+        with gpu.Solver(inst.F, inst.D, p) as s:
+            s.run(10)
+            s.run(7)
+            out.append((s.result()["accepts"], s.replica(1, 3)["E"], s.replica(0, 0)["phi"].tobytes()))
+    assert out[0] == out[1] == out[2]
