@@ -21,6 +21,14 @@ def asym(n, seed):
     return instances.Instance(n, rng.integers(-5, 40, (n, n)), rng.integers(-3, 60, (n, n)))
 
 
+def wide(n, seed):
+    """Flows up to 2e6 and distances up to 5e3: force entries and costs far beyond int32."""
+    rng = np.random.default_rng(seed)
+    F = rng.integers(0, 2_000_000, (n, n))
+    D = rng.integers(0, 5_000, (n, n))
+    return instances.Instance(n, F, D)
+
+
 def heavy_small(n, seed):
     inst = instances.heavy(n, seed)
     return instances.Instance(n, np.minimum(inst.F, 60), inst.D // 4)
@@ -33,7 +41,8 @@ CASES = {
     "asym_signed_n18": (lambda: asym(18, 13), 2, 3, 3, 0.015, 1.5, 10, {}),
     "int64_forced_n24": (lambda: instances.uniform(24, 14), 1, 4, 2, 0.01, 1.4, 10, {"force_bits": 64}),
     "heavy_n60": (lambda: heavy_small(60, 15), 1, 3, 1, 0.0005, 2.0, 4, {}),
-    "heavy_int64_n48": (lambda: instances.heavy(48, 16), 1, 3, 1, 1e-5, 2.0, 4, {}),
+    "heavy_n48": (lambda: instances.heavy(48, 16), 1, 3, 1, 1e-5, 2.0, 4, {}),
+    "wide_int64_n32": (lambda: wide(32, 26), 2, 3, 2, 1e-9, 1.5, 6, {}),
     "grid_n256_cluster": (lambda: instances.grid256(17), 1, 2, 1, 0.0015, 1.5, 2, {}),
     "grid_n256_int64_cluster4": (lambda: instances.grid256(18), 1, 1, 1, 0.0015, 1.5, 1, {"force_bits": 64}),
     "n200_single_cta": (lambda: instances.uniform(200, 19), 1, 2, 1, 0.0005, 1.5, 1, {}),
@@ -77,8 +86,10 @@ def test_force_width_and_cluster_choice(gpu, oracle):
     assert (r["force_bits"], r["cluster_size"]) == (32, 2)
     _, _, _, r = run_case(gpu, oracle, "grid_n256_int64_cluster4")
     assert (r["force_bits"], r["cluster_size"]) == (64, 4)
-    _, _, _, r = run_case(gpu, oracle, "heavy_int64_n48")
+    _, _, _, r = run_case(gpu, oracle, "wide_int64_n32")
     assert r["force_bits"] == 64
+    _, _, _, r = run_case(gpu, oracle, "plain_n32_R16")
+    assert (r["force_bits"], r["cluster_size"]) == (32, 1)
 
 
 def test_setup_matches_oracle(gpu, oracle):
