@@ -116,6 +116,21 @@ pimqap_status pimqap_read_problem(const char *path, int32_t max_n, int32_t *n,
 pimqap_status pimqap_solve(const pimqap_instance *inst, const pimqap_params *params,
                            pimqap_result *result);
 
+/* One-shot solve that allocates nothing (no counterpart in the reference, whose CPU solver
+   has no device memory).  For callers that must not call cudaMalloc while they solve: a
+   program whose device memory is all claimed by another allocator (a framework's caching
+   allocator, a service that admits work against memory reserved up front), or code that may
+   not take the allocator's locks or latency.  Same inputs, outputs and results as
+   pimqap_solve, but every device buffer lives in one file-scope device array of
+   PIMQAP_STATIC_SCRATCH_BYTES that each GPU holds from library load until exit; a solve that
+   needs more is rejected with PIMQAP_ERR_ARG.  The first call on a device looks the array's
+   address up (make it before any stream capture).  Calls share the array: this library
+   serialises its own calls per device, and calls that overlap on one GPU from elsewhere race.
+   Work runs on the legacy default stream; no stream, event or graph is created. */
+#define PIMQAP_STATIC_SCRATCH_BYTES ((size_t)8 << 20)
+pimqap_status pimqap_solve_static(const pimqap_instance *inst, const pimqap_params *params,
+                                  pimqap_result *result);
+
 /* ---------------------------------------------------------------- solver handle */
 
 typedef struct pimqap_solver pimqap_solver;

@@ -33,6 +33,12 @@ pimqap_status fail(pimqap_status st, const std::string &msg) {
     return st;
 }
 
+}  // namespace
+
+void pimqap::set_last_error(const char *msg) { g_error = msg; }
+
+namespace {
+
 #define PQ_CUDA(x)                                                                       \
     do {                                                                                 \
         cudaError_t e_ = (x);                                                            \

@@ -50,6 +50,9 @@ struct SolveDev {
     int32_t *error;            // [1]       kErr* bits
 };
 
+// Records msg as the calling thread's pimqap_last_error() text.
+void set_last_error(const char *msg);
+
 // Shared memory of one CTA of the epoch kernel.
 size_t epoch_smem_bytes(int n, int rpc, int lds, int cluster, int bits);
 

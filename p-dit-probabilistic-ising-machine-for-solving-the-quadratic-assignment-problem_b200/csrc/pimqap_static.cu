@@ -1,0 +1,401 @@
+// pimqap_static.cu - pimqap_solve_static: the one-shot solve of pimqap_solve with every device
+// buffer (instance copy, replica force matrices and permutations, exchange state) placed in
+// one fixed array of device memory that the library reserves when it is loaded, so the call
+// itself allocates nothing.
+//
+// Who needs it: a host program that must not call cudaMalloc while it solves - one that runs
+// under a strict device-memory budget owned by another allocator (a framework's caching
+// allocator that has claimed the free memory, or a service that admits work by memory it has
+// reserved up front), or real-time code that may not take the allocator's locks or its
+// latency.  Such a caller gets a solve whose device footprint is fixed when the library loads.
+//
+// Limits and rules
+//   - The array holds kStaticScratchBytes (8 MiB) on every GPU that loads the library, until
+//     the process exits.  A solve that needs more (force matrices of all replicas + instance +
+//     state) is rejected with PIMQAP_ERR_ARG and a message giving both sizes.
+//   - Every call uses the same array and leaves the last call's contents there; each call
+//     clears what must start at zero.  Calls that overlap on the same GPU would race on the
+//     array: this file serialises the calls of one process per device with a mutex, and a
+//     caller that launches work from other processes or libraries into the same context must
+//     not overlap them either.
+//   - The array's device address is looked up once per device, by the first call on that
+//     device, with that device current (cudaGetSymbolAddress on the file-scope symbol; in host
+//     code the symbol's name is only a host-side stand-in, never a device address).  Make that
+//     first call before any stream capture.
+//   - No cudaMalloc, cudaFree, cudaMallocHost, stream, event or graph creation, and no host heap
+//     allocation on the success path (small fixed-size host buffers live on the stack).  A
+//     failure records its message in the library's last-error slot.
+//   - The force-matrix width is chosen from the cheap per-row bound only (the tighter sorted
+//     bound of pimqap_solve needs heap buffers); int64 is used when that bound exceeds int32.
+//     Widths do not change results, only memory.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstdint>
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <random>
+
+#include "pimqap.h"
+#include "pimqap_internal.h"
+
+using pimqap::SolveDev;
+
+namespace {
+
+constexpr size_t kStaticScratchBytes = size_t(8) << 20;
+constexpr int kMaxDevices = 64;
+
+static __device__ __align__(256) unsigned char g_static_scratch[kStaticScratchBytes];
+
+void *g_scratch_addr[kMaxDevices] = {};
+std::mutex g_device_mutex[kMaxDevices];
+
+pimqap_status fail(pimqap_status st, const char *msg) {
+    pimqap::set_last_error(msg);
+    return st;
+}
+
+// Philox4x32-10 (Salmon et al., SC'11) and the shuffle-stream engine, as in pimqap_solve.
+void philox4x32_10(uint32_t c[4], uint32_t k0, uint32_t k1) {
+    for (int r = 0; r < 10; ++r) {
+        const uint64_t p0 = (uint64_t)0xD2511F53u * c[0];
+        const uint64_t p1 = (uint64_t)0xCD9E8D57u * c[2];
+        const uint32_t n0 = (uint32_t)(p1 >> 32) ^ c[1] ^ k0;
+        const uint32_t n2 = (uint32_t)(p0 >> 32) ^ c[3] ^ k1;
+        c[0] = n0;
+        c[1] = (uint32_t)p1;
+        c[2] = n2;
+        c[3] = (uint32_t)p0;
+        k0 += 0x9E3779B9u;
+        k1 += 0xBB67AE85u;
+    }
+}
+
+struct ShuffleEngine {
+    typedef uint_fast32_t result_type;
+    static constexpr result_type min() { return 0; }
+    static constexpr result_type max() { return 0xFFFFFFFFu; }
+    uint64_t seed = 0;
+    uint64_t k = 0;
+    result_type operator()() {
+        uint32_t c[4] = {(uint32_t)(k >> 2), (uint32_t)(k >> 34), 0u, 0xFFFFFFFFu};
+        philox4x32_10(c, (uint32_t)seed, (uint32_t)(seed >> 32));
+        return c[(k++) & 3];
+    }
+};
+
+size_t carve_size(size_t bytes) { return (bytes + 255) & ~size_t(255); }
+
+template <class T> T *carve(char *&cur, size_t count) {
+    T *p = reinterpret_cast<T *>(cur);
+    cur += carve_size(count * sizeof(T));
+    return p;
+}
+
+// Small per-call results reduced on the device (no host array of T*R entries is needed).
+struct StaticSummary {
+    long long best;
+    long long arg;
+    unsigned long long accepts;
+    long long pad;
+};
+
+__global__ void static_prepare_kernel(SolveDev d, int32_t *Dd_w, int32_t *Fd_w, int32_t *DT_w,
+                                      int32_t *FT_w) {
+    const int n = d.n;
+    const int tid = blockIdx.x * blockDim.x + threadIdx.x;
+    const int stride = gridDim.x * blockDim.x;
+    for (int q = tid; q < n * n; q += stride) {
+        const int i = q / n, j = q - i * n;
+        DT_w[q] = d.D[j * n + i];
+        FT_w[q] = d.F[j * n + i];
+    }
+    for (int q = tid; q < n; q += stride) {
+        Dd_w[q] = d.D[q * n + q];
+        Fd_w[q] = d.F[q * n + q];
+    }
+    for (int t = tid; t < d.T; t += stride) d.group_best[t] = pimqap::kNoBest;
+    if (tid == 0) {
+        *d.single_best = pimqap::kNoBest;
+        *d.stop_epoch = pimqap::kNoStop;
+        *d.target_epoch = 0x7fffffffffffffffll;
+        *d.target_ns = ~0ull;
+    }
+}
+
+__global__ void static_summary_kernel(SolveDev d, StaticSummary *out) {
+    __shared__ long long sb[256];
+    __shared__ long long sa[256];
+    __shared__ unsigned long long sc[256];
+    const int reps = d.T * d.R;
+    long long best = 0x7fffffffffffffffll, arg = 0;
+    unsigned long long acc = 0;
+    for (int k = threadIdx.x; k < reps; k += blockDim.x) {
+        const long long v = d.bestE[k];
+        if (v < best) {
+            best = v;
+            arg = k;
+        }
+        acc += d.accepts[k];
+    }
+    sb[threadIdx.x] = best;
+    sa[threadIdx.x] = arg;
+    sc[threadIdx.x] = acc;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        // lowest replica index among equal bests, as pimqap_solve picks it
+        long long b = sb[0], a = sa[0];
+        unsigned long long c = sc[0];
+        for (int k = 1; k < (int)blockDim.x; ++k) {
+            if (sb[k] < b || (sb[k] == b && sa[k] < a)) {
+                b = sb[k];
+                a = sa[k];
+            }
+            c += sc[k];
+        }
+        out->best = b;
+        out->arg = a;
+        out->accepts = c;
+    }
+}
+
+}  // namespace
+
+extern "C" pimqap_status pimqap_solve_static(const pimqap_instance *inst,
+                                              const pimqap_params *p, pimqap_result *result) {
+    const auto wall0 = std::chrono::steady_clock::now();
+    if (!inst || !p || !result) return fail(PIMQAP_ERR_ARG, "null instance, params or result");
+    const int n = inst->n;
+    if (n < 1 || n > PIMQAP_MAX_N) return fail(PIMQAP_ERR_ARG, "n must be in [1, 256]");
+    if (!inst->flow || !inst->dist) return fail(PIMQAP_ERR_ARG, "null flow or dist");
+    if (p->replicas < 1 || p->replicas > PIMQAP_MAX_REPLICAS) return fail(PIMQAP_ERR_ARG, "replicas must be in [1, 64]");
+    if (p->groups < 1 || p->groups > PIMQAP_MAX_GROUPS) return fail(PIMQAP_ERR_ARG, "groups must be in [1, 1024]");
+    if (p->sweeps_per_exchange < 1) return fail(PIMQAP_ERR_ARG, "sweeps_per_exchange must be >= 1");
+    if (p->rank_slots != 0 && (p->rank_slots < p->replicas || p->rank_slots > 4096))
+        return fail(PIMQAP_ERR_ARG, "rank_slots must be 0 or in [replicas, 4096]");
+    if (!(p->beta_max > 0) || !std::isfinite(p->beta_max)) return fail(PIMQAP_ERR_ARG, "beta_max must be a positive finite number");
+    if (!(p->beta_ratio > 0) || !std::isfinite(p->beta_ratio)) return fail(PIMQAP_ERR_ARG, "beta_ratio must be a positive finite number");
+    if (p->max_megaiters < 0) return fail(PIMQAP_ERR_ARG, "max_megaiters must be >= 0");
+    if (p->force_bits != 0 && p->force_bits != 32 && p->force_bits != 64) return fail(PIMQAP_ERR_ARG, "force_bits must be 0, 32 or 64");
+    if (p->threads_per_block != 0 && p->threads_per_block != 64 && p->threads_per_block != 128 &&
+        p->threads_per_block != 256)
+        return fail(PIMQAP_ERR_ARG, "threads_per_block must be 0, 64, 128 or 256");
+
+    // Instance analysis without heap buffers: symmetry and the per-row force bound.
+    const int32_t *F = inst->flow, *D = inst->dist;
+    bool sym = true;
+    long double A = 0, B = 0, rFmax = 0, cFmax = 0, imax = 0, ebound = 0;
+    for (int i = 0; i < n; ++i) {
+        long double rf = 0, cf = 0;
+        for (int j = 0; j < n; ++j) {
+            if (D[i * n + j] != D[j * n + i] || F[i * n + j] != F[j * n + i]) sym = false;
+            rf = std::max(rf, std::fabs((long double)F[i * n + j]));
+            cf = std::max(cf, std::fabs((long double)F[j * n + i]));
+            A = std::max(A, std::fabs((long double)D[i * n + j]));
+            B = std::max(B, std::fabs((long double)F[i * n + j]));
+        }
+        rFmax = std::max(rFmax, rf);
+        cFmax = std::max(cFmax, cf);
+    }
+    for (int i = 0; i < n; ++i) {
+        long double rd = 0, cd = 0;
+        for (int j = 0; j < n; ++j) {
+            rd += std::fabs((long double)D[i * n + j]);
+            cd += std::fabs((long double)D[j * n + i]);
+        }
+        imax = std::max(imax, rd * rFmax + cd * cFmax);
+        ebound += rd * rFmax;
+    }
+    const long double dbound = 4 * imax + 16 * A * B;
+    int bits = p->force_bits;
+    if (!bits) {
+        if (dbound < 2147483647.0L) bits = 32;
+        else if (dbound < 4.6e18L && ebound < 4.6e18L) bits = 64;
+        else return fail(PIMQAP_ERR_RANGE, "instance values can overflow int64 force matrices");
+    }
+
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return fail(PIMQAP_ERR_NO_DEVICE, "no CUDA device");
+    const int dev = p->device;
+    if (dev < 0 || dev >= ndev || dev >= kMaxDevices) return fail(PIMQAP_ERR_ARG, "bad device ordinal");
+    std::lock_guard<std::mutex> lock(g_device_mutex[dev]);
+    if (cudaSetDevice(dev) != cudaSuccess) return fail(PIMQAP_ERR_CUDA, "cudaSetDevice failed");
+    int major = 0, maxsm = 0;
+    cudaDeviceGetAttribute(&major, cudaDevAttrComputeCapabilityMajor, dev);
+    cudaDeviceGetAttribute(&maxsm, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+    if (major != 10) return fail(PIMQAP_ERR_NO_DEVICE, "the kernels are built for sm_100a only");
+    if (pimqap::prepare_kernels() != cudaSuccess) return fail(PIMQAP_ERR_CUDA, "kernel attribute setup failed");
+    if (!g_scratch_addr[dev]) {
+        void *addr = nullptr;
+        const cudaError_t e = cudaGetSymbolAddress(&addr, g_static_scratch);
+        if (e != cudaSuccess || !addr) return fail(PIMQAP_ERR_CUDA, "cudaGetSymbolAddress of the static scratch failed");
+        g_scratch_addr[dev] = addr;
+    }
+
+    // Launch shape, as pimqap_solve picks it.
+    const int T = p->groups, R = p->replicas;
+    const int cap = p->rank_slots ? p->rank_slots : std::max(R, 10);
+    const int isz = bits / 8, vec = 16 / isz;
+    const int npad = (n + 3) & ~3;
+    int lds = npad;
+    if ((lds / vec) % 2 == 0) lds += vec;
+    const int threads = p->threads_per_block ? p->threads_per_block : (n <= 64 ? 64 : (n <= 128 ? 128 : 256));
+    int cl = 0;
+    for (int c : {1, 2, 4}) {
+        if (pimqap::epoch_smem_bytes(n, (n + c - 1) / c, lds, c, bits) <= (size_t)maxsm) {
+            cl = c;
+            break;
+        }
+    }
+    if (!cl) return fail(PIMQAP_ERR_ARG, "force matrix does not fit a 4-CTA cluster");
+    const int rpc = (n + cl - 1) / cl;
+    const size_t smem = pimqap::epoch_smem_bytes(n, rpc, lds, cl, bits);
+
+    const size_t reps = (size_t)T * R, nn = (size_t)n * n;
+    const size_t need = carve_size(reps * (size_t)n * npad * isz) + 4 * carve_size(nn * 4) +
+                        2 * carve_size((size_t)n * 4) + 2 * carve_size(reps * n * 4) +
+                        4 * carve_size(reps * 8) + carve_size((size_t)T * cap * 4) +
+                        4 * carve_size((size_t)T * 8) + 8 * carve_size(8) + carve_size(sizeof(StaticSummary));
+    if (need > kStaticScratchBytes) {
+        char msg[160];
+        std::snprintf(msg, sizeof msg,
+                      "solve needs %zu bytes of device memory; the static scratch holds %zu (8 MiB)",
+                      need, kStaticScratchBytes);
+        return fail(PIMQAP_ERR_ARG, msg);
+    }
+
+    char *base = reinterpret_cast<char *>(g_scratch_addr[dev]);
+    char *cur = base;
+    SolveDev d{};
+    d.n = n; d.R = R; d.T = T; d.cap = cap; d.spe = p->sweeps_per_exchange;
+    d.ldg = npad; d.lds = lds; d.rpc = rpc;
+    d.goal = p->goal;
+    d.seed = p->seed;
+    d.I = carve<char>(cur, reps * (size_t)n * npad * isz);
+    int32_t *dD = carve<int32_t>(cur, nn), *dDT = carve<int32_t>(cur, nn);
+    int32_t *dF = carve<int32_t>(cur, nn), *dFT = carve<int32_t>(cur, nn);
+    int32_t *dDd = carve<int32_t>(cur, n), *dFd = carve<int32_t>(cur, n);
+    d.D = dD; d.DT = dDT; d.F = dF; d.FT = dFT; d.Ddiag = dDd; d.Fdiag = dFd;
+    d.phi = carve<int32_t>(cur, reps * n);
+    d.best_phi = carve<int32_t>(cur, reps * n);
+    d.E = carve<int64_t>(cur, reps);
+    d.bestE = carve<int64_t>(cur, reps);
+    d.beta = carve<double>(cur, reps);
+    d.accepts = carve<unsigned long long>(cur, reps);
+    d.order = carve<int32_t>(cur, (size_t)T * cap);
+    d.tss = carve<int32_t>(cur, T);
+    d.group_best = carve<int64_t>(cur, T);
+    d.finish = carve<unsigned int>(cur, T);
+    d.epoch = carve<int32_t>(cur, T);
+    d.single_best = carve<int64_t>(cur, 1);
+    d.stop_epoch = carve<int32_t>(cur, 1);
+    d.target_epoch = carve<int64_t>(cur, 1);
+    d.target_ns = carve<unsigned long long>(cur, 1);
+    d.start_ns = carve<unsigned long long>(cur, 1);
+    d.error = carve<int32_t>(cur, 1);
+    StaticSummary *dsum = carve<StaticSummary>(cur, 1);
+
+    const cudaStream_t q = 0;   // the legacy default stream: nothing is created per call
+#define PQS_CUDA(x)                                                     \
+    do {                                                                \
+        if ((x) != cudaSuccess) return fail(PIMQAP_ERR_CUDA, #x " failed"); \
+    } while (0)
+    PQS_CUDA(cudaMemsetAsync(base, 0, need, q));   // the previous call's contents are cleared
+    PQS_CUDA(cudaMemcpy(dD, D, nn * 4, cudaMemcpyHostToDevice));
+    PQS_CUDA(cudaMemcpy(dF, F, nn * 4, cudaMemcpyHostToDevice));
+    static_prepare_kernel<<<64, 256, 0, q>>>(d, dDd, dFd, dDT, dFT);
+    PQS_CUDA(cudaGetLastError());
+
+    // Host set-up with fixed-size stack buffers: shuffle, beta ladder, rank slots per group.
+    const double beta0 = p->beta_max * 1.44269504089;
+    ShuffleEngine eng;
+    eng.seed = p->seed;
+    int32_t perm[PIMQAP_MAX_N];
+    double ladder[PIMQAP_MAX_REPLICAS];
+    int32_t order[64];
+    for (int t = 0; t < T; ++t) {
+        for (int i = 0; i < n; ++i) perm[i] = i;
+        for (int i = 0; i < n; ++i) {
+            std::uniform_int_distribution<ShuffleEngine::result_type> distN(0, n - 1);
+            const int j = (int)distN(eng);
+            if (i != j) std::swap(perm[i], perm[j]);
+        }
+        for (int l = 0; l < R; ++l)
+            PQS_CUDA(cudaMemcpy(d.phi + ((size_t)t * R + l) * n, perm, (size_t)n * 4, cudaMemcpyHostToDevice));
+        double running = beta0;
+        for (int l = R - 1; l >= 0; --l) {
+            ladder[l] = running;
+            running /= p->beta_ratio;
+        }
+        PQS_CUDA(cudaMemcpy(d.beta + (size_t)t * R, ladder, (size_t)R * 8, cudaMemcpyHostToDevice));
+        for (int c0 = 0; c0 < cap; c0 += 64) {   // slots past R start at 0 (cleared above)
+            const int cnt = std::min(64, R - c0);
+            if (cnt <= 0) break;
+            for (int k = 0; k < cnt; ++k) order[k] = c0 + k;
+            PQS_CUDA(cudaMemcpy(d.order + (size_t)t * cap + c0, order, (size_t)cnt * 4, cudaMemcpyHostToDevice));
+        }
+    }
+    PQS_CUDA(pimqap::launch_setup(d, bits, q));
+    PQS_CUDA(cudaStreamSynchronize(q));
+
+    // Mega-iterations, one epoch launch each; goal and timeout are checked every few launches.
+    const auto run0 = std::chrono::steady_clock::now();
+    const int check_every = p->megaiters_per_launch > 0 ? p->megaiters_per_launch : 50;
+    int64_t left = p->max_megaiters;
+    bool stopped_goal = false, timed_out = false;
+    while (left > 0) {
+        const int g = (int)std::min<int64_t>(left, check_every);
+        for (int k = 0; k < g; ++k) PQS_CUDA(pimqap::launch_epoch(d, bits, cl, sym, threads, smem, q));
+        int32_t stop = 0;
+        PQS_CUDA(cudaMemcpy(&stop, d.stop_epoch, 4, cudaMemcpyDeviceToHost));
+        left -= g;
+        if (stop != pimqap::kNoStop) {
+            stopped_goal = true;
+            break;
+        }
+        if (p->timeout_s > 0 &&
+            std::chrono::duration<double>(std::chrono::steady_clock::now() - wall0).count() >= p->timeout_s) {
+            timed_out = true;
+            break;
+        }
+    }
+    static_summary_kernel<<<1, 256, 0, q>>>(d, dsum);
+    PQS_CUDA(cudaGetLastError());
+    StaticSummary sum{};
+    int32_t epoch0 = 0, err = 0;
+    int64_t single = 0, tepoch = 0;
+    unsigned long long tns = 0, sns = 0;
+    PQS_CUDA(cudaMemcpy(&sum, dsum, sizeof sum, cudaMemcpyDeviceToHost));
+    PQS_CUDA(cudaMemcpy(&epoch0, d.epoch, 4, cudaMemcpyDeviceToHost));
+    PQS_CUDA(cudaMemcpy(&err, d.error, 4, cudaMemcpyDeviceToHost));
+    PQS_CUDA(cudaMemcpy(&single, d.single_best, 8, cudaMemcpyDeviceToHost));
+    PQS_CUDA(cudaMemcpy(&tepoch, d.target_epoch, 8, cudaMemcpyDeviceToHost));
+    PQS_CUDA(cudaMemcpy(&tns, d.target_ns, 8, cudaMemcpyDeviceToHost));
+    PQS_CUDA(cudaMemcpy(&sns, d.start_ns, 8, cudaMemcpyDeviceToHost));
+    if (err) return fail(PIMQAP_ERR_DEVICE, "device check failed");
+    int32_t *perm_dst = result->best_perm;
+    std::memset(result, 0, sizeof(*result));
+    result->best_perm = perm_dst;
+    if (perm_dst)
+        PQS_CUDA(cudaMemcpy(perm_dst, d.best_phi + (size_t)sum.arg * n, (size_t)n * 4, cudaMemcpyDeviceToHost));
+#undef PQS_CUDA
+    const auto wall1 = std::chrono::steady_clock::now();
+    result->best_energy = std::min<int64_t>(sum.best, single);
+    result->target_megaiter = (tepoch == 0x7fffffffffffffffll) ? -1 : tepoch;
+    result->time_to_target_ms = (result->target_megaiter >= 0 && tns != ~0ull && tns >= sns) ? (double)(tns - sns) * 1e-6 : -1.0;
+    result->megaiters_done = epoch0;
+    result->updates = (int64_t)epoch0 * p->sweeps_per_exchange * n * (int64_t)reps;
+    result->accepts = (int64_t)sum.accepts;
+    result->device_ms = std::chrono::duration<double, std::milli>(wall1 - run0).count();
+    result->wall_ms = std::chrono::duration<double, std::milli>(wall1 - wall0).count();
+    result->force_bits = bits;
+    result->cluster_size = cl;
+    result->stopped_by = stopped_goal ? 1 : (timed_out ? 2 : 0);
+    result->h2d_bytes = (int64_t)(2 * nn * 4 + reps * n * 4 + reps * 8 + (size_t)T * std::min(cap, R) * 4);
+    result->d2h_bytes = (int64_t)(sizeof sum + 4 + 4 + 8 + 8 + 8 + 8 + (perm_dst ? (size_t)n * 4 : 0));
+    return PIMQAP_OK;
+}

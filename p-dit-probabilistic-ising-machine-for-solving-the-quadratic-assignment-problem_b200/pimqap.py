@@ -93,6 +93,8 @@ def lib() -> C.CDLL:
     L.pimqap_solver_destroy.restype = None
     L.pimqap_batch_solve.argtypes = [C.POINTER(Instance), C.POINTER(Params), C.c_int32, C.POINTER(Result)]
     L.pimqap_batch_solve.restype = st
+    L.pimqap_solve_static.argtypes = [C.POINTER(Instance), C.POINTER(Params), C.POINTER(Result)]
+    L.pimqap_solve_static.restype = st
     L.pimqap_probe_smem_bandwidth.argtypes = [C.c_int32, C.POINTER(C.c_double)]
     L.pimqap_probe_smem_bandwidth.restype = st
     _lib = L
@@ -149,6 +151,16 @@ def solve(F: np.ndarray, D: np.ndarray, params: Params) -> dict:
     r = Result()
     r.best_perm = perm.ctypes.data_as(C.POINTER(C.c_int32))
     _check(lib().pimqap_solve(C.byref(inst.c), C.byref(params), C.byref(r)))
+    return _result_dict(r, perm)
+
+
+def solve_static(F: np.ndarray, D: np.ndarray, params: Params) -> dict:
+    """pimqap_solve_static: the same solve with no device allocation (fixed 8 MiB scratch)."""
+    inst = _Inst(F, D)
+    perm = np.zeros(inst.F.shape[0], np.int32)
+    r = Result()
+    r.best_perm = perm.ctypes.data_as(C.POINTER(C.c_int32))
+    _check(lib().pimqap_solve_static(C.byref(inst.c), C.byref(params), C.byref(r)))
     return _result_dict(r, perm)
 
 
