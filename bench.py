@@ -210,7 +210,8 @@ def run_ours(args):
     params = pimqap.default_params(replicas=REPLICAS, groups=GROUPS, sweeps_per_exchange=SWEEPS_PER_EXCHANGE,
                                    beta_max=BETA_MAX, beta_ratio=BETA_RATIO, seed=1 + rank,
                                    device=local, megaiters_per_launch=MEGAITERS_PER_STEP,
-                                   max_megaiters=2 ** 31 - 1)
+                                   max_megaiters=2 ** 31 - 1, cluster_size=args.cluster_size,
+                                   threads_per_block=args.threads)
     flush = torch.empty(L2_FLUSH_BYTES, dtype=torch.uint8, device=f"cuda:{local}")
     solver = pimqap.Solver(inst.F, inst.D, params)
     for _ in range(args.warmup):
@@ -259,7 +260,8 @@ def run_ours(args):
     p2 = pimqap.default_params(replicas=REPLICAS, groups=GROUPS, sweeps_per_exchange=SWEEPS_PER_EXCHANGE,
                                beta_max=BETA_MAX, beta_ratio=BETA_RATIO, seed=1 + rank, device=local,
                                megaiters_per_launch=MEGAITERS_PER_STEP,
-                               max_megaiters=args.steps * MEGAITERS_PER_STEP)
+                               max_megaiters=args.steps * MEGAITERS_PER_STEP,
+                               cluster_size=args.cluster_size, threads_per_block=args.threads)
     barrier()
     e0 = time.perf_counter()
     res = pimqap.solve(Fp.numpy(), Dp.numpy(), p2)
@@ -321,6 +323,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cluster-size", type=int, default=0, help="CTAs per replica (0 = automatic)")
+    ap.add_argument("--threads", type=int, default=0, help="threads per CTA (0 = automatic)")
     args = ap.parse_args()
     if args.warmup < 3:
         ap.error("--warmup must be >= 3")

@@ -75,6 +75,7 @@ typedef struct pimqap_params {
     int32_t device;              /* CUDA device ordinal */
     int32_t megaiters_per_launch;/* mega-iterations per CUDA-graph launch (0 = automatic) */
     int32_t threads_per_block;   /* 0 = automatic, else 64, 128 or 256 */
+    int32_t cluster_size;        /* CTAs per replica: 0 = smallest that fits, else 1, 2 or 4 */
 } pimqap_params;
 
 /* Fills p with the reference's defaults: 10 replicas, 20 groups, 4 sweeps per exchange,

@@ -235,6 +235,8 @@ pimqap_status check_params(const pimqap_instance *inst, const pimqap_params *p) 
     if (p->threads_per_block != 0 && p->threads_per_block != 64 && p->threads_per_block != 128 &&
         p->threads_per_block != 256)
         return fail(PIMQAP_ERR_ARG, "threads_per_block must be 0, 64, 128 or 256");
+    if (p->cluster_size != 0 && p->cluster_size != 1 && p->cluster_size != 2 && p->cluster_size != 4)
+        return fail(PIMQAP_ERR_ARG, "cluster_size must be 0, 1, 2 or 4");
     return PIMQAP_OK;
 }
 
@@ -245,6 +247,371 @@ template <class T> T *carve(char *&cur, size_t count) {
 }
 
 size_t carve_size(size_t bytes) { return (bytes + 255) & ~size_t(255); }
+
+// ------------------------------------------------------------------ per-instance plan + staging
+
+// Everything decided for one instance before device memory is touched.
+struct Plan {
+    int n = 0, T = 0, R = 0, cap = 0, spe = 0;
+    int bits = 32, cl = 1, threads = 256;
+    int npad = 0, lds = 0, ldm = 0, rpc = 0;
+    bool sym = false;
+    size_t smem = 0;       // epoch kernel shared memory per CTA
+    size_t total = 0;      // device bytes of the instance's SolveDev arrays
+    int64_t h2d_bytes = 0;
+};
+
+pimqap_status open_device(int device, int *maxsm) {
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0)
+        return fail(PIMQAP_ERR_NO_DEVICE, "no CUDA device");
+    if (device < 0 || device >= ndev) return fail(PIMQAP_ERR_ARG, "bad device ordinal");
+    PQ_CUDA(cudaSetDevice(device));
+    cudaDeviceProp prop;
+    PQ_CUDA(cudaGetDeviceProperties(&prop, device));
+    if (prop.major != 10) return fail(PIMQAP_ERR_NO_DEVICE, "the kernels are built for sm_100a only");
+    PQ_CUDA(pimqap::prepare_kernels());
+    *maxsm = (int)prop.sharedMemPerBlockOptin;
+    return PIMQAP_OK;
+}
+
+// Force-matrix width, symmetry, launch shape (threads, the smallest cluster whose row share of
+// I fits one CTA, or `want_cluster`), strides and the device footprint.
+pimqap_status plan_instance(const pimqap_instance *inst, const pimqap_params *params, size_t maxsm,
+                            int want_cluster, Plan *out) {
+    const int n = inst->n;
+    const InstanceInfo info = analyse(n, inst->flow, inst->dist);
+    if (info.bits_needed == 0 && params->force_bits == 0)
+        return fail(PIMQAP_ERR_RANGE, "instance values can overflow int64 force matrices");
+    Plan P;
+    P.n = n;
+    P.T = params->groups;
+    P.R = params->replicas;
+    P.cap = params->rank_slots ? params->rank_slots : std::max(params->replicas, 10);
+    P.spe = params->sweeps_per_exchange;
+    P.sym = info.symmetric;
+    P.bits = params->force_bits ? params->force_bits : info.bits_needed;
+    const int isz = P.bits / 8, vec = 16 / isz;
+    P.npad = round_up(n, 4);
+    P.lds = P.npad;
+    if ((P.lds / vec) % 2 == 0) P.lds += vec;
+    P.threads = params->threads_per_block ? params->threads_per_block
+                                          : (n <= 64 ? 64 : (n <= 128 ? 128 : 256));
+    auto rows_per_cta = [&](int cl) { return round_up((n + cl - 1) / cl, 4); };
+    P.cl = 0;
+    for (int cl : {1, 2, 4}) {
+        if (want_cluster && cl != want_cluster) continue;
+        if (pimqap::epoch_smem_bytes(n, rows_per_cta(cl), P.lds, cl, P.bits) <= maxsm) {
+            P.cl = cl;
+            break;
+        }
+    }
+    if (!P.cl) return fail(PIMQAP_ERR_ARG, "force matrix does not fit the requested cluster size");
+    P.rpc = rows_per_cta(P.cl);
+    // D / F rows are read in 16-byte chunks up to column cl * rpc
+    P.ldm = std::max(P.npad, P.cl * P.rpc);
+    P.smem = pimqap::epoch_smem_bytes(n, P.rpc, P.lds, P.cl, P.bits);
+    const size_t reps = (size_t)P.T * P.R, nn = (size_t)n * P.ldm;
+    P.total = carve_size(reps * (size_t)n * P.npad * isz) + 4 * carve_size(nn * 4) +
+              2 * carve_size((size_t)n * 4) + 2 * carve_size(reps * n * 4) + 4 * carve_size(reps * 8) +
+              carve_size((size_t)P.T * P.cap * 4) + 4 * carve_size((size_t)P.T * 8) + 8 * carve_size(8);
+    P.h2d_bytes = (int64_t)(4 * nn * 4 + 2 * (size_t)n * 4 + reps * n * 4 + reps * 8 +
+                            (size_t)P.T * P.cap * 4 + (size_t)P.T * 8 + 8 + 4 + 8 + 8);
+    *out = P;
+    return PIMQAP_OK;
+}
+
+// setup() for one instance (CPU_PIM.cpp:109-193): carves the SolveDev arrays out of `base`
+// (plan.total bytes), uploads the padded matrices, transposes, diagonals, initial
+// permutations, beta ladder and rank slots on stream q, and enqueues the setup kernels.  The
+// host buffers of the asynchronous copies are kept in `keep` until the caller syncs q.
+pimqap_status stage_instance(const pimqap_instance *inst, const pimqap_params *params,
+                             const Plan &P, char *base, SolveDev *out, cudaStream_t q,
+                             std::vector<std::vector<char>> &keep) {
+    const int n = P.n, T = P.T, R = P.R, cap = P.cap, ldm = P.ldm;
+    const size_t reps = (size_t)T * R, nn = (size_t)n * ldm;
+    auto buffer = [&](size_t bytes) -> char * {
+        keep.emplace_back(bytes, 0);
+        return keep.back().data();
+    };
+    int32_t *Dp = reinterpret_cast<int32_t *>(buffer(nn * 4));
+    int32_t *DT = reinterpret_cast<int32_t *>(buffer(nn * 4));
+    int32_t *Fp = reinterpret_cast<int32_t *>(buffer(nn * 4));
+    int32_t *FT = reinterpret_cast<int32_t *>(buffer(nn * 4));
+    int32_t *Dd = reinterpret_cast<int32_t *>(buffer((size_t)n * 4));
+    int32_t *Fd = reinterpret_cast<int32_t *>(buffer((size_t)n * 4));
+    for (int i = 0; i < n; ++i) {
+        Dd[i] = inst->dist[i * n + i];
+        Fd[i] = inst->flow[i * n + i];
+        for (int j = 0; j < n; ++j) {
+            Dp[(size_t)i * ldm + j] = inst->dist[i * n + j];
+            Fp[(size_t)i * ldm + j] = inst->flow[i * n + j];
+            DT[(size_t)i * ldm + j] = inst->dist[j * n + i];
+            FT[(size_t)i * ldm + j] = inst->flow[j * n + i];
+        }
+    }
+    const std::vector<int32_t> perms = initial_perms(n, T, params->seed);
+    int32_t *phi = reinterpret_cast<int32_t *>(buffer(reps * n * 4));
+    for (int t = 0; t < T; ++t)
+        for (int l = 0; l < R; ++l)
+            std::memcpy(&phi[((size_t)t * R + l) * n], &perms[(size_t)t * n], sizeof(int32_t) * n);
+    // beta ladder (CPU_PIM.cpp:111-119); -b is given in natural units and stored x 1/ln 2 (:528)
+    const double beta0 = params->beta_max * 1.44269504089;
+    double *beta = reinterpret_cast<double *>(buffer(reps * 8));
+    for (int t = 0; t < T; ++t) {
+        double running = beta0;
+        for (int l = R - 1; l >= 0; --l) {
+            beta[(size_t)t * R + l] = running;
+            running /= params->beta_ratio;
+        }
+    }
+    int32_t *order = reinterpret_cast<int32_t *>(buffer((size_t)T * cap * 4));
+    for (int t = 0; t < T; ++t)
+        for (int l = 0; l < R; ++l) order[(size_t)t * cap + l] = l;
+    int64_t *nob = reinterpret_cast<int64_t *>(buffer((size_t)(T + 1) * 8));
+    for (int t = 0; t <= T; ++t) nob[t] = pimqap::kNoBest;
+    int64_t *consts = reinterpret_cast<int64_t *>(buffer(3 * 8));
+    consts[0] = pimqap::kNoStop;
+    consts[1] = std::numeric_limits<int64_t>::max();
+    consts[2] = (int64_t)~0ull;
+
+    PQ_CUDA(cudaMemsetAsync(base, 0, P.total, q));
+    char *cur = base;
+    SolveDev d{};
+    d.n = n; d.R = R; d.T = T; d.cap = cap; d.spe = P.spe;
+    d.ldg = P.npad; d.lds = P.lds; d.ldm = ldm; d.rpc = P.rpc;
+    d.goal = params->goal;
+    d.seed = params->seed;
+    d.I = carve<char>(cur, reps * (size_t)n * P.npad * (P.bits / 8));
+    int32_t *dD = carve<int32_t>(cur, nn), *dDT = carve<int32_t>(cur, nn);
+    int32_t *dF = carve<int32_t>(cur, nn), *dFT = carve<int32_t>(cur, nn);
+    int32_t *dDd = carve<int32_t>(cur, n), *dFd = carve<int32_t>(cur, n);
+    d.D = dD; d.DT = dDT; d.F = dF; d.FT = dFT; d.Ddiag = dDd; d.Fdiag = dFd;
+    d.phi = carve<int32_t>(cur, reps * n);
+    d.best_phi = carve<int32_t>(cur, reps * n);
+    d.E = carve<int64_t>(cur, reps);
+    d.bestE = carve<int64_t>(cur, reps);
+    d.beta = carve<double>(cur, reps);
+    d.accepts = carve<unsigned long long>(cur, reps);
+    d.order = carve<int32_t>(cur, (size_t)T * cap);
+    d.tss = carve<int32_t>(cur, T);
+    d.group_best = carve<int64_t>(cur, T);
+    d.finish = carve<unsigned int>(cur, T);
+    d.epoch = carve<int32_t>(cur, T);
+    d.single_best = carve<int64_t>(cur, 1);
+    d.stop_epoch = carve<int32_t>(cur, 1);
+    d.target_epoch = carve<int64_t>(cur, 1);
+    d.target_ns = carve<unsigned long long>(cur, 1);
+    d.start_ns = carve<unsigned long long>(cur, 1);
+    d.error = carve<int32_t>(cur, 1);
+    if ((size_t)(cur - base) > P.total) return fail(PIMQAP_ERR_ARG, "internal: device carve overflow");
+    PQ_CUDA(cudaMemcpyAsync(dD, Dp, nn * 4, cudaMemcpyHostToDevice, q));
+    PQ_CUDA(cudaMemcpyAsync(dF, Fp, nn * 4, cudaMemcpyHostToDevice, q));
+    PQ_CUDA(cudaMemcpyAsync(dDT, DT, nn * 4, cudaMemcpyHostToDevice, q));
+    PQ_CUDA(cudaMemcpyAsync(dFT, FT, nn * 4, cudaMemcpyHostToDevice, q));
+    PQ_CUDA(cudaMemcpyAsync(dDd, Dd, (size_t)n * 4, cudaMemcpyHostToDevice, q));
+    PQ_CUDA(cudaMemcpyAsync(dFd, Fd, (size_t)n * 4, cudaMemcpyHostToDevice, q));
+    PQ_CUDA(cudaMemcpyAsync(d.phi, phi, reps * n * 4, cudaMemcpyHostToDevice, q));
+    PQ_CUDA(cudaMemcpyAsync(d.beta, beta, reps * 8, cudaMemcpyHostToDevice, q));
+    PQ_CUDA(cudaMemcpyAsync(d.order, order, (size_t)T * cap * 4, cudaMemcpyHostToDevice, q));
+    PQ_CUDA(cudaMemcpyAsync(d.group_best, nob, (size_t)T * 8, cudaMemcpyHostToDevice, q));
+    PQ_CUDA(cudaMemcpyAsync(d.single_best, nob + T, 8, cudaMemcpyHostToDevice, q));
+    PQ_CUDA(cudaMemcpyAsync(d.stop_epoch, &consts[0], 4, cudaMemcpyHostToDevice, q));
+    PQ_CUDA(cudaMemcpyAsync(d.target_epoch, &consts[1], 8, cudaMemcpyHostToDevice, q));
+    PQ_CUDA(cudaMemcpyAsync(d.target_ns, &consts[2], 8, cudaMemcpyHostToDevice, q));
+    PQ_CUDA(pimqap::launch_setup(d, P.bits, q));
+    *out = d;
+    return PIMQAP_OK;
+}
+
+// Worker shape of a persistent class (the autotuner's knobs): threads per replica worker,
+// workers per CTA (named barriers 1..8) and the shared-memory slice of one worker.
+struct BatchShape {
+    int worker_threads = 128, workers = 1, ctas_per_sm = 1, grid = 1;
+    size_t slice = 0;
+};
+
+BatchShape batch_shape(const std::vector<Plan> &plans, const std::vector<int> &members, int bits,
+                       int sms, int maxsm) {
+    BatchShape S;
+    int nmax = 0;
+    for (int k : members) {
+        S.slice = std::max(S.slice, pimqap::batch_slice_bytes(plans[k].n, bits));
+        nmax = std::max(nmax, plans[k].n);
+    }
+    S.worker_threads = nmax <= 32 ? 32 : (nmax <= 64 ? 64 : 128);
+    S.workers = std::max(1, std::min(256 / S.worker_threads, (int)((size_t)maxsm / S.slice)));
+    int occ = 0;
+    if (pimqap::batch_occupancy(bits, S.workers * S.worker_threads, S.workers * S.slice, &occ) != cudaSuccess || occ < 1)
+        occ = 1;
+    S.ctas_per_sm = occ;
+    S.grid = sms * occ;
+    return S;
+}
+
+// Solves `members` (single-CTA replicas of one force-matrix width) in one persistent launch.
+pimqap_status run_batch_class(const pimqap_instance *insts, const pimqap_params *params,
+                              const std::vector<Plan> &plans, const std::vector<int> &members,
+                              int bits, int sms, int maxsm, pimqap_result *results) {
+    const int m = (int)members.size();
+    const BatchShape S = batch_shape(plans, members, bits, sms, maxsm);
+    size_t reps_total = 0, inst_bytes = 0;
+    std::vector<size_t> offs(m);
+    for (int q = 0; q < m; ++q) {
+        const Plan &P = plans[members[q]];
+        offs[q] = inst_bytes;
+        inst_bytes += carve_size(P.total);
+        reps_total += (size_t)P.T * P.R;
+    }
+    unsigned qcap = 1;
+    while (qcap < reps_total + 1) qcap <<= 1;
+    const size_t total = inst_bytes + carve_size(sizeof(SolveDev) * m) + 3 * carve_size(8 * (size_t)m) +
+                         2 * carve_size(8 * (size_t)qcap) + 6 * carve_size(8);
+    char *base = nullptr;
+    PQ_CUDA(cudaMalloc(&base, total));
+    struct Free {
+        char *p;
+        ~Free() { cudaFree(p); }
+    } free_guard{base};
+    cudaStream_t q = nullptr;
+    PQ_CUDA(cudaStreamCreateWithFlags(&q, cudaStreamNonBlocking));
+    struct FreeStream {
+        cudaStream_t s;
+        ~FreeStream() { cudaStreamDestroy(s); }
+    } stream_guard{q};
+
+    std::vector<SolveDev> devs(m);
+    std::vector<std::vector<char>> keep;
+    for (int i = 0; i < m; ++i) {
+        const int k = members[i];
+        pimqap_status st = stage_instance(&insts[k], &params[k], plans[k], base + offs[i], &devs[i], q, keep);
+        if (st != PIMQAP_OK) return st;
+    }
+    char *cur = base + inst_bytes;
+    SolveDev *d_inst = carve<SolveDev>(cur, m);
+    int32_t *d_sym = reinterpret_cast<int32_t *>(carve<int64_t>(cur, m));
+    int64_t *d_maxm = carve<int64_t>(cur, m);
+    unsigned int *d_finish = reinterpret_cast<unsigned int *>(carve<int64_t>(cur, m));
+    unsigned long long *d_items = carve<unsigned long long>(cur, qcap);
+    unsigned long long *d_seq = carve<unsigned long long>(cur, qcap);
+    unsigned long long *d_head = carve<unsigned long long>(cur, 1);
+    unsigned long long *d_tail = carve<unsigned long long>(cur, 1);
+    int32_t *d_active = reinterpret_cast<int32_t *>(carve<int64_t>(cur, 1));
+    int32_t *d_error = reinterpret_cast<int32_t *>(carve<int64_t>(cur, 1));
+    unsigned long long *d_start = carve<unsigned long long>(cur, 1);
+    PQ_CUDA(cudaMemsetAsync(base + inst_bytes, 0, total - inst_bytes, q));
+
+    PQ_CUDA(cudaStreamSynchronize(q));
+    keep.clear();
+    std::vector<int32_t> stop0(m);
+    for (int i = 0; i < m; ++i)
+        PQ_CUDA(cudaMemcpy(&stop0[i], devs[i].stop_epoch, 4, cudaMemcpyDeviceToHost));
+    // Epoch-0 items, largest instances first (they take longest).
+    std::vector<int> order_idx(m);
+    for (int i = 0; i < m; ++i) order_idx[i] = i;
+    std::stable_sort(order_idx.begin(), order_idx.end(), [&](int a, int b) {
+        const Plan &A = plans[members[a]], &B = plans[members[b]];
+        return (double)A.n * A.n * A.T * A.R > (double)B.n * B.n * B.T * B.R;
+    });
+    std::vector<int32_t> sym(2 * m, 0);
+    std::vector<int64_t> maxm(m);
+    std::vector<unsigned long long> items, seq;
+    int active = 0;
+    for (int i = 0; i < m; ++i) {
+        sym[i] = plans[members[i]].sym ? 1 : 0;
+        maxm[i] = params[members[i]].max_megaiters;
+    }
+    for (int i : order_idx) {
+        const Plan &P = plans[members[i]];
+        if (maxm[i] <= 0 || stop0[i] <= 0) continue;   // nothing to run, or goal met at setup
+        ++active;
+        for (int r = 0; r < P.T * P.R; ++r) {
+            items.push_back(((unsigned long long)i << 32) | (unsigned)r);
+            seq.push_back(items.size());
+        }
+    }
+    const unsigned long long tail = items.size();
+    PQ_CUDA(cudaMemcpyAsync(d_inst, devs.data(), sizeof(SolveDev) * m, cudaMemcpyHostToDevice, q));
+    PQ_CUDA(cudaMemcpyAsync(d_sym, sym.data(), 4 * (size_t)m, cudaMemcpyHostToDevice, q));
+    PQ_CUDA(cudaMemcpyAsync(d_maxm, maxm.data(), 8 * (size_t)m, cudaMemcpyHostToDevice, q));
+    if (!items.empty()) {
+        PQ_CUDA(cudaMemcpyAsync(d_items, items.data(), 8 * items.size(), cudaMemcpyHostToDevice, q));
+        PQ_CUDA(cudaMemcpyAsync(d_seq, seq.data(), 8 * seq.size(), cudaMemcpyHostToDevice, q));
+    }
+    PQ_CUDA(cudaMemcpyAsync(d_tail, &tail, 8, cudaMemcpyHostToDevice, q));
+    PQ_CUDA(cudaMemcpyAsync(d_active, &active, 4, cudaMemcpyHostToDevice, q));
+    PQ_CUDA(cudaStreamSynchronize(q));
+    keep.clear();
+
+    pimqap::BatchDev B{};
+    B.inst = d_inst; B.sym = d_sym; B.max_megaiters = d_maxm; B.finish_inst = d_finish;
+    B.count = m; B.q_items = d_items; B.q_seq = d_seq; B.q_head = d_head; B.q_tail = d_tail;
+    B.qmask = qcap - 1; B.active = d_active; B.error = d_error; B.start_ns = d_start;
+    B.worker_threads = S.worker_threads; B.workers = S.workers; B.slice_bytes = (unsigned)S.slice;
+    cudaEvent_t e0, e1;
+    PQ_CUDA(cudaEventCreate(&e0));
+    PQ_CUDA(cudaEventCreate(&e1));
+    PQ_CUDA(cudaEventRecord(e0, q));
+    if (active > 0) PQ_CUDA(pimqap::launch_batch(B, bits, S.grid, q));
+    PQ_CUDA(cudaEventRecord(e1, q));
+    PQ_CUDA(cudaStreamSynchronize(q));
+    float ms = 0;
+    cudaEventElapsedTime(&ms, e0, e1);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    int32_t err = 0;
+    unsigned long long start_ns = 0;
+    PQ_CUDA(cudaMemcpy(&err, d_error, 4, cudaMemcpyDeviceToHost));
+    PQ_CUDA(cudaMemcpy(&start_ns, d_start, 8, cudaMemcpyDeviceToHost));
+    if (err) return fail(PIMQAP_ERR_DEVICE, "batch kernel check failed (error word " + std::to_string(err) + ")");
+
+    for (int i = 0; i < m; ++i) {
+        const int k = members[i];
+        const SolveDev &d = devs[i];
+        const Plan &P = plans[k];
+        const size_t reps = (size_t)P.T * P.R;
+        std::vector<int64_t> bestE(reps);
+        std::vector<unsigned long long> acc(reps);
+        int64_t single = 0, tepoch = 0;
+        unsigned long long tns = 0;
+        int32_t epoch0 = 0, ierr = 0;
+        PQ_CUDA(cudaMemcpy(bestE.data(), d.bestE, reps * 8, cudaMemcpyDeviceToHost));
+        PQ_CUDA(cudaMemcpy(acc.data(), d.accepts, reps * 8, cudaMemcpyDeviceToHost));
+        PQ_CUDA(cudaMemcpy(&single, d.single_best, 8, cudaMemcpyDeviceToHost));
+        PQ_CUDA(cudaMemcpy(&tepoch, d.target_epoch, 8, cudaMemcpyDeviceToHost));
+        PQ_CUDA(cudaMemcpy(&tns, d.target_ns, 8, cudaMemcpyDeviceToHost));
+        PQ_CUDA(cudaMemcpy(&epoch0, d.epoch, 4, cudaMemcpyDeviceToHost));
+        PQ_CUDA(cudaMemcpy(&ierr, d.error, 4, cudaMemcpyDeviceToHost));
+        if (ierr) return fail(PIMQAP_ERR_DEVICE, "device check failed in batch instance " + std::to_string(k));
+        size_t arg = 0;
+        for (size_t r = 1; r < reps; ++r)
+            if (bestE[r] < bestE[arg]) arg = r;
+        pimqap_result &R = results[k];
+        int32_t *perm_dst = R.best_perm;
+        std::memset(&R, 0, sizeof(R));
+        R.best_perm = perm_dst;
+        R.best_energy = std::min<int64_t>(bestE[arg], single);
+        if (perm_dst)
+            PQ_CUDA(cudaMemcpy(perm_dst, d.best_phi + arg * P.n, (size_t)P.n * 4, cudaMemcpyDeviceToHost));
+        R.target_megaiter = (tepoch == std::numeric_limits<int64_t>::max()) ? -1 : tepoch;
+        R.time_to_target_ms = (R.target_megaiter >= 0 && tns != ~0ull && tns >= start_ns)
+                                  ? (double)(tns - start_ns) * 1e-6 : (R.target_megaiter >= 0 ? 0.0 : -1.0);
+        R.megaiters_done = epoch0;
+        R.updates = (int64_t)epoch0 * P.spe * P.n * (int64_t)reps;
+        int64_t a = 0;
+        for (auto v : acc) a += (int64_t)v;
+        R.accepts = a;
+        R.device_ms = ms;
+        R.force_bits = P.bits;
+        R.cluster_size = 1;
+        int32_t stop = 0;
+        PQ_CUDA(cudaMemcpy(&stop, d.stop_epoch, 4, cudaMemcpyDeviceToHost));
+        R.stopped_by = (stop != pimqap::kNoStop) ? 1 : 0;
+        R.h2d_bytes = P.h2d_bytes;
+        R.d2h_bytes = (int64_t)(reps * 16 + 40 + (perm_dst ? (size_t)P.n * 4 : 0));
+    }
+    return PIMQAP_OK;
+}
 
 }  // namespace
 
@@ -299,149 +666,37 @@ pimqap_status pimqap_solver_create(const pimqap_instance *inst, const pimqap_par
     *out = nullptr;
     pimqap_status st = check_params(inst, params);
     if (st != PIMQAP_OK) return st;
-    const int n = inst->n;
-    const InstanceInfo info = analyse(n, inst->flow, inst->dist);
-    if (info.bits_needed == 0 && params->force_bits == 0)
-        return fail(PIMQAP_ERR_RANGE, "instance values can overflow int64 force matrices");
-
     auto s = new pimqap_solver();
     std::unique_ptr<pimqap_solver> guard(s);
     s->p = *params;
-    s->n = n;
-    s->T = params->groups;
-    s->R = params->replicas;
-    s->cap = params->rank_slots ? params->rank_slots : std::max(params->replicas, 10);
-    s->spe = params->sweeps_per_exchange;
-    s->sym = info.symmetric;
-    s->bits = params->force_bits ? params->force_bits : info.bits_needed;
     s->device = params->device;
-
-    int ndev = 0;
-    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0)
-        return fail(PIMQAP_ERR_NO_DEVICE, "no CUDA device");
-    if (s->device < 0 || s->device >= ndev) return fail(PIMQAP_ERR_ARG, "bad device ordinal");
-    PQ_CUDA(cudaSetDevice(s->device));
-    cudaDeviceProp prop;
-    PQ_CUDA(cudaGetDeviceProperties(&prop, s->device));
-    if (prop.major != 10) return fail(PIMQAP_ERR_NO_DEVICE, "the kernels are built for sm_100a only");
-    PQ_CUDA(pimqap::prepare_kernels());
-
-    // Launch shape: threads per CTA and the smallest cluster whose row share fits.
-    const int isz = s->bits / 8, vec = 16 / isz;
-    const int npad = round_up(n, 4);
-    int lds = npad;
-    if ((lds / vec) % 2 == 0) lds += vec;
-    s->threads = params->threads_per_block ? params->threads_per_block
-                                           : (n <= 64 ? 64 : (n <= 128 ? 128 : 256));
-    const size_t maxsm = prop.sharedMemPerBlockOptin;
-    s->cl = 0;
-    for (int cl : {1, 2, 4}) {
-        const int rpc = (n + cl - 1) / cl;
-        if (pimqap::epoch_smem_bytes(n, rpc, lds, cl, s->bits) <= maxsm) {
-            s->cl = cl;
-            break;
-        }
-    }
-    if (!s->cl) return fail(PIMQAP_ERR_ARG, "force matrix does not fit a 4-CTA cluster");
-    const int rpc = (n + s->cl - 1) / s->cl;
-    s->smem = pimqap::epoch_smem_bytes(n, rpc, lds, s->cl, s->bits);
-
-    // Host-side setup: transposes, diagonals, permutations, beta ladder, rank slots.
-    const int T = s->T, R = s->R, cap = s->cap;
-    const size_t reps = (size_t)T * R, nn = (size_t)n * n;
-    std::vector<int32_t> DT(nn), FT(nn), Dd(n), Fd(n);
-    for (int i = 0; i < n; ++i) {
-        Dd[i] = inst->dist[i * n + i];
-        Fd[i] = inst->flow[i * n + i];
-        for (int j = 0; j < n; ++j) {
-            DT[i * n + j] = inst->dist[j * n + i];
-            FT[i * n + j] = inst->flow[j * n + i];
-        }
-    }
-    const std::vector<int32_t> perms = initial_perms(n, T, params->seed);
-    std::vector<int32_t> phi(reps * n);
-    for (int t = 0; t < T; ++t)
-        for (int l = 0; l < R; ++l)
-            std::memcpy(&phi[((size_t)t * R + l) * n], &perms[(size_t)t * n], sizeof(int32_t) * n);
-    // beta ladder (CPU_PIM.cpp:111-119); -b is given in natural units and stored x 1/ln 2 (:528)
-    const double beta0 = params->beta_max * 1.44269504089;
-    std::vector<double> beta(reps);
-    for (int t = 0; t < T; ++t) {
-        double running = beta0;
-        for (int l = R - 1; l >= 0; --l) {
-            beta[(size_t)t * R + l] = running;
-            running /= params->beta_ratio;
-        }
-    }
-    std::vector<int32_t> order((size_t)T * cap, 0);
-    for (int t = 0; t < T; ++t)
-        for (int l = 0; l < R; ++l) order[(size_t)t * cap + l] = l;
-
-    // Device memory: one allocation carved into the arrays of SolveDev.
-    const size_t Ibytes = reps * (size_t)n * npad * isz;
-    size_t total = carve_size(Ibytes) + 4 * carve_size(nn * 4) + 2 * carve_size(n * 4) +
-                   2 * carve_size(reps * n * 4) + 4 * carve_size(reps * 8) +
-                   carve_size((size_t)T * cap * 4) + 4 * carve_size((size_t)T * 8) +
-                   8 * carve_size(8);
-    PQ_CUDA(cudaMalloc(&s->dmem, total));
-    s->dbytes = total;
-    PQ_CUDA(cudaMemset(s->dmem, 0, total));
-    char *cur = reinterpret_cast<char *>(s->dmem);
-    SolveDev &d = s->dev;
-    d.n = n; d.R = R; d.T = T; d.cap = cap; d.spe = s->spe;
-    d.ldg = npad; d.lds = lds; d.rpc = rpc;
-    d.goal = params->goal;
-    d.seed = params->seed;
-    d.I = carve<char>(cur, Ibytes);
-    int32_t *dD = carve<int32_t>(cur, nn), *dDT = carve<int32_t>(cur, nn);
-    int32_t *dF = carve<int32_t>(cur, nn), *dFT = carve<int32_t>(cur, nn);
-    int32_t *dDd = carve<int32_t>(cur, n), *dFd = carve<int32_t>(cur, n);
-    d.D = dD; d.DT = dDT; d.F = dF; d.FT = dFT; d.Ddiag = dDd; d.Fdiag = dFd;
-    d.phi = carve<int32_t>(cur, reps * n);
-    d.best_phi = carve<int32_t>(cur, reps * n);
-    d.E = carve<int64_t>(cur, reps);
-    d.bestE = carve<int64_t>(cur, reps);
-    d.beta = carve<double>(cur, reps);
-    d.accepts = carve<unsigned long long>(cur, reps);
-    d.order = carve<int32_t>(cur, (size_t)T * cap);
-    d.tss = carve<int32_t>(cur, T);
-    d.group_best = carve<int64_t>(cur, T);
-    d.finish = carve<unsigned int>(cur, T);
-    d.epoch = carve<int32_t>(cur, T);
-    d.single_best = carve<int64_t>(cur, 1);
-    d.stop_epoch = carve<int32_t>(cur, 1);
-    d.target_epoch = carve<int64_t>(cur, 1);
-    d.target_ns = carve<unsigned long long>(cur, 1);
-    d.start_ns = carve<unsigned long long>(cur, 1);
-    d.error = carve<int32_t>(cur, 1);
-    if ((size_t)(cur - reinterpret_cast<char *>(s->dmem)) > total)
-        return fail(PIMQAP_ERR_ARG, "internal: device carve overflow");
-
+    int maxsm = 0;
+    st = open_device(params->device, &maxsm);
+    if (st != PIMQAP_OK) return st;
+    Plan plan;
+    st = plan_instance(inst, params, (size_t)maxsm, params->cluster_size, &plan);
+    if (st != PIMQAP_OK) return st;
+    s->n = plan.n;
+    s->T = plan.T;
+    s->R = plan.R;
+    s->cap = plan.cap;
+    s->spe = plan.spe;
+    s->sym = plan.sym;
+    s->bits = plan.bits;
+    s->cl = plan.cl;
+    s->threads = plan.threads;
+    s->smem = plan.smem;
+    PQ_CUDA(cudaMalloc(&s->dmem, plan.total));
+    s->dbytes = plan.total;
     PQ_CUDA(cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking));
     PQ_CUDA(cudaEventCreate(&s->ev0));
     PQ_CUDA(cudaEventCreate(&s->ev1));
     cudaStream_t q = s->stream;
-    s->h2d = (int64_t)(4 * nn * 4 + 2 * (size_t)n * 4 + reps * n * 4 + reps * 8 + (size_t)T * cap * 4 +
-                       (size_t)T * 8 + 8 + 4 + 8 + 8);
-    PQ_CUDA(cudaMemcpyAsync(dD, inst->dist, nn * 4, cudaMemcpyHostToDevice, q));
-    PQ_CUDA(cudaMemcpyAsync(dF, inst->flow, nn * 4, cudaMemcpyHostToDevice, q));
-    PQ_CUDA(cudaMemcpyAsync(dDT, DT.data(), nn * 4, cudaMemcpyHostToDevice, q));
-    PQ_CUDA(cudaMemcpyAsync(dFT, FT.data(), nn * 4, cudaMemcpyHostToDevice, q));
-    PQ_CUDA(cudaMemcpyAsync(dDd, Dd.data(), n * 4, cudaMemcpyHostToDevice, q));
-    PQ_CUDA(cudaMemcpyAsync(dFd, Fd.data(), n * 4, cudaMemcpyHostToDevice, q));
-    PQ_CUDA(cudaMemcpyAsync(d.phi, phi.data(), reps * n * 4, cudaMemcpyHostToDevice, q));
-    PQ_CUDA(cudaMemcpyAsync(d.beta, beta.data(), reps * 8, cudaMemcpyHostToDevice, q));
-    PQ_CUDA(cudaMemcpyAsync(d.order, order.data(), (size_t)T * cap * 4, cudaMemcpyHostToDevice, q));
-    std::vector<int64_t> nob(std::max<size_t>(T, 1), pimqap::kNoBest);
-    PQ_CUDA(cudaMemcpyAsync(d.group_best, nob.data(), (size_t)T * 8, cudaMemcpyHostToDevice, q));
-    PQ_CUDA(cudaMemcpyAsync(d.single_best, nob.data(), 8, cudaMemcpyHostToDevice, q));
-    const int32_t nostop = pimqap::kNoStop;
-    const int64_t notarget = std::numeric_limits<int64_t>::max();
-    const unsigned long long nons = ~0ull;
-    PQ_CUDA(cudaMemcpyAsync(d.stop_epoch, &nostop, 4, cudaMemcpyHostToDevice, q));
-    PQ_CUDA(cudaMemcpyAsync(d.target_epoch, &notarget, 8, cudaMemcpyHostToDevice, q));
-    PQ_CUDA(cudaMemcpyAsync(d.target_ns, &nons, 8, cudaMemcpyHostToDevice, q));
-    PQ_CUDA(pimqap::launch_setup(d, s->bits, q));
+    std::vector<std::vector<char>> keep;
+    st = stage_instance(inst, params, plan, reinterpret_cast<char *>(s->dmem), &s->dev, q, keep);
+    if (st != PIMQAP_OK) return st;
+    SolveDev &d = s->dev;
+    s->h2d = plan.h2d_bytes;
     PQ_CUDA(cudaStreamSynchronize(q));
     int32_t err = 0;
     PQ_CUDA(cudaMemcpy(&err, d.error, 4, cudaMemcpyDeviceToHost));
@@ -617,10 +872,48 @@ pimqap_status pimqap_batch_solve(const pimqap_instance *insts, const pimqap_para
                                  int32_t count, pimqap_result *results) {
     if (count < 0 || (count > 0 && (!insts || !params || !results)))
         return fail(PIMQAP_ERR_ARG, "bad batch arguments");
+    if (count == 0) return PIMQAP_OK;
+    const auto wall0 = std::chrono::steady_clock::now();
     for (int k = 0; k < count; ++k) {
-        pimqap_status st = pimqap_solve(&insts[k], &params[k], &results[k]);
+        pimqap_status st = check_params(&insts[k], &params[k]);
+        if (st != PIMQAP_OK) return st;
+        if (params[k].device != params[0].device)
+            return fail(PIMQAP_ERR_ARG, "every batch entry must use the same device");
+    }
+    int maxsm = 0;
+    pimqap_status st = open_device(params[0].device, &maxsm);
+    if (st != PIMQAP_OK) return st;
+    int sms = 0;
+    PQ_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, params[0].device));
+
+    std::vector<Plan> plans(count);
+    for (int k = 0; k < count; ++k) {
+        st = plan_instance(&insts[k], &params[k], (size_t)maxsm, params[k].cluster_size, &plans[k]);
         if (st != PIMQAP_OK) return st;
     }
+    // Persistent classes: single-CTA replicas by force-matrix width.  Replicas that need a
+    // cluster are solved by the epoch launches of pimqap_solve.
+    std::vector<int> cluster_members;
+    for (int bits : {32, 64}) {
+        std::vector<int> members;
+        for (int k = 0; k < count; ++k) {
+            if (plans[k].bits != bits) continue;
+            if (plans[k].cl != 1 || pimqap::batch_slice_bytes(plans[k].n, bits) > (size_t)maxsm) continue;
+            members.push_back(k);
+        }
+        if (members.empty()) continue;
+        st = run_batch_class(insts, params, plans, members, bits, sms, maxsm, results);
+        if (st != PIMQAP_OK) return st;
+    }
+    for (int k = 0; k < count; ++k) {
+        const bool in_class = plans[k].cl == 1 &&
+                              pimqap::batch_slice_bytes(plans[k].n, plans[k].bits) <= (size_t)maxsm;
+        if (in_class) continue;
+        st = pimqap_solve(&insts[k], &params[k], &results[k]);
+        if (st != PIMQAP_OK) return st;
+    }
+    const double el = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - wall0).count();
+    for (int k = 0; k < count; ++k) results[k].wall_ms = el;
     return PIMQAP_OK;
 }
 

@@ -18,6 +18,7 @@ constexpr int64_t kNoBest = 2147483647;  // the reference's INT_MAX sentinel
 enum : int32_t {
     kErrBadPerm = 1,      // a permutation loaded from global memory is not a bijection
     kErrShape = 2,        // launch shape does not match the solve
+    kErrTimeout = 4,      // a bounded wait for a peer CTA's data gave up
 };
 
 // Everything one solve (one instance, T groups x R replicas) keeps in device memory.
@@ -26,10 +27,11 @@ struct SolveDev {
     int n, R, T, cap, spe;     // size, replicas/group, groups, rank slots, sweeps per epoch
     int ldg;                   // row stride of I in global memory (elements, 16-byte rows)
     int lds;                   // row stride of I in shared memory (elements)
-    int rpc;                   // rows of I per CTA (= ceil(n / cluster size))
+    int ldm;                   // row stride of D, DT, F, FT (int32 elements, multiple of 4)
+    int rpc;                   // rows of I per CTA (ceil(n / cluster size) rounded up to 4)
     int64_t goal;
     uint64_t seed;
-    const int32_t *D, *DT, *F, *FT;  // n*n each, row-major (DT = D transposed)
+    const int32_t *D, *DT, *F, *FT;  // n rows of ldm each, zero padded (DT = D transposed)
     const int32_t *Ddiag, *Fdiag;    // n each
     void *I;                   // [T*R][n][ldg] of int32 or int64
     int32_t *phi;              // [T*R][n]  facility at location
@@ -49,6 +51,37 @@ struct SolveDev {
     unsigned long long *start_ns;   // [1]  %globaltimer when sweeping started
     int32_t *error;            // [1]       kErr* bits
 };
+
+// A batch of independent solves run by one persistent launch.  Work items are replica-epochs
+// (instance k, replica rep) in a ring buffer; the last replica of an instance to finish an
+// epoch runs the tracking / exchange of all its groups and enqueues the next epoch.
+struct BatchDev {
+    const SolveDev *inst;            // [count] per-instance descriptors
+    const int32_t *sym;              // [count] 1 when D and F are symmetric
+    const int64_t *max_megaiters;    // [count]
+    unsigned int *finish_inst;       // [count] replicas done with the current epoch
+    int count;
+    unsigned long long *q_items;     // [qmask + 1] (instance << 32) | replica
+    unsigned long long *q_seq;       // [qmask + 1] ticket + 1 once the slot holds that ticket
+    unsigned long long *q_head;      // [1] next ticket to pop
+    unsigned long long *q_tail;      // [1] next ticket to push
+    unsigned int qmask;
+    int32_t *active;                 // [1] instances still running
+    int32_t *error;                  // [1] kErr* bits
+    unsigned long long *start_ns;    // [1] %globaltimer when the launch began
+    int worker_threads;              // threads of one replica worker (a multiple of 32)
+    int workers;                     // workers per CTA (<= 8)
+    unsigned int slice_bytes;        // shared memory of one worker
+};
+
+// Shared memory of one replica worker of the batch kernel (single-CTA replica of size n).
+size_t batch_slice_bytes(int n, int bits);
+
+// The persistent batch launch: grid CTAs of workers * worker_threads threads.
+cudaError_t launch_batch(const BatchDev &b, int bits, int grid, cudaStream_t st);
+
+// Resident CTAs per SM of the batch kernel for this shape.
+cudaError_t batch_occupancy(int bits, int threads, size_t smem, int *ctas_per_sm);
 
 // Records msg as the calling thread's pimqap_last_error() text.
 void set_last_error(const char *msg);

@@ -46,27 +46,41 @@ template <class IT> struct alignas(16) Vec {
 __host__ __device__ inline size_t align16(size_t x) { return (x + 15) & ~size_t(15); }
 
 // Offsets (bytes) of the epoch kernel's shared-memory sections.
+//   I       rpc rows of the replica's force matrix (row stride lds)
+//   phi, inv, bphi, Dd, Fd    permutation, inverse, best permutation, diagonals of D and F
+//   A, B    [2][npad] receive buffers of the two delta halves (double-buffered by update)
+//   Drow, DTrow  [2][rpc]  D[i][own rows], D[own rows][i] for the current / next location i
+//   Frow, FTrow  [2][npad] F[a][*], F[*][a] for a = phi(i), current / next
+//   Dj, DTj, Fb, FTb        the same rows for the partner j / facility b of an accepted swap
+//   red, wsum, r, misc, bar  reductions, random number, pick, mbarriers
 struct SmemLayout {
-    size_t I, phi, inv, bphi, Dd, Fd, dE, u1, u2, v1, v2, wmax, wsum, r, misc, total;
+    size_t I, phi, inv, bphi, Dd, Fd, A, B, Drow, DTrow, Frow, FTrow, Dj, DTj, Fb, FTb;
+    size_t red, wsum, r, misc, bar, total;
     __host__ __device__ SmemLayout(int n, int rpc, int lds, int cluster, int isz) {
         const size_t npad = (size_t)((n + 3) & ~3);
-        const size_t rpad = (size_t)((rpc + 3) & ~3);
+        const size_t rp = (size_t)rpc;
         size_t o = 0;
-        I = o;    o = align16(o + (size_t)rpc * lds * isz);
-        phi = o;  o = align16(o + npad * 4);
-        inv = o;  o = align16(o + npad * 4);
-        bphi = o; o = align16(o + npad * 4);
-        Dd = o;   o = align16(o + npad * 4);
-        Fd = o;   o = align16(o + npad * 4);
-        dE = o;   o = align16(o + 2 * npad * isz);
-        u1 = o;   o = align16(o + rpad * isz);
-        u2 = o;   o = align16(o + rpad * isz);
-        v1 = o;   o = align16(o + npad * isz);
-        v2 = o;   o = align16(o + npad * isz);
-        wmax = o; o = align16(o + 2 * (size_t)cluster * kMaxWarps * isz);
-        wsum = o; o = align16(o + kMaxWarps * sizeof(double));
-        r = o;    o = align16(o + 2 * sizeof(double));
-        misc = o; o = align16(o + 4 * sizeof(int));
+        I = o;     o = align16(o + rp * lds * isz);
+        phi = o;   o = align16(o + npad * 4);
+        inv = o;   o = align16(o + npad * 4);
+        bphi = o;  o = align16(o + npad * 4);
+        Dd = o;    o = align16(o + npad * 4);
+        Fd = o;    o = align16(o + npad * 4);
+        A = o;     o = align16(o + 2 * npad * isz);
+        B = o;     o = align16(o + (cluster > 1 ? 2 * npad * isz : 0));
+        Drow = o;  o = align16(o + 2 * rp * 4);
+        DTrow = o; o = align16(o + 2 * rp * 4);
+        Frow = o;  o = align16(o + 2 * npad * 4);
+        FTrow = o; o = align16(o + 2 * npad * 4);
+        Dj = o;    o = align16(o + rp * 4);
+        DTj = o;   o = align16(o + rp * 4);
+        Fb = o;    o = align16(o + npad * 4);
+        FTb = o;   o = align16(o + npad * 4);
+        red = o;   o = align16(o + kMaxWarps * 8);
+        wsum = o;  o = align16(o + kMaxWarps * sizeof(double));
+        r = o;     o = align16(o + 2 * sizeof(double));
+        misc = o;  o = align16(o + 4 * sizeof(int));
+        bar = o;   o = align16(o + 2 * sizeof(unsigned long long));
         total = o;
     }
 };
@@ -132,6 +146,96 @@ template <class IT> __device__ __forceinline__ IT warp_max(IT v) {
     return v;
 }
 
+// ---- shared::cluster addressing, mbarriers, asynchronous remote stores, async copies
+
+__device__ __forceinline__ uint32_t smem_u32(const void *p) {
+    return (uint32_t)__cvta_generic_to_shared(p);
+}
+__device__ __forceinline__ uint32_t cluster_addr(uint32_t cta_addr, int rank) {
+    uint32_t r;
+    asm volatile("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(r) : "r"(cta_addr), "r"(rank));
+    return r;
+}
+__device__ __forceinline__ void mbar_init(uint32_t bar, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_fence_init() {
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+__device__ __forceinline__ void mbar_arrive_expect_tx(uint32_t bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes)
+                 : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint32_t bar, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.acquire.cluster.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(bar), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+// Bounded wait: gives up (returns false) after limit_ns of global time.
+__device__ __forceinline__ bool mbar_wait_bounded(uint32_t bar, uint32_t parity,
+                                                  unsigned long long limit_ns) {
+    if (mbar_try_wait(bar, parity)) return true;
+    const unsigned long long t0 = globaltimer_ns();
+    while (!mbar_try_wait(bar, parity)) {
+        if (globaltimer_ns() - t0 > limit_ns) return false;
+    }
+    return true;
+}
+__device__ __forceinline__ void st_async(uint32_t dst, int32_t v, uint32_t bar) {
+    asm volatile("st.async.shared::cluster.mbarrier::complete_tx::bytes.b32 [%0], %1, [%2];"
+                 ::"r"(dst), "r"(v), "r"(bar) : "memory");
+}
+__device__ __forceinline__ void st_async(uint32_t dst, int64_t v, uint32_t bar) {
+    asm volatile("st.async.shared::cluster.mbarrier::complete_tx::bytes.b64 [%0], %1, [%2];"
+                 ::"r"(dst), "l"(v), "r"(bar) : "memory");
+}
+__device__ __forceinline__ void st_async16(uint32_t dst, const Vec<int32_t> &v, uint32_t bar) {
+    asm volatile(
+        "st.async.shared::cluster.mbarrier::complete_tx::bytes.v4.b32 [%0], {%1, %2, %3, %4}, [%5];"
+        ::"r"(dst), "r"(v.v[0]), "r"(v.v[1]), "r"(v.v[2]), "r"(v.v[3]), "r"(bar) : "memory");
+}
+__device__ __forceinline__ void st_async16(uint32_t dst, const Vec<int64_t> &v, uint32_t bar) {
+    asm volatile(
+        "st.async.shared::cluster.mbarrier::complete_tx::bytes.v2.b64 [%0], {%1, %2}, [%3];"
+        ::"r"(dst), "l"(v.v[0]), "l"(v.v[1]), "r"(bar) : "memory");
+}
+__device__ __forceinline__ void cp_async16(void *smem, const void *gmem) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(smem_u32(smem)), "l"(gmem)
+                 : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
+
+// Copies rows of 16-byte chunks global -> shared with cp.async, spread over the CTA.
+//   D slice:  nD chunks from gD to sD (and gDT to sDT when two)
+//   F row:    nF chunks from gF to sF (and gFT to sFT)
+template <bool SYM>
+__device__ __forceinline__ void prefetch_rows(int tid, int BT, int nD, const int32_t *gD,
+                                              const int32_t *gDT, int32_t *sD, int32_t *sDT,
+                                              int nF, const int32_t *gF, const int32_t *gFT,
+                                              int32_t *sF, int32_t *sFT) {
+    const int per = SYM ? (nD + nF) : 2 * (nD + nF);
+    for (int q = tid; q < per; q += BT) {
+        int k = q;
+        if (k < nD) { cp_async16(sD + 4 * k, gD + 4 * k); continue; }
+        k -= nD;
+        if (k < nF) { cp_async16(sF + 4 * k, gF + 4 * k); continue; }
+        k -= nF;
+        if constexpr (!SYM) {
+            if (k < nD) { cp_async16(sDT + 4 * k, gDT + 4 * k); continue; }
+            k -= nD;
+            cp_async16(sFT + 4 * k, gFT + 4 * k);
+        }
+    }
+    cp_async_commit();
+}
+
 // ------------------------------------------------------------------ tracking + exchange
 
 // Best tracking, replica exchange and goal test of group g at the start of mega-iteration
@@ -143,8 +247,8 @@ __device__ void track_exchange(const SolveDev &s, int g, int e_next) {
     volatile int64_t *bestE = s.bestE + (size_t)g * R;
     volatile double *beta = s.beta + (size_t)g * R;
     volatile int32_t *order = s.order + (size_t)g * cap;
-    int tss = s.tss[g] + 1;                                  // :295
-    int64_t gb = s.group_best[g];
+    int tss = *((volatile int32_t *)s.tss + g) + 1;          // :295
+    int64_t gb = *((volatile int64_t *)s.group_best + g);
     bool found = false;
     for (int l = 0; l < R; ++l) {                            // :297-314
         const int64_t b = bestE[l];
@@ -203,10 +307,11 @@ __global__ void __launch_bounds__(256) init_force_kernel(SolveDev s) {
         const int j = j0 + tx;
         const bool jok = j < n;
         const int pj = jok ? phi[j] : 0;
-        sD[ty][tx] = (i < n && jok) ? s.D[i * n + j] : 0;
-        sDT[ty][tx] = (i < n && jok) ? s.DT[i * n + j] : 0;
-        sFp[ty][tx] = (arow < n && jok) ? s.F[arow * n + pj] : 0;
-        sFTp[ty][tx] = (arow < n && jok) ? s.FT[arow * n + pj] : 0;
+        const int ld = s.ldm;
+        sD[ty][tx] = (i < n && jok) ? s.D[i * ld + j] : 0;
+        sDT[ty][tx] = (i < n && jok) ? s.DT[i * ld + j] : 0;
+        sFp[ty][tx] = (arow < n && jok) ? s.F[arow * ld + pj] : 0;
+        sFTp[ty][tx] = (arow < n && jok) ? s.FT[arow * ld + pj] : 0;
         __syncthreads();
 #pragma unroll
         for (int k = 0; k < 16; ++k)
@@ -250,26 +355,50 @@ __global__ void init_exchange_kernel(SolveDev s) {
 
 // ------------------------------------------------------------------ the epoch kernel
 
+// Limit of one bounded wait for a peer CTA's delta halves.  A healthy wait lasts
+// microseconds; after a timeout the CTA records kErrTimeout and stops sweeping.
+constexpr unsigned long long kWaitLimitNs = 2000000000ull;
+
+// A replica worker: the whole CTA (bar == 0, __syncthreads) or a group of warps of it that
+// synchronises on its own named barrier (bar = 1..15), so several workers share one CTA.
+struct Grp {
+    int tid, BT, lane, warp, nwarps, bar;
+    __device__ __forceinline__ void sync() const {
+        if (bar == 0) __syncthreads();
+        else asm volatile("bar.sync %0, %1;" ::"r"(bar), "r"(BT) : "memory");
+    }
+    __device__ __forceinline__ bool sync_or(bool v) const {
+        if (bar == 0) return __syncthreads_or(v) != 0;
+        uint32_t r;
+        asm volatile(
+            "{\n\t.reg .pred p, q;\n\tsetp.ne.u32 p, %1, 0;\n\t"
+            "bar.red.or.pred q, %2, %3, p;\n\tselp.u32 %0, 1, 0, q;\n\t}"
+            : "=r"(r)
+            : "r"((uint32_t)v), "r"(bar), "r"(BT)
+            : "memory");
+        return r != 0;
+    }
+};
+
+template <int CL> __device__ __forceinline__ void cluster_sync(const Grp &G) {
+    if constexpr (CL == 1) G.sync();
+    else cluster_barrier<CL>();
+}
+
+// One epoch of replica rep: load its state into shared memory, spe sweeps (doMegaItera,
+// CPU_PIM.cpp:195-290), store the state back.  With CL > 1 this CTA is rank `rank` of the
+// replica's cluster and G is the whole CTA.  Replica state is read through L2 (__ldcg): the
+// previous epoch may have run on another SM.  Returns false when a bounded wait gave up.
 template <class IT, int CL, bool SYM>
-__global__ void __launch_bounds__(256) epoch_kernel(SolveDev s) {
+__device__ bool replica_epoch(const SolveDev &s, int rep, int rank, int e, const Grp &G,
+                              unsigned char *smem) {
     using U = typename Unsigned<IT>::type;
     constexpr int VEC = Vec<IT>::kN;
-    extern __shared__ __align__(16) unsigned char smem[];
-
     const int n = s.n;
-    const int tid = threadIdx.x, BT = blockDim.x;
-    const int lane = tid & 31, warp = tid >> 5, nwarps = BT >> 5;
-    int rank = 0;
-    if constexpr (CL > 1) rank = (int)cg::this_cluster().block_rank();
-    const int rep = blockIdx.x / CL;
+    const int tid = G.tid, BT = G.BT, lane = G.lane, warp = G.warp, nwarps = G.nwarps;
     const int g = rep / s.R, l = rep - g * s.R;
 
-    // Every CTA of a group reads the same epoch and stop values: stop_epoch only drops to
-    // epoch+1 during this launch, so the test below cannot differ inside a cluster or group.
-    const int e = *((volatile int32_t *)s.epoch + g);
-    if (e >= *(volatile int32_t *)s.stop_epoch) return;
-
-    const int rpc = s.rpc, lds = s.lds;
+    const int rpc = s.rpc, lds = s.lds, ldm = s.ldm;
     const int row0 = rank * rpc;
     const int rows = max(0, min(rpc, n - row0));
     const int npad = (n + 3) & ~3;
@@ -280,29 +409,36 @@ __global__ void __launch_bounds__(256) epoch_kernel(SolveDev s) {
     int32_t *s_bphi = reinterpret_cast<int32_t *>(smem + L.bphi);
     int32_t *s_Dd = reinterpret_cast<int32_t *>(smem + L.Dd);
     int32_t *s_Fd = reinterpret_cast<int32_t *>(smem + L.Fd);
-    IT *s_dE = reinterpret_cast<IT *>(smem + L.dE);
-    IT *s_u1 = reinterpret_cast<IT *>(smem + L.u1);
-    IT *s_u2 = reinterpret_cast<IT *>(smem + L.u2);
-    IT *s_v1 = reinterpret_cast<IT *>(smem + L.v1);
-    IT *s_v2 = reinterpret_cast<IT *>(smem + L.v2);
-    IT *s_wmax = reinterpret_cast<IT *>(smem + L.wmax);
+    IT *s_A = reinterpret_cast<IT *>(smem + L.A);
+    IT *s_B = reinterpret_cast<IT *>(smem + L.B);
+    int32_t *s_Drow = reinterpret_cast<int32_t *>(smem + L.Drow);
+    int32_t *s_DTrow = reinterpret_cast<int32_t *>(smem + L.DTrow);
+    int32_t *s_Frow = reinterpret_cast<int32_t *>(smem + L.Frow);
+    int32_t *s_FTrow = reinterpret_cast<int32_t *>(smem + L.FTrow);
+    int32_t *s_Dj = reinterpret_cast<int32_t *>(smem + L.Dj);
+    int32_t *s_DTj = reinterpret_cast<int32_t *>(smem + L.DTj);
+    int32_t *s_Fb = reinterpret_cast<int32_t *>(smem + L.Fb);
+    int32_t *s_FTb = reinterpret_cast<int32_t *>(smem + L.FTb);
+    IT *s_red = reinterpret_cast<IT *>(smem + L.red);
     double *s_wsum = reinterpret_cast<double *>(smem + L.wsum);
     double *s_r = reinterpret_cast<double *>(smem + L.r);
-    int *s_misc = reinterpret_cast<int *>(smem + L.misc);   // [0] pick, [1] improved-at
+    int *s_misc = reinterpret_cast<int *>(smem + L.misc);   // [0] pick, [1] improved-at, [2] error
+    unsigned long long *s_bar = reinterpret_cast<unsigned long long *>(smem + L.bar);
+    const int nDc = rpc / 4, nFc = npad / 4;                 // 16-byte chunks of a D slice / F row
 
-    // ---- load the replica
+    // ---- load the replica and prefetch the rows of update 0
     {
         const IT *gI = reinterpret_cast<const IT *>(s.I) + ((size_t)rep * n + row0) * s.ldg;
         const int nvg = s.ldg / VEC;
         for (int idx = tid; idx < rows * nvg; idx += BT) {
             const int k = idx / nvg, v = idx - k * nvg;
-            *reinterpret_cast<Vec<IT> *>(sI + (size_t)k * lds + v * VEC) =
-                *reinterpret_cast<const Vec<IT> *>(gI + (size_t)k * s.ldg + v * VEC);
+            const int4 w = __ldcg(reinterpret_cast<const int4 *>(gI + (size_t)k * s.ldg + v * VEC));
+            *reinterpret_cast<int4 *>(sI + (size_t)k * lds + v * VEC) = w;
         }
         const int32_t *gphi = s.phi + (size_t)rep * n;
         for (int q = tid; q < npad; q += BT) {
             // an entry outside [0, n) would index out of range: clamp it and flag the error
-            int p = q < n ? gphi[q] : 0;
+            int p = q < n ? __ldcg(gphi + q) : 0;
             if ((unsigned)p >= (unsigned)n) {
                 atomicOr(s.error, kErrBadPerm);
                 p = 0;
@@ -316,102 +452,146 @@ __global__ void __launch_bounds__(256) epoch_kernel(SolveDev s) {
         if (tid == 0) {
             s_misc[0] = 0x7fffffff;
             s_misc[1] = -1;
+            s_misc[2] = 0;
+            if constexpr (CL > 1) {
+                mbar_init(smem_u32(&s_bar[0]), 1);
+                mbar_init(smem_u32(&s_bar[1]), 1);
+                mbar_fence_init();
+            }
         }
+        G.sync();
+        const int a0 = s_phi[0];
+        prefetch_rows<SYM>(tid, BT, nDc, s.D + row0, s.DT + row0, s_Drow, s_DTrow, nFc,
+                           s.F + (size_t)a0 * ldm, s.FT + (size_t)a0 * ldm, s_Frow, s_FTrow);
     }
-    __syncthreads();
     for (int q = tid; q < n; q += BT) s_inv[s_phi[q]] = q;
+    cp_async_wait_all();
+    cluster_sync<CL>(G);   // every CTA of the cluster is resident, initialised, rows loaded
 
-    // Pointers into every CTA of the cluster (delta / maxima scatter, remote rows of I).
-    IT *dE_at[CL];
-    IT *wmax_at[CL];
+    // shared::cluster addresses of every CTA's receive buffers and mbarriers
+    uint32_t A_at[CL], B_at[CL], bar_at[CL];
     if constexpr (CL > 1) {
-        cg::cluster_group cluster = cg::this_cluster();
 #pragma unroll
         for (int r = 0; r < CL; ++r) {
-            dE_at[r] = cluster.map_shared_rank(s_dE, r);
-            wmax_at[r] = cluster.map_shared_rank(s_wmax, r);
+            A_at[r] = cluster_addr(smem_u32(s_A), r);
+            B_at[r] = cluster_addr(smem_u32(s_B), r);
+            bar_at[r] = cluster_addr(smem_u32(s_bar), r);
         }
-    } else {
-        dE_at[0] = s_dE;
-        wmax_at[0] = s_wmax;
     }
-    cluster_barrier<CL>();   // every CTA of the cluster is resident and initialised
+    const uint32_t tx_bytes = (uint32_t)((npad + n) * sizeof(IT));
+    uint32_t phase = 0;                                      // bit p: parity of s_bar[p]
 
-    const double beta = s.beta[rep];
+    const double beta = __ldcg(s.beta + rep);
     const double cut_span = 20.0 / beta;                    // CPU_PIM.cpp:234
-    int64_t E = s.E[rep], bestE = s.bestE[rep];
+    int64_t E = __ldcg((const long long *)s.E + rep), bestE = __ldcg((const long long *)s.bestE + rep);
     unsigned long long accepts = 0;
     const uint32_t k0 = (uint32_t)s.seed, k1 = (uint32_t)(s.seed >> 32);
     const int K = (n + BT - 1) / BT;                         // weights per thread (<= 4)
     const int nvec = npad / VEC;
+    bool failed = false;
     int upd = 0;                                             // update counter (buffer parity)
 
-    for (int sw = 0; sw < s.spe; ++sw) {
+    for (int sw = 0; sw < s.spe && !failed; ++sw) {
         const uint32_t sweep = (uint32_t)(e * s.spe + sw);
         for (int i = 0; i < n; ++i, ++upd) {
-            const int buf = upd & 1;
-            IT *dEb = s_dE + buf * npad;
+            const int p = upd & 1;
             if (tid == 0) {
                 uint32_t w0, w1;
                 philox_2words((uint32_t)i, sweep, (uint32_t)l, (uint32_t)g, k0, k1, w0, w1);
-                s_r[buf] = canonical53(w0, w1);
+                s_r[p] = canonical53(w0, w1);
+                if constexpr (CL > 1) mbar_arrive_expect_tx(smem_u32(&s_bar[p]), tx_bytes);
             }
             const int a = s_phi[i];
+            const int inext = (i + 1 == n) ? 0 : i + 1;
+            const int32_t *Di = s_Drow + p * rpc;            // D[i][own rows]
+            const int32_t *DTi = SYM ? Di : s_DTrow + p * rpc;
+            const int32_t *Fa = s_Frow + p * npad;           // F[a][*]
+            const int32_t *FTa = SYM ? Fa : s_FTrow + p * npad;
+            {   // rows of the next update (its facility assumes this update keeps phi)
+                const int an = s_phi[inext];
+                prefetch_rows<SYM>(tid, BT, nDc, s.D + (size_t)inext * ldm + row0,
+                                   s.DT + (size_t)inext * ldm + row0, s_Drow + (p ^ 1) * rpc,
+                                   s_DTrow + (p ^ 1) * rpc, nFc, s.F + (size_t)an * ldm,
+                                   s.FT + (size_t)an * ldm, s_Frow + (p ^ 1) * npad,
+                                   s_FTrow + (p ^ 1) * npad);
+            }
 
-            // ---- 1. swap deltas of the candidates this CTA owns
-            IT lmax = 0;                                     // max starts at 0 (:208)
-            {
-                const int owner = i / rpc;
-                const IT *Ii = sI + (size_t)(i - owner * rpc) * lds;
-                if constexpr (CL > 1) {
-                    if (owner != rank) Ii = cg::this_cluster().map_shared_rank(Ii, owner);
-                }
-                const IT Iia = Ii[a];
-                const int32_t Dii = s_Dd[i], Faa = s_Fd[a];
-                for (int jj = tid; jj < rows; jj += BT) {
-                    const int j = row0 + jj;
-                    const int b = s_phi[j];
-                    const IT *Ij = sI + (size_t)jj * lds;
-                    const U dd = (U)(IT)Dii + (U)(IT)s_Dd[j] - (U)(IT)__ldg(s.D + i * n + j) -
-                                 (U)(IT)__ldg(s.DT + i * n + j);
-                    const U ff = (U)(IT)Faa + (U)(IT)s_Fd[b] - (U)(IT)__ldg(s.F + a * n + b) -
-                                 (U)(IT)__ldg(s.FT + a * n + b);
-                    const IT dE = (IT)((U)Ii[b] + (U)Ij[a] - (U)Iia - (U)Ij[b] - dd * ff);
+            // ---- 1. delta halves: B from the rows this CTA owns, A from row i's owner
+            const int owner = i / rpc;
+            const int32_t Dii = s_Dd[i], Faa = s_Fd[a];
+            IT Iia = 0;
+            const IT *Ii = sI + (size_t)(i - owner * rpc) * lds;
+            if (owner == rank) Iia = Ii[a];
+            for (int jj = tid; jj < rows; jj += BT) {
+                const int j = row0 + jj;
+                const int b = s_phi[j];
+                const IT *Ij = sI + (size_t)jj * lds;
+                const U dd = (U)(IT)Dii + (U)(IT)s_Dd[j] - (U)(IT)Di[jj] - (U)(IT)DTi[jj];
+                const U ff = (U)(IT)Faa + (U)(IT)s_Fd[b] - (U)(IT)Fa[b] - (U)(IT)FTa[b];
+                const U Bv = (U)Ij[a] - (U)Ij[b] - dd * ff;
+                if constexpr (CL == 1) {
+                    s_A[p * npad + b] = (IT)(Bv + (U)Ii[b] - (U)Iia);
+                } else {
 #pragma unroll
-                    for (int r = 0; r < CL; ++r) dE_at[r][buf * npad + b] = dE;
-                    lmax = dE > lmax ? dE : lmax;
+                    for (int r = 0; r < CL; ++r)
+                        st_async(B_at[r] + (uint32_t)((p * npad + b) * sizeof(IT)), (IT)Bv, bar_at[r] + p * 8);
+                }
+            }
+            if constexpr (CL > 1) {
+                if (owner == rank) {
+                    for (int c4 = tid; c4 < npad / VEC; c4 += BT) {
+                        Vec<IT> v = *reinterpret_cast<const Vec<IT> *>(Ii + c4 * VEC);
+#pragma unroll
+                        for (int q = 0; q < VEC; ++q) v.v[q] = (IT)((U)v.v[q] - (U)Iia);
+#pragma unroll
+                        for (int r = 0; r < CL; ++r)
+                            st_async16(A_at[r] + (uint32_t)((p * npad + c4 * VEC) * sizeof(IT)), v,
+                                       bar_at[r] + p * 8);
+                    }
+                }
+            }
+
+            // ---- 2. all deltas present: max, heat-bath weights, prefix sum, threshold pick
+            bool timeout = false;
+            if constexpr (CL == 1) {
+                G.sync();
+            } else {
+                timeout = !mbar_wait_bounded(smem_u32(&s_bar[p]), (phase >> p) & 1u, kWaitLimitNs);
+                phase ^= 1u << p;
+            }
+            const int b0 = tid * K;
+            IT d[4];
+            double x[4];
+            IT lmax = 0;                                     // max starts at 0 (:208)
+#pragma unroll
+            for (int k = 0; k < 4; ++k) {
+                d[k] = 0;
+                x[k] = 0.0;
+                if (k < K && b0 + k < n) {
+                    const int b = b0 + k;
+                    d[k] = (CL == 1) ? s_A[p * npad + b]
+                                     : (IT)((U)s_A[p * npad + b] + (U)s_B[p * npad + b]);
+                    x[k] = exp2(__dmul_rn(beta, (double)d[k]));
+                    lmax = d[k] > lmax ? d[k] : lmax;
                 }
             }
             lmax = warp_max(lmax);
-            if (lane == 0) {
-#pragma unroll
-                for (int r = 0; r < CL; ++r) wmax_at[r][(buf * CL + rank) * kMaxWarps + warp] = lmax;
+            if (lane == 0) s_red[warp] = lmax;
+            if (G.sync_or(timeout)) {                 // S_max
+                if (tid == 0) atomicOr(s.error, kErrTimeout);
+                failed = true;
+                break;
             }
-            cluster_barrier<CL>();                           // S1
             if (tid == 0) s_misc[0] = 0x7fffffff;
-
-            // ---- 2. heat-bath weights, prefix sum in b order, threshold pick
-            IT M = 0;
-            for (int q = 0; q < CL * nwarps; ++q) {
-                const int rr = q / nwarps, ww = q - rr * nwarps;
-                const IT v = s_wmax[(buf * CL + rr) * kMaxWarps + ww];
-                M = v > M ? v : M;
-            }
+            IT M = s_red[0];
+            for (int w = 1; w < nwarps; ++w) M = s_red[w] > M ? s_red[w] : M;
             const long long cut = cutoff_trunc(__dsub_rn((double)M, cut_span));   // :234-235
-            double p[4];
+            double pre[4];
             double local = 0.0;
-            const int b0 = tid * K;
 #pragma unroll
             for (int k = 0; k < 4; ++k) {
-                p[k] = local;
-                if (k < K) {
-                    const int b = b0 + k;
-                    if (b < n) {
-                        const IT d = dEb[b];
-                        if ((long long)d > cut) local = __dadd_rn(local, exp2(__dmul_rn(beta, (double)d)));
-                    }
-                    p[k] = local;
-                }
+                if (k < K && (long long)d[k] > cut && b0 + k < n) local = __dadd_rn(local, x[k]);
+                pre[k] = local;
             }
             double incl = local;
 #pragma unroll
@@ -422,53 +602,48 @@ __global__ void __launch_bounds__(256) epoch_kernel(SolveDev s) {
             double excl = __shfl_up_sync(0xffffffffu, incl, 1);
             if (lane == 0) excl = 0.0;
             if (lane == 31) s_wsum[warp] = incl;
-            __syncthreads();                                 // S2
+            G.sync();                                 // S_scan
             double base = 0.0, total = 0.0;
             for (int w = 0; w < nwarps; ++w) {
                 if (w == warp) base = total;
                 total = __dadd_rn(total, s_wsum[w]);
             }
-            const double target = __dmul_rn(s_r[buf], total);   // :247
+            const double target = __dmul_rn(s_r[p], total);     // :247
             const double X = __dadd_rn(base, excl);
 #pragma unroll
             for (int k = 0; k < 4; ++k) {
                 if (k < K && b0 + k < n) {
-                    if (__dadd_rn(X, p[k]) >= target) {     // :251
+                    if (__dadd_rn(X, pre[k]) >= target) {   // :251
                         atomicMin(&s_misc[0], b0 + k);
                         break;
                     }
                 }
             }
-            __syncthreads();                                 // S3
+            cp_async_wait_all();                             // next update's rows have landed
+            G.sync();                                 // S_pick
             const int bs = s_misc[0];
             if (bs >= n || bs == a) continue;                // no move / self move (:252)
 
             // ---- 3. accepted swap: i gets facility bs, j = phiinv(bs) gets a
             const int j = s_inv[bs];
-            const IT dEsel = dEb[bs];
-            for (int k = tid; k < rows; k += BT) {
-                const int kk = row0 + k;
-                if constexpr (SYM) {
-                    s_u1[k] = (IT)(2 * ((U)(IT)__ldg(s.D + j * n + kk) - (U)(IT)__ldg(s.D + i * n + kk)));
-                } else {
-                    s_u1[k] = (IT)((U)(IT)__ldg(s.DT + j * n + kk) - (U)(IT)__ldg(s.DT + i * n + kk));
-                    s_u2[k] = (IT)((U)(IT)__ldg(s.D + j * n + kk) - (U)(IT)__ldg(s.D + i * n + kk));
-                }
-            }
-            for (int c = tid; c < npad; c += BT) {
-                if constexpr (SYM) {
-                    s_v1[c] = c < n ? (IT)((U)(IT)__ldg(s.F + bs * n + c) - (U)(IT)__ldg(s.F + a * n + c)) : (IT)0;
-                } else {
-                    s_v1[c] = c < n ? (IT)((U)(IT)__ldg(s.FT + bs * n + c) - (U)(IT)__ldg(s.FT + a * n + c)) : (IT)0;
-                    s_v2[c] = c < n ? (IT)((U)(IT)__ldg(s.F + bs * n + c) - (U)(IT)__ldg(s.F + a * n + c)) : (IT)0;
-                }
-            }
-            __syncthreads();                                 // S4
+            const IT dEsel = (CL == 1) ? s_A[p * npad + bs]
+                                       : (IT)((U)s_A[p * npad + bs] + (U)s_B[p * npad + bs]);
+            prefetch_rows<SYM>(tid, BT, nDc, s.D + (size_t)j * ldm + row0, s.DT + (size_t)j * ldm + row0,
+                               s_Dj, s_DTj, nFc, s.F + (size_t)bs * ldm, s.FT + (size_t)bs * ldm,
+                               s_Fb, s_FTb);
+            cp_async_wait_all();
+            G.sync();                                 // S4: rows j / bs in shared memory
             if (tid == 0) {
                 s_phi[i] = bs;                               // :257-261
                 s_inv[bs] = i;
                 s_phi[j] = a;
                 s_inv[a] = j;
+            }
+            if (j == inext) {   // the next location's facility became a: its F rows are Fa/FTa
+                for (int c = tid; c < npad; c += BT) {
+                    s_Frow[(p ^ 1) * npad + c] = Fa[c];
+                    if constexpr (!SYM) s_FTrow[(p ^ 1) * npad + c] = FTa[c];
+                }
             }
             E -= (int64_t)dEsel;                             // :256
             ++accepts;
@@ -477,53 +652,41 @@ __global__ void __launch_bounds__(256) epoch_kernel(SolveDev s) {
                 if (tid == 0) s_misc[1] = upd;
             }
             // I[k][c] += (D[k][j]-D[k][i])(F[c][b]-F[c][a]) + (D[j][k]-D[i][k])(F[b][c]-F[a][c])
-            if (nvec <= BT) {
-                const int kstep = BT / nvec;
-                const int cv = tid % nvec;
-                int k = tid / nvec;
-                if (k < kstep) {
-                    const Vec<IT> v1 = *reinterpret_cast<const Vec<IT> *>(s_v1 + cv * VEC);
-                    Vec<IT> v2;
-                    if constexpr (!SYM) v2 = *reinterpret_cast<const Vec<IT> *>(s_v2 + cv * VEC);
-                    for (; k < rows; k += kstep) {
-                        Vec<IT> *dst = reinterpret_cast<Vec<IT> *>(sI + (size_t)k * lds + cv * VEC);
-                        Vec<IT> x = *dst;
-                        const U u1 = (U)s_u1[k];
-                        if constexpr (SYM) {
+            for (int cv = tid % nvec, k0r = tid / nvec, kstep = max(1, BT / nvec);
+                 cv < nvec; cv += (BT >= nvec ? nvec : BT)) {
+                if (BT >= nvec && k0r >= kstep) break;
+                Vec<IT> v1, v2;
 #pragma unroll
-                            for (int q = 0; q < VEC; ++q) x.v[q] = (IT)((U)x.v[q] + u1 * (U)v1.v[q]);
-                        } else {
-                            const U u2 = (U)s_u2[k];
-#pragma unroll
-                            for (int q = 0; q < VEC; ++q)
-                                x.v[q] = (IT)((U)x.v[q] + u1 * (U)v1.v[q] + u2 * (U)v2.v[q]);
-                        }
-                        *dst = x;
+                for (int q = 0; q < VEC; ++q) {
+                    const int c = cv * VEC + q;
+                    if constexpr (SYM) {
+                        v1.v[q] = (IT)((U)(IT)s_Fb[c] - (U)(IT)Fa[c]);
+                    } else {
+                        v1.v[q] = (IT)((U)(IT)s_FTb[c] - (U)(IT)FTa[c]);
+                        v2.v[q] = (IT)((U)(IT)s_Fb[c] - (U)(IT)Fa[c]);
                     }
                 }
-            } else {
-                for (int cv = tid; cv < nvec; cv += BT) {
-                    const Vec<IT> v1 = *reinterpret_cast<const Vec<IT> *>(s_v1 + cv * VEC);
-                    Vec<IT> v2;
-                    if constexpr (!SYM) v2 = *reinterpret_cast<const Vec<IT> *>(s_v2 + cv * VEC);
-                    for (int k = 0; k < rows; ++k) {
-                        Vec<IT> *dst = reinterpret_cast<Vec<IT> *>(sI + (size_t)k * lds + cv * VEC);
-                        Vec<IT> x = *dst;
-                        const U u1 = (U)s_u1[k];
-                        if constexpr (SYM) {
+                const int kfirst = (BT >= nvec) ? k0r : 0;
+                const int kinc = (BT >= nvec) ? kstep : 1;
+#pragma unroll 2
+                for (int k = kfirst; k < rows; k += kinc) {
+                    Vec<IT> *dst = reinterpret_cast<Vec<IT> *>(sI + (size_t)k * lds + cv * VEC);
+                    Vec<IT> x = *dst;
+                    if constexpr (SYM) {
+                        const U u1 = 2u * ((U)(IT)s_Dj[k] - (U)(IT)Di[k]);
 #pragma unroll
-                            for (int q = 0; q < VEC; ++q) x.v[q] = (IT)((U)x.v[q] + u1 * (U)v1.v[q]);
-                        } else {
-                            const U u2 = (U)s_u2[k];
+                        for (int q = 0; q < VEC; ++q) x.v[q] = (IT)((U)x.v[q] + u1 * (U)v1.v[q]);
+                    } else {
+                        const U u1 = (U)(IT)s_DTj[k] - (U)(IT)DTi[k];
+                        const U u2 = (U)(IT)s_Dj[k] - (U)(IT)Di[k];
 #pragma unroll
-                            for (int q = 0; q < VEC; ++q)
-                                x.v[q] = (IT)((U)x.v[q] + u1 * (U)v1.v[q] + u2 * (U)v2.v[q]);
-                        }
-                        *dst = x;
+                        for (int q = 0; q < VEC; ++q)
+                            x.v[q] = (IT)((U)x.v[q] + u1 * (U)v1.v[q] + u2 * (U)v2.v[q]);
                     }
+                    *dst = x;
                 }
             }
-            cluster_barrier<CL>();                           // S5: new rows and phi visible
+            G.sync();                                 // S5: new rows and phi visible
             if (s_misc[1] == upd) {
                 for (int q = tid; q < n; q += BT) s_bphi[q] = s_phi[q];
             }
@@ -531,7 +694,9 @@ __global__ void __launch_bounds__(256) epoch_kernel(SolveDev s) {
     }
 
     // ---- store the replica, then the last replica of the group runs the exchange
-    cluster_barrier<CL>();   // no CTA of the cluster reads this CTA's rows any more
+    cp_async_wait_all();
+    cluster_sync<CL>(G);   // all deltas exchanged; no CTA writes into another any more
+    if (failed) return false;
     {
         IT *gI = reinterpret_cast<IT *>(s.I) + ((size_t)rep * n + row0) * s.ldg;
         const int nvg = s.ldg / VEC;
@@ -551,18 +716,126 @@ __global__ void __launch_bounds__(256) epoch_kernel(SolveDev s) {
         if (tid == 0) {
             s.E[rep] = E;
             s.bestE[rep] = bestE;
-            s.accepts[rep] += accepts;
+            s.accepts[rep] = __ldcg(s.accepts + rep) + accepts;
         }
-        __syncthreads();
-        if (tid == 0) {
+    }
+    __threadfence();   // this thread's stores reach L2 before the worker reports the epoch done
+    return true;
+}
+
+// Solve path: one launch = one epoch of every replica of the solve (grid = T*R*CL CTAs);
+// the last replica of each group to finish runs the group's tracking + exchange.
+template <class IT, int CL, bool SYM>
+__global__ void __launch_bounds__(256) epoch_kernel(SolveDev s) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    int rank = 0;
+    if constexpr (CL > 1) rank = (int)cg::this_cluster().block_rank();
+    const int rep = blockIdx.x / CL;
+    const int g = rep / s.R;
+    // Every CTA of a group reads the same epoch and stop values: stop_epoch only drops to
+    // epoch+1 during this launch, so the test below cannot differ inside a cluster or group.
+    const int e = *((volatile int32_t *)s.epoch + g);
+    if (e >= *(volatile int32_t *)s.stop_epoch) return;
+    const Grp G{(int)threadIdx.x, (int)blockDim.x, (int)(threadIdx.x & 31), (int)(threadIdx.x >> 5),
+                (int)(blockDim.x >> 5), 0};
+    const bool ok = replica_epoch<IT, CL, SYM>(s, rep, rank, e, G, smem);
+    __syncthreads();
+    if (ok && rank == 0 && threadIdx.x == 0) {
+        const unsigned prev = atomicAdd(s.finish + g, 1u);
+        if (prev == (unsigned)s.R - 1u) {
             __threadfence();
-            const unsigned prev = atomicAdd(s.finish + g, 1u);
-            if (prev == (unsigned)s.R - 1u) {
+            track_exchange(s, g, e + 1);
+            s.finish[g] = 0u;
+            s.epoch[g] = e + 1;
+            __threadfence();
+        }
+    }
+}
+
+// ------------------------------------------------------------------ the batch kernel
+
+constexpr unsigned long long kQueueWaitNs = 30000000000ull;   // 30 s without any progress
+constexpr unsigned long long kDoneItem = ~0ull;
+
+// Next work item, or kDoneItem once no instance is running.  The wait for a ticket whose item
+// is not pushed yet is bounded: the items come from other workers finishing epochs.
+__device__ unsigned long long queue_pop(const BatchDev &B) {
+    const unsigned long long idx = atomicAdd(B.q_head, 1ull);
+    const unsigned slot = (unsigned)idx & B.qmask;
+    const unsigned long long t0 = globaltimer_ns();
+    for (;;) {
+        if (*((volatile unsigned long long *)B.q_seq + slot) == idx + 1) {
+            __threadfence();
+            return *((volatile unsigned long long *)B.q_items + slot);
+        }
+        if (*(volatile int32_t *)B.active == 0) return kDoneItem;
+        if (globaltimer_ns() - t0 > kQueueWaitNs) {
+            atomicOr(B.error, kErrTimeout);
+            return kDoneItem;
+        }
+        __nanosleep(200);
+    }
+}
+
+// Enqueues every replica of instance k for its next epoch.
+__device__ void queue_push_instance(const BatchDev &B, int k, int replicas) {
+    const unsigned long long base = atomicAdd(B.q_tail, (unsigned long long)replicas);
+    for (int q = 0; q < replicas; ++q)
+        B.q_items[(unsigned)(base + q) & B.qmask] = ((unsigned long long)k << 32) | (unsigned)q;
+    __threadfence();
+    for (int q = 0; q < replicas; ++q)
+        *((volatile unsigned long long *)B.q_seq + ((unsigned)(base + q) & B.qmask)) = base + q + 1;
+}
+
+size_t batch_slice_bytes(int n, int bits) {
+    const int isz = bits / 8, vec = 16 / isz;
+    const int npad = (n + 3) & ~3;
+    int lds = npad;
+    if ((lds / vec) % 2 == 0) lds += vec;
+    return align16(16 + SmemLayout(n, npad, lds, 1, isz).total);
+}
+
+template <class IT>
+__global__ void __launch_bounds__(256) batch_kernel(BatchDev B) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    const int w = threadIdx.x / B.worker_threads;
+    const int wt = threadIdx.x - w * B.worker_threads;
+    const Grp G{wt, B.worker_threads, wt & 31, wt >> 5, B.worker_threads >> 5, 1 + w};
+    unsigned char *slice = smem + (size_t)w * B.slice_bytes;
+    volatile unsigned long long *hdr = reinterpret_cast<unsigned long long *>(slice);
+    unsigned char *work = slice + 16;
+    if (blockIdx.x == 0 && threadIdx.x == 0) *B.start_ns = globaltimer_ns();
+    for (;;) {
+        if (G.tid == 0) *hdr = queue_pop(B);
+        G.sync();
+        const unsigned long long item = *hdr;
+        G.sync();
+        if (item == kDoneItem) break;
+        const int k = (int)(item >> 32), rep = (int)(item & 0xffffffffull);
+        const SolveDev &s = B.inst[k];
+        const int e = *((volatile int32_t *)s.epoch);
+        if (B.sym[k]) replica_epoch<IT, 1, true>(s, rep, 0, e, G, work);
+        else replica_epoch<IT, 1, false>(s, rep, 0, e, G, work);
+        G.sync();
+        if (G.tid == 0) {
+            const int replicas = s.T * s.R;
+            const unsigned prev = atomicAdd(B.finish_inst + k, 1u);
+            if (prev == (unsigned)replicas - 1u) {
+                // every replica of the instance finished epoch e: all groups' tracking and
+                // exchange (lock step across groups, as one launch per epoch gives), then the
+                // next epoch or the end of the instance
                 __threadfence();
-                track_exchange(s, g, e + 1);
-                s.finish[g] = 0u;
-                s.epoch[g] = e + 1;
+                for (int g = 0; g < s.T; ++g) track_exchange(s, g, e + 1);
+                B.finish_inst[k] = 0u;
+                for (int g = 0; g < s.T; ++g) s.epoch[g] = e + 1;
                 __threadfence();
+                const int stop = *(volatile int32_t *)s.stop_epoch;
+                if (e + 1 < stop && (int64_t)(e + 1) < B.max_megaiters[k]) {
+                    queue_push_instance(B, k, replicas);
+                } else {
+                    __threadfence();
+                    atomicSub(B.active, 1);
+                }
             }
         }
     }
@@ -588,6 +861,20 @@ static void *epoch_kernel_ptr(int bits, int cl, bool sym) {
     return nullptr;
 }
 
+cudaError_t launch_batch(const BatchDev &b, int bits, int grid, cudaStream_t st) {
+    const size_t smem = (size_t)b.workers * b.slice_bytes;
+    const int threads = b.workers * b.worker_threads;
+    if (bits == 32) batch_kernel<int32_t><<<grid, threads, smem, st>>>(b);
+    else batch_kernel<int64_t><<<grid, threads, smem, st>>>(b);
+    return cudaGetLastError();
+}
+
+cudaError_t batch_occupancy(int bits, int threads, size_t smem, int *ctas_per_sm) {
+    if (bits == 32)
+        return cudaOccupancyMaxActiveBlocksPerMultiprocessor(ctas_per_sm, batch_kernel<int32_t>, threads, smem);
+    return cudaOccupancyMaxActiveBlocksPerMultiprocessor(ctas_per_sm, batch_kernel<int64_t>, threads, smem);
+}
+
 cudaError_t prepare_kernels() {
     int dev = 0;
     cudaError_t err = cudaGetDevice(&dev);
@@ -602,7 +889,9 @@ cudaError_t prepare_kernels() {
                                            cudaFuncAttributeMaxDynamicSharedMemorySize, maxsm);
                 if (err != cudaSuccess) return err;
             }
-    return cudaSuccess;
+    err = cudaFuncSetAttribute(batch_kernel<int32_t>, cudaFuncAttributeMaxDynamicSharedMemorySize, maxsm);
+    if (err != cudaSuccess) return err;
+    return cudaFuncSetAttribute(batch_kernel<int64_t>, cudaFuncAttributeMaxDynamicSharedMemorySize, maxsm);
 }
 
 cudaError_t launch_setup(const SolveDev &s, int bits, cudaStream_t st) {

@@ -104,19 +104,25 @@ struct StaticSummary {
     long long pad;
 };
 
-__global__ void static_prepare_kernel(SolveDev d, int32_t *Dd_w, int32_t *Fd_w, int32_t *DT_w,
-                                      int32_t *FT_w) {
-    const int n = d.n;
+// Pads the raw n x n matrices to rows of ldm (zeros past column n) and writes transposes
+// and diagonals, the device layout pimqap_solve builds on the host.
+__global__ void static_prepare_kernel(SolveDev d, const int32_t *Draw, const int32_t *Fraw,
+                                      int32_t *D_w, int32_t *F_w, int32_t *DT_w, int32_t *FT_w,
+                                      int32_t *Dd_w, int32_t *Fd_w) {
+    const int n = d.n, ld = d.ldm;
     const int tid = blockIdx.x * blockDim.x + threadIdx.x;
     const int stride = gridDim.x * blockDim.x;
-    for (int q = tid; q < n * n; q += stride) {
-        const int i = q / n, j = q - i * n;
-        DT_w[q] = d.D[j * n + i];
-        FT_w[q] = d.F[j * n + i];
+    for (int q = tid; q < n * ld; q += stride) {
+        const int i = q / ld, j = q - i * ld;
+        const bool in = j < n;
+        D_w[q] = in ? Draw[i * n + j] : 0;
+        F_w[q] = in ? Fraw[i * n + j] : 0;
+        DT_w[q] = in ? Draw[j * n + i] : 0;
+        FT_w[q] = in ? Fraw[j * n + i] : 0;
     }
     for (int q = tid; q < n; q += stride) {
-        Dd_w[q] = d.D[q * n + q];
-        Fd_w[q] = d.F[q * n + q];
+        Dd_w[q] = Draw[q * n + q];
+        Fd_w[q] = Fraw[q * n + q];
     }
     for (int t = tid; t < d.T; t += stride) d.group_best[t] = pimqap::kNoBest;
     if (tid == 0) {
@@ -184,6 +190,8 @@ extern "C" pimqap_status pimqap_solve_static(const pimqap_instance *inst,
     if (p->threads_per_block != 0 && p->threads_per_block != 64 && p->threads_per_block != 128 &&
         p->threads_per_block != 256)
         return fail(PIMQAP_ERR_ARG, "threads_per_block must be 0, 64, 128 or 256");
+    if (p->cluster_size != 0 && p->cluster_size != 1 && p->cluster_size != 2 && p->cluster_size != 4)
+        return fail(PIMQAP_ERR_ARG, "cluster_size must be 0, 1, 2 or 4");
 
     // Instance analysis without heap buffers: symmetry and the per-row force bound.
     const int32_t *F = inst->flow, *D = inst->dist;
@@ -244,19 +252,23 @@ extern "C" pimqap_status pimqap_solve_static(const pimqap_instance *inst,
     int lds = npad;
     if ((lds / vec) % 2 == 0) lds += vec;
     const int threads = p->threads_per_block ? p->threads_per_block : (n <= 64 ? 64 : (n <= 128 ? 128 : 256));
+    auto rows_per_cta = [&](int c) { return (((n + c - 1) / c) + 3) & ~3; };
     int cl = 0;
     for (int c : {1, 2, 4}) {
-        if (pimqap::epoch_smem_bytes(n, (n + c - 1) / c, lds, c, bits) <= (size_t)maxsm) {
+        if (p->cluster_size && c != p->cluster_size) continue;
+        if (pimqap::epoch_smem_bytes(n, rows_per_cta(c), lds, c, bits) <= (size_t)maxsm) {
             cl = c;
             break;
         }
     }
     if (!cl) return fail(PIMQAP_ERR_ARG, "force matrix does not fit a 4-CTA cluster");
-    const int rpc = (n + cl - 1) / cl;
+    const int rpc = rows_per_cta(cl);
+    const int ldm = std::max(npad, cl * rpc);
     const size_t smem = pimqap::epoch_smem_bytes(n, rpc, lds, cl, bits);
 
-    const size_t reps = (size_t)T * R, nn = (size_t)n * n;
+    const size_t reps = (size_t)T * R, nn = (size_t)n * ldm, nraw = (size_t)n * n;
     const size_t need = carve_size(reps * (size_t)n * npad * isz) + 4 * carve_size(nn * 4) +
+                        2 * carve_size(nraw * 4) +
                         2 * carve_size((size_t)n * 4) + 2 * carve_size(reps * n * 4) +
                         4 * carve_size(reps * 8) + carve_size((size_t)T * cap * 4) +
                         4 * carve_size((size_t)T * 8) + 8 * carve_size(8) + carve_size(sizeof(StaticSummary));
@@ -272,7 +284,7 @@ extern "C" pimqap_status pimqap_solve_static(const pimqap_instance *inst,
     char *cur = base;
     SolveDev d{};
     d.n = n; d.R = R; d.T = T; d.cap = cap; d.spe = p->sweeps_per_exchange;
-    d.ldg = npad; d.lds = lds; d.rpc = rpc;
+    d.ldg = npad; d.lds = lds; d.ldm = ldm; d.rpc = rpc;
     d.goal = p->goal;
     d.seed = p->seed;
     d.I = carve<char>(cur, reps * (size_t)n * npad * isz);
@@ -298,6 +310,7 @@ extern "C" pimqap_status pimqap_solve_static(const pimqap_instance *inst,
     d.start_ns = carve<unsigned long long>(cur, 1);
     d.error = carve<int32_t>(cur, 1);
     StaticSummary *dsum = carve<StaticSummary>(cur, 1);
+    int32_t *rawD = carve<int32_t>(cur, nraw), *rawF = carve<int32_t>(cur, nraw);
 
     const cudaStream_t q = 0;   // the legacy default stream: nothing is created per call
 #define PQS_CUDA(x)                                                     \
@@ -305,9 +318,9 @@ extern "C" pimqap_status pimqap_solve_static(const pimqap_instance *inst,
         if ((x) != cudaSuccess) return fail(PIMQAP_ERR_CUDA, #x " failed"); \
     } while (0)
     PQS_CUDA(cudaMemsetAsync(base, 0, need, q));   // the previous call's contents are cleared
-    PQS_CUDA(cudaMemcpy(dD, D, nn * 4, cudaMemcpyHostToDevice));
-    PQS_CUDA(cudaMemcpy(dF, F, nn * 4, cudaMemcpyHostToDevice));
-    static_prepare_kernel<<<64, 256, 0, q>>>(d, dDd, dFd, dDT, dFT);
+    PQS_CUDA(cudaMemcpy(rawD, D, nraw * 4, cudaMemcpyHostToDevice));
+    PQS_CUDA(cudaMemcpy(rawF, F, nraw * 4, cudaMemcpyHostToDevice));
+    static_prepare_kernel<<<64, 256, 0, q>>>(d, rawD, rawF, dD, dF, dDT, dFT, dDd, dFd);
     PQS_CUDA(cudaGetLastError());
 
     // Host set-up with fixed-size stack buffers: shuffle, beta ladder, rank slots per group.
@@ -395,7 +408,7 @@ extern "C" pimqap_status pimqap_solve_static(const pimqap_instance *inst,
     result->force_bits = bits;
     result->cluster_size = cl;
     result->stopped_by = stopped_goal ? 1 : (timed_out ? 2 : 0);
-    result->h2d_bytes = (int64_t)(2 * nn * 4 + reps * n * 4 + reps * 8 + (size_t)T * std::min(cap, R) * 4);
+    result->h2d_bytes = (int64_t)(2 * nraw * 4 + reps * n * 4 + reps * 8 + (size_t)T * std::min(cap, R) * 4);
     result->d2h_bytes = (int64_t)(sizeof sum + 4 + 4 + 8 + 8 + 8 + 8 + (perm_dst ? (size_t)n * 4 : 0));
     return PIMQAP_OK;
 }

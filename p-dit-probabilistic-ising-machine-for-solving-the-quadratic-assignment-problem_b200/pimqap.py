@@ -44,6 +44,7 @@ class Params(C.Structure):
         ("beta_ratio", C.c_double), ("goal", C.c_int64), ("timeout_s", C.c_double),
         ("seed", C.c_uint64), ("force_bits", C.c_int32), ("device", C.c_int32),
         ("megaiters_per_launch", C.c_int32), ("threads_per_block", C.c_int32),
+        ("cluster_size", C.c_int32),
     ]
 
 

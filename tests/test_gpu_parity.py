@@ -53,6 +53,12 @@ CASES = {
     "threads256_n40": (lambda: instances.uniform(40, 23), 1, 4, 2, 0.02, 1.3, 6, {"threads_per_block": 256}),
     "n1_trivial": (lambda: instances.uniform(1, 24), 1, 2, 1, 1.0, 1.2, 3, {}),
     "n5_tiny": (lambda: instances.uniform(5, 25), 2, 3, 2, 0.05, 1.3, 6, {}),
+    "grid_n256_cluster4": (lambda: instances.grid256(27), 1, 2, 1, 0.0015, 1.5, 2, {"cluster_size": 4}),
+    "asym_n70_cluster2": (lambda: asym(70, 28), 1, 3, 2, 0.002, 1.5, 3, {"cluster_size": 2}),
+    "asym_n37_cluster4_t64": (lambda: asym(37, 29), 2, 2, 1, 0.003, 1.5, 4,
+                              {"cluster_size": 4, "threads_per_block": 64}),
+    "wide_n50_cluster2": (lambda: wide(50, 30), 1, 3, 1, 1e-9, 1.5, 3, {"cluster_size": 2}),
+    "n250_cluster4_ragged": (lambda: instances.uniform(250, 31), 1, 2, 1, 0.0005, 1.5, 1, {"cluster_size": 4}),
 }
 
 
