@@ -76,6 +76,12 @@ typedef struct pimqap_params {
     int32_t megaiters_per_launch;/* mega-iterations per CUDA-graph launch (0 = automatic) */
     int32_t threads_per_block;   /* 0 = automatic, else 64, 128 or 256 */
     int32_t cluster_size;        /* CTAs per replica: 0 = smallest that fits, else 1, 2 or 4 */
+    int32_t beta_internal;       /* nonzero: beta_max is already in the reference's internal
+                                    (log2) units, as automatic mode sets beta0 = 2^k (:397) */
+    int32_t auto_beta;           /* nonzero: choose beta_max / beta_ratio by the reference's
+                                    automatic mode before solving (no -b flag, :645-658) */
+    double auto_lower;           /* -al lowerBetaProportion (default 0.1, :33) */
+    double auto_higher;          /* -ah higherBetaProportion (default 0.9, :34) */
 } pimqap_params;
 
 /* Fills p with the reference's defaults: 10 replicas, 20 groups, 4 sweeps per exchange,
@@ -98,6 +104,10 @@ typedef struct pimqap_result {
     int32_t stopped_by;         /* 0 = max_megaiters, 1 = goal, 2 = timeout */
     int64_t h2d_bytes;          /* host-to-device bytes copied by the solver so far */
     int64_t d2h_bytes;          /* device-to-host bytes copied by the solver so far */
+    int64_t *final_energies;    /* caller-provided, groups * replicas entries (may be NULL):
+                                   currentE of every replica at the end (CPU_PIM.cpp:54) */
+    double beta_max_used;       /* beta0 of the run in internal units (after automatic mode) */
+    double beta_ratio_used;     /* deltaBeta of the run */
 } pimqap_result;
 
 /* ---------------------------------------------------------------- instance I/O */
@@ -173,6 +183,18 @@ void pimqap_solver_destroy(pimqap_solver *s);
    Each result equals what pimqap_solve returns for that instance alone. */
 pimqap_status pimqap_batch_solve(const pimqap_instance *insts, const pimqap_params *params,
                                  int32_t count, pimqap_result *results);
+
+/* ---------------------------------------------------------------- automatic beta */
+
+/* The reference's automatic mode (autoSelectParameters, CPU_PIM.cpp:366-476): for beta0 =
+   2^k, k = -30..1, five short trials (10 mega-iterations, every replica at beta0) average the
+   final energies; the beta range is read off that curve with auto_lower / auto_higher.  All
+   160 trials run as one batched launch.  Trial (k, t) is seeded from params.seed and 5k + t.
+   Outputs: beta0 in internal units, deltaBeta, the 32 average energies (may be NULL) and the
+   best energy / permutation any trial found (may be NULL; n entries). */
+pimqap_status pimqap_auto_beta(const pimqap_instance *inst, const pimqap_params *params,
+                               double *beta0_internal, double *delta_beta, double *avg_energy,
+                               int64_t *best_energy, int32_t *best_perm);
 
 /* ---------------------------------------------------------------- misc */
 

@@ -1,0 +1,453 @@
+// pimqap_batch.cpp - batched solve: many independent instances of uneven n in persistent
+// launches (no reference counterpart: the reference solves one instance per process).
+//
+// The autotuner partitions a batch into classes: force-matrix width x CTAs per replica
+// (1, 2 or 4) x, for single-CTA replicas, a band of n.  Each class is one persistent launch
+// whose workers (a group of warps with its own named barrier and shared-memory slice, or a
+// whole cluster) pop replica-epochs from a device queue.  The classes run concurrently on
+// separate streams, their grids split the SMs in proportion to estimated work.  Results are
+// gathered on the device and read back in one copy per class.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <limits>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "pimqap.h"
+#include "pimqap_batch.h"
+#include "pimqap_internal.h"
+#include "pimqap_plan.h"
+
+namespace pimqap {
+namespace detail {
+
+namespace {
+
+// n bands of single-CTA classes: small n packs more workers into a CTA.
+constexpr int kBandEdges[] = {48, 96, 160, 256};
+
+int band_of(int n) {
+    int b = 0;
+    while (n > kBandEdges[b]) ++b;
+    return b;
+}
+
+}  // namespace
+
+double instance_work(const Plan &P, int64_t megaiters) {
+    // updates x (candidate deltas + an expected share of the n^2 force update)
+    const double upd = (double)P.T * P.R * (double)megaiters * P.spe * P.n;
+    return upd * ((double)P.n + 0.25 * (double)P.n * P.n / 8.0);
+}
+
+std::vector<BatchClass> plan_classes(const std::vector<Plan> &plans, const std::vector<int64_t> &megaiters,
+                                     int sms, int maxsm, int force_cluster) {
+    std::vector<BatchClass> classes;
+    auto find = [&](int bits, int cl, int band) -> BatchClass & {
+        for (auto &c : classes)
+            if (c.bits == bits && c.cl == cl && c.band == band) return c;
+        classes.push_back(BatchClass{});
+        BatchClass &c = classes.back();
+        c.bits = bits;
+        c.cl = cl;
+        c.band = band;
+        return c;
+    };
+    for (int k = 0; k < (int)plans.size(); ++k) {
+        const Plan &P = plans[k];
+        const bool single = P.cl == 1 && pimqap::batch_slice_bytes(P.n, P.bits) <= (size_t)maxsm && !force_cluster;
+        BatchClass &c = find(P.bits, single ? 1 : P.cl, single ? band_of(P.n) : 0);
+        c.members.push_back(k);
+        c.work += instance_work(P, megaiters[k]);
+    }
+    double total = 0;
+    for (auto &c : classes) total += c.work;
+    for (auto &c : classes) {
+        int nmax = 0;
+        size_t slice = 0;
+        for (int k : c.members) {
+            const Plan &P = plans[k];
+            nmax = std::max(nmax, P.n);
+            slice = std::max(slice, c.cl == 1 ? pimqap::batch_slice_bytes(P.n, c.bits) : 16 + P.smem);
+        }
+        c.slice = (slice + 15) & ~size_t(15);
+        if (c.cl == 1) {
+            c.worker_threads = nmax <= 32 ? 32 : (nmax <= 64 ? 64 : 128);
+            c.workers = std::max(1, std::min(256 / c.worker_threads, (int)((size_t)maxsm / c.slice)));
+        } else {
+            c.worker_threads = nmax <= 128 * c.cl ? 128 : 256;
+            c.workers = 1;
+        }
+        int occ = 0;
+        if (pimqap::batch_occupancy(c.bits, c.cl, c.workers * c.worker_threads, c.workers * c.slice, &occ) !=
+                cudaSuccess || occ < 1)
+            occ = 1;
+        // Every class gets a grid that fills the GPU: classes are launched largest first on
+        // their own streams, and a class's CTAs start on the SMs the previous classes' workers
+        // release when their work runs out.
+        c.grid = (c.cl == 1) ? sms * occ : occ * c.cl;   // occ: resident clusters for cl > 1
+        (void)total;
+    }
+    std::stable_sort(classes.begin(), classes.end(),
+                     [](const BatchClass &a, const BatchClass &b) { return a.work > b.work; });
+    return classes;
+}
+
+// One class: instance heads in one pinned image (one copy), tails cleared in one memset,
+// queue filled with every active instance's epoch-0 items, largest first.
+pimqap_status ClassRun::prepare(const pimqap_instance *insts, const pimqap_params *params,
+                                const std::vector<Plan> &plans, const BatchClass &c) {
+    cls = c;
+    const int m = (int)c.members.size();
+    size_t head_total = 0, tail_total = 0, reps_total = 0, perm_total = 0;
+    std::vector<size_t> hoff(m), toff(m);
+    perm_off.assign(m, 0);
+    energy_off.assign(m, 0);
+    for (int i = 0; i < m; ++i) {
+        const Plan &P = plans[c.members[i]];
+        hoff[i] = head_total;
+        toff[i] = tail_total;
+        head_total += carve_size(P.head);
+        tail_total += carve_size(P.tail);
+        energy_off[i] = (long long)reps_total;
+        reps_total += (size_t)P.T * P.R;
+        perm_off[i] = (long long)perm_total;
+        perm_total += (size_t)P.n;
+    }
+    energy_total = reps_total;
+    unsigned qcap = 1;
+    while (qcap < reps_total + 1) qcap <<= 1;
+    const size_t misc = carve_size(sizeof(SolveDev) * m) + 5 * carve_size(8 * (size_t)m) +
+                        2 * carve_size(8 * (size_t)qcap) + 8 * carve_size(8) +
+                        carve_size(sizeof(BatchResultDev) * m) + carve_size(4 * perm_total) +
+                        carve_size(8 * reps_total);
+    bytes = head_total + tail_total + misc;
+    trace("class: sizes");
+    PQ_CUDA(cudaMalloc(&base, bytes));
+    trace("class: cudaMalloc");
+    PQ_CUDA(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
+    PQ_CUDA(cudaMallocHost(&pinned, head_total + 64));
+    trace("class: cudaMallocHost");
+    for (int i = 0; i < m; ++i) {
+        const int k = c.members[i];
+        fill_head(&insts[k], &params[k], plans[k], pinned + hoff[i]);
+    }
+    trace("class: fill heads");
+    devs.resize(m);
+    beta0s.resize(m);
+    ratios.resize(m);
+    for (int i = 0; i < m; ++i) {
+        const int k = c.members[i];
+        beta0s[i] = params[k].beta_internal ? params[k].beta_max : params[k].beta_max * 1.44269504089;
+        ratios[i] = params[k].beta_ratio;
+        carve_instance(plans[k], base + hoff[i], base + head_total + toff[i], &devs[i]);
+        devs[i].goal = params[k].goal;
+        devs[i].seed = params[k].seed;
+    }
+    PQ_CUDA(cudaMemcpyAsync(base, pinned, head_total, cudaMemcpyHostToDevice, stream));
+    PQ_CUDA(cudaMemsetAsync(base + head_total, 0, tail_total + misc, stream));
+    for (int i = 0; i < m; ++i) PQ_CUDA(pimqap::launch_setup(devs[i], c.bits, stream));
+    trace("class: upload + setup launches");
+
+    char *cur = base + head_total + tail_total;
+    d_inst = carve<SolveDev>(cur, m);
+    int32_t *d_sym = reinterpret_cast<int32_t *>(carve<int64_t>(cur, m));
+    int64_t *d_maxm = carve<int64_t>(cur, m);
+    unsigned int *d_finish = reinterpret_cast<unsigned int *>(carve<int64_t>(cur, m));
+    long long *d_poff = carve<long long>(cur, m);
+    unsigned long long *d_items = carve<unsigned long long>(cur, qcap);
+    unsigned long long *d_seq = carve<unsigned long long>(cur, qcap);
+    unsigned long long *d_head = carve<unsigned long long>(cur, 1);
+    unsigned long long *d_tail = carve<unsigned long long>(cur, 1);
+    int32_t *d_active = reinterpret_cast<int32_t *>(carve<int64_t>(cur, 1));
+    d_error = reinterpret_cast<int32_t *>(carve<int64_t>(cur, 1));
+    d_start = carve<unsigned long long>(cur, 1);
+    int32_t *d_shutdown = reinterpret_cast<int32_t *>(carve<int64_t>(cur, 1));
+    carve<int64_t>(cur, 2);
+    d_results = carve<BatchResultDev>(cur, m);
+    d_perms = carve<int32_t>(cur, perm_total);
+    d_energies = carve<long long>(cur, reps_total);
+    d_energy_off = carve<long long>(cur, m);
+
+    // stop epochs after setup: an instance whose goal is met at mega-iteration 0 never runs
+    PQ_CUDA(cudaStreamSynchronize(stream));
+    trace("class: setup sync");
+    std::vector<int32_t> sym(2 * m, 0);
+    std::vector<int64_t> maxm(m);
+    std::vector<int32_t> stop0(m);
+    for (int i = 0; i < m; ++i) {
+        sym[i] = plans[c.members[i]].sym ? 1 : 0;
+        maxm[i] = params[c.members[i]].max_megaiters;
+        PQ_CUDA(cudaMemcpy(&stop0[i], devs[i].stop_epoch, 4, cudaMemcpyDeviceToHost));
+    }
+    std::vector<int> order_idx(m);
+    for (int i = 0; i < m; ++i) order_idx[i] = i;
+    std::stable_sort(order_idx.begin(), order_idx.end(), [&](int a, int b) {
+        const Plan &A = plans[c.members[a]], &B = plans[c.members[b]];
+        return (double)A.n * A.n * A.T * A.R > (double)B.n * B.n * B.T * B.R;
+    });
+    std::vector<unsigned long long> items, seq;
+    int active = 0;
+    for (int i : order_idx) {
+        const Plan &P = plans[c.members[i]];
+        if (maxm[i] <= 0 || stop0[i] <= 0) continue;
+        ++active;
+        for (int r = 0; r < P.T * P.R; ++r) {
+            items.push_back(((unsigned long long)i << 32) | (unsigned)r);
+            seq.push_back(items.size());
+        }
+    }
+    runnable = active;
+    const unsigned long long tail = items.size();
+    const int32_t shutdown = 1;   // a batch ends when its last instance does
+    PQ_CUDA(cudaMemcpyAsync(d_inst, devs.data(), sizeof(SolveDev) * m, cudaMemcpyHostToDevice, stream));
+    PQ_CUDA(cudaMemcpyAsync(d_sym, sym.data(), 4 * (size_t)m, cudaMemcpyHostToDevice, stream));
+    PQ_CUDA(cudaMemcpyAsync(d_maxm, maxm.data(), 8 * (size_t)m, cudaMemcpyHostToDevice, stream));
+    PQ_CUDA(cudaMemcpyAsync(d_poff, perm_off.data(), 8 * (size_t)m, cudaMemcpyHostToDevice, stream));
+    PQ_CUDA(cudaMemcpyAsync(d_energy_off, energy_off.data(), 8 * (size_t)m, cudaMemcpyHostToDevice, stream));
+    if (!items.empty()) {
+        PQ_CUDA(cudaMemcpyAsync(d_items, items.data(), 8 * items.size(), cudaMemcpyHostToDevice, stream));
+        PQ_CUDA(cudaMemcpyAsync(d_seq, seq.data(), 8 * seq.size(), cudaMemcpyHostToDevice, stream));
+    }
+    PQ_CUDA(cudaMemcpyAsync(d_tail, &tail, 8, cudaMemcpyHostToDevice, stream));
+    PQ_CUDA(cudaMemcpyAsync(d_active, &active, 4, cudaMemcpyHostToDevice, stream));
+    PQ_CUDA(cudaMemcpyAsync(d_shutdown, &shutdown, 4, cudaMemcpyHostToDevice, stream));
+    PQ_CUDA(cudaStreamSynchronize(stream));
+    trace("class: queue ready");
+    d_perm_off = d_poff;
+
+    B = pimqap::BatchDev{};
+    B.inst = d_inst; B.sym = d_sym; B.max_megaiters = d_maxm; B.finish_inst = d_finish;
+    B.count = m; B.q_items = d_items; B.q_seq = d_seq; B.q_head = d_head; B.q_tail = d_tail;
+    B.qmask = qcap - 1; B.active = d_active; B.error = d_error; B.start_ns = d_start;
+    B.shutdown = d_shutdown;
+    B.worker_threads = c.worker_threads; B.workers = c.workers; B.slice_bytes = (unsigned)c.slice;
+    return PIMQAP_OK;
+}
+
+pimqap_status ClassRun::launch() {
+    PQ_CUDA(cudaEventCreate(&e0));
+    PQ_CUDA(cudaEventCreate(&e1));
+    PQ_CUDA(cudaEventRecord(e0, stream));
+    if (runnable > 0) PQ_CUDA(pimqap::launch_batch(B, cls.bits, cls.cl, cls.grid, stream));
+    PQ_CUDA(pimqap::launch_collect(d_inst, B.count, d_results, d_perms, d_perm_off, d_energies,
+                                   d_energy_off, stream));
+    PQ_CUDA(cudaEventRecord(e1, stream));
+    return PIMQAP_OK;
+}
+
+pimqap_status ClassRun::finish(const std::vector<Plan> &plans, pimqap_result *results) {
+    PQ_CUDA(cudaStreamSynchronize(stream));
+    trace("class: kernel done");
+    float ms = 0;
+    cudaEventElapsedTime(&ms, e0, e1);
+    const int m = B.count;
+    std::vector<pimqap::BatchResultDev> out(m);
+    size_t perm_total = 0;
+    for (int k : cls.members) perm_total += (size_t)plans[k].n;
+    std::vector<int32_t> perms(perm_total);
+    std::vector<long long> energies(energy_total);
+    int32_t err = 0;
+    unsigned long long start_ns = 0;
+    PQ_CUDA(cudaMemcpy(&err, d_error, 4, cudaMemcpyDeviceToHost));
+    PQ_CUDA(cudaMemcpy(&start_ns, d_start, 8, cudaMemcpyDeviceToHost));
+    PQ_CUDA(cudaMemcpy(out.data(), d_results, sizeof(pimqap::BatchResultDev) * m, cudaMemcpyDeviceToHost));
+    if (perm_total) PQ_CUDA(cudaMemcpy(perms.data(), d_perms, 4 * perm_total, cudaMemcpyDeviceToHost));
+    if (energy_total)
+        PQ_CUDA(cudaMemcpy(energies.data(), d_energies, 8 * energy_total, cudaMemcpyDeviceToHost));
+    if (err) return fail(PIMQAP_ERR_DEVICE, "batch kernel check failed (error word " + std::to_string(err) + ")");
+    for (int i = 0; i < m; ++i) {
+        const int k = cls.members[i];
+        const Plan &P = plans[k];
+        const pimqap::BatchResultDev &o = out[i];
+        if (o.error) return fail(PIMQAP_ERR_DEVICE, "device check failed in batch instance " + std::to_string(k));
+        pimqap_result &R = results[k];
+        int32_t *perm_dst = R.best_perm;
+        int64_t *energy_dst = R.final_energies;
+        std::memset(&R, 0, sizeof(R));
+        R.best_perm = perm_dst;
+        R.final_energies = energy_dst;
+        R.best_energy = std::min<int64_t>(o.best, o.single_best);
+        if (perm_dst) std::memcpy(perm_dst, perms.data() + perm_off[i], 4 * (size_t)P.n);
+        if (energy_dst) std::memcpy(energy_dst, energies.data() + energy_off[i], 8 * (size_t)P.T * P.R);
+        R.target_megaiter = (o.target_epoch == std::numeric_limits<long long>::max()) ? -1 : o.target_epoch;
+        R.time_to_target_ms = (R.target_megaiter >= 0 && o.target_ns != ~0ull && o.target_ns >= start_ns)
+                                  ? (double)(o.target_ns - start_ns) * 1e-6
+                                  : (R.target_megaiter >= 0 ? 0.0 : -1.0);
+        R.megaiters_done = o.epoch;
+        R.updates = (int64_t)o.epoch * P.spe * P.n * (int64_t)P.T * P.R;
+        R.accepts = (int64_t)o.accepts;
+        R.device_ms = ms;
+        R.force_bits = P.bits;
+        R.cluster_size = cls.cl;
+        R.stopped_by = (o.stop_epoch != pimqap::kNoStop) ? 1 : 0;
+        R.h2d_bytes = P.h2d_bytes;
+        R.d2h_bytes = (int64_t)(sizeof(pimqap::BatchResultDev) + 4 * (size_t)P.n + 8 * (size_t)P.T * P.R);
+        R.beta_max_used = beta0s[i];
+        R.beta_ratio_used = ratios[i];
+    }
+    device_ms = ms;
+    trace("class: results");
+    return PIMQAP_OK;
+}
+
+ClassRun::~ClassRun() {
+    if (e0) cudaEventDestroy(e0);
+    if (e1) cudaEventDestroy(e1);
+    if (stream) cudaStreamDestroy(stream);
+    if (pinned) cudaFreeHost(pinned);
+    if (base) cudaFree(base);
+}
+
+}  // namespace detail
+}  // namespace pimqap
+
+using namespace pimqap::detail;
+
+extern "C" pimqap_status pimqap_batch_solve(const pimqap_instance *insts, const pimqap_params *params,
+                                            int32_t count, pimqap_result *results) {
+    if (count < 0 || (count > 0 && (!insts || !params || !results)))
+        return fail(PIMQAP_ERR_ARG, "bad batch arguments");
+    if (count == 0) return PIMQAP_OK;
+    const auto wall0 = std::chrono::steady_clock::now();
+    trace("batch: start");
+    for (int k = 0; k < count; ++k) {
+        pimqap_status st = check_params(&insts[k], &params[k]);
+        if (st != PIMQAP_OK) return st;
+        if (params[k].device != params[0].device)
+            return fail(PIMQAP_ERR_ARG, "every batch entry must use the same device");
+    }
+    int maxsm = 0;
+    pimqap_status st = open_device(params[0].device, &maxsm);
+    if (st != PIMQAP_OK) return st;
+    int sms = 0;
+    PQ_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, params[0].device));
+    std::vector<Plan> plans(count);
+    std::vector<int64_t> megaiters(count);
+    for (int k = 0; k < count; ++k) {
+        st = plan_instance(&insts[k], &params[k], (size_t)maxsm, params[k].cluster_size, &plans[k]);
+        if (st != PIMQAP_OK) return st;
+        megaiters[k] = params[k].max_megaiters;
+    }
+    trace("batch: plans");
+    const std::vector<BatchClass> classes = plan_classes(plans, megaiters, sms, maxsm, 0);
+    if (std::getenv("PIMQAP_TRACE"))
+        for (const auto &c : classes)
+            std::fprintf(stderr, "[pimqap] class bits=%d cl=%d band=%d members=%zu work=%.3g grid=%d workers=%d x %d threads slice=%zu\n",
+                         c.bits, c.cl, c.band, c.members.size(), c.work, c.grid, c.workers, c.worker_threads, c.slice);
+    trace("batch: classes");
+    std::vector<std::unique_ptr<ClassRun>> runs;
+    for (const auto &c : classes) {
+        runs.emplace_back(new ClassRun());
+        st = runs.back()->prepare(insts, params, plans, c);
+        if (st != PIMQAP_OK) return st;
+    }
+    for (auto &r : runs) {   // all classes run concurrently, each on its own stream
+        st = r->launch();
+        if (st != PIMQAP_OK) return st;
+    }
+    for (auto &r : runs) {
+        st = r->finish(plans, results);
+        if (st != PIMQAP_OK) return st;
+    }
+    runs.clear();
+    trace("batch: released");
+    const double el = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - wall0).count();
+    for (int k = 0; k < count; ++k) results[k].wall_ms = el;
+    return PIMQAP_OK;
+}
+
+namespace {
+
+uint64_t splitmix64(uint64_t x) {
+    x += 0x9E3779B97F4A7C15ull;
+    x = (x ^ (x >> 30)) * 0xBF58476D1CE4E5B9ull;
+    x = (x ^ (x >> 27)) * 0x94D049BB133111EBull;
+    return x ^ (x >> 31);
+}
+
+}  // namespace
+
+// autoSelectParameters (CPU_PIM.cpp:366-476).  The reference runs the trials one after another
+// with fresh random_device seeds; here trial (k, t) is seeded with splitmix64(seed + 5k + t + 1)
+// and all 160 trials run in one batched launch.  The averaging order and the selection rule are
+// the reference's, in the same double arithmetic.
+extern "C" pimqap_status pimqap_auto_beta(const pimqap_instance *inst, const pimqap_params *params,
+                                          double *beta0_internal, double *delta_beta, double *avg_energy,
+                                          int64_t *best_energy, int32_t *best_perm) {
+    if (!inst || !params || !beta0_internal || !delta_beta) return fail(PIMQAP_ERR_ARG, "null argument");
+    pimqap_status st = check_params(inst, params);
+    if (st != PIMQAP_OK) return st;
+    constexpr double kMinBetaToTry = -30, kBetaStep = 1;     // :366-370
+    constexpr int kTrials = 5, kSteps = 32, kMegaiters = 10;  // :368, :371, :391
+    const int T = params->groups, R = params->replicas, n = inst->n;
+    std::vector<pimqap_instance> insts(kSteps * kTrials, *inst);
+    std::vector<pimqap_params> ps(kSteps * kTrials, *params);
+    for (int i = 0; i < kSteps; ++i)
+        for (int t = 0; t < kTrials; ++t) {
+            pimqap_params &p = ps[i * kTrials + t];
+            p.auto_beta = 0;
+            p.beta_internal = 1;
+            p.beta_max = std::exp2(kMinBetaToTry + i * kBetaStep);   // :396-397
+            p.beta_ratio = 1.0;                                       // :389
+            p.max_megaiters = kMegaiters;
+            p.seed = splitmix64(params->seed + (uint64_t)(i * kTrials + t) + 1);
+            p.timeout_s = 0;
+        }
+    std::vector<pimqap_result> rs(ps.size());
+    std::vector<std::vector<int64_t>> energies(ps.size(), std::vector<int64_t>((size_t)T * R));
+    std::vector<std::vector<int32_t>> perms(ps.size(), std::vector<int32_t>(n));
+    for (size_t k = 0; k < rs.size(); ++k) {
+        std::memset(&rs[k], 0, sizeof(pimqap_result));
+        rs[k].final_energies = energies[k].data();
+        rs[k].best_perm = perms[k].data();
+    }
+    st = pimqap_batch_solve(insts.data(), ps.data(), (int32_t)ps.size(), rs.data());
+    if (st != PIMQAP_OK) return st;
+
+    double sums[kSteps] = {0};
+    const double denom = static_cast<double>(kTrials) * T * R;                    // :412
+    for (int i = 0; i < kSteps; ++i)
+        for (int t = 0; t < kTrials; ++t)
+            for (int g = 0; g < T; ++g)
+                for (int l = 0; l < R; ++l)
+                    sums[i] += (double)energies[i * kTrials + t][(size_t)g * R + l] / denom;
+    size_t arg = 0;
+    for (size_t k = 1; k < rs.size(); ++k)
+        if (rs[k].best_energy < rs[arg].best_energy) arg = k;
+    if (best_energy) *best_energy = rs[arg].best_energy;
+    if (best_perm) std::memcpy(best_perm, perms[arg].data(), 4 * (size_t)n);
+    if (avg_energy) std::memcpy(avg_energy, sums, sizeof(sums));
+
+    const int i = kSteps - 1;                                                       // :434
+    double minE = 1e30, maxE = -1e30;
+    int minEIndex = 0;
+    for (int j = 0; j < i; j++) {                                                   // :438-446
+        if (sums[j] < minE) {
+            minE = sums[j];
+            minEIndex = j;
+        }
+        if (j == 0) maxE = sums[j];
+    }
+    double minBeta = 0, maxBeta = 0;
+    const double higher = params->auto_higher, lower = params->auto_lower;
+    for (int j = 0; j < i; j++) {                                                   // :447-473
+        if (minBeta == 0 && ((j == (minEIndex - 1) && (j >= 1)) || (sums[j] < (maxE - minE) * higher + minE)))
+            minBeta = std::exp2(kMinBetaToTry + (j)*kBetaStep);
+        if (j == i - 1 || (minBeta != 0 && (j == minEIndex || (sums[j] < (maxE - minE) * lower + minE)))) {
+            if (minBeta == 0) minBeta = std::exp2(kMinBetaToTry + 0 * kBetaStep);
+            maxBeta = std::exp2(kMinBetaToTry + (j + 2) * kBetaStep);
+            *beta0_internal = maxBeta;
+            *delta_beta = std::pow(maxBeta / minBeta, 1.0 / R);
+            return PIMQAP_OK;
+        }
+    }
+    return fail(PIMQAP_ERR_ARG, "automatic beta selection found no range");
+}

@@ -1,0 +1,67 @@
+// pimqap_batch.h - classes of a batch (the autotuner's choices) and the runtime of one
+// persistent class launch.  Not part of the C ABI.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <vector>
+
+#include "pimqap.h"
+#include "pimqap_internal.h"
+#include "pimqap_plan.h"
+
+namespace pimqap {
+namespace detail {
+
+// One persistent launch: instances of one force-matrix width and cluster size (and, for
+// single-CTA replicas, one band of n), with the worker shape and grid picked for them.
+struct BatchClass {
+    int bits = 32, cl = 1, band = 0;
+    std::vector<int> members;     // indices into the batch
+    double work = 0;              // estimated cost (relative)
+    int worker_threads = 128;     // threads of one replica worker
+    int workers = 1;              // workers per CTA
+    size_t slice = 0;             // shared memory per worker
+    int grid = 1;                 // CTAs of the launch
+};
+
+// Relative cost of an instance: updates x (candidates + expected force-update share).
+double instance_work(const Plan &P, int64_t megaiters);
+
+// The autotuner: partitions plans into classes, picks worker shapes from the n range and the
+// occupancy of each shape, and splits the SMs between classes in proportion to work.
+std::vector<BatchClass> plan_classes(const std::vector<Plan> &plans, const std::vector<int64_t> &megaiters,
+                                     int sms, int maxsm, int force_cluster);
+
+// Device state and stream of one class launch.
+struct ClassRun {
+    BatchClass cls;
+    pimqap::BatchDev B{};
+    std::vector<SolveDev> devs;
+    std::vector<long long> perm_off, energy_off;
+    std::vector<double> beta0s, ratios;   // beta0 (internal units) and deltaBeta per member
+    char *base = nullptr;
+    char *pinned = nullptr;
+    size_t bytes = 0;
+    cudaStream_t stream = nullptr;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    SolveDev *d_inst = nullptr;
+    pimqap::BatchResultDev *d_results = nullptr;
+    int32_t *d_perms = nullptr;
+    long long *d_perm_off = nullptr;
+    long long *d_energies = nullptr, *d_energy_off = nullptr;
+    size_t energy_total = 0;
+    int32_t *d_error = nullptr;
+    unsigned long long *d_start = nullptr;
+    int runnable = 0;
+    double device_ms = 0;
+
+    pimqap_status prepare(const pimqap_instance *insts, const pimqap_params *params,
+                          const std::vector<Plan> &plans, const BatchClass &c);
+    pimqap_status launch();
+    pimqap_status finish(const std::vector<Plan> &plans, pimqap_result *results);
+    ~ClassRun();
+};
+
+}  // namespace detail
+}  // namespace pimqap

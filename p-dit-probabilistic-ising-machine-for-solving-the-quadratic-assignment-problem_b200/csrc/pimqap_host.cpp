@@ -11,6 +11,7 @@
 #include <chrono>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <fstream>
 #include <limits>
@@ -21,30 +22,35 @@
 
 #include "pimqap.h"
 #include "pimqap_internal.h"
+#include "pimqap_plan.h"
 
 using pimqap::SolveDev;
 
 namespace {
-
 thread_local std::string g_error;
+}  // namespace
+
+void pimqap::set_last_error(const char *msg) { g_error = msg; }
+
+namespace pimqap {
+namespace detail {
 
 pimqap_status fail(pimqap_status st, const std::string &msg) {
     g_error = msg;
     return st;
 }
 
-}  // namespace
+void trace(const char *phase) {
+    static const bool on = std::getenv("PIMQAP_TRACE") != nullptr;
+    if (!on) return;
+    static thread_local auto last = std::chrono::steady_clock::now();
+    const auto now = std::chrono::steady_clock::now();
+    std::fprintf(stderr, "[pimqap] %-32s %9.3f ms\n", phase,
+                 std::chrono::duration<double, std::milli>(now - last).count());
+    last = now;
+}
 
-void pimqap::set_last_error(const char *msg) { g_error = msg; }
 
-namespace {
-
-#define PQ_CUDA(x)                                                                       \
-    do {                                                                                 \
-        cudaError_t e_ = (x);                                                            \
-        if (e_ != cudaSuccess)                                                           \
-            return fail(PIMQAP_ERR_CUDA, std::string(#x) + ": " + cudaGetErrorString(e_)); \
-    } while (0)
 
 // ------------------------------------------------------------------ random words (host)
 
@@ -179,7 +185,10 @@ InstanceInfo analyse(int n, const int32_t *F, const int32_t *D) {
 
 int round_up(int x, int m) { return (x + m - 1) / m * m; }
 
-}  // namespace
+}  // namespace detail
+}  // namespace pimqap
+
+using namespace pimqap::detail;
 
 // ------------------------------------------------------------------ solver object
 
@@ -201,6 +210,7 @@ struct pimqap_solver {
     double device_ms = 0;
     bool stopped_goal = false;
     int64_t h2d = 0, d2h = 0;   // bytes copied over PCIe by this solver
+    double beta0_used = 0, ratio_used = 0;
 
     ~pimqap_solver() {
         if (graph) cudaGraphExecDestroy(graph);
@@ -211,7 +221,8 @@ struct pimqap_solver {
     }
 };
 
-namespace {
+namespace pimqap {
+namespace detail {
 
 pimqap_status check_params(const pimqap_instance *inst, const pimqap_params *p) {
     if (!inst || !p) return fail(PIMQAP_ERR_ARG, "null instance or params");
@@ -240,26 +251,8 @@ pimqap_status check_params(const pimqap_instance *inst, const pimqap_params *p) 
     return PIMQAP_OK;
 }
 
-template <class T> T *carve(char *&cur, size_t count) {
-    T *p = reinterpret_cast<T *>(cur);
-    cur += (count * sizeof(T) + 255) & ~size_t(255);
-    return p;
-}
-
-size_t carve_size(size_t bytes) { return (bytes + 255) & ~size_t(255); }
 
 // ------------------------------------------------------------------ per-instance plan + staging
-
-// Everything decided for one instance before device memory is touched.
-struct Plan {
-    int n = 0, T = 0, R = 0, cap = 0, spe = 0;
-    int bits = 32, cl = 1, threads = 256;
-    int npad = 0, lds = 0, ldm = 0, rpc = 0;
-    bool sym = false;
-    size_t smem = 0;       // epoch kernel shared memory per CTA
-    size_t total = 0;      // device bytes of the instance's SolveDev arrays
-    int64_t h2d_bytes = 0;
-};
 
 pimqap_status open_device(int device, int *maxsm) {
     int ndev = 0;
@@ -275,8 +268,6 @@ pimqap_status open_device(int device, int *maxsm) {
     return PIMQAP_OK;
 }
 
-// Force-matrix width, symmetry, launch shape (threads, the smallest cluster whose row share of
-// I fits one CTA, or `want_cluster`), strides and the device footprint.
 pimqap_status plan_instance(const pimqap_instance *inst, const pimqap_params *params, size_t maxsm,
                             int want_cluster, Plan *out) {
     const int n = inst->n;
@@ -312,34 +303,67 @@ pimqap_status plan_instance(const pimqap_instance *inst, const pimqap_params *pa
     P.ldm = std::max(P.npad, P.cl * P.rpc);
     P.smem = pimqap::epoch_smem_bytes(n, P.rpc, P.lds, P.cl, P.bits);
     const size_t reps = (size_t)P.T * P.R, nn = (size_t)n * P.ldm;
-    P.total = carve_size(reps * (size_t)n * P.npad * isz) + 4 * carve_size(nn * 4) +
-              2 * carve_size((size_t)n * 4) + 2 * carve_size(reps * n * 4) + 4 * carve_size(reps * 8) +
-              carve_size((size_t)P.T * P.cap * 4) + 4 * carve_size((size_t)P.T * 8) + 8 * carve_size(8);
-    P.h2d_bytes = (int64_t)(4 * nn * 4 + 2 * (size_t)n * 4 + reps * n * 4 + reps * 8 +
-                            (size_t)P.T * P.cap * 4 + (size_t)P.T * 8 + 8 + 4 + 8 + 8);
+    // head: everything uploaded from the host; tail: state that starts at zero
+    P.head = 4 * carve_size(nn * 4) + 2 * carve_size((size_t)n * 4) + carve_size(reps * n * 4) +
+             carve_size(reps * 8) + carve_size((size_t)P.T * P.cap * 4) + carve_size((size_t)P.T * 8) +
+             4 * carve_size(8);
+    P.tail = carve_size(reps * (size_t)n * P.npad * isz) + carve_size(reps * n * 4) + 3 * carve_size(reps * 8) +
+             3 * carve_size((size_t)P.T * 8) + 2 * carve_size(8);
+    P.total = P.head + P.tail;
+    P.h2d_bytes = (int64_t)P.head;
     *out = P;
     return PIMQAP_OK;
 }
 
-// setup() for one instance (CPU_PIM.cpp:109-193): carves the SolveDev arrays out of `base`
-// (plan.total bytes), uploads the padded matrices, transposes, diagonals, initial
-// permutations, beta ladder and rank slots on stream q, and enqueues the setup kernels.  The
-// host buffers of the asynchronous copies are kept in `keep` until the caller syncs q.
-pimqap_status stage_instance(const pimqap_instance *inst, const pimqap_params *params,
-                             const Plan &P, char *base, SolveDev *out, cudaStream_t q,
-                             std::vector<std::vector<char>> &keep) {
+void carve_instance(const Plan &P, char *head, char *tail, SolveDev *out) {
+    const int n = P.n, T = P.T, R = P.R, cap = P.cap;
+    const size_t reps = (size_t)T * R, nn = (size_t)n * P.ldm;
+    SolveDev d{};
+    d.n = n; d.R = R; d.T = T; d.cap = cap; d.spe = P.spe;
+    d.ldg = P.npad; d.lds = P.lds; d.ldm = P.ldm; d.rpc = P.rpc;
+    char *cur = head;
+    d.D = carve<int32_t>(cur, nn);
+    d.DT = carve<int32_t>(cur, nn);
+    d.F = carve<int32_t>(cur, nn);
+    d.FT = carve<int32_t>(cur, nn);
+    d.Ddiag = carve<int32_t>(cur, n);
+    d.Fdiag = carve<int32_t>(cur, n);
+    d.phi = carve<int32_t>(cur, reps * n);
+    d.beta = carve<double>(cur, reps);
+    d.order = carve<int32_t>(cur, (size_t)T * cap);
+    d.group_best = carve<int64_t>(cur, T);
+    d.single_best = carve<int64_t>(cur, 1);
+    d.stop_epoch = carve<int32_t>(cur, 1);
+    d.target_epoch = carve<int64_t>(cur, 1);
+    d.target_ns = carve<unsigned long long>(cur, 1);
+    cur = tail;
+    d.I = carve<char>(cur, reps * (size_t)n * P.npad * (P.bits / 8));
+    d.best_phi = carve<int32_t>(cur, reps * n);
+    d.E = carve<int64_t>(cur, reps);
+    d.bestE = carve<int64_t>(cur, reps);
+    d.accepts = carve<unsigned long long>(cur, reps);
+    d.tss = carve<int32_t>(cur, T);
+    d.finish = carve<unsigned int>(cur, T);
+    d.epoch = carve<int32_t>(cur, T);
+    d.start_ns = carve<unsigned long long>(cur, 1);
+    d.error = carve<int32_t>(cur, 1);
+    *out = d;
+}
+
+// setup() for one instance on the host side (CPU_PIM.cpp:109-162): writes the padded
+// matrices, transposes, diagonals, initial permutations, beta ladder, rank slots and the
+// sentinels into `mirror`, a host image of the instance's head region (P.head bytes) laid out
+// as carve_instance lays out the device head.
+void fill_head(const pimqap_instance *inst, const pimqap_params *params, const Plan &P,
+               char *mirror) {
+    SolveDev h;
+    carve_instance(P, mirror, mirror, &h);   // head pointers into the mirror
     const int n = P.n, T = P.T, R = P.R, cap = P.cap, ldm = P.ldm;
-    const size_t reps = (size_t)T * R, nn = (size_t)n * ldm;
-    auto buffer = [&](size_t bytes) -> char * {
-        keep.emplace_back(bytes, 0);
-        return keep.back().data();
-    };
-    int32_t *Dp = reinterpret_cast<int32_t *>(buffer(nn * 4));
-    int32_t *DT = reinterpret_cast<int32_t *>(buffer(nn * 4));
-    int32_t *Fp = reinterpret_cast<int32_t *>(buffer(nn * 4));
-    int32_t *FT = reinterpret_cast<int32_t *>(buffer(nn * 4));
-    int32_t *Dd = reinterpret_cast<int32_t *>(buffer((size_t)n * 4));
-    int32_t *Fd = reinterpret_cast<int32_t *>(buffer((size_t)n * 4));
+    const size_t reps = (size_t)T * R;
+    std::memset(mirror, 0, P.head);
+    int32_t *Dp = const_cast<int32_t *>(h.D), *DT = const_cast<int32_t *>(h.DT);
+    int32_t *Fp = const_cast<int32_t *>(h.F), *FT = const_cast<int32_t *>(h.FT);
+    int32_t *Dd = const_cast<int32_t *>(h.Ddiag), *Fd = const_cast<int32_t *>(h.Fdiag);
     for (int i = 0; i < n; ++i) {
         Dd[i] = inst->dist[i * n + i];
         Fd[i] = inst->flow[i * n + i];
@@ -351,269 +375,45 @@ pimqap_status stage_instance(const pimqap_instance *inst, const pimqap_params *p
         }
     }
     const std::vector<int32_t> perms = initial_perms(n, T, params->seed);
-    int32_t *phi = reinterpret_cast<int32_t *>(buffer(reps * n * 4));
     for (int t = 0; t < T; ++t)
         for (int l = 0; l < R; ++l)
-            std::memcpy(&phi[((size_t)t * R + l) * n], &perms[(size_t)t * n], sizeof(int32_t) * n);
+            std::memcpy(&h.phi[((size_t)t * R + l) * n], &perms[(size_t)t * n], sizeof(int32_t) * n);
     // beta ladder (CPU_PIM.cpp:111-119); -b is given in natural units and stored x 1/ln 2 (:528)
-    const double beta0 = params->beta_max * 1.44269504089;
-    double *beta = reinterpret_cast<double *>(buffer(reps * 8));
+    const double beta0 = params->beta_internal ? params->beta_max : params->beta_max * 1.44269504089;
     for (int t = 0; t < T; ++t) {
         double running = beta0;
         for (int l = R - 1; l >= 0; --l) {
-            beta[(size_t)t * R + l] = running;
+            h.beta[(size_t)t * R + l] = running;
             running /= params->beta_ratio;
         }
     }
-    int32_t *order = reinterpret_cast<int32_t *>(buffer((size_t)T * cap * 4));
     for (int t = 0; t < T; ++t)
-        for (int l = 0; l < R; ++l) order[(size_t)t * cap + l] = l;
-    int64_t *nob = reinterpret_cast<int64_t *>(buffer((size_t)(T + 1) * 8));
-    for (int t = 0; t <= T; ++t) nob[t] = pimqap::kNoBest;
-    int64_t *consts = reinterpret_cast<int64_t *>(buffer(3 * 8));
-    consts[0] = pimqap::kNoStop;
-    consts[1] = std::numeric_limits<int64_t>::max();
-    consts[2] = (int64_t)~0ull;
+        for (int l = 0; l < R; ++l) h.order[(size_t)t * cap + l] = l;
+    for (int t = 0; t < T; ++t) h.group_best[t] = pimqap::kNoBest;
+    *h.single_best = pimqap::kNoBest;
+    *h.stop_epoch = pimqap::kNoStop;
+    *h.target_epoch = std::numeric_limits<int64_t>::max();
+    *h.target_ns = ~0ull;
+    (void)reps;
+}
 
-    PQ_CUDA(cudaMemsetAsync(base, 0, P.total, q));
-    char *cur = base;
-    SolveDev d{};
-    d.n = n; d.R = R; d.T = T; d.cap = cap; d.spe = P.spe;
-    d.ldg = P.npad; d.lds = P.lds; d.ldm = ldm; d.rpc = P.rpc;
-    d.goal = params->goal;
-    d.seed = params->seed;
-    d.I = carve<char>(cur, reps * (size_t)n * P.npad * (P.bits / 8));
-    int32_t *dD = carve<int32_t>(cur, nn), *dDT = carve<int32_t>(cur, nn);
-    int32_t *dF = carve<int32_t>(cur, nn), *dFT = carve<int32_t>(cur, nn);
-    int32_t *dDd = carve<int32_t>(cur, n), *dFd = carve<int32_t>(cur, n);
-    d.D = dD; d.DT = dDT; d.F = dF; d.FT = dFT; d.Ddiag = dDd; d.Fdiag = dFd;
-    d.phi = carve<int32_t>(cur, reps * n);
-    d.best_phi = carve<int32_t>(cur, reps * n);
-    d.E = carve<int64_t>(cur, reps);
-    d.bestE = carve<int64_t>(cur, reps);
-    d.beta = carve<double>(cur, reps);
-    d.accepts = carve<unsigned long long>(cur, reps);
-    d.order = carve<int32_t>(cur, (size_t)T * cap);
-    d.tss = carve<int32_t>(cur, T);
-    d.group_best = carve<int64_t>(cur, T);
-    d.finish = carve<unsigned int>(cur, T);
-    d.epoch = carve<int32_t>(cur, T);
-    d.single_best = carve<int64_t>(cur, 1);
-    d.stop_epoch = carve<int32_t>(cur, 1);
-    d.target_epoch = carve<int64_t>(cur, 1);
-    d.target_ns = carve<unsigned long long>(cur, 1);
-    d.start_ns = carve<unsigned long long>(cur, 1);
-    d.error = carve<int32_t>(cur, 1);
-    if ((size_t)(cur - base) > P.total) return fail(PIMQAP_ERR_ARG, "internal: device carve overflow");
-    PQ_CUDA(cudaMemcpyAsync(dD, Dp, nn * 4, cudaMemcpyHostToDevice, q));
-    PQ_CUDA(cudaMemcpyAsync(dF, Fp, nn * 4, cudaMemcpyHostToDevice, q));
-    PQ_CUDA(cudaMemcpyAsync(dDT, DT, nn * 4, cudaMemcpyHostToDevice, q));
-    PQ_CUDA(cudaMemcpyAsync(dFT, FT, nn * 4, cudaMemcpyHostToDevice, q));
-    PQ_CUDA(cudaMemcpyAsync(dDd, Dd, (size_t)n * 4, cudaMemcpyHostToDevice, q));
-    PQ_CUDA(cudaMemcpyAsync(dFd, Fd, (size_t)n * 4, cudaMemcpyHostToDevice, q));
-    PQ_CUDA(cudaMemcpyAsync(d.phi, phi, reps * n * 4, cudaMemcpyHostToDevice, q));
-    PQ_CUDA(cudaMemcpyAsync(d.beta, beta, reps * 8, cudaMemcpyHostToDevice, q));
-    PQ_CUDA(cudaMemcpyAsync(d.order, order, (size_t)T * cap * 4, cudaMemcpyHostToDevice, q));
-    PQ_CUDA(cudaMemcpyAsync(d.group_best, nob, (size_t)T * 8, cudaMemcpyHostToDevice, q));
-    PQ_CUDA(cudaMemcpyAsync(d.single_best, nob + T, 8, cudaMemcpyHostToDevice, q));
-    PQ_CUDA(cudaMemcpyAsync(d.stop_epoch, &consts[0], 4, cudaMemcpyHostToDevice, q));
-    PQ_CUDA(cudaMemcpyAsync(d.target_epoch, &consts[1], 8, cudaMemcpyHostToDevice, q));
-    PQ_CUDA(cudaMemcpyAsync(d.target_ns, &consts[2], 8, cudaMemcpyHostToDevice, q));
-    PQ_CUDA(pimqap::launch_setup(d, P.bits, q));
-    *out = d;
+pimqap_status stage_instance(const pimqap_instance *inst, const pimqap_params *params,
+                             const Plan &P, char *base, SolveDev *out, cudaStream_t q,
+                             std::vector<std::vector<char>> &keep) {
+    keep.emplace_back(P.head, 0);
+    char *mirror = keep.back().data();
+    fill_head(inst, params, P, mirror);
+    carve_instance(P, base, base + P.head, out);
+    out->goal = params->goal;
+    out->seed = params->seed;
+    PQ_CUDA(cudaMemcpyAsync(base, mirror, P.head, cudaMemcpyHostToDevice, q));
+    PQ_CUDA(cudaMemsetAsync(base + P.head, 0, P.tail, q));
+    PQ_CUDA(pimqap::launch_setup(*out, P.bits, q));
     return PIMQAP_OK;
 }
 
-// Worker shape of a persistent class (the autotuner's knobs): threads per replica worker,
-// workers per CTA (named barriers 1..8) and the shared-memory slice of one worker.
-struct BatchShape {
-    int worker_threads = 128, workers = 1, ctas_per_sm = 1, grid = 1;
-    size_t slice = 0;
-};
-
-BatchShape batch_shape(const std::vector<Plan> &plans, const std::vector<int> &members, int bits,
-                       int sms, int maxsm) {
-    BatchShape S;
-    int nmax = 0;
-    for (int k : members) {
-        S.slice = std::max(S.slice, pimqap::batch_slice_bytes(plans[k].n, bits));
-        nmax = std::max(nmax, plans[k].n);
-    }
-    S.worker_threads = nmax <= 32 ? 32 : (nmax <= 64 ? 64 : 128);
-    S.workers = std::max(1, std::min(256 / S.worker_threads, (int)((size_t)maxsm / S.slice)));
-    int occ = 0;
-    if (pimqap::batch_occupancy(bits, S.workers * S.worker_threads, S.workers * S.slice, &occ) != cudaSuccess || occ < 1)
-        occ = 1;
-    S.ctas_per_sm = occ;
-    S.grid = sms * occ;
-    return S;
-}
-
-// Solves `members` (single-CTA replicas of one force-matrix width) in one persistent launch.
-pimqap_status run_batch_class(const pimqap_instance *insts, const pimqap_params *params,
-                              const std::vector<Plan> &plans, const std::vector<int> &members,
-                              int bits, int sms, int maxsm, pimqap_result *results) {
-    const int m = (int)members.size();
-    const BatchShape S = batch_shape(plans, members, bits, sms, maxsm);
-    size_t reps_total = 0, inst_bytes = 0;
-    std::vector<size_t> offs(m);
-    for (int q = 0; q < m; ++q) {
-        const Plan &P = plans[members[q]];
-        offs[q] = inst_bytes;
-        inst_bytes += carve_size(P.total);
-        reps_total += (size_t)P.T * P.R;
-    }
-    unsigned qcap = 1;
-    while (qcap < reps_total + 1) qcap <<= 1;
-    const size_t total = inst_bytes + carve_size(sizeof(SolveDev) * m) + 3 * carve_size(8 * (size_t)m) +
-                         2 * carve_size(8 * (size_t)qcap) + 6 * carve_size(8);
-    char *base = nullptr;
-    PQ_CUDA(cudaMalloc(&base, total));
-    struct Free {
-        char *p;
-        ~Free() { cudaFree(p); }
-    } free_guard{base};
-    cudaStream_t q = nullptr;
-    PQ_CUDA(cudaStreamCreateWithFlags(&q, cudaStreamNonBlocking));
-    struct FreeStream {
-        cudaStream_t s;
-        ~FreeStream() { cudaStreamDestroy(s); }
-    } stream_guard{q};
-
-    std::vector<SolveDev> devs(m);
-    std::vector<std::vector<char>> keep;
-    for (int i = 0; i < m; ++i) {
-        const int k = members[i];
-        pimqap_status st = stage_instance(&insts[k], &params[k], plans[k], base + offs[i], &devs[i], q, keep);
-        if (st != PIMQAP_OK) return st;
-    }
-    char *cur = base + inst_bytes;
-    SolveDev *d_inst = carve<SolveDev>(cur, m);
-    int32_t *d_sym = reinterpret_cast<int32_t *>(carve<int64_t>(cur, m));
-    int64_t *d_maxm = carve<int64_t>(cur, m);
-    unsigned int *d_finish = reinterpret_cast<unsigned int *>(carve<int64_t>(cur, m));
-    unsigned long long *d_items = carve<unsigned long long>(cur, qcap);
-    unsigned long long *d_seq = carve<unsigned long long>(cur, qcap);
-    unsigned long long *d_head = carve<unsigned long long>(cur, 1);
-    unsigned long long *d_tail = carve<unsigned long long>(cur, 1);
-    int32_t *d_active = reinterpret_cast<int32_t *>(carve<int64_t>(cur, 1));
-    int32_t *d_error = reinterpret_cast<int32_t *>(carve<int64_t>(cur, 1));
-    unsigned long long *d_start = carve<unsigned long long>(cur, 1);
-    PQ_CUDA(cudaMemsetAsync(base + inst_bytes, 0, total - inst_bytes, q));
-
-    PQ_CUDA(cudaStreamSynchronize(q));
-    keep.clear();
-    std::vector<int32_t> stop0(m);
-    for (int i = 0; i < m; ++i)
-        PQ_CUDA(cudaMemcpy(&stop0[i], devs[i].stop_epoch, 4, cudaMemcpyDeviceToHost));
-    // Epoch-0 items, largest instances first (they take longest).
-    std::vector<int> order_idx(m);
-    for (int i = 0; i < m; ++i) order_idx[i] = i;
-    std::stable_sort(order_idx.begin(), order_idx.end(), [&](int a, int b) {
-        const Plan &A = plans[members[a]], &B = plans[members[b]];
-        return (double)A.n * A.n * A.T * A.R > (double)B.n * B.n * B.T * B.R;
-    });
-    std::vector<int32_t> sym(2 * m, 0);
-    std::vector<int64_t> maxm(m);
-    std::vector<unsigned long long> items, seq;
-    int active = 0;
-    for (int i = 0; i < m; ++i) {
-        sym[i] = plans[members[i]].sym ? 1 : 0;
-        maxm[i] = params[members[i]].max_megaiters;
-    }
-    for (int i : order_idx) {
-        const Plan &P = plans[members[i]];
-        if (maxm[i] <= 0 || stop0[i] <= 0) continue;   // nothing to run, or goal met at setup
-        ++active;
-        for (int r = 0; r < P.T * P.R; ++r) {
-            items.push_back(((unsigned long long)i << 32) | (unsigned)r);
-            seq.push_back(items.size());
-        }
-    }
-    const unsigned long long tail = items.size();
-    PQ_CUDA(cudaMemcpyAsync(d_inst, devs.data(), sizeof(SolveDev) * m, cudaMemcpyHostToDevice, q));
-    PQ_CUDA(cudaMemcpyAsync(d_sym, sym.data(), 4 * (size_t)m, cudaMemcpyHostToDevice, q));
-    PQ_CUDA(cudaMemcpyAsync(d_maxm, maxm.data(), 8 * (size_t)m, cudaMemcpyHostToDevice, q));
-    if (!items.empty()) {
-        PQ_CUDA(cudaMemcpyAsync(d_items, items.data(), 8 * items.size(), cudaMemcpyHostToDevice, q));
-        PQ_CUDA(cudaMemcpyAsync(d_seq, seq.data(), 8 * seq.size(), cudaMemcpyHostToDevice, q));
-    }
-    PQ_CUDA(cudaMemcpyAsync(d_tail, &tail, 8, cudaMemcpyHostToDevice, q));
-    PQ_CUDA(cudaMemcpyAsync(d_active, &active, 4, cudaMemcpyHostToDevice, q));
-    PQ_CUDA(cudaStreamSynchronize(q));
-    keep.clear();
-
-    pimqap::BatchDev B{};
-    B.inst = d_inst; B.sym = d_sym; B.max_megaiters = d_maxm; B.finish_inst = d_finish;
-    B.count = m; B.q_items = d_items; B.q_seq = d_seq; B.q_head = d_head; B.q_tail = d_tail;
-    B.qmask = qcap - 1; B.active = d_active; B.error = d_error; B.start_ns = d_start;
-    B.worker_threads = S.worker_threads; B.workers = S.workers; B.slice_bytes = (unsigned)S.slice;
-    cudaEvent_t e0, e1;
-    PQ_CUDA(cudaEventCreate(&e0));
-    PQ_CUDA(cudaEventCreate(&e1));
-    PQ_CUDA(cudaEventRecord(e0, q));
-    if (active > 0) PQ_CUDA(pimqap::launch_batch(B, bits, S.grid, q));
-    PQ_CUDA(cudaEventRecord(e1, q));
-    PQ_CUDA(cudaStreamSynchronize(q));
-    float ms = 0;
-    cudaEventElapsedTime(&ms, e0, e1);
-    cudaEventDestroy(e0);
-    cudaEventDestroy(e1);
-    int32_t err = 0;
-    unsigned long long start_ns = 0;
-    PQ_CUDA(cudaMemcpy(&err, d_error, 4, cudaMemcpyDeviceToHost));
-    PQ_CUDA(cudaMemcpy(&start_ns, d_start, 8, cudaMemcpyDeviceToHost));
-    if (err) return fail(PIMQAP_ERR_DEVICE, "batch kernel check failed (error word " + std::to_string(err) + ")");
-
-    for (int i = 0; i < m; ++i) {
-        const int k = members[i];
-        const SolveDev &d = devs[i];
-        const Plan &P = plans[k];
-        const size_t reps = (size_t)P.T * P.R;
-        std::vector<int64_t> bestE(reps);
-        std::vector<unsigned long long> acc(reps);
-        int64_t single = 0, tepoch = 0;
-        unsigned long long tns = 0;
-        int32_t epoch0 = 0, ierr = 0;
-        PQ_CUDA(cudaMemcpy(bestE.data(), d.bestE, reps * 8, cudaMemcpyDeviceToHost));
-        PQ_CUDA(cudaMemcpy(acc.data(), d.accepts, reps * 8, cudaMemcpyDeviceToHost));
-        PQ_CUDA(cudaMemcpy(&single, d.single_best, 8, cudaMemcpyDeviceToHost));
-        PQ_CUDA(cudaMemcpy(&tepoch, d.target_epoch, 8, cudaMemcpyDeviceToHost));
-        PQ_CUDA(cudaMemcpy(&tns, d.target_ns, 8, cudaMemcpyDeviceToHost));
-        PQ_CUDA(cudaMemcpy(&epoch0, d.epoch, 4, cudaMemcpyDeviceToHost));
-        PQ_CUDA(cudaMemcpy(&ierr, d.error, 4, cudaMemcpyDeviceToHost));
-        if (ierr) return fail(PIMQAP_ERR_DEVICE, "device check failed in batch instance " + std::to_string(k));
-        size_t arg = 0;
-        for (size_t r = 1; r < reps; ++r)
-            if (bestE[r] < bestE[arg]) arg = r;
-        pimqap_result &R = results[k];
-        int32_t *perm_dst = R.best_perm;
-        std::memset(&R, 0, sizeof(R));
-        R.best_perm = perm_dst;
-        R.best_energy = std::min<int64_t>(bestE[arg], single);
-        if (perm_dst)
-            PQ_CUDA(cudaMemcpy(perm_dst, d.best_phi + arg * P.n, (size_t)P.n * 4, cudaMemcpyDeviceToHost));
-        R.target_megaiter = (tepoch == std::numeric_limits<int64_t>::max()) ? -1 : tepoch;
-        R.time_to_target_ms = (R.target_megaiter >= 0 && tns != ~0ull && tns >= start_ns)
-                                  ? (double)(tns - start_ns) * 1e-6 : (R.target_megaiter >= 0 ? 0.0 : -1.0);
-        R.megaiters_done = epoch0;
-        R.updates = (int64_t)epoch0 * P.spe * P.n * (int64_t)reps;
-        int64_t a = 0;
-        for (auto v : acc) a += (int64_t)v;
-        R.accepts = a;
-        R.device_ms = ms;
-        R.force_bits = P.bits;
-        R.cluster_size = 1;
-        int32_t stop = 0;
-        PQ_CUDA(cudaMemcpy(&stop, d.stop_epoch, 4, cudaMemcpyDeviceToHost));
-        R.stopped_by = (stop != pimqap::kNoStop) ? 1 : 0;
-        R.h2d_bytes = P.h2d_bytes;
-        R.d2h_bytes = (int64_t)(reps * 16 + 40 + (perm_dst ? (size_t)P.n * 4 : 0));
-    }
-    return PIMQAP_OK;
-}
-
-}  // namespace
+}  // namespace detail
+}  // namespace pimqap
 
 extern "C" {
 
@@ -630,6 +430,8 @@ void pimqap_default_params(pimqap_params *p) {
     p->timeout_s = 0;
     p->seed = 1;
     p->device = 0;
+    p->auto_lower = 0.1;            // lowerBetaProportion (:33)
+    p->auto_higher = 0.9;           // higherBetaProportion (:34)
 }
 
 const char *pimqap_last_error(void) { return g_error.c_str(); }
@@ -697,6 +499,8 @@ pimqap_status pimqap_solver_create(const pimqap_instance *inst, const pimqap_par
     if (st != PIMQAP_OK) return st;
     SolveDev &d = s->dev;
     s->h2d = plan.h2d_bytes;
+    s->beta0_used = params->beta_internal ? params->beta_max : params->beta_max * 1.44269504089;
+    s->ratio_used = params->beta_ratio;
     PQ_CUDA(cudaStreamSynchronize(q));
     int32_t err = 0;
     PQ_CUDA(cudaMemcpy(&err, d.error, 4, cudaMemcpyDeviceToHost));
@@ -783,9 +587,14 @@ pimqap_status pimqap_solver_result(pimqap_solver *s, pimqap_result *r) {
     for (size_t k = 1; k < reps; ++k)
         if (bestE[k] < bestE[arg]) arg = k;
     int32_t *perm_dst = r->best_perm;
+    int64_t *energy_dst = r->final_energies;
     std::memset(r, 0, sizeof(*r));
     r->best_perm = perm_dst;
+    r->final_energies = energy_dst;
     r->best_energy = std::min<int64_t>(bestE[arg], single);
+    if (energy_dst) PQ_CUDA(cudaMemcpy(energy_dst, s->dev.E, reps * 8, cudaMemcpyDeviceToHost));
+    r->beta_max_used = s->beta0_used;
+    r->beta_ratio_used = s->ratio_used;
     if (perm_dst)
         PQ_CUDA(cudaMemcpy(perm_dst, s->dev.best_phi + arg * s->n, (size_t)s->n * 4, cudaMemcpyDeviceToHost));
     r->target_megaiter = (tepoch == std::numeric_limits<int64_t>::max()) ? -1 : tepoch;
@@ -852,69 +661,42 @@ void pimqap_solver_destroy(pimqap_solver *s) { delete s; }
 pimqap_status pimqap_solve(const pimqap_instance *inst, const pimqap_params *params,
                            pimqap_result *result) {
     if (!result) return fail(PIMQAP_ERR_ARG, "null result");
+    if (!params) return fail(PIMQAP_ERR_ARG, "null params");
     const auto w0 = std::chrono::steady_clock::now();
+    pimqap_params p = *params;
+    int64_t auto_best = PIMQAP_NO_BEST;
+    std::vector<int32_t> auto_perm;
+    if (p.auto_beta) {   // automatic mode first (CPU_PIM.cpp:650-658)
+        pimqap_status st = check_params(inst, params);
+        if (st != PIMQAP_OK) return st;
+        double b0 = 0, db = 0;
+        auto_perm.assign(inst->n, 0);
+        st = pimqap_auto_beta(inst, params, &b0, &db, nullptr, &auto_best, auto_perm.data());
+        if (st != PIMQAP_OK) return st;
+        p.auto_beta = 0;
+        p.beta_internal = 1;
+        p.beta_max = b0;
+        p.beta_ratio = db;
+        if (auto_best <= p.goal) p.max_megaiters = 0;   // the trials reached the goal (:420-422, :661)
+    }
     pimqap_solver *s = nullptr;
-    pimqap_status st = pimqap_solver_create(inst, params, &s);
+    pimqap_status st = pimqap_solver_create(inst, &p, &s);
     if (st != PIMQAP_OK) return st;
-    st = pimqap_solver_run(s, params->max_megaiters, nullptr);
+    st = pimqap_solver_run(s, p.max_megaiters, nullptr);
     if (st == PIMQAP_OK) st = pimqap_solver_result(s, result);
     const double el = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - w0).count();
     if (st == PIMQAP_OK) {
         result->wall_ms = el;
-        if (result->stopped_by == 0 && params->timeout_s > 0 && result->megaiters_done < params->max_megaiters)
+        if (result->stopped_by == 0 && p.timeout_s > 0 && result->megaiters_done < p.max_megaiters)
             result->stopped_by = 2;
+        if (auto_best < result->best_energy) {   // the trials' best counts (singleBestE carries over)
+            result->best_energy = auto_best;
+            if (result->best_perm) std::memcpy(result->best_perm, auto_perm.data(), 4 * (size_t)inst->n);
+            if (auto_best <= p.goal) result->stopped_by = 1;
+        }
     }
     pimqap_solver_destroy(s);
     return st;
-}
-
-pimqap_status pimqap_batch_solve(const pimqap_instance *insts, const pimqap_params *params,
-                                 int32_t count, pimqap_result *results) {
-    if (count < 0 || (count > 0 && (!insts || !params || !results)))
-        return fail(PIMQAP_ERR_ARG, "bad batch arguments");
-    if (count == 0) return PIMQAP_OK;
-    const auto wall0 = std::chrono::steady_clock::now();
-    for (int k = 0; k < count; ++k) {
-        pimqap_status st = check_params(&insts[k], &params[k]);
-        if (st != PIMQAP_OK) return st;
-        if (params[k].device != params[0].device)
-            return fail(PIMQAP_ERR_ARG, "every batch entry must use the same device");
-    }
-    int maxsm = 0;
-    pimqap_status st = open_device(params[0].device, &maxsm);
-    if (st != PIMQAP_OK) return st;
-    int sms = 0;
-    PQ_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, params[0].device));
-
-    std::vector<Plan> plans(count);
-    for (int k = 0; k < count; ++k) {
-        st = plan_instance(&insts[k], &params[k], (size_t)maxsm, params[k].cluster_size, &plans[k]);
-        if (st != PIMQAP_OK) return st;
-    }
-    // Persistent classes: single-CTA replicas by force-matrix width.  Replicas that need a
-    // cluster are solved by the epoch launches of pimqap_solve.
-    std::vector<int> cluster_members;
-    for (int bits : {32, 64}) {
-        std::vector<int> members;
-        for (int k = 0; k < count; ++k) {
-            if (plans[k].bits != bits) continue;
-            if (plans[k].cl != 1 || pimqap::batch_slice_bytes(plans[k].n, bits) > (size_t)maxsm) continue;
-            members.push_back(k);
-        }
-        if (members.empty()) continue;
-        st = run_batch_class(insts, params, plans, members, bits, sms, maxsm, results);
-        if (st != PIMQAP_OK) return st;
-    }
-    for (int k = 0; k < count; ++k) {
-        const bool in_class = plans[k].cl == 1 &&
-                              pimqap::batch_slice_bytes(plans[k].n, plans[k].bits) <= (size_t)maxsm;
-        if (in_class) continue;
-        st = pimqap_solve(&insts[k], &params[k], &results[k]);
-        if (st != PIMQAP_OK) return st;
-    }
-    const double el = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - wall0).count();
-    for (int k = 0; k < count; ++k) results[k].wall_ms = el;
-    return PIMQAP_OK;
 }
 
 }  // extern "C"

@@ -67,6 +67,7 @@ struct BatchDev {
     unsigned long long *q_tail;      // [1] next ticket to push
     unsigned int qmask;
     int32_t *active;                 // [1] instances still running
+    int32_t *shutdown;               // [1] nonzero: workers exit once no instance is active
     int32_t *error;                  // [1] kErr* bits
     unsigned long long *start_ns;    // [1] %globaltimer when the launch began
     int worker_threads;              // threads of one replica worker (a multiple of 32)
@@ -77,11 +78,27 @@ struct BatchDev {
 // Shared memory of one replica worker of the batch kernel (single-CTA replica of size n).
 size_t batch_slice_bytes(int n, int bits);
 
-// The persistent batch launch: grid CTAs of workers * worker_threads threads.
-cudaError_t launch_batch(const BatchDev &b, int bits, int grid, cudaStream_t st);
+// The persistent batch launch: grid CTAs (clusters of cl) of workers * worker_threads threads.
+cudaError_t launch_batch(const BatchDev &b, int bits, int cl, int grid, cudaStream_t st);
 
-// Resident CTAs per SM of the batch kernel for this shape.
-cudaError_t batch_occupancy(int bits, int threads, size_t smem, int *ctas_per_sm);
+// Residency of the batch kernel for this shape: CTAs per SM for cl == 1, else resident
+// clusters on the device.
+cudaError_t batch_occupancy(int bits, int cl, int threads, size_t smem, int *out);
+
+// Compact per-instance result of a batch.
+struct BatchResultDev {
+    long long best, arg;
+    unsigned long long accepts;
+    long long single_best, target_epoch;
+    unsigned long long target_ns;
+    int32_t epoch, stop_epoch, error, pad;
+};
+
+// Gathers every instance's result, best permutation (perms + perm_off[k], n entries) and
+// final replica energies (energies + energy_off[k], T*R entries).
+cudaError_t launch_collect(const SolveDev *inst, int count, BatchResultDev *out, int32_t *perms,
+                           const long long *perm_off, long long *energies, const long long *energy_off,
+                           cudaStream_t st);
 
 // Records msg as the calling thread's pimqap_last_error() text.
 void set_last_error(const char *msg);

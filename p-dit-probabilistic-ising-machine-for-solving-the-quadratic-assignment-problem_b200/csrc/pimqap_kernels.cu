@@ -768,7 +768,7 @@ __device__ unsigned long long queue_pop(const BatchDev &B) {
             __threadfence();
             return *((volatile unsigned long long *)B.q_items + slot);
         }
-        if (*(volatile int32_t *)B.active == 0) return kDoneItem;
+        if (*(volatile int32_t *)B.active == 0 && *(volatile int32_t *)B.shutdown != 0) return kDoneItem;
         if (globaltimer_ns() - t0 > kQueueWaitNs) {
             atomicOr(B.error, kErrTimeout);
             return kDoneItem;
@@ -841,6 +841,116 @@ __global__ void __launch_bounds__(256) batch_kernel(BatchDev B) {
     }
 }
 
+// Batch kernel for replicas that span a cluster of CL CTAs: rank 0 pops an item and writes it
+// into every rank's header; the whole cluster runs the replica's epoch, rank 0 reports it.
+template <class IT, int CL>
+__global__ void __launch_bounds__(256) batch_cluster_kernel(BatchDev B) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    cg::cluster_group cluster = cg::this_cluster();
+    const int rank = (int)cluster.block_rank();
+    unsigned long long *hdr = reinterpret_cast<unsigned long long *>(smem);
+    unsigned char *work = smem + 16;
+    const Grp G{(int)threadIdx.x, (int)blockDim.x, (int)(threadIdx.x & 31), (int)(threadIdx.x >> 5),
+                (int)(blockDim.x >> 5), 0};
+    if (blockIdx.x == 0 && threadIdx.x == 0) *B.start_ns = globaltimer_ns();
+    cluster_barrier<CL>();
+    for (;;) {
+        if (rank == 0 && threadIdx.x == 0) {
+            const unsigned long long item = queue_pop(B);
+#pragma unroll
+            for (int r = 0; r < CL; ++r) *cluster.map_shared_rank(hdr, r) = item;
+        }
+        cluster_barrier<CL>();
+        const unsigned long long item = *(volatile unsigned long long *)hdr;
+        if (item == kDoneItem) break;
+        const int k = (int)(item >> 32), rep = (int)(item & 0xffffffffull);
+        const SolveDev &s = B.inst[k];
+        const int e = *((volatile int32_t *)s.epoch);
+        bool ok;
+        if (B.sym[k]) ok = replica_epoch<IT, CL, true>(s, rep, rank, e, G, work);
+        else ok = replica_epoch<IT, CL, false>(s, rep, rank, e, G, work);
+        __syncthreads();
+        if (!ok) {
+            if (threadIdx.x == 0) atomicOr(B.error, kErrTimeout);
+        } else if (rank == 0 && threadIdx.x == 0) {
+            const int replicas = s.T * s.R;
+            const unsigned prev = atomicAdd(B.finish_inst + k, 1u);
+            if (prev == (unsigned)replicas - 1u) {
+                __threadfence();
+                for (int g = 0; g < s.T; ++g) track_exchange(s, g, e + 1);
+                B.finish_inst[k] = 0u;
+                for (int g = 0; g < s.T; ++g) s.epoch[g] = e + 1;
+                __threadfence();
+                const int stop = *(volatile int32_t *)s.stop_epoch;
+                if (e + 1 < stop && (int64_t)(e + 1) < B.max_megaiters[k]) {
+                    queue_push_instance(B, k, replicas);
+                } else {
+                    __threadfence();
+                    atomicSub(B.active, 1);
+                }
+            }
+        }
+        // the header is rewritten only after every rank has read it (the epoch ends with a
+        // cluster barrier); this barrier also orders the next pop after rank 0's report
+        cluster_barrier<CL>();
+    }
+    cluster_barrier<CL>();
+}
+
+// Per-instance results of a batch, gathered on the device so the host reads them at once.
+__global__ void batch_collect_kernel(const SolveDev *inst, int count, BatchResultDev *out,
+                                     int32_t *perms, const long long *perm_off, long long *energies,
+                                     const long long *energy_off) {
+    const int k = blockIdx.x;
+    if (k >= count) return;
+    const SolveDev &s = inst[k];
+    const int reps = s.T * s.R;
+    __shared__ long long sb[128], sa[128];
+    __shared__ unsigned long long sc[128];
+    long long best = 0x7fffffffffffffffll, arg = 0;
+    unsigned long long acc = 0;
+    for (int r = threadIdx.x; r < reps; r += blockDim.x) {
+        const long long v = __ldcg((const long long *)s.bestE + r);
+        if (v < best) { best = v; arg = r; }
+        acc += __ldcg(s.accepts + r);
+    }
+    sb[threadIdx.x] = best; sa[threadIdx.x] = arg; sc[threadIdx.x] = acc;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        long long b = sb[0], a = sa[0];
+        unsigned long long c = sc[0];
+        for (int t = 1; t < (int)blockDim.x; ++t) {
+            if (sb[t] < b || (sb[t] == b && sa[t] < a)) { b = sb[t]; a = sa[t]; }
+            c += sc[t];
+        }
+        BatchResultDev &o = out[k];
+        o.best = b;
+        o.arg = a;
+        o.accepts = c;
+        o.single_best = __ldcg((const long long *)s.single_best);
+        o.target_epoch = __ldcg((const long long *)s.target_epoch);
+        o.target_ns = __ldcg(s.target_ns);
+        o.epoch = __ldcg(s.epoch);
+        o.stop_epoch = __ldcg(s.stop_epoch);
+        o.error = __ldcg(s.error);
+        sa[0] = a;
+    }
+    __syncthreads();
+    const long long a = sa[0];
+    for (int q = threadIdx.x; q < s.n; q += blockDim.x)
+        perms[perm_off[k] + q] = __ldcg(s.best_phi + a * s.n + q);
+    for (int r = threadIdx.x; r < reps; r += blockDim.x)
+        energies[energy_off[k] + r] = __ldcg((const long long *)s.E + r);
+}
+
+cudaError_t launch_collect(const SolveDev *inst, int count, BatchResultDev *out, int32_t *perms,
+                           const long long *perm_off, long long *energies, const long long *energy_off,
+                           cudaStream_t st) {
+    if (count <= 0) return cudaSuccess;
+    batch_collect_kernel<<<count, 128, 0, st>>>(inst, count, out, perms, perm_off, energies, energy_off);
+    return cudaGetLastError();
+}
+
 // ------------------------------------------------------------------ launchers
 
 template <class IT, int CL, bool SYM> static void *epoch_fn() {
@@ -861,18 +971,61 @@ static void *epoch_kernel_ptr(int bits, int cl, bool sym) {
     return nullptr;
 }
 
-cudaError_t launch_batch(const BatchDev &b, int bits, int grid, cudaStream_t st) {
-    const size_t smem = (size_t)b.workers * b.slice_bytes;
-    const int threads = b.workers * b.worker_threads;
-    if (bits == 32) batch_kernel<int32_t><<<grid, threads, smem, st>>>(b);
-    else batch_kernel<int64_t><<<grid, threads, smem, st>>>(b);
-    return cudaGetLastError();
+static void *batch_fn(int bits, int cl) {
+    if (bits == 32) {
+        switch (cl) {
+            case 1: return reinterpret_cast<void *>(&batch_kernel<int32_t>);
+            case 2: return reinterpret_cast<void *>(&batch_cluster_kernel<int32_t, 2>);
+            case 4: return reinterpret_cast<void *>(&batch_cluster_kernel<int32_t, 4>);
+        }
+    } else if (bits == 64) {
+        switch (cl) {
+            case 1: return reinterpret_cast<void *>(&batch_kernel<int64_t>);
+            case 2: return reinterpret_cast<void *>(&batch_cluster_kernel<int64_t, 2>);
+            case 4: return reinterpret_cast<void *>(&batch_cluster_kernel<int64_t, 4>);
+        }
+    }
+    return nullptr;
 }
 
-cudaError_t batch_occupancy(int bits, int threads, size_t smem, int *ctas_per_sm) {
-    if (bits == 32)
-        return cudaOccupancyMaxActiveBlocksPerMultiprocessor(ctas_per_sm, batch_kernel<int32_t>, threads, smem);
-    return cudaOccupancyMaxActiveBlocksPerMultiprocessor(ctas_per_sm, batch_kernel<int64_t>, threads, smem);
+cudaError_t launch_batch(const BatchDev &b, int bits, int cl, int grid, cudaStream_t st) {
+    void *fn = batch_fn(bits, cl);
+    if (!fn) return cudaErrorInvalidValue;
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3((unsigned)grid);
+    cfg.blockDim = dim3((unsigned)(b.workers * b.worker_threads));
+    cfg.dynamicSmemBytes = (size_t)b.workers * b.slice_bytes;
+    cfg.stream = st;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = (unsigned)cl;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    void *args[] = {const_cast<BatchDev *>(&b)};
+    return cudaLaunchKernelExC(&cfg, fn, args);
+}
+
+cudaError_t batch_occupancy(int bits, int cl, int threads, size_t smem, int *ctas_per_sm) {
+    void *fn = batch_fn(bits, cl);
+    if (!fn) return cudaErrorInvalidValue;
+    if (cl == 1) return cudaOccupancyMaxActiveBlocksPerMultiprocessor(ctas_per_sm, fn, threads, smem);
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3((unsigned)cl);
+    cfg.blockDim = dim3((unsigned)threads);
+    cfg.dynamicSmemBytes = smem;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = (unsigned)cl;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    int clusters = 0;
+    cudaError_t e = cudaOccupancyMaxActiveClusters(&clusters, fn, &cfg);
+    *ctas_per_sm = clusters;   // for clusters: resident clusters on the whole device
+    return e;
 }
 
 cudaError_t prepare_kernels() {
@@ -889,9 +1042,12 @@ cudaError_t prepare_kernels() {
                                            cudaFuncAttributeMaxDynamicSharedMemorySize, maxsm);
                 if (err != cudaSuccess) return err;
             }
-    err = cudaFuncSetAttribute(batch_kernel<int32_t>, cudaFuncAttributeMaxDynamicSharedMemorySize, maxsm);
-    if (err != cudaSuccess) return err;
-    return cudaFuncSetAttribute(batch_kernel<int64_t>, cudaFuncAttributeMaxDynamicSharedMemorySize, maxsm);
+    for (int bits : {32, 64})
+        for (int cl : {1, 2, 4}) {
+            err = cudaFuncSetAttribute(batch_fn(bits, cl), cudaFuncAttributeMaxDynamicSharedMemorySize, maxsm);
+            if (err != cudaSuccess) return err;
+        }
+    return cudaSuccess;
 }
 
 cudaError_t launch_setup(const SolveDev &s, int bits, cudaStream_t st) {

@@ -1,0 +1,79 @@
+// pimqap_plan.h - per-instance planning and staging shared by the solve, batch and serving
+// paths of the host runtime.  Not part of the C ABI.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstddef>
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "pimqap.h"
+#include "pimqap_internal.h"
+
+#define PQ_CUDA(x)                                                                          \
+    do {                                                                                    \
+        cudaError_t e_ = (x);                                                               \
+        if (e_ != cudaSuccess)                                                              \
+            return ::pimqap::detail::fail(PIMQAP_ERR_CUDA,                                  \
+                                          std::string(#x) + ": " + cudaGetErrorString(e_)); \
+    } while (0)
+
+namespace pimqap {
+namespace detail {
+
+// Records msg as pimqap_last_error() of the calling thread and returns st.
+pimqap_status fail(pimqap_status st, const std::string &msg);
+
+// Phase timing on stderr when the environment variable PIMQAP_TRACE is set.
+void trace(const char *phase);
+
+int round_up(int x, int m);
+inline size_t carve_size(size_t bytes) { return (bytes + 255) & ~size_t(255); }
+template <class T> T *carve(char *&cur, size_t count) {
+    T *p = reinterpret_cast<T *>(cur);
+    cur += carve_size(count * sizeof(T));
+    return p;
+}
+
+// Initial permutations of T groups (CPU_PIM.cpp:134-162) from the shuffle stream of `seed`.
+std::vector<int32_t> initial_perms(int n, int T, uint64_t seed);
+
+pimqap_status check_params(const pimqap_instance *inst, const pimqap_params *p);
+
+// Everything decided for one instance before device memory is touched.  Device memory of an
+// instance is a head (uploaded from the host) and a tail (state that starts at zero).
+struct Plan {
+    int n = 0, T = 0, R = 0, cap = 0, spe = 0;
+    int bits = 32, cl = 1, threads = 256;
+    int npad = 0, lds = 0, ldm = 0, rpc = 0;
+    bool sym = false;
+    size_t smem = 0;       // epoch kernel shared memory per CTA
+    size_t head = 0, tail = 0, total = 0;
+    int64_t h2d_bytes = 0;
+};
+
+// Makes `device` current, checks it is an sm_100 part and prepares the kernels.
+pimqap_status open_device(int device, int *maxsm);
+
+// Force-matrix width, symmetry, launch shape (threads; the smallest cluster whose row share
+// of the force matrix fits one CTA, or want_cluster), strides and device footprint.
+pimqap_status plan_instance(const pimqap_instance *inst, const pimqap_params *params, size_t maxsm,
+                            int want_cluster, Plan *out);
+
+// Device pointers of one instance carved from its head and tail regions.
+void carve_instance(const Plan &P, char *head, char *tail, SolveDev *out);
+
+// Host image of the head region (P.head bytes), laid out as carve_instance lays it out.
+void fill_head(const pimqap_instance *inst, const pimqap_params *params, const Plan &P,
+               char *mirror);
+
+// Head upload + tail clear + setup kernels for one instance in `base` (P.total bytes) on
+// stream q.  The host image is kept in `keep` until the caller syncs q.
+pimqap_status stage_instance(const pimqap_instance *inst, const pimqap_params *params,
+                             const Plan &P, char *base, SolveDev *out, cudaStream_t q,
+                             std::vector<std::vector<char>> &keep);
+
+}  // namespace detail
+}  // namespace pimqap

@@ -192,6 +192,7 @@ extern "C" pimqap_status pimqap_solve_static(const pimqap_instance *inst,
         return fail(PIMQAP_ERR_ARG, "threads_per_block must be 0, 64, 128 or 256");
     if (p->cluster_size != 0 && p->cluster_size != 1 && p->cluster_size != 2 && p->cluster_size != 4)
         return fail(PIMQAP_ERR_ARG, "cluster_size must be 0, 1, 2 or 4");
+    if (p->auto_beta) return fail(PIMQAP_ERR_ARG, "automatic beta selection needs pimqap_solve");
 
     // Instance analysis without heap buffers: symmetry and the per-row force bound.
     const int32_t *F = inst->flow, *D = inst->dist;
@@ -324,7 +325,7 @@ extern "C" pimqap_status pimqap_solve_static(const pimqap_instance *inst,
     PQS_CUDA(cudaGetLastError());
 
     // Host set-up with fixed-size stack buffers: shuffle, beta ladder, rank slots per group.
-    const double beta0 = p->beta_max * 1.44269504089;
+    const double beta0 = p->beta_internal ? p->beta_max : p->beta_max * 1.44269504089;
     ShuffleEngine eng;
     eng.seed = p->seed;
     int32_t perm[PIMQAP_MAX_N];
@@ -391,10 +392,15 @@ extern "C" pimqap_status pimqap_solve_static(const pimqap_instance *inst,
     PQS_CUDA(cudaMemcpy(&sns, d.start_ns, 8, cudaMemcpyDeviceToHost));
     if (err) return fail(PIMQAP_ERR_DEVICE, "device check failed");
     int32_t *perm_dst = result->best_perm;
+    int64_t *energy_dst = result->final_energies;
     std::memset(result, 0, sizeof(*result));
     result->best_perm = perm_dst;
+    result->final_energies = energy_dst;
     if (perm_dst)
         PQS_CUDA(cudaMemcpy(perm_dst, d.best_phi + (size_t)sum.arg * n, (size_t)n * 4, cudaMemcpyDeviceToHost));
+    if (energy_dst) PQS_CUDA(cudaMemcpy(energy_dst, d.E, reps * 8, cudaMemcpyDeviceToHost));
+    result->beta_max_used = beta0;
+    result->beta_ratio_used = p->beta_ratio;
 #undef PQS_CUDA
     const auto wall1 = std::chrono::steady_clock::now();
     result->best_energy = std::min<int64_t>(sum.best, single);

@@ -44,7 +44,8 @@ class Params(C.Structure):
         ("beta_ratio", C.c_double), ("goal", C.c_int64), ("timeout_s", C.c_double),
         ("seed", C.c_uint64), ("force_bits", C.c_int32), ("device", C.c_int32),
         ("megaiters_per_launch", C.c_int32), ("threads_per_block", C.c_int32),
-        ("cluster_size", C.c_int32),
+        ("cluster_size", C.c_int32), ("beta_internal", C.c_int32), ("auto_beta", C.c_int32),
+        ("auto_lower", C.c_double), ("auto_higher", C.c_double),
     ]
 
 
@@ -56,6 +57,8 @@ class Result(C.Structure):
         ("device_ms", C.c_double), ("wall_ms", C.c_double), ("force_bits", C.c_int32),
         ("cluster_size", C.c_int32), ("stopped_by", C.c_int32),
         ("h2d_bytes", C.c_int64), ("d2h_bytes", C.c_int64),
+        ("final_energies", C.POINTER(C.c_int64)), ("beta_max_used", C.c_double),
+        ("beta_ratio_used", C.c_double),
     ]
 
 
@@ -94,6 +97,9 @@ def lib() -> C.CDLL:
     L.pimqap_solver_destroy.restype = None
     L.pimqap_batch_solve.argtypes = [C.POINTER(Instance), C.POINTER(Params), C.c_int32, C.POINTER(Result)]
     L.pimqap_batch_solve.restype = st
+    L.pimqap_auto_beta.argtypes = [C.POINTER(Instance), C.POINTER(Params), C.POINTER(C.c_double),
+                                   C.POINTER(C.c_double), C.c_void_p, C.POINTER(C.c_int64), C.c_void_p]
+    L.pimqap_auto_beta.restype = st
     L.pimqap_solve_static.argtypes = [C.POINTER(Instance), C.POINTER(Params), C.POINTER(Result)]
     L.pimqap_solve_static.restype = st
     L.pimqap_probe_smem_bandwidth.argtypes = [C.c_int32, C.POINTER(C.c_double)]
@@ -140,19 +146,42 @@ def read_problem(path: str, max_n: int = MAX_N):
     return F, D
 
 
-def _result_dict(r: Result, perm: Optional[np.ndarray]) -> dict:
-    d = {k: getattr(r, k) for k, _ in Result._fields_ if k != "best_perm"}
+def _result_dict(r: Result, perm: Optional[np.ndarray], energies: Optional[np.ndarray] = None) -> dict:
+    d = {k: getattr(r, k) for k, _ in Result._fields_ if k not in ("best_perm", "final_energies")}
     d["best_perm"] = perm
+    d["final_energies"] = energies
     return d
+
+
+def _new_result(n: int, replicas_total: int):
+    perm = np.zeros(n, np.int32)
+    energies = np.zeros(max(1, replicas_total), np.int64)
+    r = Result()
+    r.best_perm = perm.ctypes.data_as(C.POINTER(C.c_int32))
+    r.final_energies = energies.ctypes.data_as(C.POINTER(C.c_int64))
+    return r, perm, energies
 
 
 def solve(F: np.ndarray, D: np.ndarray, params: Params) -> dict:
     inst = _Inst(F, D)
-    perm = np.zeros(inst.F.shape[0], np.int32)
-    r = Result()
-    r.best_perm = perm.ctypes.data_as(C.POINTER(C.c_int32))
+    r, perm, energies = _new_result(inst.F.shape[0], params.groups * params.replicas)
     _check(lib().pimqap_solve(C.byref(inst.c), C.byref(params), C.byref(r)))
-    return _result_dict(r, perm)
+    return _result_dict(r, perm, energies)
+
+
+def auto_beta(F: np.ndarray, D: np.ndarray, params: Params) -> dict:
+    """The reference's automatic beta selection; returns beta0 (internal units), deltaBeta,
+    the 32 average energies and the best energy / permutation of the trials."""
+    inst = _Inst(F, D)
+    b0 = C.c_double(0)
+    db = C.c_double(0)
+    avg = np.zeros(32, np.float64)
+    best = C.c_int64(0)
+    perm = np.zeros(inst.F.shape[0], np.int32)
+    _check(lib().pimqap_auto_beta(C.byref(inst.c), C.byref(params), C.byref(b0), C.byref(db),
+                                  avg.ctypes.data, C.byref(best), perm.ctypes.data))
+    return dict(beta0=b0.value, delta_beta=db.value, avg_energy=avg, best_energy=best.value,
+                best_perm=perm)
 
 
 def solve_static(F: np.ndarray, D: np.ndarray, params: Params) -> dict:
@@ -172,11 +201,13 @@ def batch_solve(instances: Sequence, params: Sequence[Params]) -> List[dict]:
     insts = (Instance * count)(*[k.c for k in keep])
     ps = (Params * count)(*params)
     perms = [np.zeros(k.F.shape[0], np.int32) for k in keep]
+    energies = [np.zeros(max(1, p.groups * p.replicas), np.int64) for p in params]
     rs = (Result * count)()
-    for r, p in zip(rs, perms):
+    for r, p, e in zip(rs, perms, energies):
         r.best_perm = p.ctypes.data_as(C.POINTER(C.c_int32))
+        r.final_energies = e.ctypes.data_as(C.POINTER(C.c_int64))
     _check(lib().pimqap_batch_solve(insts, ps, count, rs))
-    return [_result_dict(r, p) for r, p in zip(rs, perms)]
+    return [_result_dict(r, p, e) for r, p, e in zip(rs, perms, energies)]
 
 
 def probe_smem_bandwidth(device: int = 0) -> float:
@@ -204,11 +235,9 @@ class Solver:
         return ms.value
 
     def result(self) -> dict:
-        perm = np.zeros(self.n, np.int32)
-        r = Result()
-        r.best_perm = perm.ctypes.data_as(C.POINTER(C.c_int32))
+        r, perm, energies = _new_result(self.n, self.params.groups * self.params.replicas)
         _check(lib().pimqap_solver_result(self.h, C.byref(r)))
-        return _result_dict(r, perm)
+        return _result_dict(r, perm, energies)
 
     def replica(self, t: int, l: int) -> dict:
         n = self.n

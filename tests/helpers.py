@@ -35,3 +35,50 @@ def compare_solver_to_oracle(solver, st, cap):
             if not np.array_equal(r["I"], st.I[t, l]):
                 bad.append(f"replica {t}/{l} force matrix differs")
     return bad
+
+
+MASK64 = (1 << 64) - 1
+
+
+def splitmix64(x):
+    x = (x + 0x9E3779B97F4A7C15) & MASK64
+    x = ((x ^ (x >> 30)) * 0xBF58476D1CE4E5B9) & MASK64
+    x = ((x ^ (x >> 27)) * 0x94D049BB133111EB) & MASK64
+    return x ^ (x >> 31)
+
+
+def oracle_auto_beta(oracle, F, D, *, T, R, spe, seed, cap, lower=0.1, higher=0.9):
+    """autoSelectParameters (CPU_PIM.cpp:366-476) restated on the oracle, with the solver's
+    trial seeding: trial (k, t) uses splitmix64(seed + 5k + t + 1)."""
+    steps, trials = 32, 5
+    sums = [0.0] * steps
+    denom = float(trials) * T * R
+    best = None
+    for i in range(steps):
+        for t in range(trials):
+            st = oracle.setup(D, F, T, R, spe, 2.0 ** (-30 + i), 1.0,
+                              splitmix64((seed + i * trials + t + 1) & MASK64), cap=cap)
+            oracle.run(st, D, F, 10)
+            oracle.track_exchange_all(st)
+            for g in range(T):
+                for l in range(R):
+                    sums[i] += float(st.E[g, l]) / denom
+            b = min(int(st.bestE.min()), st.single_best)
+            best = b if best is None else min(best, b)
+    i = steps - 1
+    minE, maxE, minEIndex = 1e30, -1e30, 0
+    for j in range(i):
+        if sums[j] < minE:
+            minE, minEIndex = sums[j], j
+        if j == 0:
+            maxE = sums[j]
+    minBeta = 0.0
+    for j in range(i):
+        if minBeta == 0 and ((j == minEIndex - 1 and j >= 1) or sums[j] < (maxE - minE) * higher + minE):
+            minBeta = 2.0 ** (-30 + j)
+        if j == i - 1 or (minBeta != 0 and (j == minEIndex or sums[j] < (maxE - minE) * lower + minE)):
+            if minBeta == 0:
+                minBeta = 2.0 ** -30
+            maxBeta = 2.0 ** (-30 + j + 2)
+            return maxBeta, (maxBeta / minBeta) ** (1.0 / R), sums, best
+    raise AssertionError("no range")

@@ -41,6 +41,11 @@ def mixed_batch(gpu):
     insts.append(instances.grid256(901))
     params.append(gpu.default_params(replicas=2, groups=1, sweeps_per_exchange=1, beta_max=0.0015,
                                      beta_ratio=1.5, seed=78, max_megaiters=2))
+    # int64 force matrices that need a 2-CTA and a 4-CTA cluster
+    for n, seed in ((180, 903), (250, 904)):
+        insts.append(instances.Instance(n, rng.integers(0, 2_000_000, (n, n)), rng.integers(0, 5000, (n, n))))
+        params.append(gpu.default_params(replicas=2, groups=1, sweeps_per_exchange=1, beta_max=1e-9,
+                                         beta_ratio=1.5, seed=seed, max_megaiters=2))
     goal_inst = instances.uniform(24, 902)
     probe = gpu.solve(goal_inst.F, goal_inst.D, gpu.default_params(
         replicas=6, groups=2, sweeps_per_exchange=1, beta_max=0.05, beta_ratio=1.3, seed=79,
