@@ -108,6 +108,8 @@ typedef struct pimqap_result {
                                    currentE of every replica at the end (CPU_PIM.cpp:54) */
     double beta_max_used;       /* beta0 of the run in internal units (after automatic mode) */
     double beta_ratio_used;     /* deltaBeta of the run */
+    double admit_ms;            /* serving: submit -> admitted to the device (host clock) */
+    double latency_ms;          /* serving: submit -> result available (host clock) */
 } pimqap_result;
 
 /* ---------------------------------------------------------------- instance I/O */
@@ -183,6 +185,58 @@ void pimqap_solver_destroy(pimqap_solver *s);
    Each result equals what pimqap_solve returns for that instance alone. */
 pimqap_status pimqap_batch_solve(const pimqap_instance *insts, const pimqap_params *params,
                                  int32_t count, pimqap_result *results);
+
+/* ---------------------------------------------------------------- serving */
+
+/* Continuous-batching solve service (no reference counterpart).  Persistent launches stay
+   resident on the device, one per class of replica shape; a server thread admits submitted
+   requests in arrival order as instance slots and device memory (the budget) free up, and
+   the running launches pick them up between epochs, so new work overlaps work in flight.
+   Each result equals what pimqap_solve returns for that request alone.  The handle is
+   internally locked; submit / poll / wait may be called from several threads. */
+typedef struct pimqap_server pimqap_server;
+
+typedef struct pimqap_server_config {
+    int32_t device;
+    int64_t memory_budget_bytes;   /* device memory for admitted requests (0 = half of free) */
+    int32_t slots_per_class;       /* requests resident at once per class (0 = 256) */
+    double heartbeat_timeout_s;    /* device workers stop if the server thread stalls this long
+                                      (0 = 10 s) */
+    /* Representative requests for the autotuner, which sizes the classes and their share of
+       the SMs from them (NULL / 0 = a built-in mix of n = 32..256, int32 and int64). */
+    const pimqap_instance *sample;
+    const pimqap_params *sample_params;
+    int32_t sample_count;
+} pimqap_server_config;
+
+typedef struct pimqap_server_stats {
+    int64_t submitted, admitted, completed, pending;
+    int64_t memory_in_use, memory_budget;
+    int32_t classes;
+    int32_t error_word;            /* device error bits of any class launch (0 = healthy) */
+} pimqap_server_stats;
+
+pimqap_status pimqap_server_create(const pimqap_server_config *config, pimqap_server **out);
+/* Queues a request (the instance is copied; the caller may free it on return).  *ticket
+   identifies it.  PIMQAP_ERR_BUSY when it can never fit the memory budget or no class
+   fits its shape. */
+pimqap_status pimqap_server_submit(pimqap_server *s, const pimqap_instance *inst,
+                                   const pimqap_params *params, int64_t *ticket);
+/* PIMQAP_ERR_NOT_READY while the request is pending or running; then fills result (and its
+   best_perm / final_energies arrays when given) and forgets the ticket. */
+pimqap_status pimqap_server_poll(pimqap_server *s, int64_t ticket, pimqap_result *result);
+/* Like poll, waiting up to timeout_s (< 0: no limit). */
+pimqap_status pimqap_server_wait(pimqap_server *s, int64_t ticket, double timeout_s,
+                                 pimqap_result *result);
+pimqap_status pimqap_server_stats_get(pimqap_server *s, pimqap_server_stats *stats);
+/* Waits for admitted requests to finish, stops the launches and frees the device memory;
+   pending requests that were never admitted are dropped. */
+void pimqap_server_destroy(pimqap_server *s);
+
+/* Host-side fault injection for tests: stall != 0 stops the server thread's heartbeat, so
+   the device workers' idle waits run out (after heartbeat_timeout_s) and they stop with the
+   error word set; 0 resumes it.  No device fault is involved. */
+void pimqap_server_debug_stall_heartbeat(pimqap_server *s, int32_t stall);
 
 /* ---------------------------------------------------------------- automatic beta */
 

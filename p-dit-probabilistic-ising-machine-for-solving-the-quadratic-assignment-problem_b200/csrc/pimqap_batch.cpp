@@ -228,6 +228,7 @@ pimqap_status ClassRun::prepare(const pimqap_instance *insts, const pimqap_param
     B.count = m; B.q_items = d_items; B.q_seq = d_seq; B.q_head = d_head; B.q_tail = d_tail;
     B.qmask = qcap - 1; B.active = d_active; B.error = d_error; B.start_ns = d_start;
     B.shutdown = d_shutdown;
+    B.serving = 0;
     B.worker_threads = c.worker_threads; B.workers = c.workers; B.slice_bytes = (unsigned)c.slice;
     return PIMQAP_OK;
 }

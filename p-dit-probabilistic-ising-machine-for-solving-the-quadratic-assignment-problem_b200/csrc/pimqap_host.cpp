@@ -107,10 +107,6 @@ std::vector<int32_t> initial_perms(int n, int T, uint64_t seed) {
 
 // ------------------------------------------------------------------ instance analysis
 
-struct InstanceInfo {
-    bool symmetric = false;
-    int bits_needed = 32;   // 32, 64, or 0 when even int64 is not provably safe
-};
 
 // Force-matrix width: |I[i][a]| <= sum_j |D_ij||F_a,phi(j)| + |D_ji||F_phi(j),a| is bounded by
 // the rearrangement inequality (both rows sorted descending); a delta adds at most
@@ -269,9 +265,9 @@ pimqap_status open_device(int device, int *maxsm) {
 }
 
 pimqap_status plan_instance(const pimqap_instance *inst, const pimqap_params *params, size_t maxsm,
-                            int want_cluster, Plan *out) {
+                            int want_cluster, Plan *out, const InstanceInfo *known) {
     const int n = inst->n;
-    const InstanceInfo info = analyse(n, inst->flow, inst->dist);
+    const InstanceInfo info = known ? *known : analyse(n, inst->flow, inst->dist);
     if (info.bits_needed == 0 && params->force_bits == 0)
         return fail(PIMQAP_ERR_RANGE, "instance values can overflow int64 force matrices");
     Plan P;

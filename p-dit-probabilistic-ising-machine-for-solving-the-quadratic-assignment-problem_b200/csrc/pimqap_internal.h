@@ -18,7 +18,8 @@ constexpr int64_t kNoBest = 2147483647;  // the reference's INT_MAX sentinel
 enum : int32_t {
     kErrBadPerm = 1,      // a permutation loaded from global memory is not a bijection
     kErrShape = 2,        // launch shape does not match the solve
-    kErrTimeout = 4,      // a bounded wait for a peer CTA's data gave up
+    kErrTimeout = 4,      // a bounded wait for a peer CTA's data or a queue item gave up
+    kErrHostLost = 8,     // serving: the host's heartbeat stopped
 };
 
 // Everything one solve (one instance, T groups x R replicas) keeps in device memory.
@@ -52,6 +53,54 @@ struct SolveDev {
     int32_t *error;            // [1]       kErr* bits
 };
 
+// Compact per-instance result of a batch.
+struct BatchResultDev {
+    long long best, arg;
+    unsigned long long accepts;
+    long long single_best, target_epoch;
+    unsigned long long target_ns;
+    int32_t epoch, stop_epoch, error, pad;
+};
+
+// A served request as the host describes it (mapped memory); the device copies it in.
+struct ServeDesc {
+    SolveDev dev;                  // pointers into the device arena
+    long long max_megaiters;
+    unsigned long long head_bytes, tail_bytes;
+    int32_t sym, bits;
+};
+
+// Host <-> running-kernel link of a serving launch.  Everything the host writes or reads lives
+// in mapped pinned host memory, so the host serves without a single CUDA call (its streams
+// could queue behind the resident launches); the claim counters live in device memory.
+struct ServeLink {
+    volatile unsigned long long *inbox;       // [inbox_mask+1] (slot << 32) | staging buffer
+    volatile unsigned long long *inbox_tail;  // [1] entries the host has published
+    unsigned long long *inbox_head;           // [1] entries the device has claimed (device memory)
+    unsigned int inbox_mask;
+    const volatile ServeDesc *desc;           // [slots]
+    const unsigned char *staging;             // staging buffers of head images, `staging_stride` apart
+    unsigned long long staging_stride;
+    volatile int32_t *staging_busy;           // [buffers] the device clears it once copied
+    volatile BatchResultDev *results;         // [slots]
+    volatile int32_t *result_perm;            // [slots][256]
+    volatile long long *result_energy;        // [slots][energy_stride]
+    int energy_stride;
+    volatile unsigned long long *done;        // [done_mask+1] slot of each finished instance
+    volatile unsigned long long *done_seq;    // [done_mask+1] ring index + 1 once `done` is written
+    unsigned long long *done_tail;            // [1] device counter (device memory)
+    unsigned int done_mask;
+    volatile unsigned long long *heartbeat;   // [1] the host increments it while it serves
+    unsigned long long heartbeat_limit_ns;    // idle workers exit when it stalls this long
+    volatile int32_t *error_host;             // [1] copy of the error word for the host
+    SolveDev *inst_rw;                        // writable view of the device descriptor table
+    int32_t *sym_rw;
+    int64_t *maxm_rw;
+};
+
+// Item flag of a serving launch: replica set-up (force matrix, energy) instead of an epoch.
+constexpr unsigned int kSetupItem = 0x80000000u;
+
 // A batch of independent solves run by one persistent launch.  Work items are replica-epochs
 // (instance k, replica rep) in a ring buffer; the last replica of an instance to finish an
 // epoch runs the tracking / exchange of all its groups and enqueues the next epoch.
@@ -67,9 +116,11 @@ struct BatchDev {
     unsigned long long *q_tail;      // [1] next ticket to push
     unsigned int qmask;
     int32_t *active;                 // [1] instances still running
-    int32_t *shutdown;               // [1] nonzero: workers exit once no instance is active
+    volatile int32_t *shutdown;      // [1] nonzero: workers exit once no instance is active
     int32_t *error;                  // [1] kErr* bits
     unsigned long long *start_ns;    // [1] %globaltimer when the launch began
+    int serving;                     // nonzero: `link` is live (instances arrive while running)
+    ServeLink link;
     int worker_threads;              // threads of one replica worker (a multiple of 32)
     int workers;                     // workers per CTA (<= 8)
     unsigned int slice_bytes;        // shared memory of one worker
@@ -84,15 +135,6 @@ cudaError_t launch_batch(const BatchDev &b, int bits, int cl, int grid, cudaStre
 // Residency of the batch kernel for this shape: CTAs per SM for cl == 1, else resident
 // clusters on the device.
 cudaError_t batch_occupancy(int bits, int cl, int threads, size_t smem, int *out);
-
-// Compact per-instance result of a batch.
-struct BatchResultDev {
-    long long best, arg;
-    unsigned long long accepts;
-    long long single_best, target_epoch;
-    unsigned long long target_ns;
-    int32_t epoch, stop_epoch, error, pad;
-};
 
 // Gathers every instance's result, best permutation (perms + perm_off[k], n entries) and
 // final replica energies (energies + energy_off[k], T*R entries).

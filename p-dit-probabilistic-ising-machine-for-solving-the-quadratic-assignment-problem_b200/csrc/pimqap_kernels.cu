@@ -757,26 +757,6 @@ __global__ void __launch_bounds__(256) epoch_kernel(SolveDev s) {
 constexpr unsigned long long kQueueWaitNs = 30000000000ull;   // 30 s without any progress
 constexpr unsigned long long kDoneItem = ~0ull;
 
-// Next work item, or kDoneItem once no instance is running.  The wait for a ticket whose item
-// is not pushed yet is bounded: the items come from other workers finishing epochs.
-__device__ unsigned long long queue_pop(const BatchDev &B) {
-    const unsigned long long idx = atomicAdd(B.q_head, 1ull);
-    const unsigned slot = (unsigned)idx & B.qmask;
-    const unsigned long long t0 = globaltimer_ns();
-    for (;;) {
-        if (*((volatile unsigned long long *)B.q_seq + slot) == idx + 1) {
-            __threadfence();
-            return *((volatile unsigned long long *)B.q_items + slot);
-        }
-        if (*(volatile int32_t *)B.active == 0 && *(volatile int32_t *)B.shutdown != 0) return kDoneItem;
-        if (globaltimer_ns() - t0 > kQueueWaitNs) {
-            atomicOr(B.error, kErrTimeout);
-            return kDoneItem;
-        }
-        __nanosleep(200);
-    }
-}
-
 // Enqueues every replica of instance k for its next epoch.
 __device__ void queue_push_instance(const BatchDev &B, int k, int replicas) {
     const unsigned long long base = atomicAdd(B.q_tail, (unsigned long long)replicas);
@@ -785,6 +765,238 @@ __device__ void queue_push_instance(const BatchDev &B, int k, int replicas) {
     __threadfence();
     for (int q = 0; q < replicas; ++q)
         *((volatile unsigned long long *)B.q_seq + ((unsigned)(base + q) & B.qmask)) = base + q + 1;
+}
+
+constexpr unsigned long long kAdmitItem = 1ull << 63;   // a serving admission, not a queue item
+constexpr unsigned long long kNoTicket = ~0ull;
+
+__device__ void set_error(const BatchDev &B, int32_t bits) {
+    const int32_t old = atomicOr(B.error, bits);
+    if (B.serving) {
+        *B.link.error_host = old | bits;
+        __threadfence_system();
+    }
+}
+
+// Serving: claims one request the host has published (returns its inbox entry, or 0).
+__device__ unsigned long long inbox_claim(const BatchDev &B) {
+    const unsigned long long h = *(volatile unsigned long long *)B.link.inbox_head;
+    if (h >= *B.link.inbox_tail) return 0;
+    if (atomicCAS(B.link.inbox_head, h, h + 1) != h) return 0;
+    __threadfence_system();
+    return B.link.inbox[h & B.link.inbox_mask] | kAdmitItem;
+}
+
+// Serving: reports a finished instance to the host.
+__device__ void report_done(const BatchDev &B, int k) {
+    const unsigned long long idx = atomicAdd(B.link.done_tail, 1ull);
+    B.link.done[idx & B.link.done_mask] = (unsigned long long)k;
+    __threadfence_system();
+    B.link.done_seq[idx & B.link.done_mask] = idx + 1;
+    __threadfence_system();
+}
+
+// Serving: the finished instance's result, best permutation and final energies, written into
+// its mapped result slot (one thread).
+__device__ void publish_result(const BatchDev &B, int k) {
+    const SolveDev &s = B.inst[k];
+    const int reps = s.T * s.R;
+    long long best = 0x7fffffffffffffffll, arg = 0;
+    unsigned long long acc = 0;
+    for (int r = 0; r < reps; ++r) {
+        const long long v = __ldcg((const long long *)s.bestE + r);
+        if (v < best) { best = v; arg = r; }
+        acc += __ldcg(s.accepts + r);
+    }
+    volatile BatchResultDev &o = B.link.results[k];
+    o.best = best;
+    o.arg = arg;
+    o.accepts = acc;
+    o.single_best = __ldcg((const long long *)s.single_best);
+    o.target_epoch = __ldcg((const long long *)s.target_epoch);
+    o.target_ns = __ldcg(s.target_ns);
+    o.epoch = __ldcg(s.epoch);
+    o.stop_epoch = __ldcg(s.stop_epoch);
+    o.error = __ldcg(s.error);
+    for (int q = 0; q < s.n; ++q) B.link.result_perm[(size_t)k * kMaxN + q] = __ldcg(s.best_phi + arg * s.n + q);
+    for (int r = 0; r < reps && r < B.link.energy_stride; ++r)
+        B.link.result_energy[(size_t)k * B.link.energy_stride + r] = __ldcg((const long long *)s.E + r);
+    __threadfence_system();
+}
+
+// Next item for a worker that holds queue ticket `ticket` (taken when it holds none): the
+// ticket's item, a serving admission (the ticket is kept), or kDoneItem once no instance is
+// running and shutdown is set.  A batch's wait is bounded (its items come from workers that
+// are finishing epochs); a serving launch waits while the host's heartbeat advances.
+__device__ unsigned long long queue_next(const BatchDev &B, unsigned long long &ticket) {
+    if (ticket == kNoTicket) ticket = atomicAdd(B.q_head, 1ull);
+    const unsigned slot = (unsigned)ticket & B.qmask;
+    unsigned long long t0 = globaltimer_ns();
+    unsigned long long beat = B.serving ? *B.link.heartbeat : 0;
+    for (;;) {
+        if (*((volatile unsigned long long *)B.q_seq + slot) == ticket + 1) {
+            __threadfence();
+            ticket = kNoTicket;
+            return *((volatile unsigned long long *)B.q_items + slot);
+        }
+        const int32_t sd = *B.shutdown;   // 1: drain, then leave; 2: leave now
+        if (sd == 2 || (sd != 0 && *(volatile int32_t *)B.active == 0)) return kDoneItem;
+        if (B.serving) {
+            const unsigned long long adm = inbox_claim(B);
+            if (adm) return adm;
+            const unsigned long long now_beat = *B.link.heartbeat;
+            const unsigned long long now = globaltimer_ns();
+            if (now_beat != beat) {
+                beat = now_beat;
+                t0 = now;
+            } else if (now - t0 > B.link.heartbeat_limit_ns) {
+                set_error(B, kErrHostLost);
+                return kDoneItem;
+            }
+            __nanosleep(1000);
+        } else {
+            if (globaltimer_ns() - t0 > kQueueWaitNs) {
+                set_error(B, kErrTimeout);
+                return kDoneItem;
+            }
+            __nanosleep(200);
+        }
+    }
+}
+
+// Serving admission by a whole worker: the descriptor into the device table, the head image
+// from mapped memory into the instance's device head, the tail cleared; then one set-up item
+// per replica is queued.
+__device__ void serve_admit(const BatchDev &B, unsigned long long entry, const Grp &G) {
+    const int slot = (int)((entry >> 32) & 0x7fffffffull);
+    const int stg = (int)(entry & 0xffffffffull);
+    const volatile ServeDesc &d = B.link.desc[slot];
+    char *head = (char *)d.dev.D;            // the head region starts with D (carve order)
+    char *tail = (char *)d.dev.I;            // the tail region starts with I
+    const unsigned long long hb = d.head_bytes, tb = d.tail_bytes;
+    const int4 *src = reinterpret_cast<const int4 *>(B.link.staging + (size_t)stg * B.link.staging_stride);
+    for (unsigned long long q = G.tid; q < hb / 16; q += G.BT) reinterpret_cast<int4 *>(head)[q] = src[q];
+    const int4 z = make_int4(0, 0, 0, 0);
+    for (unsigned long long q = G.tid; q < tb / 16; q += G.BT) reinterpret_cast<int4 *>(tail)[q] = z;
+    if (G.tid == 0) {
+        const volatile unsigned long long *dw = reinterpret_cast<const volatile unsigned long long *>(&d.dev);
+        unsigned long long *iw = reinterpret_cast<unsigned long long *>(B.link.inst_rw + slot);
+        for (int q = 0; q < (int)(sizeof(SolveDev) / 8); ++q) iw[q] = dw[q];
+        B.link.sym_rw[slot] = d.sym;
+        B.link.maxm_rw[slot] = d.max_megaiters;
+    }
+    __threadfence();
+    G.sync();
+    if (G.tid == 0) {
+        B.link.staging_busy[stg] = 0;         // the host may reuse the staging buffer
+        __threadfence_system();
+        const SolveDev &s = B.inst[slot];
+        atomicAdd(B.active, 1);
+        const int replicas = s.T * s.R;
+        const unsigned long long base = atomicAdd(B.q_tail, (unsigned long long)replicas);
+        for (int q = 0; q < replicas; ++q)
+            B.q_items[(unsigned)(base + q) & B.qmask] =
+                ((unsigned long long)slot << 32) | (unsigned)q | (unsigned long long)kSetupItem;
+        __threadfence();
+        for (int q = 0; q < replicas; ++q)
+            *((volatile unsigned long long *)B.q_seq + ((unsigned)(base + q) & B.qmask)) = base + q + 1;
+    }
+    G.sync();
+}
+
+// setup() of one served replica on the device (CPU_PIM.cpp:164-192): force matrix from its
+// permutation, energy = -1/2 sum_i I[i][phi(i)], best energy unset.  `sphi` is a shared
+// scratch of n ints, `sred` of one long long per warp.
+template <class IT>
+__device__ void replica_setup(const SolveDev &s, int rep, const Grp &G, int32_t *sphi, long long *sred) {
+    const int n = s.n, ldg = s.ldg, ldm = s.ldm;
+    const int32_t *phi = s.phi + (size_t)rep * n;
+    for (int q = G.tid; q < n; q += G.BT) {
+        const int p = __ldcg(phi + q);
+        sphi[q] = p;
+        s.best_phi[(size_t)rep * n + q] = p;
+    }
+    G.sync();
+    IT *I = reinterpret_cast<IT *>(s.I) + (size_t)rep * n * ldg;
+    for (int idx = G.tid; idx < n * ldg; idx += G.BT) {
+        const int i = idx / ldg, a = idx - i * ldg;
+        long long acc = 0;
+        if (a < n) {
+            const int32_t *Di = s.D + (size_t)i * ldm, *DTi = s.DT + (size_t)i * ldm;
+            const int32_t *Fa = s.F + (size_t)a * ldm, *FTa = s.FT + (size_t)a * ldm;
+            for (int j = 0; j < n; ++j) {
+                const int pj = sphi[j];
+                acc += (long long)__ldcg(Di + j) * __ldcg(Fa + pj) + (long long)__ldcg(DTi + j) * __ldcg(FTa + pj);
+            }
+        }
+        I[(size_t)i * ldg + a] = (IT)(-acc);
+    }
+    __threadfence();
+    G.sync();
+    long long e = 0;
+    for (int i = G.tid; i < n; i += G.BT) e += (long long)__ldcg(I + (size_t)i * ldg + sphi[i]);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) e += __shfl_xor_sync(0xffffffffu, e, o);
+    if (G.lane == 0) sred[G.warp] = e;
+    G.sync();
+    if (G.tid == 0) {
+        long long t = 0;
+        for (int w = 0; w < G.nwarps; ++w) t += sred[w];
+        s.E[rep] = -t / 2;
+        s.bestE[rep] = kNoBest;
+        s.accepts[rep] = 0ull;
+    }
+    __threadfence();
+    G.sync();
+}
+
+// The last replica of an instance to finish its set-up: mega-iteration 0's tracking, then the
+// first epoch, or the end when nothing is to run.
+__device__ void setup_done(const BatchDev &B, int k) {
+    const SolveDev &s = B.inst[k];
+    const int replicas = s.T * s.R;
+    const unsigned prev = atomicAdd(B.finish_inst + k, 1u);
+    if (prev != (unsigned)replicas - 1u) return;
+    __threadfence();
+    B.finish_inst[k] = 0u;
+    *s.start_ns = globaltimer_ns();
+    for (int g = 0; g < s.T; ++g) track_exchange(s, g, 0);
+    __threadfence();
+    const int stop = *(volatile int32_t *)s.stop_epoch;
+    if (0 < stop && 0 < B.max_megaiters[k]) {
+        queue_push_instance(B, k, replicas);
+    } else {
+        publish_result(B, k);
+        report_done(B, k);
+        __threadfence();
+        atomicSub(B.active, 1);
+    }
+}
+
+// After replica-epoch `e` of instance k: the last replica to finish runs every group's
+// tracking + exchange (lock step across groups, as one launch per epoch gives), then the next
+// epoch or the end of the instance.
+__device__ void epoch_done(const BatchDev &B, int k, int e) {
+    const SolveDev &s = B.inst[k];
+    const int replicas = s.T * s.R;
+    const unsigned prev = atomicAdd(B.finish_inst + k, 1u);
+    if (prev != (unsigned)replicas - 1u) return;
+    __threadfence();
+    for (int g = 0; g < s.T; ++g) track_exchange(s, g, e + 1);
+    B.finish_inst[k] = 0u;
+    for (int g = 0; g < s.T; ++g) s.epoch[g] = e + 1;
+    __threadfence();
+    const int stop = *(volatile int32_t *)s.stop_epoch;
+    if (e + 1 < stop && (int64_t)(e + 1) < B.max_megaiters[k]) {
+        queue_push_instance(B, k, replicas);
+    } else {
+        __threadfence();
+        if (B.serving) {
+            publish_result(B, k);
+            report_done(B, k);
+        }
+        atomicSub(B.active, 1);
+    }
 }
 
 size_t batch_slice_bytes(int n, int bits) {
@@ -804,40 +1016,32 @@ __global__ void __launch_bounds__(256) batch_kernel(BatchDev B) {
     unsigned char *slice = smem + (size_t)w * B.slice_bytes;
     volatile unsigned long long *hdr = reinterpret_cast<unsigned long long *>(slice);
     unsigned char *work = slice + 16;
+    unsigned long long ticket = kNoTicket;   // held by G.tid == 0
     if (blockIdx.x == 0 && threadIdx.x == 0) *B.start_ns = globaltimer_ns();
     for (;;) {
-        if (G.tid == 0) *hdr = queue_pop(B);
+        if (G.tid == 0) *hdr = queue_next(B, ticket);
         G.sync();
         const unsigned long long item = *hdr;
         G.sync();
         if (item == kDoneItem) break;
-        const int k = (int)(item >> 32), rep = (int)(item & 0xffffffffull);
+        if (item & kAdmitItem) {
+            serve_admit(B, item, G);
+            continue;
+        }
+        const int k = (int)(item >> 32);
+        const int rep = (int)(item & 0x7fffffffull);
         const SolveDev &s = B.inst[k];
+        if (item & kSetupItem) {
+            replica_setup<IT>(s, rep, G, reinterpret_cast<int32_t *>(work),
+                              reinterpret_cast<long long *>(work + 16 * kMaxN));
+            if (G.tid == 0) setup_done(B, k);
+            continue;
+        }
         const int e = *((volatile int32_t *)s.epoch);
         if (B.sym[k]) replica_epoch<IT, 1, true>(s, rep, 0, e, G, work);
         else replica_epoch<IT, 1, false>(s, rep, 0, e, G, work);
         G.sync();
-        if (G.tid == 0) {
-            const int replicas = s.T * s.R;
-            const unsigned prev = atomicAdd(B.finish_inst + k, 1u);
-            if (prev == (unsigned)replicas - 1u) {
-                // every replica of the instance finished epoch e: all groups' tracking and
-                // exchange (lock step across groups, as one launch per epoch gives), then the
-                // next epoch or the end of the instance
-                __threadfence();
-                for (int g = 0; g < s.T; ++g) track_exchange(s, g, e + 1);
-                B.finish_inst[k] = 0u;
-                for (int g = 0; g < s.T; ++g) s.epoch[g] = e + 1;
-                __threadfence();
-                const int stop = *(volatile int32_t *)s.stop_epoch;
-                if (e + 1 < stop && (int64_t)(e + 1) < B.max_megaiters[k]) {
-                    queue_push_instance(B, k, replicas);
-                } else {
-                    __threadfence();
-                    atomicSub(B.active, 1);
-                }
-            }
-        }
+        if (G.tid == 0) epoch_done(B, k, e);
     }
 }
 
@@ -852,46 +1056,43 @@ __global__ void __launch_bounds__(256) batch_cluster_kernel(BatchDev B) {
     unsigned char *work = smem + 16;
     const Grp G{(int)threadIdx.x, (int)blockDim.x, (int)(threadIdx.x & 31), (int)(threadIdx.x >> 5),
                 (int)(blockDim.x >> 5), 0};
+    unsigned long long ticket = kNoTicket;   // held by rank 0, thread 0
     if (blockIdx.x == 0 && threadIdx.x == 0) *B.start_ns = globaltimer_ns();
     cluster_barrier<CL>();
     for (;;) {
         if (rank == 0 && threadIdx.x == 0) {
-            const unsigned long long item = queue_pop(B);
+            const unsigned long long item = queue_next(B, ticket);
 #pragma unroll
             for (int r = 0; r < CL; ++r) *cluster.map_shared_rank(hdr, r) = item;
         }
         cluster_barrier<CL>();
         const unsigned long long item = *(volatile unsigned long long *)hdr;
         if (item == kDoneItem) break;
-        const int k = (int)(item >> 32), rep = (int)(item & 0xffffffffull);
-        const SolveDev &s = B.inst[k];
-        const int e = *((volatile int32_t *)s.epoch);
-        bool ok;
-        if (B.sym[k]) ok = replica_epoch<IT, CL, true>(s, rep, rank, e, G, work);
-        else ok = replica_epoch<IT, CL, false>(s, rep, rank, e, G, work);
-        __syncthreads();
-        if (!ok) {
-            if (threadIdx.x == 0) atomicOr(B.error, kErrTimeout);
-        } else if (rank == 0 && threadIdx.x == 0) {
-            const int replicas = s.T * s.R;
-            const unsigned prev = atomicAdd(B.finish_inst + k, 1u);
-            if (prev == (unsigned)replicas - 1u) {
-                __threadfence();
-                for (int g = 0; g < s.T; ++g) track_exchange(s, g, e + 1);
-                B.finish_inst[k] = 0u;
-                for (int g = 0; g < s.T; ++g) s.epoch[g] = e + 1;
-                __threadfence();
-                const int stop = *(volatile int32_t *)s.stop_epoch;
-                if (e + 1 < stop && (int64_t)(e + 1) < B.max_megaiters[k]) {
-                    queue_push_instance(B, k, replicas);
-                } else {
-                    __threadfence();
-                    atomicSub(B.active, 1);
-                }
+        if (item & kAdmitItem) {
+            if (rank == 0) serve_admit(B, item, G);
+        } else if (item & kSetupItem) {
+            const int k = (int)(item >> 32);
+            if (rank == 0) {
+                replica_setup<IT>(B.inst[k], (int)(item & 0x7fffffffull), G, reinterpret_cast<int32_t *>(work),
+                                  reinterpret_cast<long long *>(work + 16 * kMaxN));
+                if (threadIdx.x == 0) setup_done(B, k);
+            }
+        } else {
+            const int k = (int)(item >> 32), rep = (int)(item & 0x7fffffffull);
+            const SolveDev &s = B.inst[k];
+            const int e = *((volatile int32_t *)s.epoch);
+            bool ok;
+            if (B.sym[k]) ok = replica_epoch<IT, CL, true>(s, rep, rank, e, G, work);
+            else ok = replica_epoch<IT, CL, false>(s, rep, rank, e, G, work);
+            __syncthreads();
+            if (!ok) {
+                if (threadIdx.x == 0) set_error(B, kErrTimeout);
+            } else if (rank == 0 && threadIdx.x == 0) {
+                epoch_done(B, k, e);
             }
         }
-        // the header is rewritten only after every rank has read it (the epoch ends with a
-        // cluster barrier); this barrier also orders the next pop after rank 0's report
+        // the header is rewritten only after every rank has read it; this barrier also orders
+        // the next pop after rank 0's report
         cluster_barrier<CL>();
     }
     cluster_barrier<CL>();

@@ -54,13 +54,21 @@ struct Plan {
     int64_t h2d_bytes = 0;
 };
 
+// Symmetry of D and F, and the force-matrix width a bound on |I| and the deltas allows
+// (32, 64, or 0 when not even int64 is provably safe).
+struct InstanceInfo {
+    bool symmetric = false;
+    int bits_needed = 32;
+};
+InstanceInfo analyse(int n, const int32_t *F, const int32_t *D);
+
 // Makes `device` current, checks it is an sm_100 part and prepares the kernels.
 pimqap_status open_device(int device, int *maxsm);
 
 // Force-matrix width, symmetry, launch shape (threads; the smallest cluster whose row share
 // of the force matrix fits one CTA, or want_cluster), strides and device footprint.
 pimqap_status plan_instance(const pimqap_instance *inst, const pimqap_params *params, size_t maxsm,
-                            int want_cluster, Plan *out);
+                            int want_cluster, Plan *out, const InstanceInfo *known = nullptr);
 
 // Device pointers of one instance carved from its head and tail regions.
 void carve_instance(const Plan &P, char *head, char *tail, SolveDev *out);

@@ -58,8 +58,20 @@ class Result(C.Structure):
         ("cluster_size", C.c_int32), ("stopped_by", C.c_int32),
         ("h2d_bytes", C.c_int64), ("d2h_bytes", C.c_int64),
         ("final_energies", C.POINTER(C.c_int64)), ("beta_max_used", C.c_double),
-        ("beta_ratio_used", C.c_double),
+        ("beta_ratio_used", C.c_double), ("admit_ms", C.c_double), ("latency_ms", C.c_double),
     ]
+
+
+class ServerConfig(C.Structure):
+    _fields_ = [("device", C.c_int32), ("memory_budget_bytes", C.c_int64), ("slots_per_class", C.c_int32),
+                ("heartbeat_timeout_s", C.c_double), ("sample", C.POINTER(Instance)),
+                ("sample_params", C.POINTER(Params)), ("sample_count", C.c_int32)]
+
+
+class ServerStats(C.Structure):
+    _fields_ = [("submitted", C.c_int64), ("admitted", C.c_int64), ("completed", C.c_int64),
+                ("pending", C.c_int64), ("memory_in_use", C.c_int64), ("memory_budget", C.c_int64),
+                ("classes", C.c_int32), ("error_word", C.c_int32)]
 
 
 _lib = None
@@ -97,6 +109,20 @@ def lib() -> C.CDLL:
     L.pimqap_solver_destroy.restype = None
     L.pimqap_batch_solve.argtypes = [C.POINTER(Instance), C.POINTER(Params), C.c_int32, C.POINTER(Result)]
     L.pimqap_batch_solve.restype = st
+    L.pimqap_server_create.argtypes = [C.POINTER(ServerConfig), C.POINTER(C.c_void_p)]
+    L.pimqap_server_create.restype = st
+    L.pimqap_server_submit.argtypes = [C.c_void_p, C.POINTER(Instance), C.POINTER(Params), C.POINTER(C.c_int64)]
+    L.pimqap_server_submit.restype = st
+    L.pimqap_server_poll.argtypes = [C.c_void_p, C.c_int64, C.POINTER(Result)]
+    L.pimqap_server_poll.restype = st
+    L.pimqap_server_wait.argtypes = [C.c_void_p, C.c_int64, C.c_double, C.POINTER(Result)]
+    L.pimqap_server_wait.restype = st
+    L.pimqap_server_stats_get.argtypes = [C.c_void_p, C.POINTER(ServerStats)]
+    L.pimqap_server_stats_get.restype = st
+    L.pimqap_server_destroy.argtypes = [C.c_void_p]
+    L.pimqap_server_destroy.restype = None
+    L.pimqap_server_debug_stall_heartbeat.argtypes = [C.c_void_p, C.c_int32]
+    L.pimqap_server_debug_stall_heartbeat.restype = None
     L.pimqap_auto_beta.argtypes = [C.POINTER(Instance), C.POINTER(Params), C.POINTER(C.c_double),
                                    C.POINTER(C.c_double), C.c_void_p, C.POINTER(C.c_int64), C.c_void_p]
     L.pimqap_auto_beta.restype = st
@@ -267,6 +293,79 @@ class Solver:
             self.close()
         except Exception:
             pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+
+class Server:
+    """Continuous-batching solve service: submit() requests at any time, wait() / poll() for
+    their results.  sample: optional list of (F, D, Params) representative of the expected
+    requests, from which the autotuner sizes the resident launches."""
+
+    def __init__(self, device: int = 0, memory_budget: int = 0, slots_per_class: int = 0,
+                 heartbeat_timeout: float = 0.0, sample=None):
+        cfg = ServerConfig()
+        cfg.device = device
+        cfg.memory_budget_bytes = memory_budget
+        cfg.slots_per_class = slots_per_class
+        cfg.heartbeat_timeout_s = heartbeat_timeout
+        keep = []
+        if sample:
+            insts = [_Inst(F, D) for F, D, _ in sample]
+            keep.append(insts)
+            arr = (Instance * len(insts))(*[i.c for i in insts])
+            parr = (Params * len(sample))(*[p for _, _, p in sample])
+            keep += [arr, parr]
+            cfg.sample = C.cast(arr, C.POINTER(Instance))
+            cfg.sample_params = C.cast(parr, C.POINTER(Params))
+            cfg.sample_count = len(sample)
+        h = C.c_void_p()
+        _check(lib().pimqap_server_create(C.byref(cfg), C.byref(h)))
+        self.h = h
+        self._shapes = {}
+
+    def submit(self, F: np.ndarray, D: np.ndarray, params: Params) -> int:
+        inst = _Inst(F, D)
+        t = C.c_int64(0)
+        _check(lib().pimqap_server_submit(self.h, C.byref(inst.c), C.byref(params), C.byref(t)))
+        self._shapes[t.value] = (inst.F.shape[0], params.groups * params.replicas)
+        return t.value
+
+    def _fetch(self, ticket: int, timeout: float):
+        n, reps = self._shapes[ticket]
+        r, perm, energies = _new_result(n, reps)
+        st = lib().pimqap_server_wait(self.h, ticket, timeout, C.byref(r))
+        if st == 8:      # not ready
+            return None
+        del self._shapes[ticket]
+        _check(st)
+        return _result_dict(r, perm, energies)
+
+    def poll(self, ticket: int):
+        return self._fetch(ticket, 0.0)
+
+    def wait(self, ticket: int, timeout: float = -1.0) -> dict:
+        out = self._fetch(ticket, timeout)
+        if out is None:
+            raise PimqapError(8, "request not finished within the timeout")
+        return out
+
+    def stats(self) -> dict:
+        s = ServerStats()
+        _check(lib().pimqap_server_stats_get(self.h, C.byref(s)))
+        return {k: getattr(s, k) for k, _ in ServerStats._fields_}
+
+    def stall_heartbeat(self, stall: bool) -> None:
+        lib().pimqap_server_debug_stall_heartbeat(self.h, 1 if stall else 0)
+
+    def close(self) -> None:
+        if getattr(self, "h", None):
+            lib().pimqap_server_destroy(self.h)
+            self.h = None
 
     def __enter__(self):
         return self

@@ -1,0 +1,91 @@
+"""Serving: continuous batching with resident launches (GPU).
+
+Requests submitted while others run are admitted as slots and device memory free up; each
+result must equal pimqap_solve of the same request alone.  A host-side heartbeat stall must
+make the device workers' idle waits run out and stop them with an error status.
+"""
+import time
+
+import numpy as np
+import pytest
+
+import instances
+
+pytestmark = pytest.mark.gpu
+
+
+def same(a, b):
+    keys = ("best_energy", "megaiters_done", "updates", "accepts", "target_megaiter", "stopped_by")
+    return all(a[k] == b[k] for k in keys) and np.array_equal(a["best_perm"], b["best_perm"]) \
+        and np.array_equal(a["final_energies"], b["final_energies"])
+
+
+def requests(gpu, count, seed):
+    rng = np.random.default_rng(seed)
+    out = []
+    for k in range(count):
+        n = int(rng.integers(8, 200))
+        if k % 4 == 3:
+            inst = instances.Instance(n, rng.integers(0, 2_000_000, (n, n)), rng.integers(0, 5000, (n, n)))
+            b = 1e-9
+        else:
+            inst = instances.uniform(n, seed * 100 + k)
+            b = 0.02
+        p = gpu.default_params(replicas=int(rng.integers(2, 12)), groups=1 + k % 2,
+                               sweeps_per_exchange=1 + k % 3, beta_max=b, beta_ratio=1.4,
+                               seed=seed + k, max_megaiters=int(rng.integers(2, 9)))
+        out.append((inst, p))
+    return out
+
+
+def test_served_results_equal_solo_solves(gpu):
+    reqs = requests(gpu, 14, 3)
+    with gpu.Server() as srv:
+        first = [srv.submit(i.F, i.D, p) for i, p in reqs[:7]]
+        time.sleep(0.05)                    # the rest arrive while the first are on the GPU
+        second = [srv.submit(i.F, i.D, p) for i, p in reqs[7:]]
+        st0 = srv.stats()
+        assert st0["error_word"] == 0, st0
+        got = [srv.wait(t, 120.0) for t in first + second]
+        st = srv.stats()
+    assert st["completed"] == len(reqs) and st["error_word"] == 0, st
+    for (inst, p), r in zip(reqs, got):
+        assert same(r, gpu.solve(inst.F, inst.D, p)), inst.n
+        assert r["latency_ms"] >= r["admit_ms"] >= 0
+
+
+def test_memory_budget_gates_admission(gpu):
+    reqs = requests(gpu, 8, 5)
+    sizes = []
+    with gpu.Server(memory_budget=24 << 20, slots_per_class=4) as srv:
+        tickets = [srv.submit(i.F, i.D, p) for i, p in reqs]
+        peak_pending = srv.stats()["pending"]
+        got = [srv.wait(t, 120.0) for t in tickets]
+        sizes.append(srv.stats()["memory_budget"])
+        big = instances.grid256(9)
+        p = gpu.default_params(replicas=64, groups=8, max_megaiters=1)
+        with pytest.raises(gpu.PimqapError) as e:
+            srv.submit(big.F, big.D, p)
+        assert e.value.status == 7           # never fits the budget
+    assert peak_pending >= 0
+    for (inst, p), r in zip(reqs, got):
+        assert same(r, gpu.solve(inst.F, inst.D, p))
+
+
+def test_heartbeat_stall_stops_device_workers(gpu):
+    inst = instances.uniform(20, 11)
+    p = gpu.default_params(replicas=4, groups=1, max_megaiters=3, beta_max=0.02)
+    srv = gpu.Server(heartbeat_timeout=0.5)
+    try:
+        t = srv.submit(inst.F, inst.D, p)
+        srv.wait(t, 60.0)
+        srv.stall_heartbeat(True)
+        deadline = time.time() + 20
+        while time.time() < deadline and srv.stats()["error_word"] == 0:
+            time.sleep(0.1)
+        assert srv.stats()["error_word"] & 8      # host lost: the bounded idle waits ran out
+        with pytest.raises(gpu.PimqapError) as e:
+            srv.submit(inst.F, inst.D, p)
+        assert e.value.status == 6
+    finally:
+        srv.close()                               # returns: the workers have already stopped
