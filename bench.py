@@ -46,9 +46,14 @@ REPLICAS = 64
 GROUPS = 1
 SWEEPS_PER_EXCHANGE = 4
 MEGAITERS_PER_STEP = 25
-# Geometric ladder: beta_max in the reference's -b units (natural), ratio between neighbours.
-BETA_MAX = 0.05
-BETA_RATIO = 1.104
+# Geometric ladder chosen by the reference's automatic mode (pimqap_auto_beta on this
+# instance, 64 replicas, seed 1: beta0 = 2^-5 in the reference's internal log2 units, deltaBeta
+# = 64^(1/64)), then fixed for the run.
+BETA_MAX = 2.0 ** -5           # internal units
+BETA_RATIO = 1.0671404006768237
+# Ladders of the batch / serving suites, chosen the same way on representative instances.
+LADDER_UNIFORM = (2.0 ** -9, 1.1387886347566916)    # uniform n = 85, 32 replicas
+LADDER_HEAVY = (2.0 ** -13, 1.0787607977571199)     # heavy-tailed n = 180, 64 replicas
 METRIC = "swap proposals/sec"
 UNIT = "proposals/s"
 L2_FLUSH_BYTES = 256 << 20
@@ -131,7 +136,7 @@ def ref_cpu_throughput(F, D, budget_s: float, replicas: int = REPLICAS):
     ref = RefHarness("big_mt")
     cores = max(1, min(os.cpu_count() or 1, ref.maxt))
     ref.load(F, D)
-    ref.setup_replicated(cores, replicas, SWEEPS_PER_EXCHANGE, BETA_MAX * 1.44269504089, BETA_RATIO, 1)
+    ref.setup_replicated(cores, replicas, SWEEPS_PER_EXCHANGE, BETA_MAX, BETA_RATIO, 1)
     t1 = ref.run(1)
     m = max(1, int(budget_s / max(t1, 1e-3)))
     el = ref.run(m)
@@ -157,7 +162,7 @@ def run_reference(args):
     ref = RefHarness("big_mt")
     cores = max(1, min(os.cpu_count() or 1, ref.maxt))
     ref.load(inst.F, inst.D)
-    ref.setup_replicated(cores, REPLICAS, SWEEPS_PER_EXCHANGE, BETA_MAX * 1.44269504089, BETA_RATIO, 1)
+    ref.setup_replicated(cores, REPLICAS, SWEEPS_PER_EXCHANGE, BETA_MAX, BETA_RATIO, 1)
     t1 = ref.run(1)
     # each step a bounded sample: the whole run stays within ~3 minutes
     per_step = min(2.0, 180.0 / max(1, args.steps + args.warmup))
@@ -208,7 +213,7 @@ def run_ours(args):
 
     inst = instances.grid256(1000 + rank)
     params = pimqap.default_params(replicas=REPLICAS, groups=GROUPS, sweeps_per_exchange=SWEEPS_PER_EXCHANGE,
-                                   beta_max=BETA_MAX, beta_ratio=BETA_RATIO, seed=1 + rank,
+                                   beta_max=BETA_MAX, beta_ratio=BETA_RATIO, beta_internal=1, seed=1 + rank,
                                    device=local, megaiters_per_launch=MEGAITERS_PER_STEP,
                                    max_megaiters=2 ** 31 - 1, cluster_size=args.cluster_size,
                                    threads_per_block=args.threads)
@@ -258,7 +263,8 @@ def run_ours(args):
     Fp = torch.from_numpy(inst.F).pin_memory()
     Dp = torch.from_numpy(inst.D).pin_memory()
     p2 = pimqap.default_params(replicas=REPLICAS, groups=GROUPS, sweeps_per_exchange=SWEEPS_PER_EXCHANGE,
-                               beta_max=BETA_MAX, beta_ratio=BETA_RATIO, seed=1 + rank, device=local,
+                               beta_max=BETA_MAX, beta_ratio=BETA_RATIO, beta_internal=1, seed=1 + rank,
+                               device=local,
                                megaiters_per_launch=MEGAITERS_PER_STEP,
                                max_megaiters=args.steps * MEGAITERS_PER_STEP,
                                cluster_size=args.cluster_size, threads_per_block=args.threads)
@@ -288,7 +294,9 @@ def run_ours(args):
                                    "64 replicas, geometric beta ladder, exchange every 4 sweeps, "
                                    "10^4 sweeps = 100 steps",
                        "n": N, "replicas": reps, "sweeps_per_step": MEGAITERS_PER_STEP * SWEEPS_PER_EXCHANGE,
-                       "beta_max": BETA_MAX, "beta_ratio": BETA_RATIO, "parallelism": f"instances x{world}",
+                       "beta0_internal": BETA_MAX, "beta_ratio": BETA_RATIO,
+                       "ladder": "reference automatic mode on this instance (pimqap_auto_beta, seed 1), then fixed",
+                       "parallelism": f"instances x{world}",
                        "cluster_size": r1["cluster_size"], "force_bits": r1["force_bits"],
                        "l2": "flushed between steps (256 MiB write)"},
             "candidate_deltas_per_s": cand * world / (ms_max * 1e-3),
@@ -316,6 +324,115 @@ def run_ours(args):
     return line
 
 
+# ------------------------------------------------------------------ batch and serving suites
+
+def _sweeps_proposals(n: int, replicas: int, sweeps: int) -> float:
+    return float(replicas) * sweeps * n * (n - 1) / 2.0
+
+
+def run_batch_suite(args):
+    """512 instances, n ~ U[20, 150], uniform [0, 99] flows and distances, 32 replicas each,
+    2000 sweeps (500 mega-iterations of 4), in persistent launches.  Reports throughput of the
+    fixed-work batch and time-to-target against per-instance targets from a run twice as long
+    (gap <= 0.1 %), for the batch and for the plain form (one pimqap_solve per instance, one
+    instance per launch), the latter timed on every 16th instance and scaled to 512."""
+    import pimqap
+    batch = instances.uniform_batch(512)
+    M = 500
+    b0, ratio = LADDER_UNIFORM
+
+    def params(seed, **kw):
+        return pimqap.default_params(replicas=32, groups=1, sweeps_per_exchange=4, beta_max=b0,
+                                     beta_ratio=ratio, beta_internal=1, seed=seed, **kw)
+
+    pairs = [(b.F, b.D) for b in batch]
+    pimqap.batch_solve(pairs[:2], [params(1, max_megaiters=2), params(2, max_megaiters=2)])   # warm-up
+    t0 = time.perf_counter()
+    fixed = pimqap.batch_solve(pairs, [params(k + 1, max_megaiters=M) for k in range(len(batch))])
+    fixed_wall = time.perf_counter() - t0
+    props = sum(_sweeps_proposals(b.n, 32, 4 * M) for b in batch)
+    t0 = time.perf_counter()
+    longrun = pimqap.batch_solve(pairs, [params(10 ** 6 + k, max_megaiters=2 * M) for k in range(len(batch))])
+    long_wall = time.perf_counter() - t0
+    targets = [min(l["best_energy"], f["best_energy"]) for l, f in zip(longrun, fixed)]
+    goals = [int(t * 1.001) for t in targets]
+    t0 = time.perf_counter()
+    res = pimqap.batch_solve(pairs, [params(k + 1, max_megaiters=M, goal=goals[k]) for k in range(len(batch))])
+    batch_ttt = time.perf_counter() - t0
+    reached = sum(1 for r in res if r["stopped_by"] == 1)
+    sample = list(range(0, len(batch), 16))
+    t0 = time.perf_counter()
+    plain_reached = 0
+    for k in sample:
+        r = pimqap.solve(batch[k].F, batch[k].D, params(k + 1, max_megaiters=M, goal=goals[k]))
+        plain_reached += r["stopped_by"] == 1
+    plain_sample = time.perf_counter() - t0
+    plain_total = plain_sample * len(batch) / len(sample)
+    line = {"suite": "batch", "metric": "time-to-target (<=0.1% gap) and swap proposals/sec",
+            "instances": len(batch), "n_range": [20, 150], "replicas": 32, "sweeps": 4 * M,
+            "ladder": {"beta0_internal": b0, "beta_ratio": ratio},
+            "fixed_work": {"wall_s": fixed_wall, "device_ms_first_class": fixed[0]["device_ms"],
+                           "proposals_per_s_wall": props / fixed_wall,
+                           "accept_rate": sum(r["accepts"] for r in fixed) / sum(r["updates"] for r in fixed)},
+            "targets": "best of a 4000-sweep batch run (other seeds) and the 2000-sweep run; goal = target * 1.001",
+            "long_run_wall_s": long_wall,
+            "batch_time_to_target_s": batch_ttt, "batch_reached": reached,
+            "plain_time_to_target_s_est": plain_total, "plain_sampled": len(sample),
+            "plain_reached_in_sample": plain_reached,
+            "speedup_vs_plain": plain_total / batch_ttt}
+    print(json.dumps(line))
+
+
+def run_serve_suite(args):
+    """Poisson arrivals (rate --rate, --duration s) of QAP solves, n ~ U[30, 256], half uniform,
+    half heavy-tailed instances, 32 replicas and 2000 sweeps each, into the continuous-batching
+    server; reports p50/p99 latency of completed requests, throughput and backlog."""
+    import pimqap
+    trace = list(instances.serving_trace(rate_hz=args.rate, duration_s=args.duration))
+
+    def params(inst, k):
+        b0, ratio = LADDER_UNIFORM if inst.name.startswith("uniform") else LADDER_HEAVY
+        return pimqap.default_params(replicas=32, groups=1, sweeps_per_exchange=4, beta_max=b0,
+                                     beta_ratio=ratio, beta_internal=1, seed=k + 1, max_megaiters=500)
+
+    sample = [(inst.F, inst.D, params(inst, k)) for k, (_, inst) in enumerate(trace[:64])]
+    srv = pimqap.Server(sample=sample)
+    t_start = time.perf_counter()
+    tickets = []
+    for k, (t_arr, inst) in enumerate(trace):
+        now = time.perf_counter() - t_start
+        if t_arr > now:
+            time.sleep(t_arr - now)
+        tickets.append((srv.submit(inst.F, inst.D, params(inst, k)), inst))
+    done = {}
+    deadline = t_start + args.duration + args.drain
+    while len(done) < len(tickets) and time.perf_counter() < deadline:
+        for t, inst in tickets:
+            if t in done:
+                continue
+            r = srv.poll(t)
+            if r is not None:
+                done[t] = (r, inst, time.perf_counter() - t_start)
+        time.sleep(0.01)
+    st = srv.stats()
+    srv.close()
+    lat = sorted(r["latency_ms"] for r, _, _ in done.values())
+    t_last = max((t for _, _, t in done.values()), default=0.0)
+    props = sum(_sweeps_proposals(inst.n, 32, r["megaiters_done"] * 4) for r, inst, _ in done.values())
+
+    def pct(q):
+        return lat[min(len(lat) - 1, int(q * len(lat)))] if lat else None
+
+    line = {"suite": "serve", "metric": "serve p50/p99 latency and throughput",
+            "rate_hz": args.rate, "duration_s": args.duration, "submitted": len(tickets),
+            "completed": len(done), "backlog_at_end": len(tickets) - len(done),
+            "p50_ms": pct(0.50), "p99_ms": pct(0.99), "max_ms": lat[-1] if lat else None,
+            "throughput_req_per_s": len(done) / t_last if t_last else 0.0,
+            "proposals_per_s": props / t_last if t_last else 0.0,
+            "classes": st["classes"], "error_word": st["error_word"]}
+    print(json.dumps(line))
+
+
 def main():
     ap = argparse.ArgumentParser(description=__doc__.split("\n")[0])
     ap.add_argument("--gpus", type=int, default=1)
@@ -325,9 +442,20 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cluster-size", type=int, default=0, help="CTAs per replica (0 = automatic)")
     ap.add_argument("--threads", type=int, default=0, help="threads per CTA (0 = automatic)")
+    ap.add_argument("--suite", choices=["headline", "batch", "serve"], default="headline",
+                    help="headline: the n=256 workload (the driver's line); batch / serve: the other workloads")
+    ap.add_argument("--rate", type=float, default=200.0, help="serve suite: arrivals per second")
+    ap.add_argument("--duration", type=float, default=5.0, help="serve suite: seconds of arrivals")
+    ap.add_argument("--drain", type=float, default=180.0, help="serve suite: seconds allowed after arrivals end")
     args = ap.parse_args()
     if args.warmup < 3:
         ap.error("--warmup must be >= 3")
+    if args.suite == "batch":
+        run_batch_suite(args)
+        return
+    if args.suite == "serve":
+        run_serve_suite(args)
+        return
     if args.impl == "reference":
         run_reference(args)
     else:
