@@ -82,6 +82,12 @@ typedef struct pimqap_params {
                                     automatic mode before solving (no -b flag, :645-658) */
     double auto_lower;           /* -al lowerBetaProportion (default 0.1, :33) */
     double auto_higher;          /* -ah higherBetaProportion (default 0.9, :34) */
+    int64_t goal_print;          /* -G  record a replica whose best falls below this during a
+                                    sweep, with its permutation (goalPrint, :271-282); acts only
+                                    when > 0, as in the reference.  Needs event_capacity > 0 */
+    int32_t event_capacity;      /* progress events kept per run call (0 = no event log); see
+                                    pimqap_solver_events */
+    int32_t event_perm_capacity; /* goal_print permutations kept per run call (0 = 256) */
 } pimqap_params;
 
 /* Fills p with the reference's defaults: 10 replicas, 20 groups, 4 sweeps per exchange,
@@ -175,6 +181,41 @@ pimqap_status pimqap_solver_replica(pimqap_solver *s, int32_t t, int32_t l, int3
 pimqap_status pimqap_solver_group(pimqap_solver *s, int32_t t, int32_t *order,
                                   int32_t *time_since_swap, int64_t *group_best);
 
+/* A progress event: what the reference prints while it runs, recorded on the device with
+   the time it happened.  Recorded only when params.event_capacity > 0. */
+#define PIMQAP_EVENT_GROUP_BEST 0 /* tracking of mega-iteration `megaiter` found replica
+                                     `replica` below group `group`'s best (threadBestE); one
+                                     event per lowering, in the reference's replica order
+                                     (CPU_PIM.cpp:297-314).  "Best Energy Found" lines are the
+                                     events that also lower the best over all groups (:303-311)
+                                     and sweep<t>.txt holds the last event of each (m, t) (:317-321) */
+#define PIMQAP_EVENT_GOAL_PRINT 1 /* a sweep of mega-iteration `megaiter` lowered the replica's
+                                     best below params.goal_print (:271-282) */
+typedef struct pimqap_event {
+    int64_t megaiter;
+    int64_t energy;
+    double time_ms;             /* device time since setup (solver) or the batch start */
+    int32_t kind;               /* PIMQAP_EVENT_* */
+    int32_t group;
+    int32_t replica;
+    int32_t perm_index;         /* GOAL_PRINT: argument of pimqap_solver_event_perm, -1 when the
+                                   permutation store of that run call was full */
+    int32_t trial;              /* automatic mode: trial index (beta step * 5 + trial); else 0 */
+    int32_t pad;
+} pimqap_event;
+
+/* Events recorded so far, in the reference's order (mega-iteration, then tracking before the
+   sweeps, then group, then replica): copies events [first, first + capacity) into `events`
+   and sets *count to the number copied.  *total (may be NULL) receives the number recorded;
+   *dropped (may be NULL) the number lost because a run call recorded more than
+   params.event_capacity. */
+pimqap_status pimqap_solver_events(pimqap_solver *s, int64_t first, int32_t capacity,
+                                   pimqap_event *events, int32_t *count, int64_t *total,
+                                   int64_t *dropped);
+
+/* The permutation (n entries) of a GOAL_PRINT event. */
+pimqap_status pimqap_solver_event_perm(pimqap_solver *s, int32_t perm_index, int32_t *perm);
+
 void pimqap_solver_destroy(pimqap_solver *s);
 
 /* ---------------------------------------------------------------- batched solve */
@@ -249,6 +290,40 @@ void pimqap_server_debug_stall_heartbeat(pimqap_server *s, int32_t stall);
 pimqap_status pimqap_auto_beta(const pimqap_instance *inst, const pimqap_params *params,
                                double *beta0_internal, double *delta_beta, double *avg_energy,
                                int64_t *best_energy, int32_t *best_perm);
+
+/* Everything the reference's automatic mode prints and decides, for a drop-in of its log
+   (CPU_PIM.cpp:373-476).  The trials run as in pimqap_auto_beta; in the reference they run one
+   after another, so the first trial (in that order) whose tracked best reaches params.goal ends
+   automatic mode: goal_trial is that trial and the later trials are ignored. */
+#define PIMQAP_AUTO_STEPS 32
+#define PIMQAP_AUTO_TRIALS 5
+typedef struct pimqap_auto_report {
+    double beta0_internal;      /* beta0 after automatic mode: maxBeta, or exp2(-30 + step) of
+                                   the goal trial's step (:397, :420-422) */
+    double delta_beta;          /* deltaBeta after automatic mode (1 when the goal ended it) */
+    double min_beta, max_beta;  /* "Selecting minimum / maximum beta of" values (:449-461);
+                                   0 when the goal ended automatic mode */
+    int32_t min_beta_printed;   /* nonzero when the reference prints the minimum-beta line (it
+                                   falls back to exp2(-30) silently otherwise, :454-456) */
+    int32_t pad0;
+    double avg_energy[PIMQAP_AUTO_STEPS];          /* "Average Energy" of each beta step */
+    int64_t trial_best[PIMQAP_AUTO_STEPS * PIMQAP_AUTO_TRIALS];
+                                /* best energy each trial's tracking saw (mega-iterations 0-9;
+                                   the sweeps of the last one are not tracked, :293-362) */
+    int32_t steps_printed;      /* beta steps whose "Beta:" line the reference prints */
+    int32_t goal_trial;         /* -1, or the trial that reached the goal */
+    int64_t best_energy;        /* best energy of any visited state over the trials used */
+    int32_t *best_perm;         /* caller-provided, n entries (may be NULL) */
+    pimqap_event *events;       /* caller-provided GROUP_BEST events of the trials used, in
+                                   the reference's order (may be NULL) */
+    int32_t event_capacity;     /* entries of events */
+    int32_t event_count;        /* entries written */
+    int64_t events_dropped;     /* events that did not fit */
+    double device_ms;           /* device time of the trials */
+} pimqap_auto_report;
+
+pimqap_status pimqap_auto_beta_report(const pimqap_instance *inst, const pimqap_params *params,
+                                      pimqap_auto_report *report);
 
 /* ---------------------------------------------------------------- misc */
 

@@ -13,6 +13,8 @@
 #   _ref/libref_big_mt.so  MAXN 256, 64 replicas, 256 threads, the reference's own
 #                          std::mt19937 (no shim): the timed CPU baseline
 #   _ref/cpu_pim_stock     the unmodified reference CLI (for output-format checks)
+#   _ref/cpu_pim_philox    the reference CLI with stock capacities on the solver's Philox
+#                          streams (ref_cli_main.cpp; for the CLI parity fixtures)
 #
 # The reference source path is $PIMQAP_REF_ROOT (default /root/reference).  When it is
 # absent the script does nothing and exits 0.
@@ -37,8 +39,10 @@ if [ ! -f "$SRC" ]; then
 fi
 mkdir -p "$OUT"
 
-# Exactly one line must match each capacity constant, or the recipe fails.
-for pat in '^const int MAXN = 160;' '^const int MAXNUMREPLICAS = 10;' '^const int MAXNUMTHREADS = 20;'; do
+# Exactly one line must match each capacity constant (and the last statement of main), or
+# the recipe fails.
+for pat in '^const int MAXN = 160;' '^const int MAXNUMREPLICAS = 10;' '^const int MAXNUMTHREADS = 20;' \
+           '^    cout << "Elapsed time: " << duration.count() / 1000.0 << " seconds." << endl;$'; do
     c=$(grep -c "$pat" "$SRC" || true)
     if [ "$c" != "1" ]; then
         echo "build_ref.sh: pattern '$pat' matched $c lines in $SRC" >&2
@@ -46,10 +50,14 @@ for pat in '^const int MAXN = 160;' '^const int MAXNUMREPLICAS = 10;' '^const in
     fi
 done
 
+# main() is renamed (ref_prelude.h), and a renamed int function that runs off its end is
+# undefined behaviour (only main has the implicit return 0): the recipe adds that return 0
+# after main's last statement.
 patched() {  # maxn maxr maxt
     sed -e "s/^const int MAXN = 160;/const int MAXN = $1;/" \
         -e "s/^const int MAXNUMREPLICAS = 10;/const int MAXNUMREPLICAS = $2;/" \
-        -e "s/^const int MAXNUMTHREADS = 20;/const int MAXNUMTHREADS = $3;/" "$SRC"
+        -e "s/^const int MAXNUMTHREADS = 20;/const int MAXNUMTHREADS = $3;/" \
+        -e 's/^    cout << "Elapsed time: " << duration.count() \/ 1000.0 << " seconds." << endl;$/& return 0;/' "$SRC"
 }
 
 build_lib() {  # out maxn maxr maxt extra-flags
@@ -64,4 +72,9 @@ build_lib libref_stock.so 160 10 20
 build_lib libref_big.so 256 64 64
 build_lib libref_big_mt.so 256 64 256 -DPIMQAP_REF_NO_SHIM -mcmodel=medium
 $CXX $CXXFLAGS "$SRC" -o "$OUT/cpu_pim_stock.tmp" && mv "$OUT/cpu_pim_stock.tmp" "$OUT/cpu_pim_stock"
+{ patched 160 10 20; cat "$HERE/ref_harness.cpp"; } |
+    $CXX $CXXFLAGS -include "$HERE/ref_prelude.h" -c -x c++ - -o "$OUT/cpu_pim_philox.o"
+$CXX $CXXFLAGS "$HERE/ref_cli_main.cpp" "$OUT/cpu_pim_philox.o" -o "$OUT/cpu_pim_philox.tmp"
+rm -f "$OUT/cpu_pim_philox.o"
+mv "$OUT/cpu_pim_philox.tmp" "$OUT/cpu_pim_philox"
 echo "build_ref.sh: built $(ls "$OUT" | tr '\n' ' ')"

@@ -168,5 +168,23 @@ int64_t ref_single_best() { return singleBestE.load(); }
 /* The reference CLI in process (argv[0] is the program name). */
 int ref_main(int argc, char **argv) { return pimqap_ref_main(argc, argv); }
 
+#ifndef PIMQAP_REF_NO_SHIM
+/* The reference's own main() on the solver's Philox streams (see the CLI mode of
+   ref_prelude.h): same flags, same files, same stdout, so its outputs can be compared line by
+   line with the pimqap CLI run with --seed. */
+int ref_cli(uint64_t seed, int argc, char **argv) {
+    pimqap_ref::g_cli = true;
+    pimqap_ref::g_cli_seed = seed;
+    pimqap_ref::g_ctor_calls = 0;
+    pimqap_ref::g_rng_base = reinterpret_cast<const char *>(&rng[0]);
+    pimqap_ref::g_N = &N;
+    pimqap_ref::g_R = &NUMREPLICAS;
+    pimqap_ref::g_IT = &NUMITERA;
+    pimqap_ref::g_T = &NUMTHREADS;
+    pimqap_ref::g_main = std::this_thread::get_id();
+    return pimqap_ref_main(argc, argv);
+}
+#endif
+
 }  // extern "C"
 #pragma GCC visibility pop

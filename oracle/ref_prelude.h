@@ -20,6 +20,7 @@
 
 #include <cstdint>
 #include <random>
+#include <thread>
 
 namespace pimqap_ref {
 
@@ -42,6 +43,36 @@ inline void philox4x32_10(uint32_t c[4], uint32_t k0, uint32_t k1) {
 inline uint64_t g_seed = 0;
 inline uint64_t g_shuffle_calls = 0;
 
+/* CLI mode (ref_cli in ref_harness.cpp): the reference's own main() runs, so nothing calls
+   bind_sweep.  Instead each engine binds itself: calls from the main thread are setup()'s
+   shuffle, calls from a worker thread are the sweeps of group (engine index in rng[]).  Every
+   setup() re-seeds all NUMTHREADS engines (CPU_PIM.cpp:128-132); the j-th setup takes the key
+   the solver gives the same run: setup 0 is the run itself (key = seed), setups 1..160 are
+   automatic mode's trials (key = splitmix64(seed + j), trial j - 1 = 5 * step + trial), and
+   setup 161 is the run after automatic mode (key = seed). */
+inline bool g_cli = false;
+inline const char *g_rng_base = nullptr;
+inline const int *g_N = nullptr, *g_R = nullptr, *g_IT = nullptr, *g_T = nullptr;
+inline std::thread::id g_main;
+inline uint64_t g_cli_seed = 0, g_ctor_calls = 0;
+
+inline uint64_t splitmix64(uint64_t x) {
+    x += 0x9E3779B97F4A7C15ull;
+    x = (x ^ (x >> 30)) * 0xBF58476D1CE4E5B9ull;
+    x = (x ^ (x >> 27)) * 0x94D049BB133111EBull;
+    return x ^ (x >> 31);
+}
+
+inline void on_seed() {
+    const uint64_t T = (uint64_t)*g_T;
+    if (g_ctor_calls % T == 0) {
+        const uint64_t j = g_ctor_calls / T;
+        g_shuffle_calls = 0;
+        g_seed = (j >= 1 && j <= 160) ? splitmix64(g_cli_seed + j) : g_cli_seed;
+    }
+    ++g_ctor_calls;
+}
+
 }  // namespace pimqap_ref
 
 #ifndef PIMQAP_REF_NO_SHIM
@@ -52,7 +83,9 @@ struct pimqap_ref_engine {
     static constexpr result_type max() { return 0xFFFFFFFFu; }
 
     pimqap_ref_engine() {}
-    explicit pimqap_ref_engine(result_type) {}  // the random_device seed is ignored
+    explicit pimqap_ref_engine(result_type) {  // the random_device seed is ignored
+        if (pimqap_ref::g_cli) pimqap_ref::on_seed();
+    }
 
     /* After setup() the harness binds each group's engine to its sweep stream. */
     void bind_sweep(uint32_t group, int n, int replicas, int numitera) {
@@ -62,6 +95,10 @@ struct pimqap_ref_engine {
     result_type operator()() {
         uint32_t c[4];
         uint64_t idx;
+        if (pimqap_ref::g_cli && !bound && std::this_thread::get_id() != pimqap_ref::g_main)
+            bind_sweep((uint32_t)((reinterpret_cast<const char *>(this) - pimqap_ref::g_rng_base) /
+                                  sizeof(pimqap_ref_engine)),
+                       *pimqap_ref::g_N, *pimqap_ref::g_R, *pimqap_ref::g_IT);
         if (!bound) {
             idx = pimqap_ref::g_shuffle_calls++;
             c[0] = (uint32_t)(idx >> 2); c[1] = (uint32_t)(idx >> 34); c[2] = 0; c[3] = 0xFFFFFFFFu;

@@ -103,7 +103,8 @@ std::vector<BatchClass> plan_classes(const std::vector<Plan> &plans, const std::
 // One class: instance heads in one pinned image (one copy), tails cleared in one memset,
 // queue filled with every active instance's epoch-0 items, largest first.
 pimqap_status ClassRun::prepare(const pimqap_instance *insts, const pimqap_params *params,
-                                const std::vector<Plan> &plans, const BatchClass &c) {
+                                const std::vector<Plan> &plans, const BatchClass &c,
+                                const EventLink *ev) {
     cls = c;
     const int m = (int)c.members.size();
     size_t head_total = 0, tail_total = 0, reps_total = 0, perm_total = 0;
@@ -150,6 +151,10 @@ pimqap_status ClassRun::prepare(const pimqap_instance *insts, const pimqap_param
         carve_instance(plans[k], base + hoff[i], base + head_total + toff[i], &devs[i]);
         devs[i].goal = params[k].goal;
         devs[i].seed = params[k].seed;
+        if (ev) {
+            devs[i].ev = *ev;
+            devs[i].ev.tag = k;
+        }
     }
     PQ_CUDA(cudaMemcpyAsync(base, pinned, head_total, cudaMemcpyHostToDevice, stream));
     PQ_CUDA(cudaMemsetAsync(base + head_total, 0, tail_total + misc, stream));
@@ -259,6 +264,7 @@ pimqap_status ClassRun::finish(const std::vector<Plan> &plans, pimqap_result *re
     unsigned long long start_ns = 0;
     PQ_CUDA(cudaMemcpy(&err, d_error, 4, cudaMemcpyDeviceToHost));
     PQ_CUDA(cudaMemcpy(&start_ns, d_start, 8, cudaMemcpyDeviceToHost));
+    this->start_ns = start_ns;
     PQ_CUDA(cudaMemcpy(out.data(), d_results, sizeof(pimqap::BatchResultDev) * m, cudaMemcpyDeviceToHost));
     if (perm_total) PQ_CUDA(cudaMemcpy(perms.data(), d_perms, 4 * perm_total, cudaMemcpyDeviceToHost));
     if (energy_total)
@@ -314,6 +320,14 @@ using namespace pimqap::detail;
 
 extern "C" pimqap_status pimqap_batch_solve(const pimqap_instance *insts, const pimqap_params *params,
                                             int32_t count, pimqap_result *results) {
+    return batch_solve(insts, params, count, results, nullptr);
+}
+
+namespace pimqap {
+namespace detail {
+
+pimqap_status batch_solve(const pimqap_instance *insts, const pimqap_params *params, int32_t count,
+                          pimqap_result *results, EventBuffer *ev) {
     if (count < 0 || (count > 0 && (!insts || !params || !results)))
         return fail(PIMQAP_ERR_ARG, "bad batch arguments");
     if (count == 0) return PIMQAP_OK;
@@ -347,15 +361,21 @@ extern "C" pimqap_status pimqap_batch_solve(const pimqap_instance *insts, const 
     std::vector<std::unique_ptr<ClassRun>> runs;
     for (const auto &c : classes) {
         runs.emplace_back(new ClassRun());
-        st = runs.back()->prepare(insts, params, plans, c);
+        st = runs.back()->prepare(insts, params, plans, c, ev ? &ev->link : nullptr);
         if (st != PIMQAP_OK) return st;
     }
     for (auto &r : runs) {   // all classes run concurrently, each on its own stream
         st = r->launch();
         if (st != PIMQAP_OK) return st;
     }
+    unsigned long long t0 = ~0ull;
     for (auto &r : runs) {
         st = r->finish(plans, results);
+        if (st != PIMQAP_OK) return st;
+        if (r->runnable > 0) t0 = std::min(t0, r->start_ns);
+    }
+    if (ev) {
+        st = ev->drain(runs.front()->stream, t0 == ~0ull ? 0ull : t0, false);
         if (st != PIMQAP_OK) return st;
     }
     runs.clear();
@@ -364,6 +384,9 @@ extern "C" pimqap_status pimqap_batch_solve(const pimqap_instance *insts, const 
     for (int k = 0; k < count; ++k) results[k].wall_ms = el;
     return PIMQAP_OK;
 }
+
+}  // namespace detail
+}  // namespace pimqap
 
 namespace {
 
@@ -379,15 +402,16 @@ uint64_t splitmix64(uint64_t x) {
 // autoSelectParameters (CPU_PIM.cpp:366-476).  The reference runs the trials one after another
 // with fresh random_device seeds; here trial (k, t) is seeded with splitmix64(seed + 5k + t + 1)
 // and all 160 trials run in one batched launch.  The averaging order and the selection rule are
-// the reference's, in the same double arithmetic.
-extern "C" pimqap_status pimqap_auto_beta(const pimqap_instance *inst, const pimqap_params *params,
-                                          double *beta0_internal, double *delta_beta, double *avg_energy,
-                                          int64_t *best_energy, int32_t *best_perm) {
-    if (!inst || !params || !beta0_internal || !delta_beta) return fail(PIMQAP_ERR_ARG, "null argument");
+// the reference's, in the same double arithmetic.  Because the reference's trials run in order
+// and its best energy carries over between them, the first trial (in that order) whose tracked
+// best reaches the goal ends automatic mode (:419-422); the trials after it are ignored.
+extern "C" pimqap_status pimqap_auto_beta_report(const pimqap_instance *inst, const pimqap_params *params,
+                                                 pimqap_auto_report *rep) {
+    if (!inst || !params || !rep) return fail(PIMQAP_ERR_ARG, "null argument");
     pimqap_status st = check_params(inst, params);
     if (st != PIMQAP_OK) return st;
     constexpr double kMinBetaToTry = -30, kBetaStep = 1;     // :366-370
-    constexpr int kTrials = 5, kSteps = 32, kMegaiters = 10;  // :368, :371, :391
+    constexpr int kTrials = PIMQAP_AUTO_TRIALS, kSteps = PIMQAP_AUTO_STEPS, kMegaiters = 10;  // :368, :371, :391
     const int T = params->groups, R = params->replicas, n = inst->n;
     std::vector<pimqap_instance> insts(kSteps * kTrials, *inst);
     std::vector<pimqap_params> ps(kSteps * kTrials, *params);
@@ -401,6 +425,8 @@ extern "C" pimqap_status pimqap_auto_beta(const pimqap_instance *inst, const pim
             p.max_megaiters = kMegaiters;
             p.seed = splitmix64(params->seed + (uint64_t)(i * kTrials + t) + 1);
             p.timeout_s = 0;
+            p.goal_print = 0;
+            p.event_capacity = 0;
         }
     std::vector<pimqap_result> rs(ps.size());
     std::vector<std::vector<int64_t>> energies(ps.size(), std::vector<int64_t>((size_t)T * R));
@@ -410,8 +436,31 @@ extern "C" pimqap_status pimqap_auto_beta(const pimqap_instance *inst, const pim
         rs[k].final_energies = energies[k].data();
         rs[k].best_perm = perms[k].data();
     }
-    st = pimqap_batch_solve(insts.data(), ps.data(), (int32_t)ps.size(), rs.data());
+    // Group-best events of every trial: the tracked bests (mega-iterations 0-9) decide the goal
+    // and give the "Best Energy Found" lines printed during automatic mode.
+    EventBuffer ev;
+    {
+        int maxsm = 0;
+        st = open_device(params->device, &maxsm);
+        if (st != PIMQAP_OK) return st;
+        const unsigned cap = (unsigned)std::min<size_t>((size_t)1 << 22, (size_t)ps.size() * T * R * (kMegaiters + 1));
+        st = ev.allocate(cap, 0, n, 0, 0);
+        if (st != PIMQAP_OK) return st;
+        PQ_CUDA(cudaStreamSynchronize(0));
+    }
+    st = batch_solve(insts.data(), ps.data(), (int32_t)ps.size(), rs.data(), &ev);
     if (st != PIMQAP_OK) return st;
+    if (ev.dropped) return fail(PIMQAP_ERR_ARG, "automatic mode: event log overflow");
+
+    const int ntrial = kSteps * kTrials;
+    for (int k = 0; k < ntrial; ++k) rep->trial_best[k] = PIMQAP_NO_BEST;
+    for (const pimqap_event &e : ev.events)
+        if (e.kind == PIMQAP_EVENT_GROUP_BEST && e.megaiter < kMegaiters)
+            rep->trial_best[e.trial] = std::min<int64_t>(rep->trial_best[e.trial], e.energy);
+    int goal_trial = -1;
+    for (int k = 0; k < ntrial && goal_trial < 0; ++k)
+        if (rep->trial_best[k] <= params->goal) goal_trial = k;
+    const int used = goal_trial >= 0 ? goal_trial + 1 : ntrial;
 
     double sums[kSteps] = {0};
     const double denom = static_cast<double>(kTrials) * T * R;                    // :412
@@ -421,12 +470,29 @@ extern "C" pimqap_status pimqap_auto_beta(const pimqap_instance *inst, const pim
                 for (int l = 0; l < R; ++l)
                     sums[i] += (double)energies[i * kTrials + t][(size_t)g * R + l] / denom;
     size_t arg = 0;
-    for (size_t k = 1; k < rs.size(); ++k)
+    for (int k = 1; k < used; ++k)
         if (rs[k].best_energy < rs[arg].best_energy) arg = k;
-    if (best_energy) *best_energy = rs[arg].best_energy;
-    if (best_perm) std::memcpy(best_perm, perms[arg].data(), 4 * (size_t)n);
-    if (avg_energy) std::memcpy(avg_energy, sums, sizeof(sums));
-
+    rep->best_energy = rs[arg].best_energy;
+    if (rep->best_perm) std::memcpy(rep->best_perm, perms[arg].data(), 4 * (size_t)n);
+    std::memcpy(rep->avg_energy, sums, sizeof(sums));
+    rep->goal_trial = goal_trial;
+    rep->device_ms = rs[0].device_ms;
+    rep->event_count = 0;
+    rep->events_dropped = 0;
+    for (const pimqap_event &e : ev.events) {
+        if (e.kind != PIMQAP_EVENT_GROUP_BEST || e.megaiter >= kMegaiters || e.trial >= used) continue;
+        if (rep->events && rep->event_count < rep->event_capacity) rep->events[rep->event_count++] = e;
+        else ++rep->events_dropped;
+    }
+    rep->min_beta = rep->max_beta = 0;
+    rep->min_beta_printed = 0;
+    if (goal_trial >= 0) {                   // :419-422: beta0 stays at the step's beta
+        rep->steps_printed = goal_trial / kTrials;
+        rep->beta0_internal = std::exp2(kMinBetaToTry + (goal_trial / kTrials) * kBetaStep);
+        rep->delta_beta = 1.0;
+        return PIMQAP_OK;
+    }
+    rep->steps_printed = kSteps;
     const int i = kSteps - 1;                                                       // :434
     double minE = 1e30, maxE = -1e30;
     int minEIndex = 0;
@@ -440,15 +506,35 @@ extern "C" pimqap_status pimqap_auto_beta(const pimqap_instance *inst, const pim
     double minBeta = 0, maxBeta = 0;
     const double higher = params->auto_higher, lower = params->auto_lower;
     for (int j = 0; j < i; j++) {                                                   // :447-473
-        if (minBeta == 0 && ((j == (minEIndex - 1) && (j >= 1)) || (sums[j] < (maxE - minE) * higher + minE)))
+        if (minBeta == 0 && ((j == (minEIndex - 1) && (j >= 1)) || (sums[j] < (maxE - minE) * higher + minE))) {
             minBeta = std::exp2(kMinBetaToTry + (j)*kBetaStep);
+            rep->min_beta_printed = 1;
+        }
         if (j == i - 1 || (minBeta != 0 && (j == minEIndex || (sums[j] < (maxE - minE) * lower + minE)))) {
             if (minBeta == 0) minBeta = std::exp2(kMinBetaToTry + 0 * kBetaStep);
             maxBeta = std::exp2(kMinBetaToTry + (j + 2) * kBetaStep);
-            *beta0_internal = maxBeta;
-            *delta_beta = std::pow(maxBeta / minBeta, 1.0 / R);
+            rep->min_beta = minBeta;
+            rep->max_beta = maxBeta;
+            rep->beta0_internal = maxBeta;
+            rep->delta_beta = std::pow(maxBeta / minBeta, 1.0 / R);
             return PIMQAP_OK;
         }
     }
     return fail(PIMQAP_ERR_ARG, "automatic beta selection found no range");
+}
+
+extern "C" pimqap_status pimqap_auto_beta(const pimqap_instance *inst, const pimqap_params *params,
+                                          double *beta0_internal, double *delta_beta, double *avg_energy,
+                                          int64_t *best_energy, int32_t *best_perm) {
+    if (!beta0_internal || !delta_beta) return fail(PIMQAP_ERR_ARG, "null argument");
+    std::unique_ptr<pimqap_auto_report> rep(new pimqap_auto_report());
+    std::memset(rep.get(), 0, sizeof(pimqap_auto_report));
+    rep->best_perm = best_perm;
+    pimqap_status st = pimqap_auto_beta_report(inst, params, rep.get());
+    if (st != PIMQAP_OK) return st;
+    *beta0_internal = rep->beta0_internal;
+    *delta_beta = rep->delta_beta;
+    if (avg_energy) std::memcpy(avg_energy, rep->avg_energy, sizeof(rep->avg_energy));
+    if (best_energy) *best_energy = rep->best_energy;
+    return PIMQAP_OK;
 }

@@ -9,6 +9,7 @@
 #include "pimqap.h"
 #include "pimqap_internal.h"
 #include "pimqap_plan.h"
+#include "pimqap_events.h"
 
 namespace pimqap {
 namespace detail {
@@ -55,13 +56,21 @@ struct ClassRun {
     unsigned long long *d_start = nullptr;
     int runnable = 0;
     double device_ms = 0;
+    unsigned long long start_ns = 0;   // %globaltimer when the launch started
 
+    // `ev` (may be null): the event log every member appends to, tagged with its batch index.
     pimqap_status prepare(const pimqap_instance *insts, const pimqap_params *params,
-                          const std::vector<Plan> &plans, const BatchClass &c);
+                          const std::vector<Plan> &plans, const BatchClass &c,
+                          const EventLink *ev = nullptr);
     pimqap_status launch();
     pimqap_status finish(const std::vector<Plan> &plans, pimqap_result *results);
     ~ClassRun();
 };
+
+// pimqap_batch_solve with an optional event log shared by all members (tag = batch index);
+// the log is drained (times from the earliest class start) before this returns.
+pimqap_status batch_solve(const pimqap_instance *insts, const pimqap_params *params, int32_t count,
+                          pimqap_result *results, EventBuffer *ev);
 
 }  // namespace detail
 }  // namespace pimqap

@@ -23,6 +23,7 @@
 #include "pimqap.h"
 #include "pimqap_internal.h"
 #include "pimqap_plan.h"
+#include "pimqap_events.h"
 
 using pimqap::SolveDev;
 
@@ -207,8 +208,11 @@ struct pimqap_solver {
     bool stopped_goal = false;
     int64_t h2d = 0, d2h = 0;   // bytes copied over PCIe by this solver
     double beta0_used = 0, ratio_used = 0;
+    std::unique_ptr<pimqap::detail::EventBuffer> events;   // params.event_capacity > 0
+    unsigned long long start_ns = 0;                        // %globaltimer at setup
 
     ~pimqap_solver() {
+        events.reset();
         if (graph) cudaGraphExecDestroy(graph);
         if (ev0) cudaEventDestroy(ev0);
         if (ev1) cudaEventDestroy(ev1);
@@ -237,6 +241,8 @@ pimqap_status check_params(const pimqap_instance *inst, const pimqap_params *p) 
     if (!(p->beta_ratio > 0) || !std::isfinite(p->beta_ratio))
         return fail(PIMQAP_ERR_ARG, "beta_ratio must be a positive finite number");
     if (p->max_megaiters < 0) return fail(PIMQAP_ERR_ARG, "max_megaiters must be >= 0");
+    if (p->event_capacity < 0 || p->event_perm_capacity < 0)
+        return fail(PIMQAP_ERR_ARG, "event capacities must be >= 0");
     if (p->force_bits != 0 && p->force_bits != 32 && p->force_bits != 64)
         return fail(PIMQAP_ERR_ARG, "force_bits must be 0, 32 or 64");
     if (p->threads_per_block != 0 && p->threads_per_block != 64 && p->threads_per_block != 128 &&
@@ -395,13 +401,14 @@ void fill_head(const pimqap_instance *inst, const pimqap_params *params, const P
 
 pimqap_status stage_instance(const pimqap_instance *inst, const pimqap_params *params,
                              const Plan &P, char *base, SolveDev *out, cudaStream_t q,
-                             std::vector<std::vector<char>> &keep) {
+                             std::vector<std::vector<char>> &keep, const EventLink *ev) {
     keep.emplace_back(P.head, 0);
     char *mirror = keep.back().data();
     fill_head(inst, params, P, mirror);
     carve_instance(P, base, base + P.head, out);
     out->goal = params->goal;
     out->seed = params->seed;
+    if (ev) out->ev = *ev;
     PQ_CUDA(cudaMemcpyAsync(base, mirror, P.head, cudaMemcpyHostToDevice, q));
     PQ_CUDA(cudaMemsetAsync(base + P.head, 0, P.tail, q));
     PQ_CUDA(pimqap::launch_setup(*out, P.bits, q));
@@ -490,8 +497,19 @@ pimqap_status pimqap_solver_create(const pimqap_instance *inst, const pimqap_par
     PQ_CUDA(cudaEventCreate(&s->ev0));
     PQ_CUDA(cudaEventCreate(&s->ev1));
     cudaStream_t q = s->stream;
+    if (params->event_capacity > 0) {
+        s->events.reset(new pimqap::detail::EventBuffer());
+        const unsigned pcap = params->goal_print > 0
+                                  ? (unsigned)(params->event_perm_capacity > 0 ? params->event_perm_capacity : 256)
+                                  : 0u;
+        // goalPrint acts only when positive (CPU_PIM.cpp:273)
+        st = s->events->allocate((unsigned)params->event_capacity, pcap, plan.n,
+                                 params->goal_print > 0 ? params->goal_print : 0, q);
+        if (st != PIMQAP_OK) return st;
+    }
     std::vector<std::vector<char>> keep;
-    st = stage_instance(inst, params, plan, reinterpret_cast<char *>(s->dmem), &s->dev, q, keep);
+    st = stage_instance(inst, params, plan, reinterpret_cast<char *>(s->dmem), &s->dev, q, keep,
+                        s->events ? &s->events->link : nullptr);
     if (st != PIMQAP_OK) return st;
     SolveDev &d = s->dev;
     s->h2d = plan.h2d_bytes;
@@ -502,6 +520,11 @@ pimqap_status pimqap_solver_create(const pimqap_instance *inst, const pimqap_par
     PQ_CUDA(cudaMemcpy(&err, d.error, 4, cudaMemcpyDeviceToHost));
     s->d2h += 4;
     if (err) return fail(PIMQAP_ERR_DEVICE, "device check failed during setup");
+    if (s->events) {
+        PQ_CUDA(cudaMemcpy(&s->start_ns, d.start_ns, 8, cudaMemcpyDeviceToHost));
+        st = s->events->drain(q, s->start_ns, true);
+        if (st != PIMQAP_OK) return st;
+    }
     *out = guard.release();
     return PIMQAP_OK;
 }
@@ -549,6 +572,10 @@ pimqap_status pimqap_solver_run(pimqap_solver *s, int64_t megaiters, double *dev
         ms_total += ms;
         left -= g;
         if (stop != pimqap::kNoStop) s->stopped_goal = true;
+        if (s->events) {
+            pimqap_status est = s->events->drain(s->stream, s->start_ns, true);
+            if (est != PIMQAP_OK) return est;
+        }
         if (s->p.timeout_s > 0) {
             const double el = std::chrono::duration<double>(std::chrono::steady_clock::now() - wall0).count();
             if (el >= s->p.timeout_s) break;
@@ -649,6 +676,30 @@ pimqap_status pimqap_solver_group(pimqap_solver *s, int32_t t, int32_t *order,
     if (order) PQ_CUDA(cudaMemcpy(order, s->dev.order + (size_t)t * s->cap, (size_t)s->cap * 4, cudaMemcpyDeviceToHost));
     if (time_since_swap) PQ_CUDA(cudaMemcpy(time_since_swap, s->dev.tss + t, 4, cudaMemcpyDeviceToHost));
     if (group_best) PQ_CUDA(cudaMemcpy(group_best, s->dev.group_best + t, 8, cudaMemcpyDeviceToHost));
+    return PIMQAP_OK;
+}
+
+pimqap_status pimqap_solver_events(pimqap_solver *s, int64_t first, int32_t capacity,
+                                   pimqap_event *events, int32_t *count, int64_t *total,
+                                   int64_t *dropped) {
+    if (!s || !count || capacity < 0 || first < 0 || (capacity > 0 && !events))
+        return fail(PIMQAP_ERR_ARG, "bad event arguments");
+    *count = 0;
+    const int64_t have = s->events ? (int64_t)s->events->events.size() : 0;
+    if (total) *total = have;
+    if (dropped) *dropped = s->events ? s->events->dropped : 0;
+    if (first >= have) return PIMQAP_OK;
+    const int64_t k = std::min<int64_t>(capacity, have - first);
+    std::memcpy(events, s->events->events.data() + first, sizeof(pimqap_event) * (size_t)k);
+    *count = (int32_t)k;
+    return PIMQAP_OK;
+}
+
+pimqap_status pimqap_solver_event_perm(pimqap_solver *s, int32_t perm_index, int32_t *perm) {
+    if (!s || !perm) return fail(PIMQAP_ERR_ARG, "null solver or permutation");
+    if (!s->events || perm_index < 0 || (size_t)perm_index * s->n >= s->events->perms.size())
+        return fail(PIMQAP_ERR_ARG, "no permutation with that index");
+    std::memcpy(perm, s->events->perms.data() + (size_t)perm_index * s->n, 4 * (size_t)s->n);
     return PIMQAP_OK;
 }
 

@@ -22,6 +22,31 @@ enum : int32_t {
     kErrHostLost = 8,     // serving: the host's heartbeat stopped
 };
 
+// One progress event, appended by the device for the reference's log lines.
+//   kind_slot == -1: the tracking step of mega-iteration `megaiter` found replica `replica`
+//                    of group `group` below the group's best (CPU_PIM.cpp:297-314); one event
+//                    per lowering, in replica order, as the reference prints them.
+//   kind_slot >= -2: a sweep of mega-iteration `megaiter` lowered the replica's best below
+//                    goal_print (CPU_PIM.cpp:271-282); >= 0 is the slot of its permutation
+//                    in EventLink::perm, -2 means the permutation store was full.
+struct EventDev {
+    int32_t megaiter, group, replica, kind_slot;
+    int64_t energy;
+    unsigned long long ns;     // %globaltimer
+    int32_t tag, pad;          // batch member index (0 for a single solve)
+};
+
+// Where a solve appends its events (log == nullptr: no events).  Several solves of a batch
+// may share one log and tell their events apart by tag.
+struct EventLink {
+    EventDev *log;
+    int32_t *perm;             // [pcap][n] permutations of goal_print events
+    unsigned int *count;       // [2] events appended, permutation slots taken (may pass caps)
+    unsigned int cap, pcap;
+    int64_t goal_print;        // 0: no goal_print events
+    int32_t tag, pad;
+};
+
 // Everything one solve (one instance, T groups x R replicas) keeps in device memory.
 // Arrays are indexed by replica slot rep = t * R + l or by group t.
 struct SolveDev {
@@ -51,6 +76,7 @@ struct SolveDev {
     unsigned long long *target_ns;  // [1]  %globaltimer at that tracking
     unsigned long long *start_ns;   // [1]  %globaltimer when sweeping started
     int32_t *error;            // [1]       kErr* bits
+    EventLink ev;              // progress events (optional)
 };
 
 // Compact per-instance result of a batch.

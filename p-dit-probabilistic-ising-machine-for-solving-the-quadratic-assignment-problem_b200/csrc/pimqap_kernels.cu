@@ -256,6 +256,10 @@ __device__ void track_exchange(const SolveDev &s, int g, int e_next) {
             found = true;
             gb = b;
             tss = 0;
+            if (s.ev.log) {
+                const unsigned idx = atomicAdd(s.ev.count, 1u);
+                if (idx < s.ev.cap) s.ev.log[idx] = EventDev{e_next, g, l, -1, b, globaltimer_ns(), s.ev.tag, 0};
+            }
         }
     }
     if (found) atomicMin((long long *)s.single_best, (long long)gb);
@@ -389,7 +393,21 @@ template <int CL> __device__ __forceinline__ void cluster_sync(const Grp &G) {
 // CPU_PIM.cpp:195-290), store the state back.  With CL > 1 this CTA is rank `rank` of the
 // replica's cluster and G is the whole CTA.  Replica state is read through L2 (__ldcg): the
 // previous epoch may have run on another SM.  Returns false when a bounded wait gave up.
-template <class IT, int CL, bool SYM>
+// A replica's best fell below goal_print during a sweep of mega-iteration e (the reference
+// prints the replica and its permutation, CPU_PIM.cpp:271-282).  One thread claims a
+// permutation slot and appends the event; the CTA fills the slot after its next barrier.
+// Returns the slot, or -1 when the permutation store is full.
+__device__ __forceinline__ int goal_print_claim(const EventLink &v, int g, int l, int e, int64_t E) {
+    if (!v.log) return -1;
+    const unsigned slot = atomicAdd(v.count + 1, 1u);
+    const bool stored = slot < v.pcap;
+    const unsigned idx = atomicAdd(v.count, 1u);
+    if (idx < v.cap)
+        v.log[idx] = EventDev{e, g, l, stored ? (int32_t)slot : -2, E, globaltimer_ns(), v.tag, 0};
+    return stored ? (int)slot : -1;
+}
+
+template <class IT, int CL, bool SYM, bool GP = false>
 __device__ bool replica_epoch(const SolveDev &s, int rep, int rank, int e, const Grp &G,
                               unsigned char *smem) {
     using U = typename Unsigned<IT>::type;
@@ -422,7 +440,7 @@ __device__ bool replica_epoch(const SolveDev &s, int rep, int rank, int e, const
     IT *s_red = reinterpret_cast<IT *>(smem + L.red);
     double *s_wsum = reinterpret_cast<double *>(smem + L.wsum);
     double *s_r = reinterpret_cast<double *>(smem + L.r);
-    int *s_misc = reinterpret_cast<int *>(smem + L.misc);   // [0] pick, [1] improved-at, [2] error
+    int *s_misc = reinterpret_cast<int *>(smem + L.misc);   // [0] pick, [1] improved-at, [2] error, [3] goal-print slot
     unsigned long long *s_bar = reinterpret_cast<unsigned long long *>(smem + L.bar);
     const int nDc = rpc / 4, nFc = npad / 4;                 // 16-byte chunks of a D slice / F row
 
@@ -649,7 +667,12 @@ __device__ bool replica_epoch(const SolveDev &s, int rep, int rank, int e, const
             ++accepts;
             if (E < bestE) {                                 // :271-272
                 bestE = E;
-                if (tid == 0) s_misc[1] = upd;
+                if (tid == 0) {
+                    s_misc[1] = upd;
+                    if constexpr (GP) {
+                        if (E < s.ev.goal_print && rank == 0) s_misc[3] = goal_print_claim(s.ev, g, l, e, E);
+                    }
+                }
             }
             // I[k][c] += (D[k][j]-D[k][i])(F[c][b]-F[c][a]) + (D[j][k]-D[i][k])(F[b][c]-F[a][c])
             for (int cv = tid % nvec, k0r = tid / nvec, kstep = max(1, BT / nvec);
@@ -689,6 +712,13 @@ __device__ bool replica_epoch(const SolveDev &s, int rep, int rank, int e, const
             G.sync();                                 // S5: new rows and phi visible
             if (s_misc[1] == upd) {
                 for (int q = tid; q < n; q += BT) s_bphi[q] = s_phi[q];
+                if constexpr (GP) {
+                    if (E < s.ev.goal_print && rank == 0) {
+                        const int slot = s_misc[3];
+                        if (slot >= 0)
+                            for (int q = tid; q < n; q += BT) s.ev.perm[(size_t)slot * n + q] = s_phi[q];
+                    }
+                }
             }
         }
     }
@@ -725,8 +755,8 @@ __device__ bool replica_epoch(const SolveDev &s, int rep, int rank, int e, const
 
 // Solve path: one launch = one epoch of every replica of the solve (grid = T*R*CL CTAs);
 // the last replica of each group to finish runs the group's tracking + exchange.
-template <class IT, int CL, bool SYM>
-__global__ void __launch_bounds__(256) epoch_kernel(SolveDev s) {
+template <class IT, int CL, bool SYM, bool GP>
+__global__ void __launch_bounds__(256, CL == 4 ? 2 : 1) epoch_kernel(SolveDev s) {
     extern __shared__ __align__(16) unsigned char smem[];
     int rank = 0;
     if constexpr (CL > 1) rank = (int)cg::this_cluster().block_rank();
@@ -738,7 +768,7 @@ __global__ void __launch_bounds__(256) epoch_kernel(SolveDev s) {
     if (e >= *(volatile int32_t *)s.stop_epoch) return;
     const Grp G{(int)threadIdx.x, (int)blockDim.x, (int)(threadIdx.x & 31), (int)(threadIdx.x >> 5),
                 (int)(blockDim.x >> 5), 0};
-    const bool ok = replica_epoch<IT, CL, SYM>(s, rep, rank, e, G, smem);
+    const bool ok = replica_epoch<IT, CL, SYM, GP>(s, rep, rank, e, G, smem);
     __syncthreads();
     if (ok && rank == 0 && threadIdx.x == 0) {
         const unsigned prev = atomicAdd(s.finish + g, 1u);
@@ -1154,17 +1184,19 @@ cudaError_t launch_collect(const SolveDev *inst, int count, BatchResultDev *out,
 
 // ------------------------------------------------------------------ launchers
 
-template <class IT, int CL, bool SYM> static void *epoch_fn() {
-    return reinterpret_cast<void *>(&epoch_kernel<IT, CL, SYM>);
+template <class IT, int CL, bool SYM> static void *epoch_fn(bool gp) {
+    return gp ? reinterpret_cast<void *>(&epoch_kernel<IT, CL, SYM, true>)
+              : reinterpret_cast<void *>(&epoch_kernel<IT, CL, SYM, false>);
 }
 
-static void *epoch_kernel_ptr(int bits, int cl, bool sym) {
-#define PIMQAP_PICK(IT)                                                        \
-    switch (cl) {                                                              \
-        case 1: return sym ? epoch_fn<IT, 1, true>() : epoch_fn<IT, 1, false>(); \
-        case 2: return sym ? epoch_fn<IT, 2, true>() : epoch_fn<IT, 2, false>(); \
-        case 4: return sym ? epoch_fn<IT, 4, true>() : epoch_fn<IT, 4, false>(); \
-        default: return nullptr;                                               \
+// gp: the variant that records goal_print events (solver handles with goal_print set).
+static void *epoch_kernel_ptr(int bits, int cl, bool sym, bool gp) {
+#define PIMQAP_PICK(IT)                                                              \
+    switch (cl) {                                                                    \
+        case 1: return sym ? epoch_fn<IT, 1, true>(gp) : epoch_fn<IT, 1, false>(gp); \
+        case 2: return sym ? epoch_fn<IT, 2, true>(gp) : epoch_fn<IT, 2, false>(gp); \
+        case 4: return sym ? epoch_fn<IT, 4, true>(gp) : epoch_fn<IT, 4, false>(gp); \
+        default: return nullptr;                                                     \
     }
     if (bits == 32) { PIMQAP_PICK(int32_t) }
     if (bits == 64) { PIMQAP_PICK(int64_t) }
@@ -1238,11 +1270,12 @@ cudaError_t prepare_kernels() {
     if (err != cudaSuccess) return err;
     for (int bits : {32, 64})
         for (int cl : {1, 2, 4})
-            for (int sym = 0; sym < 2; ++sym) {
-                err = cudaFuncSetAttribute(epoch_kernel_ptr(bits, cl, sym != 0),
-                                           cudaFuncAttributeMaxDynamicSharedMemorySize, maxsm);
-                if (err != cudaSuccess) return err;
-            }
+            for (int sym = 0; sym < 2; ++sym)
+                for (int gp = 0; gp < 2; ++gp) {
+                    err = cudaFuncSetAttribute(epoch_kernel_ptr(bits, cl, sym != 0, gp != 0),
+                                               cudaFuncAttributeMaxDynamicSharedMemorySize, maxsm);
+                    if (err != cudaSuccess) return err;
+                }
     for (int bits : {32, 64})
         for (int cl : {1, 2, 4}) {
             err = cudaFuncSetAttribute(batch_fn(bits, cl), cudaFuncAttributeMaxDynamicSharedMemorySize, maxsm);
@@ -1267,7 +1300,7 @@ cudaError_t launch_setup(const SolveDev &s, int bits, cudaStream_t st) {
 
 cudaError_t launch_epoch(const SolveDev &s, int bits, int cluster, bool sym, int threads,
                          size_t smem, cudaStream_t st) {
-    void *fn = epoch_kernel_ptr(bits, cluster, sym);
+    void *fn = epoch_kernel_ptr(bits, cluster, sym, s.ev.log != nullptr && s.ev.goal_print != 0);
     if (!fn) return cudaErrorInvalidValue;
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3((unsigned)(s.T * s.R * cluster));

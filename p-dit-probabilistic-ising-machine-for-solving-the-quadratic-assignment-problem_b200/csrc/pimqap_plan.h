@@ -78,10 +78,11 @@ void fill_head(const pimqap_instance *inst, const pimqap_params *params, const P
                char *mirror);
 
 // Head upload + tail clear + setup kernels for one instance in `base` (P.total bytes) on
-// stream q.  The host image is kept in `keep` until the caller syncs q.
+// stream q.  The host image is kept in `keep` until the caller syncs q.  `ev` (may be null)
+// is the event log the solve appends to.
 pimqap_status stage_instance(const pimqap_instance *inst, const pimqap_params *params,
                              const Plan &P, char *base, SolveDev *out, cudaStream_t q,
-                             std::vector<std::vector<char>> &keep);
+                             std::vector<std::vector<char>> &keep, const EventLink *ev = nullptr);
 
 }  // namespace detail
 }  // namespace pimqap

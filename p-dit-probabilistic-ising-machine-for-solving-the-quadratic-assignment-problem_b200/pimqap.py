@@ -45,8 +45,33 @@ class Params(C.Structure):
         ("seed", C.c_uint64), ("force_bits", C.c_int32), ("device", C.c_int32),
         ("megaiters_per_launch", C.c_int32), ("threads_per_block", C.c_int32),
         ("cluster_size", C.c_int32), ("beta_internal", C.c_int32), ("auto_beta", C.c_int32),
-        ("auto_lower", C.c_double), ("auto_higher", C.c_double),
+        ("auto_lower", C.c_double), ("auto_higher", C.c_double), ("goal_print", C.c_int64),
+        ("event_capacity", C.c_int32), ("event_perm_capacity", C.c_int32),
     ]
+
+
+EVENT_GROUP_BEST = 0
+EVENT_GOAL_PRINT = 1
+AUTO_STEPS = 32
+AUTO_TRIALS = 5
+
+
+class Event(C.Structure):
+    _fields_ = [("megaiter", C.c_int64), ("energy", C.c_int64), ("time_ms", C.c_double),
+                ("kind", C.c_int32), ("group", C.c_int32), ("replica", C.c_int32),
+                ("perm_index", C.c_int32), ("trial", C.c_int32), ("pad", C.c_int32)]
+
+
+class AutoReport(C.Structure):
+    _fields_ = [("beta0_internal", C.c_double), ("delta_beta", C.c_double),
+                ("min_beta", C.c_double), ("max_beta", C.c_double),
+                ("min_beta_printed", C.c_int32), ("pad0", C.c_int32),
+                ("avg_energy", C.c_double * AUTO_STEPS),
+                ("trial_best", C.c_int64 * (AUTO_STEPS * AUTO_TRIALS)),
+                ("steps_printed", C.c_int32), ("goal_trial", C.c_int32),
+                ("best_energy", C.c_int64), ("best_perm", C.POINTER(C.c_int32)),
+                ("events", C.POINTER(Event)), ("event_capacity", C.c_int32),
+                ("event_count", C.c_int32), ("events_dropped", C.c_int64), ("device_ms", C.c_double)]
 
 
 class Result(C.Structure):
@@ -126,6 +151,13 @@ def lib() -> C.CDLL:
     L.pimqap_auto_beta.argtypes = [C.POINTER(Instance), C.POINTER(Params), C.POINTER(C.c_double),
                                    C.POINTER(C.c_double), C.c_void_p, C.POINTER(C.c_int64), C.c_void_p]
     L.pimqap_auto_beta.restype = st
+    L.pimqap_solver_events.argtypes = [C.c_void_p, C.c_int64, C.c_int32, C.POINTER(Event),
+                                       C.POINTER(C.c_int32), C.POINTER(C.c_int64), C.POINTER(C.c_int64)]
+    L.pimqap_solver_events.restype = st
+    L.pimqap_solver_event_perm.argtypes = [C.c_void_p, C.c_int32, C.c_void_p]
+    L.pimqap_solver_event_perm.restype = st
+    L.pimqap_auto_beta_report.argtypes = [C.POINTER(Instance), C.POINTER(Params), C.POINTER(AutoReport)]
+    L.pimqap_auto_beta_report.restype = st
     L.pimqap_solve_static.argtypes = [C.POINTER(Instance), C.POINTER(Params), C.POINTER(Result)]
     L.pimqap_solve_static.restype = st
     L.pimqap_probe_smem_bandwidth.argtypes = [C.c_int32, C.POINTER(C.c_double)]
@@ -210,6 +242,31 @@ def auto_beta(F: np.ndarray, D: np.ndarray, params: Params) -> dict:
                 best_perm=perm)
 
 
+def _event_dict(e: Event) -> dict:
+    return dict(megaiter=int(e.megaiter), energy=int(e.energy), time_ms=float(e.time_ms),
+                kind=int(e.kind), group=int(e.group), replica=int(e.replica),
+                perm_index=int(e.perm_index), trial=int(e.trial))
+
+
+def auto_beta_report(F: np.ndarray, D: np.ndarray, params: Params, event_capacity: int = 1 << 16) -> dict:
+    """pimqap_auto_beta_report: everything automatic mode prints and decides."""
+    inst = _Inst(F, D)
+    rep = AutoReport()
+    perm = np.zeros(inst.F.shape[0], np.int32)
+    evs = (Event * max(1, event_capacity))()
+    rep.best_perm = perm.ctypes.data_as(C.POINTER(C.c_int32))
+    rep.events = evs
+    rep.event_capacity = event_capacity
+    _check(lib().pimqap_auto_beta_report(C.byref(inst.c), C.byref(params), C.byref(rep)))
+    return dict(beta0=rep.beta0_internal, delta_beta=rep.delta_beta, min_beta=rep.min_beta,
+                max_beta=rep.max_beta, min_beta_printed=bool(rep.min_beta_printed),
+                avg_energy=np.array(rep.avg_energy[:]),
+                trial_best=np.array(rep.trial_best[:], np.int64), steps_printed=rep.steps_printed,
+                goal_trial=rep.goal_trial, best_energy=rep.best_energy, best_perm=perm,
+                events=[_event_dict(evs[k]) for k in range(rep.event_count)],
+                events_dropped=rep.events_dropped, device_ms=rep.device_ms)
+
+
 def solve_static(F: np.ndarray, D: np.ndarray, params: Params) -> dict:
     """pimqap_solve_static: the same solve with no device allocation (fixed 8 MiB scratch)."""
     inst = _Inst(F, D)
@@ -275,6 +332,23 @@ class Solver:
         _check(lib().pimqap_solver_replica(self.h, t, l, phi.ctypes.data, I.ctypes.data,
                                            E.ctypes.data, bE.ctypes.data, b.ctypes.data))
         return dict(phi=phi, I=I, E=int(E[0]), bestE=int(bE[0]), beta=float(b[0]))
+
+    def events(self, first: int = 0) -> List[dict]:
+        """Progress events recorded so far (params.event_capacity > 0), in the reference's order."""
+        total = C.c_int64(0)
+        dropped = C.c_int64(0)
+        count = C.c_int32(0)
+        _check(lib().pimqap_solver_events(self.h, 0, 0, None, C.byref(count), C.byref(total), C.byref(dropped)))
+        k = max(0, total.value - first)
+        buf = (Event * max(1, k))()
+        _check(lib().pimqap_solver_events(self.h, first, k, buf, C.byref(count), None, None))
+        self.events_dropped = dropped.value
+        return [_event_dict(buf[i]) for i in range(count.value)]
+
+    def event_perm(self, perm_index: int) -> np.ndarray:
+        perm = np.zeros(self.n, np.int32)
+        _check(lib().pimqap_solver_event_perm(self.h, perm_index, perm.ctypes.data))
+        return perm
 
     def group(self, t: int, rank_slots: int) -> dict:
         order = np.zeros(rank_slots, np.int32)

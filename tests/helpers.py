@@ -82,3 +82,34 @@ def oracle_auto_beta(oracle, F, D, *, T, R, spe, seed, cap, lower=0.1, higher=0.
             maxBeta = 2.0 ** (-30 + j + 2)
             return maxBeta, (maxBeta / minBeta) ** (1.0 / R), sums, best
     raise AssertionError("no range")
+
+
+NO_BEST = 2147483647
+
+
+def oracle_cli_trace(oracle, F, D, *, T, R, spe, beta0, ratio, seed, megaiters, goal=0,
+                     single=NO_BEST, cap=10):
+    """What the reference's threadToRun loop (CPU_PIM.cpp:292-362) prints, restated on the
+    oracle with lock-step groups: the "Best Energy Found" energies in (mega-iteration, group,
+    replica) order, each group's sweep<t>.txt pairs [m, threadBestE], and the final single
+    best.  `single` is the best carried in (automatic mode's trials share it)."""
+    st = oracle.setup(D, F, T, R, spe, beta0, ratio, seed, cap=cap)
+    thread = [NO_BEST] * T
+    lines, sweeps = [], {t: [] for t in range(T)}
+    for m in range(megaiters):
+        bestE = st.bestE.copy()
+        for t in range(T):
+            found = False
+            for l in range(R):
+                if bestE[t, l] < thread[t]:
+                    thread[t] = int(bestE[t, l])
+                    found = True
+                    if thread[t] < single:
+                        single = thread[t]
+                        lines.append(single)
+            if found:
+                sweeps[t].append([m, thread[t]])
+        if single <= goal:
+            break
+        oracle.run(st, D, F, 1, -(1 << 62))
+    return lines, sweeps, single
