@@ -337,8 +337,8 @@ def run_batch_suite(args):
     (gap <= 0.1 %), for the batch and for the plain form (one pimqap_solve per instance, one
     instance per launch), the latter timed on every 16th instance and scaled to 512."""
     import pimqap
-    batch = instances.uniform_batch(512)
-    M = 500
+    batch = instances.uniform_batch(args.batch_instances)
+    M = max(1, args.batch_sweeps // 4)
     b0, ratio = LADDER_UNIFORM
 
     def params(seed, **kw):
@@ -351,6 +351,10 @@ def run_batch_suite(args):
     fixed = pimqap.batch_solve(pairs, [params(k + 1, max_megaiters=M) for k in range(len(batch))])
     fixed_wall = time.perf_counter() - t0
     props = sum(_sweeps_proposals(b.n, 32, 4 * M) for b in batch)
+    if args.batch_fixed_only:   # the fixed-work batch alone (profiling)
+        print(json.dumps({"suite": "batch", "instances": len(batch), "sweeps": 4 * M, "wall_s": fixed_wall,
+                          "proposals_per_s_wall": props / fixed_wall}))
+        return
     t0 = time.perf_counter()
     longrun = pimqap.batch_solve(pairs, [params(10 ** 6 + k, max_megaiters=2 * M) for k in range(len(batch))])
     long_wall = time.perf_counter() - t0
@@ -395,7 +399,10 @@ def run_serve_suite(args):
         return pimqap.default_params(replicas=32, groups=1, sweeps_per_exchange=4, beta_max=b0,
                                      beta_ratio=ratio, beta_internal=1, seed=k + 1, max_megaiters=500)
 
-    sample = [(inst.F, inst.D, params(inst, k)) for k, (_, inst) in enumerate(trace[:64])]
+    # the autotuner's sample: 64 requests spread over the trace (it picks classes and SM shares
+    # from them; shapes it misses still get a launch of their own)
+    step = max(1, len(trace) // 64)
+    sample = [(inst.F, inst.D, params(inst, k)) for k, (_, inst) in enumerate(trace) if k % step == 0][:64]
     srv = pimqap.Server(sample=sample)
     t_start = time.perf_counter()
     tickets = []
@@ -444,6 +451,10 @@ def main():
     ap.add_argument("--threads", type=int, default=0, help="threads per CTA (0 = automatic)")
     ap.add_argument("--suite", choices=["headline", "batch", "serve"], default="headline",
                     help="headline: the n=256 workload (the driver's line); batch / serve: the other workloads")
+    ap.add_argument("--batch-instances", type=int, default=512, help="batch suite: instances")
+    ap.add_argument("--batch-sweeps", type=int, default=2000, help="batch suite: sweeps per instance")
+    ap.add_argument("--batch-fixed-only", action="store_true",
+                    help="batch suite: run only the fixed-work batch (profiling)")
     ap.add_argument("--rate", type=float, default=200.0, help="serve suite: arrivals per second")
     ap.add_argument("--duration", type=float, default=5.0, help="serve suite: seconds of arrivals")
     ap.add_argument("--drain", type=float, default=180.0, help="serve suite: seconds allowed after arrivals end")

@@ -270,8 +270,8 @@ pimqap_status pimqap_server_poll(pimqap_server *s, int64_t ticket, pimqap_result
 pimqap_status pimqap_server_wait(pimqap_server *s, int64_t ticket, double timeout_s,
                                  pimqap_result *result);
 pimqap_status pimqap_server_stats_get(pimqap_server *s, pimqap_server_stats *stats);
-/* Waits for admitted requests to finish, stops the launches and frees the device memory;
-   pending requests that were never admitted are dropped. */
+/* Stops the launches and frees the device memory.  Requests not finished yet are abandoned
+   (their tickets become invalid): wait for the ones whose results are needed first. */
 void pimqap_server_destroy(pimqap_server *s);
 
 /* Host-side fault injection for tests: stall != 0 stops the server thread's heartbeat, so

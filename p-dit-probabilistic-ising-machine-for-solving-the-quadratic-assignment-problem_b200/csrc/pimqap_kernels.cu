@@ -864,13 +864,14 @@ __device__ unsigned long long queue_next(const BatchDev &B, unsigned long long &
     unsigned long long t0 = globaltimer_ns();
     unsigned long long beat = B.serving ? *B.link.heartbeat : 0;
     for (;;) {
+        const int32_t sd = *B.shutdown;   // 1: drain, then leave; 2: leave now
+        if (sd == 2) return kDoneItem;    // even with work queued (the host abandons it)
         if (*((volatile unsigned long long *)B.q_seq + slot) == ticket + 1) {
             __threadfence();
             ticket = kNoTicket;
             return *((volatile unsigned long long *)B.q_items + slot);
         }
-        const int32_t sd = *B.shutdown;   // 1: drain, then leave; 2: leave now
-        if (sd == 2 || (sd != 0 && *(volatile int32_t *)B.active == 0)) return kDoneItem;
+        if (sd != 0 && *(volatile int32_t *)B.active == 0) return kDoneItem;
         if (B.serving) {
             const unsigned long long adm = inbox_claim(B);
             if (adm) return adm;

@@ -107,10 +107,12 @@ struct Request {
     std::vector<int32_t> perm;
     std::vector<int64_t> energies;
     int64_t maxm = 0;
+    double work = 0;           // estimated cost, counted in its class's load until it completes
 };
 
 struct ServeClass {
     BatchClass shape;
+    double load = 0;           // estimated cost of the requests routed here and not yet done
     int slots = 0;
     std::vector<int> free_slots;
     std::vector<int64_t> slot_ticket;
@@ -286,23 +288,46 @@ pimqap_status open_class(Server &S, ServeClass &C) {
 
 // The class that runs a request most cheaply: exact force width first, then the smallest
 // cluster and slice that fit.  The request is re-planned for that class's width and cluster.
+// Whether an instance needing `bits`-wide forces can run in a launch of shape sh (and its
+// plan there, in *out).
+bool class_fits(const BatchClass &sh, const pimqap_instance &inst, const pimqap_params &params,
+                const InstanceInfo &info, int bits, int maxsm, Plan *out = nullptr) {
+    if (sh.bits < bits) return false;
+    pimqap_params p = params;
+    p.force_bits = sh.bits;
+    Plan P;
+    if (plan_instance(&inst, &p, (size_t)maxsm, sh.cl, &P, &info) != PIMQAP_OK) return false;
+    const size_t need = sh.cl == 1 ? pimqap::batch_slice_bytes(P.n, sh.bits) : 16 + P.smem;
+    if (need > sh.slice) return false;
+    if (out) *out = P;
+    return true;
+}
+
+// The class a request joins: among the launches it fits, the one that would finish the work
+// routed to it (this request included) first, by estimated cost per SM of the launch.  The
+// request's cost is added to that class's load (under S.mu) until it completes.
 int route(Server &S, Request &R) {
+    std::vector<std::pair<int, double>> fits;
+    for (int c = 0; c < (int)S.classes.size(); ++c) {
+        Plan P;
+        if (!class_fits(S.classes[c].shape, R.inst, R.params, R.info, R.plan.bits, S.maxsm, &P)) continue;
+        fits.push_back({c, instance_work(P, std::min<int64_t>(R.params.max_megaiters, 1000000))});
+    }
+    std::lock_guard<std::mutex> lk(S.mu);
     int best = -1;
     double best_cost = 1e300;
-    for (int c = 0; c < (int)S.classes.size(); ++c) {
-        const BatchClass &sh = S.classes[c].shape;
-        if (sh.bits < R.plan.bits) continue;
-        pimqap_params p = R.params;
-        p.force_bits = sh.bits;
-        Plan P;
-        if (plan_instance(&R.inst, &p, (size_t)S.maxsm, sh.cl, &P, &R.info) != PIMQAP_OK) continue;
-        const size_t need = sh.cl == 1 ? pimqap::batch_slice_bytes(P.n, sh.bits) : 16 + P.smem;
-        if (need > sh.slice) continue;
-        const double cost = (sh.bits == R.plan.bits ? 0 : 1e6) + sh.cl * 1e3 + (double)sh.slice / 1e6;
+    for (const auto &f : fits) {
+        const ServeClass &C = S.classes[f.first];
+        const double cost = (C.load + f.second) / std::max(1, C.shape.grid);
         if (cost < best_cost) {
             best_cost = cost;
-            best = c;
+            best = f.first;
         }
+    }
+    if (best >= 0) {
+        for (const auto &f : fits)
+            if (f.first == best) R.work = f.second;
+        S.classes[best].load += R.work;
     }
     return best;
 }
@@ -340,6 +365,7 @@ void release(Server &S, Request &R) {
     C.free_slots.push_back(R.slot);
     C.slot_ticket[R.slot] = 0;
     C.replicas_in_flight -= (size_t)R.plan.T * R.plan.R;
+    C.load = std::max(0.0, C.load - R.work);
 }
 
 // One pass of admissions in arrival order: every pending request whose class has a free slot
@@ -359,7 +385,13 @@ bool admit_some(Server &S) {
             }
         if (stg < 0) break;
         size_t off = 0;
-        if (C.free_slots.empty() || C.replicas_in_flight + reps > C.qcap - 1 ||
+        // At most about two rounds of the launch's workers in flight: the queue serves the
+        // admitted instances' epochs in turn, so admitting more only spreads the workers over
+        // more requests and delays them all (the rest wait here, in arrival order).
+        const size_t workers = C.shape.cl == 1 ? (size_t)C.shape.grid * C.shape.workers
+                                               : (size_t)(C.shape.grid / C.shape.cl);
+        const bool crowded = C.replicas_in_flight > 0 && C.replicas_in_flight + reps > 2 * workers;
+        if (C.free_slots.empty() || crowded || C.replicas_in_flight + reps > C.qcap - 1 ||
             !S.arena.alloc(R.plan.total, &off)) {
             ++it;
             continue;
@@ -437,13 +469,7 @@ void serve_loop(Server *S) {
         }
         bool busy = complete_some(*S);
         busy |= admit_some(*S);
-        if (S->stopping.load()) {
-            std::lock_guard<std::mutex> lk(S->mu);
-            bool inflight = false;
-            for (auto &C : S->classes)
-                if (C.replicas_in_flight) inflight = true;
-            if (!inflight || err) break;
-        }
+        if (S->stopping.load()) break;   // destroy: running requests are abandoned
         if (!busy) std::this_thread::sleep_for(std::chrono::microseconds(100));
     }
 }
@@ -503,6 +529,37 @@ pimqap_status pimqap_server_create(const pimqap_server_config *config, pimqap_se
         megaiters[k] = sparams[k].max_megaiters;
     }
     std::vector<BatchClass> shapes = plan_classes(plans, megaiters, S.sms, S.maxsm, 0);
+    if (config->sample && config->sample_count > 0) {
+        // Every shape a request can have (n <= PIMQAP_MAX_N, int32 or int64 forces) must find a
+        // resident launch: shapes of the built-in sample that no class from the caller's sample
+        // fits get a class of their own, with the smallest SM share.
+        std::vector<pimqap_instance> dsample;
+        std::vector<pimqap_params> dparams;
+        std::vector<std::vector<int32_t>> dkeep;
+        default_sample(dsample, dparams, dkeep);
+        std::vector<Plan> missing;
+        std::vector<int64_t> mmega;
+        for (size_t k = 0; k < dsample.size(); ++k) {
+            const InstanceInfo info = analyse(dsample[k].n, dsample[k].flow, dsample[k].dist);
+            Plan P;
+            st = plan_instance(&dsample[k], &dparams[k], (size_t)S.maxsm, 0, &P, &info);
+            if (st != PIMQAP_OK) return st;
+            bool fits = false;
+            for (const auto &c : shapes) fits = fits || class_fits(c, dsample[k], dparams[k], info, P.bits, S.maxsm);
+            if (!fits) {
+                missing.push_back(P);
+                mmega.push_back(1);
+            }
+        }
+        if (!missing.empty()) {
+            std::vector<BatchClass> extra = plan_classes(missing, mmega, S.sms, S.maxsm, 0);
+            for (auto &c : extra) {
+                c.work = 0;
+                c.members.clear();
+                shapes.push_back(c);
+            }
+        }
+    }
     // Resident side by side: each class gets a share of the SMs by work and one CTA per SM of
     // its share.  With no more CTAs than SMs in total, every CTA finds an SM it fits alone,
     // so no class is left without resident workers.  Cluster classes launch first.
@@ -596,9 +653,15 @@ pimqap_status pimqap_server_submit(pimqap_server *h, const pimqap_instance *inst
     st = plan_instance(&R->inst, &p, (size_t)S.maxsm, S.classes[R->cls].shape.cl, &R->plan, &R->info);
     if (st != PIMQAP_OK) return st;
     R->params.force_bits = p.force_bits;
-    if (carve_size(R->plan.total) > S.arena.size())
+    if (carve_size(R->plan.total) > S.arena.size()) {
+        {
+            std::lock_guard<std::mutex> lk(S.mu);
+            S.classes[R->cls].load = std::max(0.0, S.classes[R->cls].load - R->work);
+        }
         return fail(PIMQAP_ERR_BUSY, "request needs " + std::to_string(R->plan.total) +
-                                         " bytes of device memory; the budget is " + std::to_string(S.arena.size()));
+                                         " bytes of device memory; the budget is " +
+                                         std::to_string(S.arena.size()));
+    }
     R->t_submit = Clock::now();
     std::lock_guard<std::mutex> lk(S.mu);
     R->ticket = S.next_ticket++;
@@ -672,7 +735,8 @@ void pimqap_server_destroy(pimqap_server *h) {
     for (auto &C : S.classes)
         if (C.replicas_in_flight) inflight = true;
     for (auto &C : S.classes) {
-        // drain when nothing is in flight; leave at once after a device error
+        // drain when nothing is in flight; leave at once (abandoning running requests) when
+        // something is, or after a device error
         if (C.h_shutdown) *C.h_shutdown = (inflight || S.error_word.load()) ? 2 : 1;
         std::atomic_thread_fence(std::memory_order_seq_cst);
     }

@@ -89,3 +89,39 @@ def test_heartbeat_stall_stops_device_workers(gpu):
         assert e.value.status == 6
     finally:
         srv.close()                               # returns: the workers have already stopped
+
+
+def test_requests_outside_the_sample_still_find_a_launch(gpu):
+    """A server tuned on a sample of small int32 instances still serves a large int64 one
+    (classes for the uncovered shapes are added at creation)."""
+    small = instances.uniform(24, 5)
+    ps = gpu.default_params(replicas=4, groups=1, beta_max=0.02, beta_ratio=1.3, max_megaiters=3)
+    n = 240
+    rng = np.random.default_rng(11)
+    big = instances.Instance(n, rng.integers(0, 30_000_000, (n, n)), rng.integers(0, 100, (n, n)))
+    pb = gpu.default_params(replicas=3, groups=1, beta_max=1e-9, beta_ratio=1.3, seed=4, max_megaiters=2)
+    with gpu.Server(sample=[(small.F, small.D, ps)]) as srv:
+        t = srv.submit(big.F, big.D, pb)
+        r = srv.wait(t, 120.0)
+        assert srv.stats()["error_word"] == 0
+    solo = gpu.solve(big.F, big.D, pb)
+    assert r["force_bits"] == 64 and same(r, solo)
+
+
+def test_destroy_abandons_running_requests_promptly(gpu):
+    """Closing the server with long requests still running stops the resident launches at
+    once instead of running the requests to the end."""
+    inst = instances.uniform(96, 12)
+    p = gpu.default_params(replicas=16, groups=2, beta_max=0.02, beta_ratio=1.3, max_megaiters=10 ** 7)
+    srv = gpu.Server()
+    for k in range(6):
+        p.seed = k + 1
+        srv.submit(inst.F, inst.D, p)
+    time.sleep(0.5)
+    st = srv.stats()
+    assert st["admitted"] >= 1 and st["completed"] == 0 and st["error_word"] == 0, st
+    t0 = time.perf_counter()
+    srv.close()
+    assert time.perf_counter() - t0 < 10.0
+    r = gpu.solve(inst.F, inst.D, gpu.default_params(replicas=4, groups=1, max_megaiters=3))
+    assert r["megaiters_done"] == 3      # the device is usable afterwards
