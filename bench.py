@@ -436,6 +436,7 @@ def run_serve_suite(args):
             "p50_ms": pct(0.50), "p99_ms": pct(0.99), "max_ms": lat[-1] if lat else None,
             "throughput_req_per_s": len(done) / t_last if t_last else 0.0,
             "proposals_per_s": props / t_last if t_last else 0.0,
+            "admitted": st["admitted"], "pending_at_end": st["pending"],
             "classes": st["classes"], "error_word": st["error_word"]}
     print(json.dumps(line))
 

@@ -20,6 +20,7 @@ enum : int32_t {
     kErrShape = 2,        // launch shape does not match the solve
     kErrTimeout = 4,      // a bounded wait for a peer CTA's data or a queue item gave up
     kErrHostLost = 8,     // serving: the host's heartbeat stopped
+    kErrLaunchEnded = 16, // serving: a resident launch ended while serving (host-detected)
 };
 
 // One progress event, appended by the device for the reference's log lines.
@@ -119,6 +120,7 @@ struct ServeLink {
     volatile unsigned long long *heartbeat;   // [1] the host increments it while it serves
     unsigned long long heartbeat_limit_ns;    // idle workers exit when it stalls this long
     volatile int32_t *error_host;             // [1] copy of the error word for the host
+    volatile int32_t *resident;               // [grid] each CTA sets its entry when it starts
     SolveDev *inst_rw;                        // writable view of the device descriptor table
     int32_t *sym_rw;
     int64_t *maxm_rw;

@@ -159,6 +159,11 @@ __device__ __forceinline__ uint32_t cluster_addr(uint32_t cta_addr, int rank) {
 __device__ __forceinline__ void mbar_init(uint32_t bar, uint32_t count) {
     asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(count) : "memory");
 }
+// Ends an mbarrier's life, so the same shared-memory word can be initialised again for the
+// next replica a persistent worker runs.
+__device__ __forceinline__ void mbar_inval(uint32_t bar) {
+    asm volatile("mbarrier.inval.shared::cta.b64 [%0];" ::"r"(bar) : "memory");
+}
 __device__ __forceinline__ void mbar_fence_init() {
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
 }
@@ -265,6 +270,10 @@ __device__ void track_exchange(const SolveDev &s, int g, int e_next) {
     if (found) atomicMin((long long *)s.single_best, (long long)gb);
     for (int l = 0; l < R - 1; ++l) {                        // :324-337
         const int i1 = order[l], i2 = order[l + 1];
+        if ((unsigned)i1 >= (unsigned)R || (unsigned)i2 >= (unsigned)R) {   // never in a valid state
+            atomicOr(s.error, kErrShape);
+            return;
+        }
         const double e1 = (double)E[i1], e2 = (double)E[i2];
         if (e1 < e2) {
             order[l] = i2;
@@ -277,6 +286,10 @@ __device__ void track_exchange(const SolveDev &s, int g, int e_next) {
     }
     if (tss > 100) {                                         // :339-344, slot cap-1
         const int i1 = order[cap - 1], i2 = order[0];
+        if ((unsigned)i1 >= (unsigned)R || (unsigned)i2 >= (unsigned)R) {
+            atomicOr(s.error, kErrShape);
+            return;
+        }
         order[cap - 1] = i2;
         order[0] = i1;
         const double tb = beta[i1];
@@ -464,8 +477,8 @@ __device__ bool replica_epoch(const SolveDev &s, int rep, int rank, int e, const
             s_phi[q] = p;
             s_bphi[q] = p;
             s_inv[q] = 0;
-            s_Dd[q] = q < n ? s.Ddiag[q] : 0;
-            s_Fd[q] = q < n ? s.Fdiag[q] : 0;
+            s_Dd[q] = q < n ? __ldcg(s.Ddiag + q) : 0;
+            s_Fd[q] = q < n ? __ldcg(s.Fdiag + q) : 0;
         }
         if (tid == 0) {
             s_misc[0] = 0x7fffffff;
@@ -726,6 +739,12 @@ __device__ bool replica_epoch(const SolveDev &s, int rep, int rank, int e, const
     // ---- store the replica, then the last replica of the group runs the exchange
     cp_async_wait_all();
     cluster_sync<CL>(G);   // all deltas exchanged; no CTA writes into another any more
+    if constexpr (CL > 1) {
+        if (tid == 0) {
+            mbar_inval(smem_u32(&s_bar[0]));
+            mbar_inval(smem_u32(&s_bar[1]));
+        }
+    }
     if (failed) return false;
     {
         IT *gI = reinterpret_cast<IT *>(s.I) + ((size_t)rep * n + row0) * s.ldg;
@@ -787,6 +806,22 @@ __global__ void __launch_bounds__(256, CL == 4 ? 2 : 1) epoch_kernel(SolveDev s)
 constexpr unsigned long long kQueueWaitNs = 30000000000ull;   // 30 s without any progress
 constexpr unsigned long long kDoneItem = ~0ull;
 
+// An instance descriptor read through L2.  A serving launch rewrites descriptors while it
+// runs (a slot is reused by the next request), and another SM's L1 may still hold the old
+// lines, so device code never reads B.inst[k] (nor B.sym / B.max_megaiters) through L1.
+// (The words are assembled in a word array and copied into the struct with memcpy: storing
+// them through an unsigned long long pointer into a SolveDev would break type-based aliasing,
+// and the compiler may then read the fields before or without those stores.)
+__device__ __forceinline__ void load_desc(SolveDev &d, const SolveDev *p) {
+    constexpr int kWords = (int)(sizeof(SolveDev) / 8);
+    static_assert(sizeof(SolveDev) % 8 == 0, "descriptor copied in 8-byte words");
+    const unsigned long long *src = reinterpret_cast<const unsigned long long *>(p);
+    unsigned long long w[kWords];
+#pragma unroll
+    for (int q = 0; q < kWords; ++q) w[q] = __ldcg(src + q);
+    memcpy(&d, w, sizeof(SolveDev));
+}
+
 // Enqueues every replica of instance k for its next epoch.
 __device__ void queue_push_instance(const BatchDev &B, int k, int replicas) {
     const unsigned long long base = atomicAdd(B.q_tail, (unsigned long long)replicas);
@@ -829,7 +864,8 @@ __device__ void report_done(const BatchDev &B, int k) {
 // Serving: the finished instance's result, best permutation and final energies, written into
 // its mapped result slot (one thread).
 __device__ void publish_result(const BatchDev &B, int k) {
-    const SolveDev &s = B.inst[k];
+    SolveDev s;
+    load_desc(s, B.inst + k);
     const int reps = s.T * s.R;
     long long best = 0x7fffffffffffffffll, arg = 0;
     unsigned long long acc = 0;
@@ -905,8 +941,11 @@ __device__ void serve_admit(const BatchDev &B, unsigned long long entry, const G
     char *head = (char *)d.dev.D;            // the head region starts with D (carve order)
     char *tail = (char *)d.dev.I;            // the tail region starts with I
     const unsigned long long hb = d.head_bytes, tb = d.tail_bytes;
+    // The staging buffers are mapped host memory that the host refills for the next request:
+    // read them uncached (ld.global.cv), or this SM's L1 could return the previous request's
+    // image of the same buffer.
     const int4 *src = reinterpret_cast<const int4 *>(B.link.staging + (size_t)stg * B.link.staging_stride);
-    for (unsigned long long q = G.tid; q < hb / 16; q += G.BT) reinterpret_cast<int4 *>(head)[q] = src[q];
+    for (unsigned long long q = G.tid; q < hb / 16; q += G.BT) reinterpret_cast<int4 *>(head)[q] = __ldcv(src + q);
     const int4 z = make_int4(0, 0, 0, 0);
     for (unsigned long long q = G.tid; q < tb / 16; q += G.BT) reinterpret_cast<int4 *>(tail)[q] = z;
     if (G.tid == 0) {
@@ -921,7 +960,8 @@ __device__ void serve_admit(const BatchDev &B, unsigned long long entry, const G
     if (G.tid == 0) {
         B.link.staging_busy[stg] = 0;         // the host may reuse the staging buffer
         __threadfence_system();
-        const SolveDev &s = B.inst[slot];
+        SolveDev s;
+        load_desc(s, B.inst + slot);
         atomicAdd(B.active, 1);
         const int replicas = s.T * s.R;
         const unsigned long long base = atomicAdd(B.q_tail, (unsigned long long)replicas);
@@ -984,7 +1024,8 @@ __device__ void replica_setup(const SolveDev &s, int rep, const Grp &G, int32_t 
 // The last replica of an instance to finish its set-up: mega-iteration 0's tracking, then the
 // first epoch, or the end when nothing is to run.
 __device__ void setup_done(const BatchDev &B, int k) {
-    const SolveDev &s = B.inst[k];
+    SolveDev s;
+    load_desc(s, B.inst + k);
     const int replicas = s.T * s.R;
     const unsigned prev = atomicAdd(B.finish_inst + k, 1u);
     if (prev != (unsigned)replicas - 1u) return;
@@ -994,7 +1035,7 @@ __device__ void setup_done(const BatchDev &B, int k) {
     for (int g = 0; g < s.T; ++g) track_exchange(s, g, 0);
     __threadfence();
     const int stop = *(volatile int32_t *)s.stop_epoch;
-    if (0 < stop && 0 < B.max_megaiters[k]) {
+    if (0 < stop && 0 < __ldcg(B.max_megaiters + k)) {
         queue_push_instance(B, k, replicas);
     } else {
         publish_result(B, k);
@@ -1008,7 +1049,8 @@ __device__ void setup_done(const BatchDev &B, int k) {
 // tracking + exchange (lock step across groups, as one launch per epoch gives), then the next
 // epoch or the end of the instance.
 __device__ void epoch_done(const BatchDev &B, int k, int e) {
-    const SolveDev &s = B.inst[k];
+    SolveDev s;
+    load_desc(s, B.inst + k);
     const int replicas = s.T * s.R;
     const unsigned prev = atomicAdd(B.finish_inst + k, 1u);
     if (prev != (unsigned)replicas - 1u) return;
@@ -1018,7 +1060,7 @@ __device__ void epoch_done(const BatchDev &B, int k, int e) {
     for (int g = 0; g < s.T; ++g) s.epoch[g] = e + 1;
     __threadfence();
     const int stop = *(volatile int32_t *)s.stop_epoch;
-    if (e + 1 < stop && (int64_t)(e + 1) < B.max_megaiters[k]) {
+    if (e + 1 < stop && (int64_t)(e + 1) < __ldcg(B.max_megaiters + k)) {
         queue_push_instance(B, k, replicas);
     } else {
         __threadfence();
@@ -1049,6 +1091,10 @@ __global__ void __launch_bounds__(256) batch_kernel(BatchDev B) {
     unsigned char *work = slice + 16;
     unsigned long long ticket = kNoTicket;   // held by G.tid == 0
     if (blockIdx.x == 0 && threadIdx.x == 0) *B.start_ns = globaltimer_ns();
+    if (B.serving && threadIdx.x == 0) {   // tell the host this CTA is resident
+        B.link.resident[blockIdx.x] = 1;
+        __threadfence_system();
+    }
     for (;;) {
         if (G.tid == 0) *hdr = queue_next(B, ticket);
         G.sync();
@@ -1061,7 +1107,8 @@ __global__ void __launch_bounds__(256) batch_kernel(BatchDev B) {
         }
         const int k = (int)(item >> 32);
         const int rep = (int)(item & 0x7fffffffull);
-        const SolveDev &s = B.inst[k];
+        SolveDev s;
+        load_desc(s, B.inst + k);
         if (item & kSetupItem) {
             replica_setup<IT>(s, rep, G, reinterpret_cast<int32_t *>(work),
                               reinterpret_cast<long long *>(work + 16 * kMaxN));
@@ -1069,7 +1116,7 @@ __global__ void __launch_bounds__(256) batch_kernel(BatchDev B) {
             continue;
         }
         const int e = *((volatile int32_t *)s.epoch);
-        if (B.sym[k]) replica_epoch<IT, 1, true>(s, rep, 0, e, G, work);
+        if (__ldcg(B.sym + k)) replica_epoch<IT, 1, true>(s, rep, 0, e, G, work);
         else replica_epoch<IT, 1, false>(s, rep, 0, e, G, work);
         G.sync();
         if (G.tid == 0) epoch_done(B, k, e);
@@ -1089,6 +1136,10 @@ __global__ void __launch_bounds__(256) batch_cluster_kernel(BatchDev B) {
                 (int)(blockDim.x >> 5), 0};
     unsigned long long ticket = kNoTicket;   // held by rank 0, thread 0
     if (blockIdx.x == 0 && threadIdx.x == 0) *B.start_ns = globaltimer_ns();
+    if (B.serving && threadIdx.x == 0) {   // tell the host this CTA is resident
+        B.link.resident[blockIdx.x] = 1;
+        __threadfence_system();
+    }
     cluster_barrier<CL>();
     for (;;) {
         if (rank == 0 && threadIdx.x == 0) {
@@ -1104,18 +1155,24 @@ __global__ void __launch_bounds__(256) batch_cluster_kernel(BatchDev B) {
         } else if (item & kSetupItem) {
             const int k = (int)(item >> 32);
             if (rank == 0) {
-                replica_setup<IT>(B.inst[k], (int)(item & 0x7fffffffull), G, reinterpret_cast<int32_t *>(work),
+                SolveDev s;
+                load_desc(s, B.inst + k);
+                replica_setup<IT>(s, (int)(item & 0x7fffffffull), G, reinterpret_cast<int32_t *>(work),
                                   reinterpret_cast<long long *>(work + 16 * kMaxN));
                 if (threadIdx.x == 0) setup_done(B, k);
             }
         } else {
             const int k = (int)(item >> 32), rep = (int)(item & 0x7fffffffull);
-            const SolveDev &s = B.inst[k];
+            SolveDev s;
+            load_desc(s, B.inst + k);
             const int e = *((volatile int32_t *)s.epoch);
             bool ok;
-            if (B.sym[k]) ok = replica_epoch<IT, CL, true>(s, rep, rank, e, G, work);
+            if (__ldcg(B.sym + k)) ok = replica_epoch<IT, CL, true>(s, rep, rank, e, G, work);
             else ok = replica_epoch<IT, CL, false>(s, rep, rank, e, G, work);
-            __syncthreads();
+            // every rank has stored its rows of the force matrix (and fenced them) before rank 0
+            // reports the epoch: the next epoch, or, once the instance ends, the next request
+            // in its slot and memory, must not meet a late store
+            cluster_barrier<CL>();
             if (!ok) {
                 if (threadIdx.x == 0) set_error(B, kErrTimeout);
             } else if (rank == 0 && threadIdx.x == 0) {

@@ -124,7 +124,7 @@ struct ServeClass {
     char *hbase = nullptr;   // mapped pinned host block
     volatile unsigned long long *h_inbox = nullptr, *h_inbox_tail = nullptr;
     volatile unsigned long long *h_done = nullptr, *h_done_seq = nullptr, *h_heartbeat = nullptr;
-    volatile int32_t *h_shutdown = nullptr, *h_error = nullptr;
+    volatile int32_t *h_shutdown = nullptr, *h_error = nullptr, *h_resident = nullptr;
     volatile ServeDesc *h_desc = nullptr;
     volatile BatchResultDev *h_res = nullptr;
     volatile int32_t *h_perm = nullptr;
@@ -139,6 +139,7 @@ struct ServeClass {
 constexpr int kServeMaxReplicas = 1024;
 constexpr int kServeMaxRankSlots = 65536;   // groups x rank slots of a served request
 constexpr int kStagingBuffers = 8;
+constexpr int kMaxResidentCtas = 1024;     // CTAs of one resident launch (at most one per SM)
 
 struct Server {
     pimqap_server_config cfg{};
@@ -159,6 +160,7 @@ struct Server {
     std::atomic<bool> stopping{false};
     std::atomic<bool> stall_heartbeat{false};
     std::atomic<int32_t> error_word{0};
+    std::string launch_error;             // the CUDA error that ended a launch (under mu)
 };
 
 namespace {
@@ -217,7 +219,8 @@ pimqap_status open_class(Server &S, ServeClass &C) {
     unsigned long long *d_done_tail = carve<unsigned long long>(cur, 1);
 
     // mapped block: inbox | done | done_seq | flags | descriptors | results | perms | energies
-    const size_t ring_bytes = 8 * ((size_t)C.inbox_cap + 2 * C.done_cap + 8);
+    const size_t ring_words = (size_t)C.inbox_cap + 2 * C.done_cap + 8;
+    const size_t ring_bytes = 8 * ring_words + 4 * (size_t)kMaxResidentCtas;
     const size_t desc_off = carve_size(ring_bytes);
     const size_t res_off = desc_off + carve_size(sizeof(ServeDesc) * m);
     const size_t perm_off = res_off + carve_size(sizeof(BatchResultDev) * m);
@@ -233,6 +236,7 @@ pimqap_status open_class(Server &S, ServeClass &C) {
     C.h_heartbeat = h + C.inbox_cap + 2 * C.done_cap + 1;
     C.h_shutdown = reinterpret_cast<volatile int32_t *>(h + C.inbox_cap + 2 * C.done_cap + 2);
     C.h_error = reinterpret_cast<volatile int32_t *>(h + C.inbox_cap + 2 * C.done_cap + 3);
+    C.h_resident = reinterpret_cast<volatile int32_t *>(h + ring_words);
     C.h_desc = reinterpret_cast<volatile ServeDesc *>(C.hbase + desc_off);
     C.h_res = reinterpret_cast<volatile BatchResultDev *>(C.hbase + res_off);
     C.h_perm = reinterpret_cast<volatile int32_t *>(C.hbase + perm_off);
@@ -276,6 +280,7 @@ pimqap_status open_class(Server &S, ServeClass &C) {
     L.heartbeat_limit_ns =
         (unsigned long long)((S.cfg.heartbeat_timeout_s > 0 ? S.cfg.heartbeat_timeout_s : 10.0) * 1e9);
     L.error_host = reinterpret_cast<volatile int32_t *>(dq + C.inbox_cap + 2 * C.done_cap + 3);
+    L.resident = reinterpret_cast<volatile int32_t *>(dq + ring_words);
     L.inst_rw = C.d_inst;
     L.sym_rw = C.d_sym;
     L.maxm_rw = C.d_maxm;
@@ -303,9 +308,15 @@ bool class_fits(const BatchClass &sh, const pimqap_instance &inst, const pimqap_
     return true;
 }
 
-// The class a request joins: among the launches it fits, the one that would finish the work
-// routed to it (this request included) first, by estimated cost per SM of the launch.  The
-// request's cost is added to that class's load (under S.mu) until it completes.
+// Replica workers of a launch: replicas it runs at once.
+size_t class_workers(const BatchClass &sh) {
+    return sh.cl == 1 ? (size_t)sh.grid * sh.workers : (size_t)(sh.grid / sh.cl);
+}
+
+// The class a request joins: among the launches it fits, the one expected to finish it first:
+// the work already routed there spread over its workers, plus the request's own work spread
+// over the workers it can use (one per replica).  The request's cost is added to that class's
+// load (under S.mu) until it completes.
 int route(Server &S, Request &R) {
     std::vector<std::pair<int, double>> fits;
     for (int c = 0; c < (int)S.classes.size(); ++c) {
@@ -313,12 +324,14 @@ int route(Server &S, Request &R) {
         if (!class_fits(S.classes[c].shape, R.inst, R.params, R.info, R.plan.bits, S.maxsm, &P)) continue;
         fits.push_back({c, instance_work(P, std::min<int64_t>(R.params.max_megaiters, 1000000))});
     }
+    const double reps = (double)R.plan.T * R.plan.R;
     std::lock_guard<std::mutex> lk(S.mu);
     int best = -1;
     double best_cost = 1e300;
     for (const auto &f : fits) {
         const ServeClass &C = S.classes[f.first];
-        const double cost = (C.load + f.second) / std::max(1, C.shape.grid);
+        const double W = (double)std::max<size_t>(1, class_workers(C.shape));
+        const double cost = C.load / W + f.second / std::min(reps, W);
         if (cost < best_cost) {
             best_cost = cost;
             best = f.first;
@@ -385,12 +398,10 @@ bool admit_some(Server &S) {
             }
         if (stg < 0) break;
         size_t off = 0;
-        // At most about two rounds of the launch's workers in flight: the queue serves the
+        // About two rounds of the launch's workers in flight at most: the queue serves the
         // admitted instances' epochs in turn, so admitting more only spreads the workers over
         // more requests and delays them all (the rest wait here, in arrival order).
-        const size_t workers = C.shape.cl == 1 ? (size_t)C.shape.grid * C.shape.workers
-                                               : (size_t)(C.shape.grid / C.shape.cl);
-        const bool crowded = C.replicas_in_flight > 0 && C.replicas_in_flight + reps > 2 * workers;
+        const bool crowded = C.replicas_in_flight >= 2 * class_workers(C.shape);
         if (C.free_slots.empty() || crowded || C.replicas_in_flight + reps > C.qcap - 1 ||
             !S.arena.alloc(R.plan.total, &off)) {
             ++it;
@@ -454,16 +465,30 @@ bool complete_some(Server &S) {
     return any;
 }
 
-// The server thread: no CUDA calls while the resident launches run.
+// The server thread: no work is enqueued while the resident launches run (the only CUDA
+// call is a periodic stream query, which enqueues nothing): a launch that ended while serving
+// (a device fault ends them all) sets kErrLaunchEnded, so waiters fail instead of waiting.
 void serve_loop(Server *S) {
     unsigned long long beat = 1;
+    auto last_query = Clock::now();
     for (;;) {
         if (!S->stall_heartbeat.load())
             for (auto &C : S->classes) *C.h_heartbeat = ++beat;
         int32_t err = 0;
         for (auto &C : S->classes) err |= *C.h_error;
-        if (err && !S->error_word.load()) {
-            S->error_word.store(err);
+        if (std::chrono::duration<double>(Clock::now() - last_query).count() > 0.05) {
+            last_query = Clock::now();
+            for (size_t k = 0; k < S->classes.size(); ++k) {
+                const cudaError_t q = cudaStreamQuery(S->classes[k].stream);
+                if (q == cudaErrorNotReady) continue;
+                err |= pimqap::kErrLaunchEnded;
+                std::lock_guard<std::mutex> lk(S->mu);
+                if (S->launch_error.empty())
+                    S->launch_error = "serving launch " + std::to_string(k) + " ended: " + cudaGetErrorString(q);
+            }
+        }
+        if (err && (S->error_word.load() | err) != S->error_word.load()) {
+            S->error_word.fetch_or(err);
             std::lock_guard<std::mutex> lk(S->mu);
             S->cv.notify_all();
         }
@@ -612,9 +637,29 @@ pimqap_status pimqap_server_create(const pimqap_server_config *config, pimqap_se
         if (st != PIMQAP_OK) return st;
     }
     PQ_CUDA(cudaDeviceSynchronize());
-    // every buffer exists: now the resident launches (cluster classes first)
-    for (auto &C : S.classes)
+    // every buffer exists: now the resident launches, cluster classes first, each one only
+    // after every CTA of the previous one has started (launches on different streams may be
+    // placed in any order, and CTAs of a later launch could take the SMs a cluster needs)
+    unsigned long long beat = 1;
+    for (size_t k = 0; k < S.classes.size(); ++k) {
+        ServeClass &C = S.classes[k];
         PQ_CUDA(pimqap::launch_batch(C.B, C.shape.bits, C.shape.cl, C.shape.grid, C.stream));
+        const auto t0 = Clock::now();
+        for (;;) {
+            int up = 0;
+            for (int b = 0; b < C.shape.grid; ++b) up += C.h_resident[b] ? 1 : 0;
+            if (up == C.shape.grid) break;
+            for (size_t q = 0; q <= k; ++q) *S.classes[q].h_heartbeat = ++beat;
+            if (std::chrono::duration<double>(Clock::now() - t0).count() > 10.0) {
+                const std::string why = "serving launch " + std::to_string(k) + " (" +
+                                        std::to_string(C.shape.grid) + " CTAs, cluster " +
+                                        std::to_string(C.shape.cl) + ") did not become resident";
+                pimqap_server_destroy(h.release());
+                return fail(PIMQAP_ERR_CUDA, why);
+            }
+            std::this_thread::sleep_for(std::chrono::microseconds(50));
+        }
+    }
     S.loop = std::thread(serve_loop, &S);
     *out = h.release();
     return PIMQAP_OK;
@@ -634,8 +679,11 @@ pimqap_status pimqap_server_submit(pimqap_server *h, const pimqap_instance *inst
         if ((int64_t)params->groups * cap > kServeMaxRankSlots)
             return fail(PIMQAP_ERR_ARG, "groups x rank slots too large for serving");
     }
-    if (S.error_word.load()) return fail(PIMQAP_ERR_DEVICE, "the server's device launches stopped (error word " +
-                                                               std::to_string(S.error_word.load()) + ")");
+    if (S.error_word.load()) {
+        std::lock_guard<std::mutex> lk(S.mu);
+        return fail(PIMQAP_ERR_DEVICE, "the server's device launches stopped (error word " +
+                                           std::to_string(S.error_word.load()) + ") " + S.launch_error);
+    }
     auto R = std::unique_ptr<Request>(new Request());
     const int n = inst->n;
     R->F.assign(inst->flow, inst->flow + (size_t)n * n);
@@ -698,7 +746,7 @@ pimqap_status pimqap_server_wait(pimqap_server *h, int64_t ticket, double timeou
     if (R.state != Request::kDone) {
         if (S.error_word.load())
             return fail(PIMQAP_ERR_DEVICE, "the server's device launches stopped (error word " +
-                                               std::to_string(S.error_word.load()) + ")");
+                                               std::to_string(S.error_word.load()) + ") " + S.launch_error);
         return fail(PIMQAP_ERR_NOT_READY, "request not finished");
     }
     fill_out(R, result);
@@ -726,6 +774,21 @@ void pimqap_server_destroy(pimqap_server *h) {
     Server &S = h->s;
     {
         std::lock_guard<std::mutex> lk(S.mu);
+        if (std::getenv("PIMQAP_TRACE")) {   // state of every class at shutdown
+            std::vector<int> pend(S.classes.size(), 0);
+            for (int64_t t : S.pending) ++pend[S.reqs[t]->cls];
+            int busy = 0;
+            for (int b = 0; b < kStagingBuffers; ++b) busy += S.staging_busy[b] ? 1 : 0;
+            std::fprintf(stderr, "[pimqap] server: %zu pending, %d staging buffers busy, error word %d %s\n",
+                         S.pending.size(), busy, S.error_word.load(), S.launch_error.c_str());
+            for (size_t k = 0; k < S.classes.size(); ++k) {
+                const ServeClass &C = S.classes[k];
+                std::fprintf(stderr, "[pimqap] class %zu bits=%d cl=%d band=%d grid=%d workers=%d: load %.3g, "
+                                     "replicas in flight %zu, free slots %zu/%d, pending %d, inbox %llu\n",
+                             k, C.shape.bits, C.shape.cl, C.shape.band, C.shape.grid, C.shape.workers, C.load,
+                             C.replicas_in_flight, C.free_slots.size(), C.slots, pend[k], C.inbox_tail);
+            }
+        }
         S.pending.clear();
     }
     S.stopping.store(true);
@@ -749,6 +812,21 @@ void pimqap_server_destroy(pimqap_server *h) {
         if (!running) break;
         for (auto &D : S.classes) *D.h_heartbeat = ++beat;
         std::this_thread::sleep_for(std::chrono::microseconds(200));
+    }
+    if (std::getenv("PIMQAP_TRACE")) {   // where every abandoned request had got to
+        for (auto &kv : S.reqs) {
+            const Request &R = *kv.second;
+            if (R.state != Request::kRunning) continue;
+            int32_t e = -1, err = 0;
+            const cudaError_t c1 = cudaMemcpy(&e, R.dev.epoch, 4, cudaMemcpyDeviceToHost);
+            cudaMemcpy(&err, R.dev.error, 4, cudaMemcpyDeviceToHost);
+            if (c1 != cudaSuccess) std::fprintf(stderr, "[pimqap] read-back: %s\n", cudaGetErrorString(c1));
+            const double age = std::chrono::duration<double>(Clock::now() - R.t_admit).count();
+            std::fprintf(stderr, "[pimqap] running ticket %lld class %d slot %d n=%d reps=%d: epoch %d of %lld, "
+                                 "error %d, admitted %.1f s ago\n",
+                         (long long)R.ticket, R.cls, R.slot, R.plan.n, R.plan.T * R.plan.R, e,
+                         (long long)R.params.max_megaiters, err, age);
+        }
     }
     for (auto &C : S.classes) {
         if (C.stream) cudaStreamDestroy(C.stream);
