@@ -196,6 +196,27 @@ def read_traffic():
     return float(m.group(1)) if m else None
 
 
+def rank_instance(rank):
+    """The instance rank `rank` solves: one grid256 instance per GPU (the work is sharded by
+    instance; ranks never exchange data)."""
+    return instances.grid256(1000 + rank)
+
+
+def max_over_ranks(x, world, device):
+    """The largest x over all ranks (the slowest rank bounds the whole job)."""
+    import torch
+    t = torch.tensor([float(x)], dtype=torch.float64, device=device)
+    if world > 1:
+        import torch.distributed as dist
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def whole_job_rate(units_per_rank, world, seconds_max):
+    """Units all ranks processed / the slowest rank's time."""
+    return units_per_rank * world / seconds_max
+
+
 def run_ours(args):
     import torch
     import torch.distributed as dist
@@ -211,7 +232,7 @@ def run_ours(args):
         import datetime
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
 
-    inst = instances.grid256(1000 + rank)
+    inst = rank_instance(rank)
     params = pimqap.default_params(replicas=REPLICAS, groups=GROUPS, sweeps_per_exchange=SWEEPS_PER_EXCHANGE,
                                    beta_max=BETA_MAX, beta_ratio=BETA_RATIO, beta_internal=1, seed=1 + rank,
                                    device=local, megaiters_per_launch=MEGAITERS_PER_STEP,
@@ -241,13 +262,10 @@ def run_ours(args):
         wall = time.perf_counter() - w0
     r1 = solver.result()
     solver.close()
-    t = torch.tensor([ms_total], dtype=torch.float64, device=f"cuda:{local}")
-    if world > 1:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    ms_max = float(t.item())
+    ms_max = max_over_ranks(ms_total, world, f"cuda:{local}")
     sweeps = args.steps * MEGAITERS_PER_STEP * SWEEPS_PER_EXCHANGE
     reps = REPLICAS * GROUPS
-    value = proposals(reps, sweeps) * world / (ms_max * 1e-3)
+    value = whole_job_rate(proposals(reps, sweeps), world, ms_max * 1e-3)
 
     # roofline of the sweep kernel (every timed launch is that kernel)
     accepts = r1["accepts"] - r0["accepts"]
@@ -272,10 +290,7 @@ def run_ours(args):
     e0 = time.perf_counter()
     res = pimqap.solve(Fp.numpy(), Dp.numpy(), p2)
     e_wall = time.perf_counter() - e0
-    te = torch.tensor([e_wall], dtype=torch.float64, device=f"cuda:{local}")
-    if world > 1:
-        dist.all_reduce(te, op=dist.ReduceOp.MAX)
-    e2e_value = proposals(reps, sweeps) * world / float(te.item())
+    e2e_value = whole_job_rate(proposals(reps, sweeps), world, max_over_ranks(e_wall, world, f"cuda:{local}"))
 
     line = None
     if rank == 0:
