@@ -55,7 +55,7 @@ __host__ __device__ inline size_t align16(size_t x) { return (x + 15) & ~size_t(
 //   red, wsum, r, misc, bar  reductions, random number, pick, mbarriers
 struct SmemLayout {
     size_t I, phi, inv, bphi, Dd, Fd, A, B, Drow, DTrow, Frow, FTrow, Dj, DTj, Fb, FTb;
-    size_t red, wsum, r, misc, bar, total;
+    size_t u1, u2, red, wsum, r, misc, bar, total;
     __host__ __device__ SmemLayout(int n, int rpc, int lds, int cluster, int isz) {
         const size_t npad = (size_t)((n + 3) & ~3);
         const size_t rp = (size_t)rpc;
@@ -76,6 +76,8 @@ struct SmemLayout {
         DTj = o;   o = align16(o + rp * 4);
         Fb = o;    o = align16(o + npad * 4);
         FTb = o;   o = align16(o + npad * 4);
+        u1 = o;    o = align16(o + rp * isz);
+        u2 = o;    o = align16(o + rp * isz);
         red = o;   o = align16(o + kMaxWarps * 8);
         wsum = o;  o = align16(o + kMaxWarps * sizeof(double));
         r = o;     o = align16(o + 2 * sizeof(double));
@@ -402,10 +404,6 @@ template <int CL> __device__ __forceinline__ void cluster_sync(const Grp &G) {
     else cluster_barrier<CL>();
 }
 
-// One epoch of replica rep: load its state into shared memory, spe sweeps (doMegaItera,
-// CPU_PIM.cpp:195-290), store the state back.  With CL > 1 this CTA is rank `rank` of the
-// replica's cluster and G is the whole CTA.  Replica state is read through L2 (__ldcg): the
-// previous epoch may have run on another SM.  Returns false when a bounded wait gave up.
 // A replica's best fell below goal_print during a sweep of mega-iteration e (the reference
 // prints the replica and its permutation, CPU_PIM.cpp:271-282).  One thread claims a
 // permutation slot and appends the event; the CTA fills the slot after its next barrier.
@@ -420,6 +418,10 @@ __device__ __forceinline__ int goal_print_claim(const EventLink &v, int g, int l
     return stored ? (int)slot : -1;
 }
 
+// One epoch of replica rep: load its state into shared memory, spe sweeps (doMegaItera,
+// CPU_PIM.cpp:195-290), store the state back.  With CL > 1 this CTA is rank `rank` of the
+// replica's cluster and G is the whole CTA.  Replica state is read through L2 (__ldcg): the
+// previous epoch may have run on another SM.  Returns false when a bounded wait gave up.
 template <class IT, int CL, bool SYM, bool GP = false>
 __device__ bool replica_epoch(const SolveDev &s, int rep, int rank, int e, const Grp &G,
                               unsigned char *smem) {
@@ -450,6 +452,8 @@ __device__ bool replica_epoch(const SolveDev &s, int rep, int rank, int e, const
     int32_t *s_DTj = reinterpret_cast<int32_t *>(smem + L.DTj);
     int32_t *s_Fb = reinterpret_cast<int32_t *>(smem + L.Fb);
     int32_t *s_FTb = reinterpret_cast<int32_t *>(smem + L.FTb);
+    IT *s_u1 = reinterpret_cast<IT *>(smem + L.u1);          // row factors of the accepted swap
+    IT *s_u2 = reinterpret_cast<IT *>(smem + L.u2);
     IT *s_red = reinterpret_cast<IT *>(smem + L.red);
     double *s_wsum = reinterpret_cast<double *>(smem + L.wsum);
     double *s_r = reinterpret_cast<double *>(smem + L.r);
@@ -663,7 +667,26 @@ __device__ bool replica_epoch(const SolveDev &s, int rep, int rank, int e, const
                                s_Dj, s_DTj, nFc, s.F + (size_t)bs * ldm, s.FT + (size_t)bs * ldm,
                                s_Fb, s_FTb);
             cp_async_wait_all();
-            G.sync();                                 // S4: rows j / bs in shared memory
+            // the row factors of the rank-2 update, each computed by the thread that fetched
+            // its 16-byte chunk of row j (prefetch_rows' chunk order), so no extra barrier
+            for (int q = tid; q < (SYM ? nDc : 2 * nDc + nFc); q += BT) {
+                if (q < nDc) {
+#pragma unroll
+                    for (int r = 0; r < 4; ++r) {
+                        const int k = 4 * q + r;
+                        const U d = (U)(IT)s_Dj[k] - (U)(IT)Di[k];
+                        if constexpr (SYM) s_u1[k] = (IT)(2u * d);
+                        else s_u2[k] = (IT)d;
+                    }
+                } else if (!SYM && q >= nDc + nFc) {
+#pragma unroll
+                    for (int r = 0; r < 4; ++r) {
+                        const int k = 4 * (q - nDc - nFc) + r;
+                        s_u1[k] = (IT)((U)(IT)s_DTj[k] - (U)(IT)DTi[k]);
+                    }
+                }
+            }
+            G.sync();                                 // S4: rows j / bs and the row factors in shared memory
             if (tid == 0) {
                 s_phi[i] = bs;                               // :257-261
                 s_inv[bs] = i;
@@ -704,21 +727,36 @@ __device__ bool replica_epoch(const SolveDev &s, int rep, int rank, int e, const
                 }
                 const int kfirst = (BT >= nvec) ? k0r : 0;
                 const int kinc = (BT >= nvec) ? kstep : 1;
-#pragma unroll 2
-                for (int k = kfirst; k < rows; k += kinc) {
-                    Vec<IT> *dst = reinterpret_cast<Vec<IT> *>(sI + (size_t)k * lds + cv * VEC);
-                    Vec<IT> x = *dst;
+                auto upd_row = [&](int k, Vec<IT> &x) {
+                    const U u1 = (U)s_u1[k];
                     if constexpr (SYM) {
-                        const U u1 = 2u * ((U)(IT)s_Dj[k] - (U)(IT)Di[k]);
 #pragma unroll
                         for (int q = 0; q < VEC; ++q) x.v[q] = (IT)((U)x.v[q] + u1 * (U)v1.v[q]);
                     } else {
-                        const U u1 = (U)(IT)s_DTj[k] - (U)(IT)DTi[k];
-                        const U u2 = (U)(IT)s_Dj[k] - (U)(IT)Di[k];
+                        const U u2 = (U)s_u2[k];
 #pragma unroll
                         for (int q = 0; q < VEC; ++q)
                             x.v[q] = (IT)((U)x.v[q] + u1 * (U)v1.v[q] + u2 * (U)v2.v[q]);
                     }
+                };
+                // rows in batches: the loads of a batch are in flight together
+                constexpr int RB = sizeof(IT) == 8 ? 2 : 8;
+                int k = kfirst;
+                for (; k + (RB - 1) * kinc < rows; k += RB * kinc) {
+                    Vec<IT> x[RB];
+#pragma unroll
+                    for (int m = 0; m < RB; ++m)
+                        x[m] = *reinterpret_cast<const Vec<IT> *>(sI + (size_t)(k + m * kinc) * lds + cv * VEC);
+#pragma unroll
+                    for (int m = 0; m < RB; ++m) upd_row(k + m * kinc, x[m]);
+#pragma unroll
+                    for (int m = 0; m < RB; ++m)
+                        *reinterpret_cast<Vec<IT> *>(sI + (size_t)(k + m * kinc) * lds + cv * VEC) = x[m];
+                }
+                for (; k < rows; k += kinc) {
+                    Vec<IT> *dst = reinterpret_cast<Vec<IT> *>(sI + (size_t)k * lds + cv * VEC);
+                    Vec<IT> x = *dst;
+                    upd_row(k, x);
                     *dst = x;
                 }
             }
@@ -1126,7 +1164,7 @@ __global__ void __launch_bounds__(256) batch_kernel(BatchDev B) {
 // Batch kernel for replicas that span a cluster of CL CTAs: rank 0 pops an item and writes it
 // into every rank's header; the whole cluster runs the replica's epoch, rank 0 reports it.
 template <class IT, int CL>
-__global__ void __launch_bounds__(256) batch_cluster_kernel(BatchDev B) {
+__global__ void __launch_bounds__(256, 1) batch_cluster_kernel(BatchDev B) {
     extern __shared__ __align__(16) unsigned char smem[];
     cg::cluster_group cluster = cg::this_cluster();
     const int rank = (int)cluster.block_rank();
