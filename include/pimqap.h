@@ -88,6 +88,10 @@ typedef struct pimqap_params {
     int32_t event_capacity;      /* progress events kept per run call (0 = no event log); see
                                     pimqap_solver_events */
     int32_t event_perm_capacity; /* goal_print permutations kept per run call (0 = 256) */
+    int32_t compact_instance;    /* 0 = automatic: a symmetric instance with 0/1 flows and
+                                    int16 distances keeps D and F in shared memory beside the
+                                    force rows (same results); 1 = never */
+    int32_t pad1;
 } pimqap_params;
 
 /* Fills p with the reference's defaults: 10 replicas, 20 groups, 4 sweeps per exchange,

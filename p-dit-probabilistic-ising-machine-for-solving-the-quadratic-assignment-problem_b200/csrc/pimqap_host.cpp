@@ -123,6 +123,12 @@ InstanceInfo analyse(int n, const int32_t *F, const int32_t *D) {
                 break;
             }
     info.symmetric = sym;
+    info.binary_flow = true;
+    info.dist16 = true;
+    for (int k = 0; k < n * n; ++k) {
+        if (F[k] != 0 && F[k] != 1) info.binary_flow = false;
+        if (D[k] < -32768 || D[k] > 32767) info.dist16 = false;
+    }
     std::vector<long double> rD(n, 0), cD(n, 0);
     long double rFmax = 0, cFmax = 0;
     for (int i = 0; i < n; ++i)
@@ -193,7 +199,7 @@ struct pimqap_solver {
     pimqap_params p{};
     int n = 0, T = 0, R = 0, cap = 0, spe = 0;
     int bits = 32, cl = 1, threads = 256;
-    bool sym = false;
+    bool sym = false, bin = false;
     size_t smem = 0;
     int device = 0;
     cudaStream_t stream = nullptr;
@@ -243,6 +249,8 @@ pimqap_status check_params(const pimqap_instance *inst, const pimqap_params *p) 
     if (p->max_megaiters < 0) return fail(PIMQAP_ERR_ARG, "max_megaiters must be >= 0");
     if (p->event_capacity < 0 || p->event_perm_capacity < 0)
         return fail(PIMQAP_ERR_ARG, "event capacities must be >= 0");
+    if (p->compact_instance != 0 && p->compact_instance != 1)
+        return fail(PIMQAP_ERR_ARG, "compact_instance must be 0 or 1");
     if (p->force_bits != 0 && p->force_bits != 32 && p->force_bits != 64)
         return fail(PIMQAP_ERR_ARG, "force_bits must be 0, 32 or 64");
     if (p->threads_per_block != 0 && p->threads_per_block != 64 && p->threads_per_block != 128 &&
@@ -304,6 +312,14 @@ pimqap_status plan_instance(const pimqap_instance *inst, const pimqap_params *pa
     // D / F rows are read in 16-byte chunks up to column cl * rpc
     P.ldm = std::max(P.npad, P.cl * P.rpc);
     P.smem = pimqap::epoch_smem_bytes(n, P.rpc, P.lds, P.cl, P.bits);
+    // binary flows and int16 distances: the instance itself fits next to the force rows
+    if (info.symmetric && info.binary_flow && info.dist16 && P.bits == 32 && params->compact_instance == 0) {
+        const size_t sb = pimqap::epoch_smem_bytes_bin(n, P.rpc, P.lds, P.cl);
+        if (sb <= maxsm) {
+            P.bin = true;
+            P.smem_bin = sb;
+        }
+    }
     const size_t reps = (size_t)P.T * P.R, nn = (size_t)n * P.ldm;
     // head: everything uploaded from the host; tail: state that starts at zero
     P.head = 4 * carve_size(nn * 4) + 2 * carve_size((size_t)n * 4) + carve_size(reps * n * 4) +
@@ -487,10 +503,11 @@ pimqap_status pimqap_solver_create(const pimqap_instance *inst, const pimqap_par
     s->cap = plan.cap;
     s->spe = plan.spe;
     s->sym = plan.sym;
+    s->bin = plan.bin;
     s->bits = plan.bits;
     s->cl = plan.cl;
     s->threads = plan.threads;
-    s->smem = plan.smem;
+    s->smem = plan.bin ? plan.smem_bin : plan.smem;
     PQ_CUDA(cudaMalloc(&s->dmem, plan.total));
     s->dbytes = plan.total;
     PQ_CUDA(cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking));
@@ -547,7 +564,7 @@ pimqap_status pimqap_solver_run(pimqap_solver *s, int64_t megaiters, double *dev
             cudaGraph_t graph;
             PQ_CUDA(cudaStreamBeginCapture(s->stream, cudaStreamCaptureModeThreadLocal));
             for (int k = 0; k < g; ++k) {
-                cudaError_t e = pimqap::launch_epoch(s->dev, s->bits, s->cl, s->sym, s->threads,
+                cudaError_t e = pimqap::launch_epoch(s->dev, s->bits, s->cl, s->sym, s->bin, s->threads,
                                                      s->smem, s->stream);
                 if (e != cudaSuccess) {
                     cudaStreamEndCapture(s->stream, &graph);

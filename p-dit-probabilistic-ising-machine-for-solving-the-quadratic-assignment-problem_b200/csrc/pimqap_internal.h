@@ -175,6 +175,8 @@ void set_last_error(const char *msg);
 
 // Shared memory of one CTA of the epoch kernel.
 size_t epoch_smem_bytes(int n, int rpc, int lds, int cluster, int bits);
+// Shared memory of the binary-flow epoch kernel (0 / 1 flows and int16 distances resident).
+size_t epoch_smem_bytes_bin(int n, int rpc, int lds, int cluster);
 
 // One-time kernel attributes (dynamic shared memory, non-portable cluster size).
 cudaError_t prepare_kernels();
@@ -184,7 +186,7 @@ cudaError_t prepare_kernels();
 cudaError_t launch_setup(const SolveDev &s, int bits, cudaStream_t st);
 
 // One epoch: spe sweeps of every replica, then each group's tracking + exchange.
-cudaError_t launch_epoch(const SolveDev &s, int bits, int cluster, bool sym, int threads,
+cudaError_t launch_epoch(const SolveDev &s, int bits, int cluster, bool sym, bool bin, int threads,
                          size_t smem, cudaStream_t st);
 
 }  // namespace pimqap

@@ -810,9 +810,356 @@ __device__ bool replica_epoch(const SolveDev &s, int rep, int rank, int e, const
     return true;
 }
 
+// Shared-memory layout of the binary-flow epoch (replica_epoch_bin): the instance itself is
+// resident next to the force-matrix rows, D as int16 columns of this CTA's rows and F as bit
+// rows, so no update waits for a row from L2.
+struct BinLayout {
+    size_t I, phi, inv, bphi, Dd, A, B, Ds, Fb, red, wsum, r, misc, bar, total;
+    __host__ __device__ BinLayout(int n, int rpc, int lds, int cluster) {
+        const size_t npad = (size_t)((n + 3) & ~3), rp = (size_t)rpc, nw = (size_t)((n + 31) / 32);
+        size_t o = 0;
+        I = o;     o = align16(o + rp * lds * 4);
+        phi = o;   o = align16(o + npad * 4);
+        inv = o;   o = align16(o + npad * 4);
+        bphi = o;  o = align16(o + npad * 4);
+        Dd = o;    o = align16(o + npad * 4);
+        A = o;     o = align16(o + 2 * npad * 4);
+        B = o;     o = align16(o + (cluster > 1 ? 2 * npad * 4 : 0));
+        Ds = o;    o = align16(o + (size_t)n * rp * 2);   // Ds[r][k] = D[r][row0 + k]
+        Fb = o;    o = align16(o + (size_t)n * nw * 4);   // bit b % 32 of Fb[a][b / 32] = F[a][b]
+        red = o;   o = align16(o + kMaxWarps * 8);
+        wsum = o;  o = align16(o + kMaxWarps * sizeof(double));
+        r = o;     o = align16(o + 2 * sizeof(double));
+        misc = o;  o = align16(o + 4 * sizeof(int));
+        bar = o;   o = align16(o + 2 * sizeof(unsigned long long));
+        total = o;
+    }
+};
+
+size_t epoch_smem_bytes_bin(int n, int rpc, int lds, int cluster) {
+    return BinLayout(n, rpc, lds, cluster).total;
+}
+
+// One epoch of replica rep for a symmetric instance whose flows are 0 / 1 and whose distances
+// fit in int16 (int32 force matrix): replica_epoch with the instance resident in shared memory.
+// Every delta, weight and update is the same integer / fp64 computation as replica_epoch's:
+// dd = Dii + Djj - 2 Dij, ff = Faa + Fbb - 2 Fab, and the rank-2 update
+// I[k][c] += 2 (Djk - Dik)(Fbc - Fac) (CPU_PIM.cpp:220-232, :262-268 with D = Dᵀ, F = Fᵀ).
+template <int CL>
+__device__ bool replica_epoch_bin(const SolveDev &s, int rep, int rank, int e, const Grp &G,
+                                  unsigned char *smem) {
+    using IT = int32_t;
+    using U = uint32_t;
+    constexpr int VEC = 4;
+    const int n = s.n;
+    const int tid = G.tid, BT = G.BT, lane = G.lane, warp = G.warp, nwarps = G.nwarps;
+    const int g = rep / s.R, l = rep - g * s.R;
+    const int rpc = s.rpc, lds = s.lds, ldm = s.ldm;
+    const int row0 = rank * rpc;
+    const int rows = max(0, min(rpc, n - row0));
+    const int npad = (n + 3) & ~3;
+    const int nw = (n + 31) / 32;
+    const BinLayout L(n, rpc, lds, CL);
+    IT *sI = reinterpret_cast<IT *>(smem + L.I);
+    int32_t *s_phi = reinterpret_cast<int32_t *>(smem + L.phi);
+    int32_t *s_inv = reinterpret_cast<int32_t *>(smem + L.inv);
+    int32_t *s_bphi = reinterpret_cast<int32_t *>(smem + L.bphi);
+    int32_t *s_Dd = reinterpret_cast<int32_t *>(smem + L.Dd);
+    IT *s_A = reinterpret_cast<IT *>(smem + L.A);
+    IT *s_B = reinterpret_cast<IT *>(smem + L.B);
+    int16_t *s_Ds = reinterpret_cast<int16_t *>(smem + L.Ds);
+    uint32_t *s_Fb = reinterpret_cast<uint32_t *>(smem + L.Fb);
+    IT *s_red = reinterpret_cast<IT *>(smem + L.red);
+    double *s_wsum = reinterpret_cast<double *>(smem + L.wsum);
+    double *s_r = reinterpret_cast<double *>(smem + L.r);
+    int *s_misc = reinterpret_cast<int *>(smem + L.misc);   // [0] pick key, [1] improved-at
+    unsigned long long *s_bar = reinterpret_cast<unsigned long long *>(smem + L.bar);
+    auto fbit = [&](int a, int b) -> int { return (int)((s_Fb[a * nw + (b >> 5)] >> (b & 31)) & 1u); };
+
+    // ---- load the replica and the instance
+    {
+        const IT *gI = reinterpret_cast<const IT *>(s.I) + ((size_t)rep * n + row0) * s.ldg;
+        const int nvg = s.ldg / VEC;
+        for (int idx = tid; idx < rows * nvg; idx += BT) {
+            const int k = idx / nvg, v = idx - k * nvg;
+            const int4 w = __ldcg(reinterpret_cast<const int4 *>(gI + (size_t)k * s.ldg + v * VEC));
+            *reinterpret_cast<int4 *>(sI + (size_t)k * lds + v * VEC) = w;
+        }
+        const int32_t *gphi = s.phi + (size_t)rep * n;
+        for (int q = tid; q < npad; q += BT) {
+            int p = q < n ? __ldcg(gphi + q) : 0;
+            if ((unsigned)p >= (unsigned)n) {
+                atomicOr(s.error, kErrBadPerm);
+                p = 0;
+            }
+            s_phi[q] = p;
+            s_bphi[q] = p;
+            s_inv[q] = 0;
+            s_Dd[q] = q < n ? __ldcg(s.Ddiag + q) : 0;
+        }
+        for (int idx = tid; idx < n * rows; idx += BT) {
+            const int r = idx / rows, k = idx - r * rows;
+            s_Ds[(size_t)r * rpc + k] = (int16_t)__ldcg(s.D + (size_t)r * ldm + row0 + k);
+        }
+        for (int widx = warp; widx < n * nw; widx += nwarps) {
+            const int r = widx / nw, w = widx - r * nw, b = 32 * w + lane;
+            const bool one = b < n && __ldcg(s.F + (size_t)r * ldm + b) != 0;
+            const unsigned bits = __ballot_sync(0xffffffffu, one);
+            if (lane == 0) s_Fb[widx] = bits;
+        }
+        if (tid == 0) {
+            s_misc[0] = 0x7fffffff;
+            s_misc[1] = -1;
+            if constexpr (CL > 1) {
+                mbar_init(smem_u32(&s_bar[0]), 1);
+                mbar_init(smem_u32(&s_bar[1]), 1);
+                mbar_fence_init();
+            }
+        }
+        G.sync();
+    }
+    for (int q = tid; q < n; q += BT) s_inv[s_phi[q]] = q;
+    cluster_sync<CL>(G);
+
+    uint32_t A_at[CL], B_at[CL], bar_at[CL];
+    if constexpr (CL > 1) {
+#pragma unroll
+        for (int r = 0; r < CL; ++r) {
+            A_at[r] = cluster_addr(smem_u32(s_A), r);
+            B_at[r] = cluster_addr(smem_u32(s_B), r);
+            bar_at[r] = cluster_addr(smem_u32(s_bar), r);
+        }
+    }
+    const uint32_t tx_bytes = (uint32_t)((npad + n) * sizeof(IT));
+    uint32_t phase = 0;
+
+    const double beta = __ldcg(s.beta + rep);
+    const double cut_span = 20.0 / beta;                    // CPU_PIM.cpp:234
+    int64_t E = __ldcg((const long long *)s.E + rep), bestE = __ldcg((const long long *)s.bestE + rep);
+    unsigned long long accepts = 0;
+    const uint32_t k0 = (uint32_t)s.seed, k1 = (uint32_t)(s.seed >> 32);
+    const int K = (n + BT - 1) / BT;                         // weights per thread (<= 4)
+    const int nvec = npad / VEC;
+    bool failed = false;
+    int upd = 0;
+
+    for (int sw = 0; sw < s.spe && !failed; ++sw) {
+        const uint32_t sweep = (uint32_t)(e * s.spe + sw);
+        for (int i = 0; i < n; ++i, ++upd) {
+            const int p = upd & 1;
+            if (tid == 0) {
+                uint32_t w0, w1;
+                philox_2words((uint32_t)i, sweep, (uint32_t)l, (uint32_t)g, k0, k1, w0, w1);
+                s_r[p] = canonical53(w0, w1);
+                if constexpr (CL > 1) mbar_arrive_expect_tx(smem_u32(&s_bar[p]), tx_bytes);
+            }
+            const int a = s_phi[i];
+            const int16_t *Di = s_Ds + (size_t)i * rpc;      // D[i][own rows]
+            const int owner = i / rpc;
+            const int Dii = s_Dd[i], Faa = fbit(a, a);
+            IT Iia = 0;
+            const IT *Ii = sI + (size_t)(i - owner * rpc) * lds;
+            if (owner == rank) Iia = Ii[a];
+            for (int jj = tid; jj < rows; jj += BT) {
+                const int j = row0 + jj;
+                const int b = s_phi[j];
+                const IT *Ij = sI + (size_t)jj * lds;
+                const U dd = (U)Dii + (U)s_Dd[j] - 2u * (U)(IT)Di[jj];
+                const U ff = (U)Faa + (U)fbit(b, b) - 2u * (U)fbit(a, b);
+                const U Bv = (U)Ij[a] - (U)Ij[b] - dd * ff;
+                if constexpr (CL == 1) {
+                    s_A[p * npad + b] = (IT)(Bv + (U)Ii[b] - (U)Iia);
+                } else {
+#pragma unroll
+                    for (int r = 0; r < CL; ++r)
+                        st_async(B_at[r] + (uint32_t)((p * npad + b) * sizeof(IT)), (IT)Bv, bar_at[r] + p * 8);
+                }
+            }
+            if constexpr (CL > 1) {
+                if (owner == rank) {
+                    for (int c4 = tid; c4 < nvec; c4 += BT) {
+                        Vec<IT> v = *reinterpret_cast<const Vec<IT> *>(Ii + c4 * VEC);
+#pragma unroll
+                        for (int q = 0; q < VEC; ++q) v.v[q] = (IT)((U)v.v[q] - (U)Iia);
+#pragma unroll
+                        for (int r = 0; r < CL; ++r)
+                            st_async16(A_at[r] + (uint32_t)((p * npad + c4 * VEC) * sizeof(IT)), v,
+                                       bar_at[r] + p * 8);
+                    }
+                }
+            }
+
+            bool timeout = false;
+            if constexpr (CL == 1) {
+                G.sync();
+            } else {
+                timeout = !mbar_wait_bounded(smem_u32(&s_bar[p]), (phase >> p) & 1u, kWaitLimitNs);
+                phase ^= 1u << p;
+            }
+            const int b0 = tid * K;
+            IT d[4];
+            double x[4];
+            IT lmax = 0;                                     // max starts at 0 (:208)
+#pragma unroll
+            for (int k = 0; k < 4; ++k) {
+                d[k] = 0;
+                x[k] = 0.0;
+                if (k < K && b0 + k < n) {
+                    const int b = b0 + k;
+                    d[k] = (CL == 1) ? s_A[p * npad + b] : (IT)((U)s_A[p * npad + b] + (U)s_B[p * npad + b]);
+                    x[k] = exp2(__dmul_rn(beta, (double)d[k]));
+                    lmax = d[k] > lmax ? d[k] : lmax;
+                }
+            }
+            lmax = warp_max(lmax);
+            if (lane == 0) s_red[warp] = lmax;
+            if (G.sync_or(timeout)) {
+                if (tid == 0) atomicOr(s.error, kErrTimeout);
+                failed = true;
+                break;
+            }
+            if (tid == 0) s_misc[0] = 0x7fffffff;
+            IT M = s_red[0];
+            for (int w = 1; w < nwarps; ++w) M = s_red[w] > M ? s_red[w] : M;
+            const long long cut = cutoff_trunc(__dsub_rn((double)M, cut_span));   // :234-235
+            double pre[4];
+            double local = 0.0;
+#pragma unroll
+            for (int k = 0; k < 4; ++k) {
+                if (k < K && (long long)d[k] > cut && b0 + k < n) local = __dadd_rn(local, x[k]);
+                pre[k] = local;
+            }
+            double incl = local;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const double y = __shfl_up_sync(0xffffffffu, incl, o);
+                if (lane >= o) incl = __dadd_rn(incl, y);
+            }
+            double excl = __shfl_up_sync(0xffffffffu, incl, 1);
+            if (lane == 0) excl = 0.0;
+            if (lane == 31) s_wsum[warp] = incl;
+            G.sync();
+            double base = 0.0, total = 0.0;
+            for (int w = 0; w < nwarps; ++w) {
+                if (w == warp) base = total;
+                total = __dadd_rn(total, s_wsum[w]);
+            }
+            const double target = __dmul_rn(s_r[p], total);     // :247
+            const double X = __dadd_rn(base, excl);
+#pragma unroll
+            for (int k = 0; k < 4; ++k) {
+                if (k < K && b0 + k < n) {
+                    if (__dadd_rn(X, pre[k]) >= target) {   // :251
+                        // the candidate with its partner j = phiinv(b), read before anyone swaps
+                        atomicMin(&s_misc[0], ((b0 + k) << 9) | s_inv[b0 + k]);
+                        break;
+                    }
+                }
+            }
+            G.sync();
+            const int key = s_misc[0];
+            const int bs = key >> 9;
+            if (bs >= n || bs == a) continue;                // no move / self move (:252)
+
+            // ---- accepted swap: every row and bit row it needs is already in shared memory
+            const int j = key & 511;
+            const IT dEsel = (CL == 1) ? s_A[p * npad + bs] : (IT)((U)s_A[p * npad + bs] + (U)s_B[p * npad + bs]);
+            if (tid == 0) {                                  // :257-261
+                s_phi[i] = bs;
+                s_inv[bs] = i;
+                s_phi[j] = a;
+                s_inv[a] = j;
+            }
+            E -= (int64_t)dEsel;                             // :256
+            ++accepts;
+            if (E < bestE) {                                 // :271-272
+                bestE = E;
+                if (tid == 0) s_misc[1] = upd;
+            }
+            const int16_t *Dj = s_Ds + (size_t)j * rpc;
+            // I[k][c] += 2 (D[j][k] - D[i][k]) (F[bs][c] - F[a][c])
+            for (int cv = tid % nvec, k0r = tid / nvec, kstep = max(1, BT / nvec);
+                 cv < nvec; cv += (BT >= nvec ? nvec : BT)) {
+                if (BT >= nvec && k0r >= kstep) break;
+                const int c0 = cv * VEC;
+                const unsigned fb = (s_Fb[bs * nw + (c0 >> 5)] >> (c0 & 31)) & 15u;
+                const unsigned fa = (s_Fb[a * nw + (c0 >> 5)] >> (c0 & 31)) & 15u;
+                U v1[VEC];
+#pragma unroll
+                for (int q = 0; q < VEC; ++q) v1[q] = (U)((fb >> q) & 1u) - (U)((fa >> q) & 1u);
+                const int kfirst = (BT >= nvec) ? k0r : 0;
+                const int kinc = (BT >= nvec) ? kstep : 1;
+                constexpr int RB = 8;
+                int k = kfirst;
+                for (; k + (RB - 1) * kinc < rows; k += RB * kinc) {
+                    Vec<IT> xv[RB];
+#pragma unroll
+                    for (int m = 0; m < RB; ++m)
+                        xv[m] = *reinterpret_cast<const Vec<IT> *>(sI + (size_t)(k + m * kinc) * lds + c0);
+#pragma unroll
+                    for (int m = 0; m < RB; ++m) {
+                        const int kk = k + m * kinc;
+                        const U u1 = 2u * ((U)(IT)Dj[kk] - (U)(IT)Di[kk]);
+#pragma unroll
+                        for (int q = 0; q < VEC; ++q) xv[m].v[q] = (IT)((U)xv[m].v[q] + u1 * v1[q]);
+                    }
+#pragma unroll
+                    for (int m = 0; m < RB; ++m)
+                        *reinterpret_cast<Vec<IT> *>(sI + (size_t)(k + m * kinc) * lds + c0) = xv[m];
+                }
+                for (; k < rows; k += kinc) {
+                    Vec<IT> *dst = reinterpret_cast<Vec<IT> *>(sI + (size_t)k * lds + c0);
+                    Vec<IT> xv = *dst;
+                    const U u1 = 2u * ((U)(IT)Dj[k] - (U)(IT)Di[k]);
+#pragma unroll
+                    for (int q = 0; q < VEC; ++q) xv.v[q] = (IT)((U)xv.v[q] + u1 * v1[q]);
+                    *dst = xv;
+                }
+            }
+            G.sync();                                        // new rows and phi visible
+            if (s_misc[1] == upd) {
+                for (int q = tid; q < n; q += BT) s_bphi[q] = s_phi[q];
+            }
+        }
+    }
+
+    cluster_sync<CL>(G);
+    if constexpr (CL > 1) {
+        if (tid == 0) {
+            mbar_inval(smem_u32(&s_bar[0]));
+            mbar_inval(smem_u32(&s_bar[1]));
+        }
+    }
+    if (failed) return false;
+    {
+        IT *gI = reinterpret_cast<IT *>(s.I) + ((size_t)rep * n + row0) * s.ldg;
+        const int nvg = s.ldg / VEC;
+        for (int idx = tid; idx < rows * nvg; idx += BT) {
+            const int k = idx / nvg, v = idx - k * nvg;
+            *reinterpret_cast<Vec<IT> *>(gI + (size_t)k * s.ldg + v * VEC) =
+                *reinterpret_cast<const Vec<IT> *>(sI + (size_t)k * lds + v * VEC);
+        }
+    }
+    if (rank == 0) {
+        int32_t *gphi = s.phi + (size_t)rep * n;
+        for (int q = tid; q < n; q += BT) gphi[q] = s_phi[q];
+        if (s_misc[1] >= 0) {
+            int32_t *gb = s.best_phi + (size_t)rep * n;
+            for (int q = tid; q < n; q += BT) gb[q] = s_bphi[q];
+        }
+        if (tid == 0) {
+            s.E[rep] = E;
+            s.bestE[rep] = bestE;
+            s.accepts[rep] = __ldcg(s.accepts + rep) + accepts;
+        }
+    }
+    __threadfence();
+    return true;
+}
+
 // Solve path: one launch = one epoch of every replica of the solve (grid = T*R*CL CTAs);
 // the last replica of each group to finish runs the group's tracking + exchange.
-template <class IT, int CL, bool SYM, bool GP>
+template <class IT, int CL, bool SYM, bool GP, bool BIN = false>
 __global__ void __launch_bounds__(256, CL == 4 ? 2 : 1) epoch_kernel(SolveDev s) {
     extern __shared__ __align__(16) unsigned char smem[];
     int rank = 0;
@@ -825,7 +1172,9 @@ __global__ void __launch_bounds__(256, CL == 4 ? 2 : 1) epoch_kernel(SolveDev s)
     if (e >= *(volatile int32_t *)s.stop_epoch) return;
     const Grp G{(int)threadIdx.x, (int)blockDim.x, (int)(threadIdx.x & 31), (int)(threadIdx.x >> 5),
                 (int)(blockDim.x >> 5), 0};
-    const bool ok = replica_epoch<IT, CL, SYM, GP>(s, rep, rank, e, G, smem);
+    bool ok;
+    if constexpr (BIN) ok = replica_epoch_bin<CL>(s, rep, rank, e, G, smem);
+    else ok = replica_epoch<IT, CL, SYM, GP>(s, rep, rank, e, G, smem);
     __syncthreads();
     if (ok && rank == 0 && threadIdx.x == 0) {
         const unsigned prev = atomicAdd(s.finish + g, 1u);
@@ -1300,6 +1649,16 @@ static void *epoch_kernel_ptr(int bits, int cl, bool sym, bool gp) {
     return nullptr;
 }
 
+// The binary-flow epoch (int32 forces, symmetric instance, no goal_print events).
+static void *epoch_bin_ptr(int cl) {
+    switch (cl) {
+        case 1: return reinterpret_cast<void *>(&epoch_kernel<int32_t, 1, true, false, true>);
+        case 2: return reinterpret_cast<void *>(&epoch_kernel<int32_t, 2, true, false, true>);
+        case 4: return reinterpret_cast<void *>(&epoch_kernel<int32_t, 4, true, false, true>);
+        default: return nullptr;
+    }
+}
+
 static void *batch_fn(int bits, int cl) {
     if (bits == 32) {
         switch (cl) {
@@ -1377,6 +1736,10 @@ cudaError_t prepare_kernels() {
             err = cudaFuncSetAttribute(batch_fn(bits, cl), cudaFuncAttributeMaxDynamicSharedMemorySize, maxsm);
             if (err != cudaSuccess) return err;
         }
+    for (int cl : {1, 2, 4}) {
+        err = cudaFuncSetAttribute(epoch_bin_ptr(cl), cudaFuncAttributeMaxDynamicSharedMemorySize, maxsm);
+        if (err != cudaSuccess) return err;
+    }
     return cudaSuccess;
 }
 
@@ -1394,9 +1757,10 @@ cudaError_t launch_setup(const SolveDev &s, int bits, cudaStream_t st) {
     return cudaGetLastError();
 }
 
-cudaError_t launch_epoch(const SolveDev &s, int bits, int cluster, bool sym, int threads,
+cudaError_t launch_epoch(const SolveDev &s, int bits, int cluster, bool sym, bool bin, int threads,
                          size_t smem, cudaStream_t st) {
-    void *fn = epoch_kernel_ptr(bits, cluster, sym, s.ev.log != nullptr && s.ev.goal_print != 0);
+    const bool gp = s.ev.log != nullptr && s.ev.goal_print != 0;
+    void *fn = (bin && !gp && bits == 32 && sym) ? epoch_bin_ptr(cluster) : epoch_kernel_ptr(bits, cluster, sym, gp);
     if (!fn) return cudaErrorInvalidValue;
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3((unsigned)(s.T * s.R * cluster));

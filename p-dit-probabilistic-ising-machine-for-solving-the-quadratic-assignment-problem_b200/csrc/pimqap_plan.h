@@ -49,7 +49,9 @@ struct Plan {
     int bits = 32, cl = 1, threads = 256;
     int npad = 0, lds = 0, ldm = 0, rpc = 0;
     bool sym = false;
-    size_t smem = 0;       // epoch kernel shared memory per CTA
+    bool bin = false;      // the solve path may run the binary-flow epoch kernel
+    size_t smem = 0;       // epoch kernel shared memory per CTA (the generic kernel)
+    size_t smem_bin = 0;   // the binary-flow kernel's (when bin)
     size_t head = 0, tail = 0, total = 0;
     int64_t h2d_bytes = 0;
 };
@@ -59,6 +61,8 @@ struct Plan {
 struct InstanceInfo {
     bool symmetric = false;
     int bits_needed = 32;
+    bool binary_flow = false;   // every flow is 0 or 1
+    bool dist16 = false;        // every distance fits in int16
 };
 InstanceInfo analyse(int n, const int32_t *F, const int32_t *D);
 

@@ -363,7 +363,7 @@ extern "C" pimqap_status pimqap_solve_static(const pimqap_instance *inst,
     bool stopped_goal = false, timed_out = false;
     while (left > 0) {
         const int g = (int)std::min<int64_t>(left, check_every);
-        for (int k = 0; k < g; ++k) PQS_CUDA(pimqap::launch_epoch(d, bits, cl, sym, threads, smem, q));
+        for (int k = 0; k < g; ++k) PQS_CUDA(pimqap::launch_epoch(d, bits, cl, sym, false, threads, smem, q));
         int32_t stop = 0;
         PQS_CUDA(cudaMemcpy(&stop, d.stop_epoch, 4, cudaMemcpyDeviceToHost));
         left -= g;

@@ -29,6 +29,14 @@ def wide(n, seed):
     return instances.Instance(n, F, D)
 
 
+def binary(n, seed, dmax=300):
+    """Symmetric 0/1 flows and int16 distances: solved by the binary-flow epoch kernel."""
+    rng = np.random.default_rng(seed)
+    F = np.triu((rng.random((n, n)) < 0.4).astype(np.int64), 1)
+    D = np.triu(rng.integers(0, dmax, (n, n)), 1)
+    return instances.Instance(n, F + F.T, D + D.T)
+
+
 def heavy_small(n, seed):
     inst = instances.heavy(n, seed)
     return instances.Instance(n, np.minimum(inst.F, 60), inst.D // 4)
@@ -59,6 +67,12 @@ CASES = {
                               {"cluster_size": 4, "threads_per_block": 64}),
     "wide_n50_cluster2": (lambda: wide(50, 30), 1, 3, 1, 1e-9, 1.5, 3, {"cluster_size": 2}),
     "n250_cluster4_ragged": (lambda: instances.uniform(250, 31), 1, 2, 1, 0.0005, 1.5, 1, {"cluster_size": 4}),
+    # symmetric 0/1 flows, int16 distances: the binary-flow kernel (and the generic one for the
+    # same instance, compact_instance = 1)
+    "binary_n90_single_cta": (lambda: binary(90, 32), 2, 3, 2, 0.01, 1.4, 4, {}),
+    "binary_n37_t64_ragged": (lambda: binary(37, 33), 1, 4, 3, 0.02, 1.3, 6, {"threads_per_block": 64}),
+    "binary_n200_cluster2": (lambda: binary(200, 34, 30000), 1, 2, 1, 0.0001, 1.5, 2, {"cluster_size": 2}),
+    "grid_n256_generic_kernel": (lambda: instances.grid256(17), 1, 2, 1, 0.0015, 1.5, 2, {"compact_instance": 1}),
 }
 
 
