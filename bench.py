@@ -196,9 +196,12 @@ def read_traffic():
     return float(m.group(1)) if m else None
 
 
-def rank_instance(rank):
-    """The instance rank `rank` solves: one grid256 instance per GPU (the work is sharded by
-    instance; ranks never exchange data)."""
+def rank_instance(rank, workload="grid256"):
+    """The instance rank `rank` solves: one instance per GPU (the work is sharded by
+    instance; ranks never exchange data).  clique92: the structure of the reference's tai256c
+    program (unit flows among 92 of 256 facilities), solved with its moves."""
+    if workload == "clique92":
+        return instances.clique_flow(1000 + rank)
     return instances.grid256(1000 + rank)
 
 
@@ -232,12 +235,13 @@ def run_ours(args):
         import datetime
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
 
-    inst = rank_instance(rank)
+    inst = rank_instance(rank, args.workload)
+    act = 92 if args.workload == "clique92" else 0
     params = pimqap.default_params(replicas=REPLICAS, groups=GROUPS, sweeps_per_exchange=SWEEPS_PER_EXCHANGE,
                                    beta_max=BETA_MAX, beta_ratio=BETA_RATIO, beta_internal=1, seed=1 + rank,
                                    device=local, megaiters_per_launch=MEGAITERS_PER_STEP,
                                    max_megaiters=2 ** 31 - 1, cluster_size=args.cluster_size,
-                                   threads_per_block=args.threads)
+                                   threads_per_block=args.threads, active_facilities=act)
     flush = torch.empty(L2_FLUSH_BYTES, dtype=torch.uint8, device=f"cuda:{local}")
     solver = pimqap.Solver(inst.F, inst.D, params)
     for _ in range(args.warmup):
@@ -285,7 +289,8 @@ def run_ours(args):
                                device=local,
                                megaiters_per_launch=MEGAITERS_PER_STEP,
                                max_megaiters=args.steps * MEGAITERS_PER_STEP,
-                               cluster_size=args.cluster_size, threads_per_block=args.threads)
+                               cluster_size=args.cluster_size, threads_per_block=args.threads,
+                               active_facilities=act)
     barrier()
     e0 = time.perf_counter()
     res = pimqap.solve(Fp.numpy(), Dp.numpy(), p2)
@@ -295,7 +300,7 @@ def run_ours(args):
     line = None
     if rank == 0:
         cpu = None
-        if world == 1 and not args.no_cpu_baseline:
+        if world == 1 and not args.no_cpu_baseline and args.workload == "grid256":
             got = ref_cpu_throughput(inst.F, inst.D, budget_s=12.0)
             if got:
                 v, cores, kind, sample = got
@@ -305,7 +310,10 @@ def run_ours(args):
             "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": f"int{8 * s}",
             "data": "synthetic (seeded grid256 instance per GPU)",
-            "config": {"workload": "grid256: n=256 Bernoulli(0.36) flow, 16x16 grid sq. distance + U[0,3]; "
+            "config": {"workload": ("grid256: n=256 Bernoulli(0.36) flow, 16x16 grid sq. distance + U[0,3]; "
+                                    if args.workload == "grid256" else
+                                    "clique92: n=256, unit flows among facilities 0..91, 16x16 grid sq. "
+                                    "distance + U[0,3]; the tai256c program's moves; ") +
                                    "64 replicas, geometric beta ladder, exchange every 4 sweeps, "
                                    "10^4 sweeps = 100 steps",
                        "n": N, "replicas": reps, "sweeps_per_step": MEGAITERS_PER_STEP * SWEEPS_PER_EXCHANGE,
@@ -463,6 +471,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--workload", choices=["grid256", "clique92"], default="grid256",
+                    help="headline instance (clique92: the tai256c program's structure and moves)")
     ap.add_argument("--cluster-size", type=int, default=0, help="CTAs per replica (0 = automatic)")
     ap.add_argument("--threads", type=int, default=0, help="threads per CTA (0 = automatic)")
     ap.add_argument("--suite", choices=["headline", "batch", "serve"], default="headline",

@@ -91,7 +91,12 @@ typedef struct pimqap_params {
     int32_t compact_instance;    /* 0 = automatic: a symmetric instance with 0/1 flows and
                                     int16 distances keeps D and F in shared memory beside the
                                     force rows (same results); 1 = never */
-    int32_t pad1;
+    int32_t active_facilities;   /* > 0: the moves of the reference's tai256c program
+                                    (CPU-PIM/CPU_PIM_tai256c.cpp, which hard-wires 92 of 256):
+                                    facilities 0..A-1 must form a clique of unit flows and the
+                                    others carry none; a location holding an inactive facility
+                                    weighs the actives and all inactives as one lumped move.
+                                    pimqap_solve / solver handles only; no goal_print events */
 } pimqap_params;
 
 /* Fills p with the reference's defaults: 10 replicas, 20 groups, 4 sweeps per exchange,

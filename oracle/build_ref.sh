@@ -15,6 +15,9 @@
 #   _ref/cpu_pim_stock     the unmodified reference CLI (for output-format checks)
 #   _ref/cpu_pim_philox    the reference CLI with stock capacities on the solver's Philox
 #                          streams (ref_cli_main.cpp; for the CLI parity fixtures)
+#   _ref/libref_tai.so     CPU-PIM/CPU_PIM_tai256c.cpp (n = 256, 92 active facilities hard-wired
+#                          there; 10 replicas, 20 threads), Philox engine shim; its lumped draw
+#                          goes to the shim's second engine (ref_prelude.h)
 #
 # The reference source path is $PIMQAP_REF_ROOT (default /root/reference).  When it is
 # absent the script does nothing and exits 0.
@@ -67,6 +70,27 @@ build_lib() {  # out maxn maxr maxt extra-flags
         $CXX $CXXFLAGS $LIBFLAGS "$@" -shared -include "$HERE/ref_prelude.h" -x c++ - -o "$OUT/$out.tmp"
     mv "$OUT/$out.tmp" "$OUT/$out"
 }
+
+# CPU_PIM_tai256c.cpp: N becomes assignable (the harness loads instances), doMegaIteraTai
+# takes the name the harness calls, and the lumped move's draw reads the shim's second engine.
+TAI="$REF_ROOT/CPU-PIM/CPU_PIM_tai256c.cpp"
+if [ -f "$TAI" ]; then
+    for pat in '^const int N = 256;$' 'randomNonActiveIndex(rng\[t\])' \
+               '^    cout << "Elapsed time: " << duration.count() / 1000.0 << " seconds." << endl;$'; do
+        c=$(grep -c "$pat" "$TAI" || true)
+        if [ "$c" != "1" ]; then
+            echo "build_ref.sh: pattern '$pat' matched $c lines in $TAI" >&2
+            exit 1
+        fi
+    done
+    { sed -e 's/^const int N = 256;$/int N = 256;/' \
+          -e 's/doMegaIteraTai/doMegaItera/g' \
+          -e 's/randomNonActiveIndex(rng\[t\])/randomNonActiveIndex(pimqap_ref::lumped(rng[t]))/' \
+          -e 's/^    cout << "Elapsed time: " << duration.count() \/ 1000.0 << " seconds." << endl;$/& return 0;/' "$TAI"
+      cat "$HERE/ref_harness.cpp"; } |
+        $CXX $CXXFLAGS $LIBFLAGS -shared -include "$HERE/ref_prelude.h" -x c++ - -o "$OUT/libref_tai.so.tmp"
+    mv "$OUT/libref_tai.so.tmp" "$OUT/libref_tai.so"
+fi
 
 build_lib libref_stock.so 160 10 20
 build_lib libref_big.so 256 64 64

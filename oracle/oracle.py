@@ -34,7 +34,7 @@ class _RunState(C.Structure):
         ("E", C.c_void_p), ("bestE", C.c_void_p), ("beta", C.c_void_p),
         ("order", C.c_void_p), ("time_since_swap", C.c_void_p), ("thread_best", C.c_void_p),
         ("single_best", C.c_int64), ("megaiters_done", C.c_int64), ("accepts", C.c_int64),
-        ("target_megaiter", C.c_int64),
+        ("target_megaiter", C.c_int64), ("active", C.c_int32), ("pad", C.c_int32),
     ]
 
 
@@ -142,9 +142,12 @@ class Oracle:
                                           picks.ctypes.data if record_picks else None)
         return int(acc), picks
 
-    def setup(self, D, F, T, R, numitera, beta0, delta_beta, seed, cap=None) -> RunState:
+    def setup(self, D, F, T, R, numitera, beta0, delta_beta, seed, cap=None, active=0) -> RunState:
+        """active > 0: the clique-flow update of CPU_PIM_tai256c.cpp with that many active
+        facilities (orc_update_clique)."""
         n = D.shape[0]
         st = RunState(n, T, R, cap if cap is not None else R, numitera, seed)
+        st.c.active = active
         self.lib.orc_setup(C.byref(st.c), np.ascontiguousarray(D, np.int32),
                            np.ascontiguousarray(F, np.int32), beta0, delta_beta)
         return st

@@ -193,6 +193,103 @@ int orc_update(int n, const int32_t *D, const int32_t *F, int64_t *I, int32_t *p
     return -1;
 }
 
+uint32_t orc_lumped_word(uint64_t seed, uint32_t group, uint32_t replica, uint32_t sweep,
+                         uint32_t loc, uint32_t k) {
+    const uint32_t key[2] = {(uint32_t)seed, (uint32_t)(seed >> 32)};
+    uint32_t out[4];
+    if (k < 2) {
+        const uint32_t ctr[4] = {loc, sweep, replica, group};
+        orc_philox4x32_10(ctr, key, out);
+        return out[2 + k];
+    }
+    const uint32_t m = (k - 2) / 4 + 1;
+    const uint32_t ctr[4] = {loc, sweep, replica, group + 0x10000u * m};
+    orc_philox4x32_10(ctr, key, out);
+    return out[(k - 2) % 4];
+}
+
+int orc_update_clique(int n, int act, const int32_t *D, const int32_t *F, int64_t *I,
+                      int32_t *phi, int32_t *phiinv, int64_t *E, int64_t *bestE, double beta,
+                      int i, uint32_t w0, uint32_t w1, uint64_t seed, uint32_t group,
+                      uint32_t replica, uint32_t sweep) {
+    long double probs[256];
+    int64_t dEs[256];
+    int64_t maxDeltaE = 0;
+    const double r = orc_canonical(w0, w1);             /* :228 */
+    double probSum = 0.0;
+    const int a = phi[i];
+    const int ncand = a < act ? n : act + 1;            /* :236, act = the lumped candidate */
+    const int64_t *Ii = I + (size_t)i * n;
+    for (int b = 0; b < ncand; ++b) {                   /* :236-249, zero diagonals */
+        int j = phiinv[b];
+        const int64_t *Ij = I + (size_t)j * n;
+        int64_t dE = Ii[b] + Ij[a] - Ii[a] - Ij[b] -
+                     (-(int64_t)D[i * n + j] - D[j * n + i]) * (-(int64_t)F[a * n + b] - F[b * n + a]);
+        dEs[b] = dE;
+        if (dE > maxDeltaE) maxDeltaE = dE;
+    }
+    const int64_t cut = trunc_cutoff((double)maxDeltaE - 20.0 / beta);   /* :251-252 */
+    for (int b = 0; b < ncand; ++b) {                   /* :253-266 */
+        probs[b] = 0.0L;
+        const int lumped = a >= act && b == act;
+        if (dEs[b] > cut || lumped) {
+            long double expr = (long double)(beta * (double)dEs[b]);
+            probs[b] = exp2l(expr);
+            if (lumped) probs[b] *= (long double)(n - act);
+            probSum = (double)((long double)probSum + probs[b]);
+        }
+    }
+    const double scaledR = r * probSum;                  /* :268 */
+    double cumulativeProb = 0.0;
+    const int npick = a < act ? n : act;                 /* the lumped candidate is not scanned */
+    for (int b = 0; b < npick; ++b) {                    /* :270-320 */
+        cumulativeProb = (double)((long double)cumulativeProb + probs[b]);
+        if (cumulativeProb >= scaledR) {
+            if (b != a) {
+                int j = phiinv[b];
+                *E -= dEs[b];
+                phi[i] = b;
+                phiinv[b] = i;
+                phi[j] = a;
+                phiinv[a] = j;
+                /* the reference's region-split update equals the full rank-2 update for a
+                   clique of unit flows (:286-302) */
+                for (int k = 0; k < n; ++k) {
+                    int64_t d1 = (int64_t)D[k * n + j] - D[k * n + i];
+                    int64_t d2 = (int64_t)D[j * n + k] - D[i * n + k];
+                    int64_t *Ik = I + (size_t)k * n;
+                    for (int c = 0; c < n; ++c)
+                        Ik[c] += d1 * ((int64_t)F[c * n + b] - F[c * n + a]) +
+                                 d2 * ((int64_t)F[b * n + c] - F[a * n + c]);
+                }
+                if (*E < *bestE) *bestE = *E;
+            }
+            return b;
+        }
+    }
+    if (a >= act) {                                      /* :323-336, inactive to inactive */
+        const uint32_t range = (uint32_t)(n - act);
+        uint32_t k = 0;
+        uint64_t product = (uint64_t)orc_lumped_word(seed, group, replica, sweep, (uint32_t)i, k++) * range;
+        uint32_t low = (uint32_t)product;
+        if (low < range) {
+            uint32_t threshold = (uint32_t)(0u - range) % range;
+            while (low < threshold) {
+                product = (uint64_t)orc_lumped_word(seed, group, replica, sweep, (uint32_t)i, k++) * range;
+                low = (uint32_t)product;
+            }
+        }
+        const int b = act + (int)(product >> 32);
+        const int j = phiinv[b];
+        phi[i] = b;
+        phiinv[b] = i;
+        phi[j] = a;
+        phiinv[a] = j;
+        return b;
+    }
+    return -1;
+}
+
 int64_t orc_replica_sweeps(int n, const int32_t *D, const int32_t *F, int64_t *I,
                            int32_t *phi, int32_t *phiinv, int64_t *E, int64_t *bestE,
                            double beta, uint64_t seed, uint32_t group, uint32_t replica,
@@ -300,6 +397,21 @@ int orc_run(orc_run_state *st, const int32_t *D, const int32_t *F, int64_t megai
         for (int t = 0; t < T; ++t) {
             for (int l = 0; l < R; ++l) {                /* :360-362 */
                 size_t rep = (size_t)t * R + l;
+                if (st->active > 0) {
+                    for (int s2 = 0; s2 < st->numitera; ++s2)
+                        for (int i = 0; i < n; ++i) {
+                            const uint32_t sw = sweep0 + (uint32_t)s2;
+                            const int a = st->phi[rep * n + i];
+                            const int b = orc_update_clique(
+                                n, st->active, D, F, st->I + rep * (size_t)n * n, st->phi + rep * n,
+                                st->phiinv + rep * n, &st->E[rep], &st->bestE[rep], st->beta[rep], i,
+                                orc_sweep_word(st->seed, (uint32_t)t, (uint32_t)l, sw, (uint32_t)i, 0),
+                                orc_sweep_word(st->seed, (uint32_t)t, (uint32_t)l, sw, (uint32_t)i, 1),
+                                st->seed, (uint32_t)t, (uint32_t)l, sw);
+                            if (b >= 0 && b != a) st->accepts++;
+                        }
+                    continue;
+                }
                 st->accepts += orc_replica_sweeps(
                     n, D, F, st->I + rep * (size_t)n * n, st->phi + rep * n,
                     st->phiinv + rep * n, &st->E[rep], &st->bestE[rep], st->beta[rep],

@@ -13,6 +13,7 @@
  *   orc_beta_ladder ................... beta ladder (CPU_PIM.cpp:111-119)
  *   orc_force_init .................... force matrix + energy (CPU_PIM.cpp:164-192)
  *   orc_update ........................ one p-dit update (CPU_PIM.cpp:207-287)
+ *   orc_update_clique ................. one update of CPU_PIM_tai256c.cpp (:209-337)
  *   orc_replica_sweeps ................ doMegaItera (CPU_PIM.cpp:195-290)
  *   orc_track_exchange ................ best tracking + replica exchange (CPU_PIM.cpp:293-344)
  *   orc_run ........................... threadToRun for all groups in lock step (CPU_PIM.cpp:292-364)
@@ -102,7 +103,28 @@ typedef struct orc_run_state {
     int64_t megaiters_done;   /* mega-iterations completed (exchange + sweeps) */
     int64_t accepts;
     int64_t target_megaiter;  /* first mega-iteration whose tracking saw single_best <= goal, or -1 */
+    int32_t active;           /* 0: orc_update; A > 0: orc_update_clique with A active facilities */
+    int32_t pad;
 } orc_run_state;
+
+/* The clique-flow update of CPU-PIM/CPU_PIM_tai256c.cpp (doMegaIteraTai, :209-337), with the
+   reference's hard-wired 92 active facilities and n = 256 made parameters: facilities
+   0..act-1 form a clique of unit flows, the others have no flow at all (so every swap between
+   two of them leaves the energy and the force matrix unchanged), and D, F have zero diagonals.
+   A location holding an inactive facility weighs the active facilities one by one and all
+   inactive ones as one lumped candidate (weight (n - act) * exp2(beta * dE(act)), never cut
+   off, :253-266); when the lumped candidate is drawn, the facility to swap with is
+   act + uniform_int(n - act) (:324-336) on the words of orc_lumped_word.  Returns the facility
+   swapped in (phi[i] for no move) or -1. */
+int orc_update_clique(int n, int act, const int32_t *D, const int32_t *F, int64_t *I,
+                      int32_t *phi, int32_t *phiinv, int64_t *E, int64_t *bestE, double beta,
+                      int i, uint32_t w0, uint32_t w1, uint64_t seed, uint32_t group,
+                      uint32_t replica, uint32_t sweep);
+
+/* Words of the lumped draw of update (group, replica, sweep, loc): words 2 and 3 of the
+   update's Philox block, then blocks with counter word 3 = group + 0x10000 * m, m >= 1. */
+uint32_t orc_lumped_word(uint64_t seed, uint32_t group, uint32_t replica, uint32_t sweep,
+                         uint32_t loc, uint32_t k);
 
 /* setup(): ladder, shuffle, force matrices, energies (CPU_PIM.cpp:109-193).  The caller
    allocates every array of st and fills n, T, R, cap, numitera, seed. */

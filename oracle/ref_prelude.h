@@ -112,6 +112,7 @@ struct pimqap_ref_engine {
             uint32_t rep = (uint32_t)(rest % (uint64_t)rr);
             uint64_t mega = rest / (uint64_t)rr;
             c[0] = loc; c[1] = (uint32_t)(mega * (uint64_t)it + itera); c[2] = rep; c[3] = grp;
+            for (int q = 0; q < 4; ++q) last[q] = c[q];
             idx &= 1;
         }
         pimqap_ref::philox4x32_10(c, (uint32_t)pimqap_ref::g_seed,
@@ -123,8 +124,44 @@ struct pimqap_ref_engine {
     uint32_t grp = 0;
     int nn = 1, rr = 1, it = 1;
     uint64_t calls = 0;
+    uint32_t last[4] = {0, 0, 0, 0};   // counter of the update whose words were drawn last
+};
+
+/* CPU_PIM_tai256c.cpp draws the lumped move's facility from rng[t] after the update's two
+   words; the tai harness build routes that draw here instead (oracle/build_ref.sh), so the
+   sweep engine keeps exactly two words per update.  The words are 2 and 3 of the update's
+   Philox block, then blocks with counter word 3 = group + 0x10000 * m (orc_lumped_word). */
+struct pimqap_ref_lumped_engine {
+    typedef uint_fast32_t result_type;
+    static constexpr result_type min() { return 0; }
+    static constexpr result_type max() { return 0xFFFFFFFFu; }
+    uint32_t ctr[4] = {0, 0, 0, 0};
+    uint32_t k = 0;
+    result_type operator()() {
+        uint32_t c[4] = {ctr[0], ctr[1], ctr[2], ctr[3]};
+        uint32_t w;
+        if (k < 2) {
+            w = 2 + k;
+        } else {
+            const uint32_t m = (k - 2) / 4 + 1;
+            c[3] = ctr[3] + 0x10000u * m;
+            w = (k - 2) % 4;
+        }
+        ++k;
+        pimqap_ref::philox4x32_10(c, (uint32_t)pimqap_ref::g_seed, (uint32_t)(pimqap_ref::g_seed >> 32));
+        return c[w];
+    }
 };
 }  // namespace std
+
+namespace pimqap_ref {
+inline std::pimqap_ref_lumped_engine &lumped(const std::pimqap_ref_engine &e) {
+    static thread_local std::pimqap_ref_lumped_engine L;
+    for (int q = 0; q < 4; ++q) L.ctr[q] = e.last[q];
+    L.k = 0;
+    return L;
+}
+}  // namespace pimqap_ref
 #define mt19937 pimqap_ref_engine
 #endif
 

@@ -47,6 +47,7 @@ struct Options {
     unsigned long long seed = 1;
     std::string json;
     int device = 0, force_bits = 0;
+    int active = 0;                      // --active-facilities: the tai256c program's moves
 };
 
 void usage(const char *argv0) {   // :486-503
@@ -73,6 +74,8 @@ void usage(const char *argv0) {   // :486-503
     cout << "--json PATH     write the best cost, permutation and time to target as JSON" << endl;
     cout << "--device D      CUDA device ordinal (default 0)" << endl;
     cout << "--force-bits B  force-matrix width 32 or 64 (default: from the instance bound)" << endl;
+    cout << "--active-facilities A  the moves of the reference's CPU_PIM_tai256c program: facilities" << endl;
+    cout << "                0..A-1 form a clique of unit flows, the others carry none (A = 92 there)" << endl;
 }
 
 // std::stoi / std::stod as the reference uses them, with a message instead of an abort.
@@ -164,6 +167,9 @@ int parse(int argc, char **argv, Options &o) {
         } else if (arg == "--device") {
             if (!(s = value()) || !to_ll(arg, s, &v)) return 1;
             o.device = (int)v;
+        } else if (arg == "--active-facilities") {
+            if (!(s = value()) || !to_ll(arg, s, &v)) return 1;
+            o.active = (int)v;
         } else if (arg == "--force-bits") {
             if (!(s = value()) || !to_ll(arg, s, &v)) return 1;
             o.force_bits = (int)v;
@@ -265,6 +271,7 @@ int run(int argc, char **argv) {
     p.seed = o.seed;
     p.device = o.device;
     p.force_bits = o.force_bits;
+    p.active_facilities = o.active;
     p.auto_lower = o.lower;
     p.auto_higher = o.higher;
     p.beta_internal = 1;

@@ -129,6 +129,16 @@ InstanceInfo analyse(int n, const int32_t *F, const int32_t *D) {
         if (F[k] != 0 && F[k] != 1) info.binary_flow = false;
         if (D[k] < -32768 || D[k] > 32767) info.dist16 = false;
     }
+    if (info.binary_flow) {   // clique of unit flows on a prefix of the facilities?
+        int A = 0;
+        while (A < n && [&] { for (int b = 0; b < n; ++b) if (F[A * n + b]) return true; return false; }()) ++A;
+        bool ok = A >= 2 && A < n;
+        for (int a = 0; a < n && ok; ++a) {
+            ok = D[a * n + a] == 0;
+            for (int b = 0; b < n && ok; ++b) ok = F[a * n + b] == ((a != b && a < A && b < A) ? 1 : 0);
+        }
+        info.clique = ok ? A : 0;
+    }
     std::vector<long double> rD(n, 0), cD(n, 0);
     long double rFmax = 0, cFmax = 0;
     for (int i = 0; i < n; ++i)
@@ -251,6 +261,8 @@ pimqap_status check_params(const pimqap_instance *inst, const pimqap_params *p) 
         return fail(PIMQAP_ERR_ARG, "event capacities must be >= 0");
     if (p->compact_instance != 0 && p->compact_instance != 1)
         return fail(PIMQAP_ERR_ARG, "compact_instance must be 0 or 1");
+    if (p->active_facilities < 0 || p->active_facilities >= inst->n && p->active_facilities != 0)
+        return fail(PIMQAP_ERR_ARG, "active_facilities must be 0 or in [2, n)");
     if (p->force_bits != 0 && p->force_bits != 32 && p->force_bits != 64)
         return fail(PIMQAP_ERR_ARG, "force_bits must be 0, 32 or 64");
     if (p->threads_per_block != 0 && p->threads_per_block != 64 && p->threads_per_block != 128 &&
@@ -313,12 +325,20 @@ pimqap_status plan_instance(const pimqap_instance *inst, const pimqap_params *pa
     P.ldm = std::max(P.npad, P.cl * P.rpc);
     P.smem = pimqap::epoch_smem_bytes(n, P.rpc, P.lds, P.cl, P.bits);
     // binary flows and int16 distances: the instance itself fits next to the force rows
-    if (info.symmetric && info.binary_flow && info.dist16 && P.bits == 32 && params->compact_instance == 0) {
+    if (info.symmetric && info.binary_flow && info.dist16 && P.bits == 32 &&
+        (params->compact_instance == 0 || params->active_facilities > 0)) {
         const size_t sb = pimqap::epoch_smem_bytes_bin(n, P.rpc, P.lds, P.cl);
         if (sb <= maxsm) {
             P.bin = true;
             P.smem_bin = sb;
         }
+    }
+    if (params->active_facilities > 0) {   // the tai256c program's moves (CPU_PIM_tai256c.cpp)
+        if (!P.bin || !info.symmetric || info.clique != params->active_facilities)
+            return fail(PIMQAP_ERR_ARG, "active_facilities needs a symmetric instance whose flows are a clique of "
+                                        "unit flows on facilities 0..active_facilities-1 (zero diagonals, "
+                                        "distances within int16, int32 forces)");
+        P.act = params->active_facilities;
     }
     const size_t reps = (size_t)P.T * P.R, nn = (size_t)n * P.ldm;
     // head: everything uploaded from the host; tail: state that starts at zero
@@ -338,6 +358,7 @@ void carve_instance(const Plan &P, char *head, char *tail, SolveDev *out) {
     const size_t reps = (size_t)T * R, nn = (size_t)n * P.ldm;
     SolveDev d{};
     d.n = n; d.R = R; d.T = T; d.cap = cap; d.spe = P.spe;
+    d.act = P.act;
     d.ldg = P.npad; d.lds = P.lds; d.ldm = P.ldm; d.rpc = P.rpc;
     char *cur = head;
     d.D = carve<int32_t>(cur, nn);

@@ -78,6 +78,8 @@ struct SolveDev {
     unsigned long long *start_ns;   // [1]  %globaltimer when sweeping started
     int32_t *error;            // [1]       kErr* bits
     EventLink ev;              // progress events (optional)
+    int32_t act;               // > 0: clique-flow moves with facilities 0..act-1 active
+    int32_t pad_act;
 };
 
 // Compact per-instance result of a batch.

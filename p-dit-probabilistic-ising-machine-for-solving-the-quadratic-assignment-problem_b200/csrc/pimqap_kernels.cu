@@ -108,6 +108,53 @@ __device__ __forceinline__ void philox_2words(uint32_t c0, uint32_t c1, uint32_t
     w1 = c1;
 }
 
+// All four words of the block (the lumped draw of a clique-flow update).
+__device__ __forceinline__ void philox_4words(uint32_t c0, uint32_t c1, uint32_t c2, uint32_t c3,
+                                              uint32_t k0, uint32_t k1, uint32_t w[4]) {
+#pragma unroll
+    for (int r = 0; r < 10; ++r) {
+        const uint32_t hi0 = __umulhi(0xD2511F53u, c0), lo0 = 0xD2511F53u * c0;
+        const uint32_t hi1 = __umulhi(0xCD9E8D57u, c2), lo1 = 0xCD9E8D57u * c2;
+        const uint32_t n0 = hi1 ^ c1 ^ k0, n2 = hi0 ^ c3 ^ k1;
+        c0 = n0; c1 = lo1; c2 = n2; c3 = lo0;
+        k0 += 0x9E3779B9u;
+        k1 += 0xBB67AE85u;
+    }
+    w[0] = c0; w[1] = c1; w[2] = c2; w[3] = c3;
+}
+
+// Facility of a lumped clique-flow move (CPU_PIM_tai256c.cpp:326): act + uniform_int(range)
+// by Lemire's method on words 2 and 3 of the update's block, then on blocks whose counter
+// word 3 is group + 0x10000 m, m = 1, 2, ... (one thread).
+__device__ __noinline__ int lumped_facility(uint32_t loc, uint32_t sweep, uint32_t rep, uint32_t grp,
+                                            uint32_t k0, uint32_t k1, int act, uint32_t range) {
+    uint32_t w[4];
+    philox_4words(loc, sweep, rep, grp, k0, k1, w);
+    uint32_t k = 0;
+    auto word = [&]() -> uint32_t {
+        uint32_t v;
+        if (k < 2) {
+            v = w[2 + k];
+        } else {
+            const uint32_t m = (k - 2) / 4 + 1;
+            if ((k - 2) % 4 == 0) philox_4words(loc, sweep, rep, grp + 0x10000u * m, k0, k1, w);
+            v = w[(k - 2) % 4];
+        }
+        ++k;
+        return v;
+    };
+    unsigned long long product = (unsigned long long)word() * range;
+    uint32_t low = (uint32_t)product;
+    if (low < range) {
+        const uint32_t threshold = (0u - range) % range;
+        while (low < threshold) {
+            product = (unsigned long long)word() * range;
+            low = (uint32_t)product;
+        }
+    }
+    return act + (int)(product >> 32);
+}
+
 // std::generate_canonical<double, 53> over two 32-bit words (CPU_PIM.cpp:212):
 // (w0 + w1 * 2^32) rounded once to double, times 2^-64, clamped below 1.
 __device__ __forceinline__ double canonical53(uint32_t w0, uint32_t w1) {
@@ -940,6 +987,7 @@ __device__ bool replica_epoch_bin(const SolveDev &s, int rep, int rank, int e, c
     const uint32_t k0 = (uint32_t)s.seed, k1 = (uint32_t)(s.seed >> 32);
     const int K = (n + BT - 1) / BT;                         // weights per thread (<= 4)
     const int nvec = npad / VEC;
+    const int act = s.act;
     bool failed = false;
     int upd = 0;
 
@@ -954,6 +1002,10 @@ __device__ bool replica_epoch_bin(const SolveDev &s, int rep, int rank, int e, c
                 if constexpr (CL > 1) mbar_arrive_expect_tx(smem_u32(&s_bar[p]), tx_bytes);
             }
             const int a = s_phi[i];
+            // clique flows (act > 0): an inactive facility weighs the actives and one lumped
+            // candidate b = act for all inactives (CPU_PIM_tai256c.cpp:236, :253-266)
+            const bool inact = act > 0 && a >= act;
+            const int ncand = inact ? act + 1 : n, npick = inact ? act : n;
             const int16_t *Di = s_Ds + (size_t)i * rpc;      // D[i][own rows]
             const int owner = i / rpc;
             const int Dii = s_Dd[i], Faa = fbit(a, a);
@@ -1004,10 +1056,11 @@ __device__ bool replica_epoch_bin(const SolveDev &s, int rep, int rank, int e, c
             for (int k = 0; k < 4; ++k) {
                 d[k] = 0;
                 x[k] = 0.0;
-                if (k < K && b0 + k < n) {
+                if (k < K && b0 + k < ncand) {
                     const int b = b0 + k;
                     d[k] = (CL == 1) ? s_A[p * npad + b] : (IT)((U)s_A[p * npad + b] + (U)s_B[p * npad + b]);
                     x[k] = exp2(__dmul_rn(beta, (double)d[k]));
+                    if (inact && b == act) x[k] = __dmul_rn(x[k], (double)(n - act));   // :261-264
                     lmax = d[k] > lmax ? d[k] : lmax;
                 }
             }
@@ -1026,7 +1079,8 @@ __device__ bool replica_epoch_bin(const SolveDev &s, int rep, int rank, int e, c
             double local = 0.0;
 #pragma unroll
             for (int k = 0; k < 4; ++k) {
-                if (k < K && (long long)d[k] > cut && b0 + k < n) local = __dadd_rn(local, x[k]);
+                const bool lumped = inact && b0 + k == act;      // never cut off (:256)
+                if (k < K && ((long long)d[k] > cut || lumped) && b0 + k < ncand) local = __dadd_rn(local, x[k]);
                 pre[k] = local;
             }
             double incl = local;
@@ -1048,7 +1102,7 @@ __device__ bool replica_epoch_bin(const SolveDev &s, int rep, int rank, int e, c
             const double X = __dadd_rn(base, excl);
 #pragma unroll
             for (int k = 0; k < 4; ++k) {
-                if (k < K && b0 + k < n) {
+                if (k < K && b0 + k < npick) {               // the lumped candidate is not scanned
                     if (__dadd_rn(X, pre[k]) >= target) {   // :251
                         // the candidate with its partner j = phiinv(b), read before anyone swaps
                         atomicMin(&s_misc[0], ((b0 + k) << 9) | s_inv[b0 + k]);
@@ -1059,6 +1113,22 @@ __device__ bool replica_epoch_bin(const SolveDev &s, int rep, int rank, int e, c
             G.sync();
             const int key = s_misc[0];
             const int bs = key >> 9;
+            if (bs >= n && inact) {
+                // lumped move between two inactive facilities: energy and forces unchanged
+                // (CPU_PIM_tai256c.cpp:323-336)
+                if (tid == 0) {
+                    const int b = lumped_facility((uint32_t)i, sweep, (uint32_t)l, (uint32_t)g, k0, k1, act,
+                                                  (uint32_t)(n - act));
+                    const int j = s_inv[b];
+                    s_phi[i] = b;
+                    s_inv[b] = i;
+                    s_phi[j] = a;
+                    s_inv[a] = j;
+                    if (b != a) ++accepts;                   // tid 0's count is the one stored
+                }
+                G.sync();
+                continue;
+            }
             if (bs >= n || bs == a) continue;                // no move / self move (:252)
 
             // ---- accepted swap: every row and bit row it needs is already in shared memory
@@ -1077,9 +1147,25 @@ __device__ bool replica_epoch_bin(const SolveDev &s, int rep, int rank, int e, c
                 if (tid == 0) s_misc[1] = upd;
             }
             const int16_t *Dj = s_Ds + (size_t)j * rpc;
-            // I[k][c] += 2 (D[j][k] - D[i][k]) (F[bs][c] - F[a][c])
+            // I[k][c] += 2 (D[j][k] - D[i][k]) (F[bs][c] - F[a][c]).  With clique flows only
+            // columns a and bs change when both facilities are active, and only the active
+            // columns when one is (CPU_PIM_tai256c.cpp:286-302): the other differences are 0.
+            int nv = nvec;
+            if (act > 0) {
+                if (a < act && bs < act) {
+                    for (int k = tid; k < rows; k += BT) {
+                        const U u1 = 2u * ((U)(IT)Dj[k] - (U)(IT)Di[k]);
+                        IT *Ik = sI + (size_t)k * lds;
+                        Ik[a] = (IT)((U)Ik[a] + u1);         // F[bs][a] - F[a][a] = 1
+                        Ik[bs] = (IT)((U)Ik[bs] - u1);       // F[bs][bs] - F[a][bs] = -1
+                    }
+                    nv = 0;
+                } else {
+                    nv = min(nvec, (act + VEC - 1) / VEC);
+                }
+            }
             for (int cv = tid % nvec, k0r = tid / nvec, kstep = max(1, BT / nvec);
-                 cv < nvec; cv += (BT >= nvec ? nvec : BT)) {
+                 cv < nv; cv += (BT >= nvec ? nvec : BT)) {
                 if (BT >= nvec && k0r >= kstep) break;
                 const int c0 = cv * VEC;
                 const unsigned fb = (s_Fb[bs * nw + (c0 >> 5)] >> (c0 & 31)) & 15u;
@@ -1760,7 +1846,9 @@ cudaError_t launch_setup(const SolveDev &s, int bits, cudaStream_t st) {
 cudaError_t launch_epoch(const SolveDev &s, int bits, int cluster, bool sym, bool bin, int threads,
                          size_t smem, cudaStream_t st) {
     const bool gp = s.ev.log != nullptr && s.ev.goal_print != 0;
-    void *fn = (bin && !gp && bits == 32 && sym) ? epoch_bin_ptr(cluster) : epoch_kernel_ptr(bits, cluster, sym, gp);
+    // clique-flow solves (s.act > 0) exist only in the binary-flow kernel
+    void *fn = (bin && bits == 32 && sym && (!gp || s.act > 0)) ? epoch_bin_ptr(cluster)
+                                                                 : epoch_kernel_ptr(bits, cluster, sym, gp);
     if (!fn) return cudaErrorInvalidValue;
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3((unsigned)(s.T * s.R * cluster));

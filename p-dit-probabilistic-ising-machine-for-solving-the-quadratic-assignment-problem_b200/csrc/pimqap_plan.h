@@ -52,6 +52,7 @@ struct Plan {
     bool bin = false;      // the solve path may run the binary-flow epoch kernel
     size_t smem = 0;       // epoch kernel shared memory per CTA (the generic kernel)
     size_t smem_bin = 0;   // the binary-flow kernel's (when bin)
+    int act = 0;           // clique-flow moves with facilities 0..act-1 active (0 = off)
     size_t head = 0, tail = 0, total = 0;
     int64_t h2d_bytes = 0;
 };
@@ -63,6 +64,7 @@ struct InstanceInfo {
     int bits_needed = 32;
     bool binary_flow = false;   // every flow is 0 or 1
     bool dist16 = false;        // every distance fits in int16
+    int clique = 0;             // A > 0: F[a][b] = 1 exactly for a != b < A, and diag(D) = 0
 };
 InstanceInfo analyse(int n, const int32_t *F, const int32_t *D);
 

@@ -69,6 +69,22 @@ def grid256(seed: int, side: int = 16, p: float = 0.36) -> Instance:
     return Instance(n, F, D, name=f"grid256_s{seed}")
 
 
+def clique_flow(seed: int, side: int = 16, active: int = 92) -> Instance:
+    """The structure CPU_PIM_tai256c.cpp is written for: n = side^2 locations on a grid
+    (squared Euclidean distance plus a symmetric uniform [0, 3] perturbation, zero diagonal) and
+    unit flows between every pair of the first `active` facilities, none elsewhere."""
+    n = side * side
+    rng = np.random.default_rng(seed)
+    F = np.zeros((n, n), np.int64)
+    F[:active, :active] = 1
+    np.fill_diagonal(F, 0)
+    ys, xs = np.divmod(np.arange(n), side)
+    d2 = (xs[:, None] - xs[None, :]) ** 2 + (ys[:, None] - ys[None, :]) ** 2
+    D = d2 + _symmetric_from_upper(rng.integers(0, 4, size=(n, n), dtype=np.int64))
+    np.fill_diagonal(D, 0)
+    return Instance(n, F, D, name=f"clique{active}_n{n}_s{seed}")
+
+
 def heavy(n: int, seed: int, mu: float = 2.0, sigma: float = 1.5, zero_frac: float = 0.7,
           square: float = 1000.0) -> Instance:
     rng = np.random.default_rng(seed)

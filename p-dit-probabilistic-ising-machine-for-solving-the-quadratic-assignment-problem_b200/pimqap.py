@@ -47,7 +47,7 @@ class Params(C.Structure):
         ("cluster_size", C.c_int32), ("beta_internal", C.c_int32), ("auto_beta", C.c_int32),
         ("auto_lower", C.c_double), ("auto_higher", C.c_double), ("goal_print", C.c_int64),
         ("event_capacity", C.c_int32), ("event_perm_capacity", C.c_int32),
-        ("compact_instance", C.c_int32), ("pad1", C.c_int32),
+        ("compact_instance", C.c_int32), ("active_facilities", C.c_int32),
     ]
 
 

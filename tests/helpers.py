@@ -4,11 +4,11 @@ import numpy as np
 LN2_INV = 1.44269504089
 
 
-def oracle_after(oracle, F, D, *, T, R, spe, beta_max, beta_ratio, seed, cap, megaiters):
+def oracle_after(oracle, F, D, *, T, R, spe, beta_max, beta_ratio, seed, cap, megaiters, active=0):
     """Oracle state after `megaiters` mega-iterations followed by each group's tracking /
     exchange step of the next mega-iteration (the solver runs that step at the end of every
-    epoch, on the device, before the next launch)."""
-    st = oracle.setup(D, F, T, R, spe, beta_max * LN2_INV, beta_ratio, seed, cap=cap)
+    epoch, on the device, before the next launch).  active > 0: clique-flow moves."""
+    st = oracle.setup(D, F, T, R, spe, beta_max * LN2_INV, beta_ratio, seed, cap=cap, active=active)
     oracle.run(st, D, F, megaiters)
     oracle.track_exchange_all(st)
     return st

@@ -73,6 +73,12 @@ CASES = {
     "binary_n37_t64_ragged": (lambda: binary(37, 33), 1, 4, 3, 0.02, 1.3, 6, {"threads_per_block": 64}),
     "binary_n200_cluster2": (lambda: binary(200, 34, 30000), 1, 2, 1, 0.0001, 1.5, 2, {"cluster_size": 2}),
     "grid_n256_generic_kernel": (lambda: instances.grid256(17), 1, 2, 1, 0.0015, 1.5, 2, {"compact_instance": 1}),
+    # clique flows with the moves of the reference's tai256c program (lumped inactive moves)
+    "clique92_n256_tai": (lambda: instances.clique_flow(35), 2, 3, 1, 0.002, 1.5, 3, {"active_facilities": 92}),
+    "clique20_n64_single_cta": (lambda: instances.clique_flow(36, side=8, active=20), 2, 4, 2, 0.01, 1.3, 8,
+                                {"active_facilities": 20}),
+    "clique9_n36_t64": (lambda: instances.clique_flow(37, side=6, active=9), 1, 5, 3, 0.05, 1.2, 20,
+                        {"active_facilities": 9, "threads_per_block": 64}),
 }
 
 
@@ -86,7 +92,8 @@ def run_case(gpu, oracle, name, seed=7):
     with gpu.Solver(inst.F, inst.D, p) as s:
         s.run(M)
         st = oracle_after(oracle, inst.F, inst.D, T=T, R=R, spe=spe, beta_max=bmax,
-                          beta_ratio=ratio, seed=seed, cap=cap, megaiters=M)
+                          beta_ratio=ratio, seed=seed, cap=cap, megaiters=M,
+                          active=extra.get("active_facilities", 0))
         bad = compare_solver_to_oracle(s, st, cap)
         res = s.result()
     return inst, st, bad, res
@@ -99,6 +106,16 @@ def test_trajectory_matches_oracle(gpu, oracle, name):
     assert res["megaiters_done"] == CASES[name][6]
     assert res["accepts"] == st.accepts
     assert res["best_energy"] == min(int(st.bestE.min()), st.single_best)
+
+
+def test_clique_moves_are_rejected_where_unsupported(gpu):
+    inst = instances.clique_flow(38, side=6, active=9)
+    p = gpu.default_params(replicas=3, groups=1, beta_max=0.05, max_megaiters=2, active_facilities=10)
+    with pytest.raises(gpu.PimqapError):            # not the instance's clique
+        gpu.solve(inst.F, inst.D, p)
+    p.active_facilities = 9
+    with pytest.raises(gpu.PimqapError):
+        gpu.batch_solve([(inst.F, inst.D)], [p])
 
 
 def test_force_width_and_cluster_choice(gpu, oracle):

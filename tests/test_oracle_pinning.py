@@ -90,3 +90,37 @@ def test_reference_file_reader_matches(tmp_path):
     assert np.array_equal(F, inst.F) and np.array_equal(D, inst.D)
     back = instances.read_instance(path)
     assert np.array_equal(back.F, inst.F) and np.array_equal(back.D, inst.D)
+
+
+# (n = 256, 92 active facilities are hard-wired in the reference's tai256c program)
+TAI_CASES = [
+    (2, 3, 1, 0.002, 1.5, 2, 29),
+    (1, 4, 2, 0.02, 1.3, 2, 31),          # colder: the lumped candidate dominates inactive picks
+]
+
+
+@pytest.mark.skipif(not ref_available("tai"), reason="reference tai256c harness not built")
+@pytest.mark.parametrize("case", TAI_CASES, ids=[f"T{c[0]}-R{c[1]}-i{c[2]}-b{c[3]}" for c in TAI_CASES])
+def test_clique_restatement_matches_reference_tai256c(oracle, case):
+    """orc_update_clique against CPU_PIM_tai256c.cpp (doMegaIteraTai) on a 92-clique instance."""
+    T, R, it, b0, db, M, seed = case
+    ref = RefHarness("tai")
+    inst = instances.clique_flow(seed)
+    ref.load(inst.F, inst.D)
+    ref.setup(T, R, it, b0, db, seed)
+    st = oracle.setup(inst.D, inst.F, T, R, it, b0, db, seed, cap=ref.maxr, active=92)
+    before = st.phi.copy()
+    ref.run(M)
+    oracle.run(st, inst.D, inst.F, M)
+    moved_inactive = 0
+    for t in range(T):
+        g = ref.group(t)
+        assert np.array_equal(g["order"], st.order[t])
+        assert g["thread_best"] == st.thread_best[t]
+        for l in range(R):
+            r = ref.replica(t, l)
+            assert np.array_equal(r["phi"], st.phi[t, l]), (t, l)
+            assert np.array_equal(r["I"], st.I[t, l]), (t, l)
+            assert (r["E"], r["bestE"], r["beta"]) == (st.E[t, l], st.bestE[t, l], st.beta[t, l])
+            moved_inactive += int(((before[t, l] >= 92) & (st.phi[t, l] >= 92) & (before[t, l] != st.phi[t, l])).sum())
+    assert moved_inactive > 0, "expected lumped inactive-to-inactive moves"
