@@ -187,9 +187,9 @@ def run_reference(args):
 
 # ------------------------------------------------------------------ our arm
 
-def read_traffic():
+def read_traffic(summary="epoch_kernel_grid256.md"):
     """dram bytes per launch of the sweep kernel from the committed ncu summary, or None."""
-    path = os.path.join(ROOT, "profiles", "epoch_kernel_grid256.md")
+    path = os.path.join(ROOT, "profiles", summary)
     if not os.path.exists(path):
         return None
     m = re.search(r"dram_bytes_per_launch:\s*([0-9.eE+]+)", open(path).read())
@@ -237,11 +237,12 @@ def run_ours(args):
 
     inst = rank_instance(rank, args.workload)
     act = 92 if args.workload == "clique92" else 0
+    rule = pimqap.RULE_ONE_SHOT if args.update_rule == "one-shot" else pimqap.RULE_SEQUENTIAL
     params = pimqap.default_params(replicas=REPLICAS, groups=GROUPS, sweeps_per_exchange=SWEEPS_PER_EXCHANGE,
                                    beta_max=BETA_MAX, beta_ratio=BETA_RATIO, beta_internal=1, seed=1 + rank,
                                    device=local, megaiters_per_launch=MEGAITERS_PER_STEP,
                                    max_megaiters=2 ** 31 - 1, cluster_size=args.cluster_size,
-                                   threads_per_block=args.threads, active_facilities=act)
+                                   threads_per_block=args.threads, active_facilities=act, update_rule=rule)
     flush = torch.empty(L2_FLUSH_BYTES, dtype=torch.uint8, device=f"cuda:{local}")
     solver = pimqap.Solver(inst.F, inst.D, params)
     for _ in range(args.warmup):
@@ -275,11 +276,18 @@ def run_ours(args):
     accepts = r1["accepts"] - r0["accepts"]
     cand = float(reps) * sweeps * N * N
     s = r1["force_bits"] // 8
-    alg_bytes = (3 * s + 20) * cand + (2 * N * N * s + 32 * N) * float(accepts)
+    if rule == pimqap.RULE_ONE_SHOT:
+        # one read-modify-write of the force matrix per replica step, whatever the number of
+        # swaps it applies, plus the swaps' D / F rows
+        alg_bytes = (3 * s + 20) * cand + 2 * N * N * s * float(reps) * sweeps + 32 * N * float(accepts)
+        bytes_model = f"({3 * s}+20) B per candidate delta + 2 n^2 {s} B per replica step + 32 n B per accept"
+    else:
+        alg_bytes = (3 * s + 20) * cand + (2 * N * N * s + 32 * N) * float(accepts)
+        bytes_model = f"({3 * s}+20) B per candidate delta + (2 n^2 {s} + 32 n) B per accept"
     launches = args.steps * MEGAITERS_PER_STEP
     achieved = alg_bytes / (ms_total * 1e-3) / 1e9
     smem_peak = pimqap.probe_smem_bandwidth(local)
-    traffic = read_traffic()
+    traffic = read_traffic("epoch_kernel_oneshot_grid256.md" if rule else "epoch_kernel_grid256.md")
 
     # e2e through the C ABI from pinned host buffers
     Fp = torch.from_numpy(inst.F).pin_memory()
@@ -290,7 +298,7 @@ def run_ours(args):
                                megaiters_per_launch=MEGAITERS_PER_STEP,
                                max_megaiters=args.steps * MEGAITERS_PER_STEP,
                                cluster_size=args.cluster_size, threads_per_block=args.threads,
-                               active_facilities=act)
+                               active_facilities=act, update_rule=rule)
     barrier()
     e0 = time.perf_counter()
     res = pimqap.solve(Fp.numpy(), Dp.numpy(), p2)
@@ -300,7 +308,7 @@ def run_ours(args):
     line = None
     if rank == 0:
         cpu = None
-        if world == 1 and not args.no_cpu_baseline and args.workload == "grid256":
+        if world == 1 and not args.no_cpu_baseline and args.workload == "grid256" and rule == 0:
             got = ref_cpu_throughput(inst.F, inst.D, budget_s=12.0)
             if got:
                 v, cores, kind, sample = got
@@ -315,7 +323,10 @@ def run_ours(args):
                                     "clique92: n=256, unit flows among facilities 0..91, 16x16 grid sq. "
                                     "distance + U[0,3]; the tai256c program's moves; ") +
                                    "64 replicas, geometric beta ladder, exchange every 4 sweeps, "
-                                   "10^4 sweeps = 100 steps",
+                                   "10^4 sweeps = 100 steps" +
+                                   ("; GPU-CUPIM's one-shot rule (a sweep = one parallel step)"
+                                    if rule else ""),
+                       "update_rule": args.update_rule,
                        "n": N, "replicas": reps, "sweeps_per_step": MEGAITERS_PER_STEP * SWEEPS_PER_EXCHANGE,
                        "beta0_internal": BETA_MAX, "beta_ratio": BETA_RATIO,
                        "ladder": "reference automatic mode on this instance (pimqap_auto_beta, seed 1), then fixed",
@@ -333,7 +344,7 @@ def run_ours(args):
                                         "read-modify-write, 128-bit, 2 CTAs/SM)",
                          "traffic": traffic,
                          "alg_bytes_per_launch": alg_bytes / launches,
-                         "bytes_model": f"({3 * s}+20) B per candidate delta + (2 n^2 {s} + 32 n) B per accept"},
+                         "bytes_model": bytes_model},
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": res["h2d_bytes"],
                     "d2h_bytes_per_step": res["d2h_bytes"], "wall_s": e_wall,
                     "note": "one step = one pimqap_solve of the whole workload (upload, set-up, sweeps, result)"},
@@ -473,6 +484,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--workload", choices=["grid256", "clique92"], default="grid256",
                     help="headline instance (clique92: the tai256c program's structure and moves)")
+    ap.add_argument("--update-rule", choices=["sequential", "one-shot"], default="sequential",
+                    help="sequential: CPU_PIM's sweeps (the headline); one-shot: GPU-CUPIM's parallel step")
     ap.add_argument("--cluster-size", type=int, default=0, help="CTAs per replica (0 = automatic)")
     ap.add_argument("--threads", type=int, default=0, help="threads per CTA (0 = automatic)")
     ap.add_argument("--suite", choices=["headline", "batch", "serve"], default="headline",

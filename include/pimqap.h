@@ -97,7 +97,18 @@ typedef struct pimqap_params {
                                     others carry none; a location holding an inactive facility
                                     weighs the actives and all inactives as one lumped move.
                                     pimqap_solve / solver handles only; no goal_print events */
+    int32_t update_rule;         /* PIMQAP_RULE_SEQUENTIAL (0): CPU_PIM's sweeps, one location
+                                    after another; PIMQAP_RULE_ONE_SHOT (1): the one-shot
+                                    parallel step of GPU-CUPIM (perl-gpu/src/lib/qap/qap.cu:
+                                    1038-1458), which every location of a replica proposes a
+                                    partner in against the same snapshot, collisions go to the
+                                    larger delta and the surviving swaps apply together; a
+                                    "sweep" is then one such step.  pimqap_solve / solver
+                                    handles only */
 } pimqap_params;
+
+#define PIMQAP_RULE_SEQUENTIAL 0
+#define PIMQAP_RULE_ONE_SHOT 1
 
 /* Fills p with the reference's defaults: 10 replicas, 20 groups, 4 sweeps per exchange,
    beta_ratio 1.2 (CPU_PIM.cpp:19-31), no goal, no timeout, seed 1, automatic shapes. */
@@ -339,6 +350,10 @@ pimqap_status pimqap_auto_beta_report(const pimqap_instance *inst, const pimqap_
 /* Diagnostic with no reference counterpart: measures the shared-memory read-modify-write
    bandwidth of the device (GB/s, reads + writes), the ceiling of the resident sweep. */
 pimqap_status pimqap_probe_smem_bandwidth(int32_t device, double *gbs);
+
+/* Diagnostic with no reference counterpart: evaluates the one-shot rule's binary32 weight
+   function 2^x (x <= 0; exact bits of the solver's device code) on `count` inputs. */
+pimqap_status pimqap_probe_weight_exp2(int32_t device, const float *x, float *y, int64_t count);
 
 const char *pimqap_last_error(void);
 const char *pimqap_version(void);

@@ -34,7 +34,7 @@ class _RunState(C.Structure):
         ("E", C.c_void_p), ("bestE", C.c_void_p), ("beta", C.c_void_p),
         ("order", C.c_void_p), ("time_since_swap", C.c_void_p), ("thread_best", C.c_void_p),
         ("single_best", C.c_int64), ("megaiters_done", C.c_int64), ("accepts", C.c_int64),
-        ("target_megaiter", C.c_int64), ("active", C.c_int32), ("pad", C.c_int32),
+        ("target_megaiter", C.c_int64), ("active", C.c_int32), ("rule", C.c_int32),
     ]
 
 
@@ -104,6 +104,16 @@ class Oracle:
         L.orc_setup.argtypes = [C.POINTER(_RunState), _i32p, _i32p, C.c_double, C.c_double]
         L.orc_run.argtypes = [C.POINTER(_RunState), _i32p, _i32p, C.c_int64, C.c_int64]
         L.orc_run.restype = C.c_int
+        L.orc_exp2f_neg.argtypes = [C.c_float]
+        L.orc_exp2f_neg.restype = C.c_float
+        L.orc_oneshot_uniform.argtypes = [C.c_uint32]
+        L.orc_oneshot_uniform.restype = C.c_float
+        L.orc_oneshot_pick.argtypes = [C.c_int, _i64p, C.c_float, C.c_float, _i64p]
+        L.orc_oneshot_pick.restype = C.c_int
+        L.orc_oneshot_step.argtypes = [C.c_int, _i32p, _i32p, _i64p, _i32p, _i32p, _i64p, _i64p,
+                                       C.c_double, C.c_uint64, C.c_uint32, C.c_uint32, C.c_uint32,
+                                       C.c_void_p]
+        L.orc_oneshot_step.restype = C.c_int
 
     def philox(self, ctr, key) -> np.ndarray:
         out = np.zeros(4, np.uint32)
@@ -142,12 +152,15 @@ class Oracle:
                                           picks.ctypes.data if record_picks else None)
         return int(acc), picks
 
-    def setup(self, D, F, T, R, numitera, beta0, delta_beta, seed, cap=None, active=0) -> RunState:
+    def setup(self, D, F, T, R, numitera, beta0, delta_beta, seed, cap=None, active=0,
+              rule=0) -> RunState:
         """active > 0: the clique-flow update of CPU_PIM_tai256c.cpp with that many active
-        facilities (orc_update_clique)."""
+        facilities (orc_update_clique).  rule = 1: GPU-CUPIM's one-shot parallel steps
+        (orc_oneshot_step) instead of sequential sweeps."""
         n = D.shape[0]
         st = RunState(n, T, R, cap if cap is not None else R, numitera, seed)
         st.c.active = active
+        st.c.rule = rule
         self.lib.orc_setup(C.byref(st.c), np.ascontiguousarray(D, np.int32),
                            np.ascontiguousarray(F, np.int32), beta0, delta_beta)
         return st
@@ -164,6 +177,28 @@ class Oracle:
             st.time_since_swap[t] = tss[0]
             st.thread_best[t] = tb[0]
         st.c.single_best = int(sb[0])
+
+    def exp2f_neg(self, x: float) -> float:
+        return float(self.lib.orc_exp2f_neg(x))
+
+    def oneshot_uniform(self, w0: int) -> float:
+        return float(self.lib.orc_oneshot_uniform(w0))
+
+    def oneshot_pick(self, d: np.ndarray, beta_f: float, u: float):
+        """(target, delta) of one proposal from the deltas d of every partner location."""
+        out = np.zeros(1, np.int64)
+        j = self.lib.orc_oneshot_pick(len(d), np.ascontiguousarray(d, np.int64), beta_f, u, out)
+        return int(j), int(out[0])
+
+    def oneshot_step(self, D, F, I, phi, phiinv, E, bestE, beta, seed, group, replica, step):
+        """One one-shot step in place (I int64 [n,n], phi/phiinv int32 [n], E/bestE int64 [1]).
+        Returns (swaps applied, every location's proposal)."""
+        n = D.shape[0]
+        tg = np.zeros(n, np.int32)
+        np_ = self.lib.orc_oneshot_step(n, np.ascontiguousarray(D, np.int32), np.ascontiguousarray(F, np.int32),
+                                        I, phi, phiinv, E, bestE, beta, seed, group, replica, step,
+                                        tg.ctypes.data)
+        return int(np_), tg
 
     def run(self, st: RunState, D, F, megaiters: int, goal: int = 0) -> int:
         return self.lib.orc_run(C.byref(st.c), np.ascontiguousarray(D, np.int32),

@@ -309,6 +309,163 @@ int64_t orc_replica_sweeps(int n, const int32_t *D, const int32_t *F, int64_t *I
     return accepts;
 }
 
+/* ---------------------------------------------------------------- one-shot parallel update */
+
+/* 2^x in binary32 for x <= 0 (Cody-Waite reduction x = k + f, |f| <= 1/2, then the degree-7
+   Taylor polynomial of 2^f = e^(f ln 2) by Horner's rule with fused multiply-adds, scaled by
+   2^k).  Every step is one correctly rounded IEEE operation, so the solver's device copy of
+   this function returns the same bits.  Error below 1 ulp over the normal range. */
+static const float kExp2Coef[8] = {0x1p+0f,         0x1.62e430p-1f, 0x1.ebfbe0p-3f,
+                                   0x1.c6b08ep-5f,  0x1.3b2ab6p-7f, 0x1.5d87fep-10f,
+                                   0x1.430912p-13f, 0x1.ffcbfcp-17f};
+
+static float bits_float(uint32_t u) {
+    float f;
+    memcpy(&f, &u, 4);
+    return f;
+}
+
+float orc_exp2f_neg(float x) {
+    if (!(x > -150.0f)) return 0.0f;
+    if (x > 0.0f) x = 0.0f;
+    const float k = rintf(x);
+    const float f = x - k;                               /* exact */
+    float p = kExp2Coef[7];
+    for (int c = 6; c >= 0; --c) p = fmaf(p, f, kExp2Coef[c]);
+    const int ki = (int)k;
+    if (ki >= -126) return p * bits_float((uint32_t)(ki + 127) << 23);
+    return (p * bits_float((uint32_t)(ki + 64 + 127) << 23)) * 0x1p-64f;
+}
+
+/* The threshold of a one-shot proposal: word 0 of the update's Philox block as an odd
+   multiple of 2^-24, in (0, 1). */
+float orc_oneshot_uniform(uint32_t w0) {
+    return (float)(((w0 >> 9) << 1) | 1u) * 0x1p-24f;
+}
+
+/* The proposal of one location (GPU-CUPIM qap.cu:1040-1146, os_pwc_d): deltas d[j] of every
+   partner location j, weights 2^(beta (d[j] - max)) in binary32 with no cutoff, summed in the
+   reference's warp order (lane t holds j = t, t+32, ...: a running sum per lane, then an
+   inclusive Hillis-Steele scan of the lane totals over 32 lanes), and the first lane whose
+   span [prev, cur) contains u * total picks its j; when no lane does, j = n - 1
+   (:1136-1144).  Returns j; *delta_out = d[j]. */
+int orc_oneshot_pick(int n, const int64_t *d, float beta_f, float u, int64_t *delta_out) {
+    int64_t mx = d[0];
+    for (int j = 1; j < n; ++j)
+        if (d[j] > mx) mx = d[j];
+    const int K = (n + 31) / 32;
+    float s[32][8], tot[32], x[32], y[32], off[32];
+    for (int t = 0; t < 32; ++t) {
+        float run = 0.0f;
+        for (int k = 0; k < K; ++k) {
+            const int j = t + 32 * k;
+            const float w = (j < n) ? orc_exp2f_neg(beta_f * (float)(d[j] - mx)) : 0.0f;
+            run = (k == 0) ? w : w + run;                /* :1094-1099 */
+            s[t][k] = run;
+        }
+        tot[t] = run;
+        x[t] = run;
+    }
+    for (int dd = 1; dd < 32; dd <<= 1) {                /* :1101-1110 */
+        for (int t = 0; t < 32; ++t) y[t] = (t >= dd) ? x[t] + x[t - dd] : x[t];
+        memcpy(x, y, sizeof(x));
+    }
+    for (int t = 0; t < 32; ++t) off[t] = x[t] - tot[t];
+    const float total = off[31] + tot[31];
+    const float thresh = u * total;                      /* :1114 */
+    for (int t = 0; t < 32; ++t) {                       /* :1119-1135, lowest lane wins */
+        int win = -1;
+        for (int k = 0; k < K; ++k) {
+            const int j = t + 32 * k;
+            if (j >= n) break;
+            const float cur = off[t] + s[t][k];
+            const float prev = (k == 0) ? off[t] : off[t] + s[t][k - 1];
+            if (cur >= thresh && prev < thresh) win = j;
+        }
+        if (win >= 0) {
+            *delta_out = d[win];
+            return win;
+        }
+    }
+    *delta_out = d[n - 1];
+    return n - 1;
+}
+
+/* Ballot word of a proposal (i -> target with delta): the larger delta wins, then the lower i
+   (GPU-CUPIM qap.cu:1184-1198); deltas beyond int32 are saturated (the reference's are int32). */
+static uint64_t oneshot_ballot(int64_t delta, int i) {
+    const int32_t d32 = delta > INT32_MAX ? INT32_MAX : (delta < INT32_MIN ? INT32_MIN : (int32_t)delta);
+    const uint32_t biased = ~((uint32_t)d32 ^ 0x80000000u);
+    return ((uint64_t)biased << 32) | (uint32_t)i;
+}
+
+int orc_oneshot_step(int n, const int32_t *D, const int32_t *F, int64_t *I, int32_t *phi,
+                     int32_t *phiinv, int64_t *E, int64_t *bestE, double beta, uint64_t seed,
+                     uint32_t group, uint32_t replica, uint32_t step, int32_t *targets) {
+    int32_t tgt[256], acc_i[256], acc_j[256], acc_a[256], acc_b[256];
+    int64_t dl[256], d[256];
+    uint64_t own[256];
+    const float beta_f = (float)beta;
+    /* 1. every location proposes against the same snapshot */
+    for (int i = 0; i < n; ++i) {
+        const int a = phi[i];
+        const int64_t *Ii = I + (size_t)i * n;
+        for (int j = 0; j < n; ++j) {                    /* qap.cu:609-646 */
+            const int b = phi[j];
+            const int64_t dd = (int64_t)D[i * n + i] + D[j * n + j] - D[i * n + j] - D[j * n + i];
+            const int64_t ff = (int64_t)F[a * n + a] + F[b * n + b] - F[a * n + b] - F[b * n + a];
+            d[j] = Ii[b] + I[(size_t)j * n + a] - Ii[a] - I[(size_t)j * n + b] - dd * ff;
+        }
+        const float u = orc_oneshot_uniform(orc_sweep_word(seed, group, replica, step, (uint32_t)i, 0));
+        tgt[i] = orc_oneshot_pick(n, d, beta_f, u, &dl[i]);
+        if (targets) targets[i] = tgt[i];
+    }
+    /* 2. collisions: a location goes to the best ballot touching it (qap.cu:1150-1225) */
+    for (int i = 0; i < n; ++i) own[i] = UINT64_MAX;
+    for (int i = 0; i < n; ++i) {
+        if (tgt[i] == i) continue;
+        const uint64_t w = oneshot_ballot(dl[i], i);
+        if (w < own[tgt[i]]) own[tgt[i]] = w;
+        if (w < own[i]) own[i] = w;
+    }
+    int np = 0;
+    for (int i = 0; i < n; ++i) {
+        const int j = tgt[i];
+        if (j == i || (uint32_t)own[i] != (uint32_t)i || (uint32_t)own[j] != (uint32_t)i) continue;
+        acc_i[np] = i;
+        acc_j[np] = j;
+        acc_a[np] = phi[i];
+        acc_b[np] = phi[j];
+        ++np;
+    }
+    /* 3. the accepted swaps are disjoint, so their rank-2 force updates add up exactly
+          (qap.cu:1337-1412); facilities are those before the step */
+    for (int p = 0; p < np; ++p) {
+        const int i = acc_i[p], j = acc_j[p], a = acc_a[p], b = acc_b[p];
+        for (int k = 0; k < n; ++k) {
+            const int64_t u1 = (int64_t)D[k * n + j] - D[k * n + i];
+            const int64_t u2 = (int64_t)D[j * n + k] - D[i * n + k];
+            int64_t *Ik = I + (size_t)k * n;
+            for (int c = 0; c < n; ++c)
+                Ik[c] += u1 * ((int64_t)F[c * n + b] - F[c * n + a]) +
+                         u2 * ((int64_t)F[b * n + c] - F[a * n + c]);
+        }
+    }
+    for (int p = 0; p < np; ++p) {                       /* qap.cu:1311-1332 */
+        const int i = acc_i[p], j = acc_j[p], a = acc_a[p], b = acc_b[p];
+        phi[i] = b;
+        phi[j] = a;
+        phiinv[a] = j;
+        phiinv[b] = i;
+    }
+    /* 4. the energy from the new force matrix, E = -1/2 sum_k I[k][phi(k)] (qap.cu:1420-1458) */
+    int64_t sum = 0;
+    for (int k = 0; k < n; ++k) sum += I[(size_t)k * n + phi[k]];
+    *E = -sum / 2;
+    if (*E < *bestE) *bestE = *E;
+    return np;
+}
+
 /* ---------------------------------------------------------------- tracking + exchange */
 
 int orc_track_exchange(int R, int cap, const int64_t *E, const int64_t *bestE, double *beta,
@@ -397,6 +554,14 @@ int orc_run(orc_run_state *st, const int32_t *D, const int32_t *F, int64_t megai
         for (int t = 0; t < T; ++t) {
             for (int l = 0; l < R; ++l) {                /* :360-362 */
                 size_t rep = (size_t)t * R + l;
+                if (st->rule == 1) {
+                    for (int s2 = 0; s2 < st->numitera; ++s2)
+                        st->accepts += orc_oneshot_step(
+                            n, D, F, st->I + rep * (size_t)n * n, st->phi + rep * n, st->phiinv + rep * n,
+                            &st->E[rep], &st->bestE[rep], st->beta[rep], st->seed, (uint32_t)t,
+                            (uint32_t)l, sweep0 + (uint32_t)s2, 0);
+                    continue;
+                }
                 if (st->active > 0) {
                     for (int s2 = 0; s2 < st->numitera; ++s2)
                         for (int i = 0; i < n; ++i) {

@@ -17,6 +17,9 @@
  *   orc_replica_sweeps ................ doMegaItera (CPU_PIM.cpp:195-290)
  *   orc_track_exchange ................ best tracking + replica exchange (CPU_PIM.cpp:293-344)
  *   orc_run ........................... threadToRun for all groups in lock step (CPU_PIM.cpp:292-364)
+ *   orc_oneshot_* ..................... the one-shot parallel step of GPU-CUPIM (qap.cu:1038-1458),
+ *                                       run by orc_run when rule == 1 (parity unpinned: that
+ *                                       code needs cuRANDDx and a GPU, neither available here)
  *
  * Random stream.  The reference draws from std::mt19937 seeded by std::random_device, which
  * makes its runs irreproducible.  The solver and this oracle replace the engine by a
@@ -104,8 +107,23 @@ typedef struct orc_run_state {
     int64_t accepts;
     int64_t target_megaiter;  /* first mega-iteration whose tracking saw single_best <= goal, or -1 */
     int32_t active;           /* 0: orc_update; A > 0: orc_update_clique with A active facilities */
-    int32_t pad;
+    int32_t rule;             /* 0: the sequential p-dit sweeps; 1: one-shot steps (orc_oneshot_step) */
 } orc_run_state;
+
+/* ---- the one-shot parallel update of GPU-CUPIM (perl-gpu/src/lib/qap/qap.cu:1038-1458) ----
+   One step of a replica: every location i proposes a partner j against the same snapshot
+   (heat-bath weights over all n partners in binary32, no cutoff, summed in the reference's
+   warp order), collisions go to the proposal with the larger delta (then the lower i), the
+   surviving swaps (disjoint pairs) are applied together, and the energy is recomputed from the
+   updated force matrix.  The reference's cuRANDDx uniforms are replaced by word 0 of the
+   update's Philox block (orc_sweep_word with sweep = step).  Returns the swaps applied;
+   targets (optional, n entries) receives every location's proposal. */
+float orc_exp2f_neg(float x);
+float orc_oneshot_uniform(uint32_t w0);
+int orc_oneshot_pick(int n, const int64_t *d, float beta_f, float u, int64_t *delta_out);
+int orc_oneshot_step(int n, const int32_t *D, const int32_t *F, int64_t *I, int32_t *phi,
+                     int32_t *phiinv, int64_t *E, int64_t *bestE, double beta, uint64_t seed,
+                     uint32_t group, uint32_t replica, uint32_t step, int32_t *targets);
 
 /* The clique-flow update of CPU-PIM/CPU_PIM_tai256c.cpp (doMegaIteraTai, :209-337), with the
    reference's hard-wired 92 active facilities and n = 256 made parameters: facilities

@@ -338,6 +338,8 @@ pimqap_status batch_solve(const pimqap_instance *insts, const pimqap_params *par
         if (st != PIMQAP_OK) return st;
         if (params[k].active_facilities > 0)
             return fail(PIMQAP_ERR_ARG, "active_facilities is supported by pimqap_solve and solver handles only");
+        if (params[k].update_rule != PIMQAP_RULE_SEQUENTIAL)
+            return fail(PIMQAP_ERR_ARG, "the one-shot rule is supported by pimqap_solve and solver handles only");
         if (params[k].device != params[0].device)
             return fail(PIMQAP_ERR_ARG, "every batch entry must use the same device");
     }
@@ -414,6 +416,8 @@ extern "C" pimqap_status pimqap_auto_beta_report(const pimqap_instance *inst, co
     if (st != PIMQAP_OK) return st;
     if (params->active_facilities > 0)
         return fail(PIMQAP_ERR_ARG, "automatic mode with active_facilities is not supported: give beta_max");
+    if (params->update_rule != PIMQAP_RULE_SEQUENTIAL)
+        return fail(PIMQAP_ERR_ARG, "automatic mode with the one-shot rule is not supported: give beta_max");
     constexpr double kMinBetaToTry = -30, kBetaStep = 1;     // :366-370
     constexpr int kTrials = PIMQAP_AUTO_TRIALS, kSteps = PIMQAP_AUTO_STEPS, kMegaiters = 10;  // :368, :371, :391
     const int T = params->groups, R = params->replicas, n = inst->n;

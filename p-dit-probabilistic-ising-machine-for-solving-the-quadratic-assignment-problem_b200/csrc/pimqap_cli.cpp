@@ -5,7 +5,8 @@
 // folder (<file>.out unless -o), the same log.txt and sweep<t>.txt files and the same stdout
 // lines, so the reference's drivers (CPU-PIM/run_all.py, run_timed.py) can call it unchanged.
 // Added flags: --seed S (Philox key), --json PATH (best cost, permutation, time to target),
-// --device D, --force-bits 32|64.
+// --device D, --force-bits 32|64, --active-facilities A (the tai256c program's moves),
+// --one-shot (GPU-CUPIM's one-shot parallel step instead of sequential sweeps).
 //
 // The solver records every group-best lowering and goal-print hit on the device with its time
 // (pimqap_solver_events); this program prints them in the reference's order after each chunk
@@ -48,6 +49,7 @@ struct Options {
     std::string json;
     int device = 0, force_bits = 0;
     int active = 0;                      // --active-facilities: the tai256c program's moves
+    bool one_shot = false;               // --one-shot: GPU-CUPIM's parallel step
 };
 
 void usage(const char *argv0) {   // :486-503
@@ -76,6 +78,8 @@ void usage(const char *argv0) {   // :486-503
     cout << "--force-bits B  force-matrix width 32 or 64 (default: from the instance bound)" << endl;
     cout << "--active-facilities A  the moves of the reference's CPU_PIM_tai256c program: facilities" << endl;
     cout << "                0..A-1 form a clique of unit flows, the others carry none (A = 92 there)" << endl;
+    cout << "--one-shot      GPU-CUPIM's one-shot step: every location proposes at once, collisions" << endl;
+    cout << "                go to the larger delta (a sweep is one such step; needs -b)" << endl;
 }
 
 // std::stoi / std::stod as the reference uses them, with a message instead of an abort.
@@ -170,6 +174,8 @@ int parse(int argc, char **argv, Options &o) {
         } else if (arg == "--active-facilities") {
             if (!(s = value()) || !to_ll(arg, s, &v)) return 1;
             o.active = (int)v;
+        } else if (arg == "--one-shot") {
+            o.one_shot = true;
         } else if (arg == "--force-bits") {
             if (!(s = value()) || !to_ll(arg, s, &v)) return 1;
             o.force_bits = (int)v;
@@ -272,6 +278,7 @@ int run(int argc, char **argv) {
     p.device = o.device;
     p.force_bits = o.force_bits;
     p.active_facilities = o.active;
+    p.update_rule = o.one_shot ? PIMQAP_RULE_ONE_SHOT : PIMQAP_RULE_SEQUENTIAL;
     p.auto_lower = o.lower;
     p.auto_higher = o.higher;
     p.beta_internal = 1;

@@ -263,11 +263,15 @@ pimqap_status check_params(const pimqap_instance *inst, const pimqap_params *p) 
         return fail(PIMQAP_ERR_ARG, "compact_instance must be 0 or 1");
     if (p->active_facilities < 0 || p->active_facilities >= inst->n && p->active_facilities != 0)
         return fail(PIMQAP_ERR_ARG, "active_facilities must be 0 or in [2, n)");
+    if (p->update_rule != PIMQAP_RULE_SEQUENTIAL && p->update_rule != PIMQAP_RULE_ONE_SHOT)
+        return fail(PIMQAP_ERR_ARG, "update_rule must be 0 (sequential) or 1 (one-shot)");
+    if (p->update_rule == PIMQAP_RULE_ONE_SHOT && p->active_facilities != 0)
+        return fail(PIMQAP_ERR_ARG, "active_facilities applies to the sequential rule only");
     if (p->force_bits != 0 && p->force_bits != 32 && p->force_bits != 64)
         return fail(PIMQAP_ERR_ARG, "force_bits must be 0, 32 or 64");
     if (p->threads_per_block != 0 && p->threads_per_block != 64 && p->threads_per_block != 128 &&
-        p->threads_per_block != 256)
-        return fail(PIMQAP_ERR_ARG, "threads_per_block must be 0, 64, 128 or 256");
+        p->threads_per_block != 256 && !(p->threads_per_block == 512 && p->update_rule == PIMQAP_RULE_ONE_SHOT))
+        return fail(PIMQAP_ERR_ARG, "threads_per_block must be 0, 64, 128 or 256 (or 512 with the one-shot rule)");
     if (p->cluster_size != 0 && p->cluster_size != 1 && p->cluster_size != 2 && p->cluster_size != 4)
         return fail(PIMQAP_ERR_ARG, "cluster_size must be 0, 1, 2 or 4");
     return PIMQAP_OK;
@@ -311,6 +315,34 @@ pimqap_status plan_instance(const pimqap_instance *inst, const pimqap_params *pa
     P.threads = params->threads_per_block ? params->threads_per_block
                                           : (n <= 64 ? 64 : (n <= 128 ? 128 : 256));
     auto rows_per_cta = [&](int cl) { return round_up((n + cl - 1) / cl, 4); };
+    if (params->update_rule == PIMQAP_RULE_ONE_SHOT) {
+        // the one-shot epoch: odd row stride (column reads by 32 lanes hit 32 banks), the
+        // smallest cluster that holds its rows with a force-update chunk of 32, 16, 8 or 4 swaps,
+        // preferring the layout whose peers push the columns the proposals need
+        P.lds = P.npad + 1;
+        P.cl = 0;
+        for (int cl : {1, 2, 4}) {
+            if (want_cluster && cl != want_cluster) continue;
+            for (int xcol = (cl > 1 ? 1 : 0); xcol >= 0 && !P.cl; --xcol)
+                for (int pc : {32, 16, 8, 4}) {
+                    const size_t sm = pimqap::epoch_smem_bytes_os(n, rows_per_cta(cl), P.lds, cl, P.bits, pc,
+                                                                  P.sym, xcol != 0);
+                    if (sm <= maxsm) {
+                        P.cl = cl;
+                        P.os_chunk = pc;
+                        P.os_xcol = xcol;
+                        P.smem = sm;
+                        break;
+                    }
+                }
+            if (P.cl) break;
+        }
+        if (!P.cl) return fail(PIMQAP_ERR_ARG, "force matrix does not fit the requested cluster size");
+        P.rpc = rows_per_cta(P.cl);
+        P.ldm = std::max(P.npad, P.cl * P.rpc);
+        if (!params->threads_per_block) P.threads = P.rpc > 64 ? 512 : (P.rpc > 32 ? 256 : 128);
+    }
+    if (!P.os_chunk) {
     P.cl = 0;
     for (int cl : {1, 2, 4}) {
         if (want_cluster && cl != want_cluster) continue;
@@ -324,8 +356,9 @@ pimqap_status plan_instance(const pimqap_instance *inst, const pimqap_params *pa
     // D / F rows are read in 16-byte chunks up to column cl * rpc
     P.ldm = std::max(P.npad, P.cl * P.rpc);
     P.smem = pimqap::epoch_smem_bytes(n, P.rpc, P.lds, P.cl, P.bits);
+    }
     // binary flows and int16 distances: the instance itself fits next to the force rows
-    if (info.symmetric && info.binary_flow && info.dist16 && P.bits == 32 &&
+    if (info.symmetric && info.binary_flow && info.dist16 && P.bits == 32 && !P.os_chunk &&
         (params->compact_instance == 0 || params->active_facilities > 0)) {
         const size_t sb = pimqap::epoch_smem_bytes_bin(n, P.rpc, P.lds, P.cl);
         if (sb <= maxsm) {
@@ -359,6 +392,8 @@ void carve_instance(const Plan &P, char *head, char *tail, SolveDev *out) {
     SolveDev d{};
     d.n = n; d.R = R; d.T = T; d.cap = cap; d.spe = P.spe;
     d.act = P.act;
+    d.os_chunk = P.os_chunk;
+    d.os_xcol = P.os_xcol;
     d.ldg = P.npad; d.lds = P.lds; d.ldm = P.ldm; d.rpc = P.rpc;
     char *cur = head;
     d.D = carve<int32_t>(cur, nn);

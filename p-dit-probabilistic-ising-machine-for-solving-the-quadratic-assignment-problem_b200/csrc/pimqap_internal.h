@@ -11,6 +11,7 @@ namespace pimqap {
 
 constexpr int kMaxN = 256;
 constexpr int kMaxWarps = 8;           // kernels run with 64, 128 or 256 threads
+constexpr int kMaxWarpsOs = 16;        // the one-shot epoch runs with up to 512
 constexpr int32_t kNoStop = 0x7fffffff;
 constexpr int64_t kNoBest = 2147483647;  // the reference's INT_MAX sentinel
 
@@ -79,7 +80,11 @@ struct SolveDev {
     int32_t *error;            // [1]       kErr* bits
     EventLink ev;              // progress events (optional)
     int32_t act;               // > 0: clique-flow moves with facilities 0..act-1 active
-    int32_t pad_act;
+    int32_t os_chunk;          // > 0: the one-shot update rule, force update in chunks of this
+                               //      many swaps (0: sequential sweeps)
+    int32_t os_xcol;           // one-shot with a cluster: peers push the force-matrix columns
+                               //      the proposals need (0: the proposals read them remotely)
+    int32_t pad_os;
 };
 
 // Compact per-instance result of a batch.
@@ -179,6 +184,8 @@ void set_last_error(const char *msg);
 size_t epoch_smem_bytes(int n, int rpc, int lds, int cluster, int bits);
 // Shared memory of the binary-flow epoch kernel (0 / 1 flows and int16 distances resident).
 size_t epoch_smem_bytes_bin(int n, int rpc, int lds, int cluster);
+// Shared memory of the one-shot epoch kernel (force update in chunks of `chunk` swaps).
+size_t epoch_smem_bytes_os(int n, int rpc, int lds, int cluster, int bits, int chunk, bool sym, bool xcol);
 
 // One-time kernel attributes (dynamic shared memory, non-portable cluster size).
 cudaError_t prepare_kernels();

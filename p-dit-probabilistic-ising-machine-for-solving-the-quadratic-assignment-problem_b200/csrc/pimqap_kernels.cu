@@ -27,6 +27,7 @@
 #include <cstdint>
 
 #include "pimqap_internal.h"
+#include "pimqap_weights.cuh"
 
 namespace cg = cooperative_groups;
 
@@ -1243,10 +1244,599 @@ __device__ bool replica_epoch_bin(const SolveDev &s, int rep, int rank, int e, c
     return true;
 }
 
+// ------------------------------------------------------------------ the one-shot epoch
+
+// Shared-memory layout of the one-shot epoch (replica_epoch_os).
+//   I       rpc rows of the force matrix; odd row stride lds, so 32 lanes reading one column
+//           of 32 rows hit 32 banks
+//   phi, inv, bphi, Dd, Fd   permutation, inverse, best permutation, diagonals of D and F
+//   diag    I[j][phi(j)] of every location (each CTA stores its rows' entries into all CTAs)
+//   tgt, dlt   [2][npad] every location's proposal (partner, delta), stored by the CTA that
+//           owns the location into all CTAs; double-buffered by step
+//   own     ballot words of the collision resolution
+//   pair    accepted swaps: i, j, phi(i), phi(j) before the step ([4][npad])
+//   uni     thresholds of this CTA's locations for the coming step (binary32)
+//   T       (xcol) [rpc][(CL-1) rpc]: for each location i of this CTA, column phi(i) of the
+//           other CTAs' rows, pushed by those CTAs (coalesced remote stores) after every step
+//           that moved something, so the proposals read no remote memory
+//   U, V    factors of one chunk of pc accepted swaps: U[p][k] = 2 (D[k][j] - D[k][i]) over
+//           this CTA's rows (row stride rpc), V[p][c] = F[c][b] - F[c][a] (row stride 256, zero
+//           beyond n); asymmetric instances use U = D[k][j] - D[k][i] and add
+//           U2 = D[j][k] - D[i][k], V2 = F[b][c] - F[a][c].  They share T's space: they are
+//           live only between a step's proposals and its column exchange
+//   part    [CL] every CTA's share of sum_k I[k][phi(k)], then [kMaxWarpsOs] warp sums
+//   misc    [kMaxWarpsOs] warp counts of the pair compaction, [8] flags
+struct OsLayout {
+    size_t I, phi, inv, bphi, Dd, Fd, diag, tgt, dlt, own, pair, uni, T, U, V, U2, V2, part, misc, total;
+    int tld;   // row stride of T (elements)
+    __host__ __device__ OsLayout(int n, int rpc, int lds, int cluster, int isz, int pc, bool sym, bool xcol) {
+        const size_t npad = (size_t)((n + 3) & ~3), rp = (size_t)rpc, vld = 256;
+        size_t o = 0;
+        I = o;    o = align16(o + rp * lds * isz);
+        phi = o;  o = align16(o + npad * 4);
+        inv = o;  o = align16(o + npad * 4);
+        bphi = o; o = align16(o + npad * 4);
+        Dd = o;   o = align16(o + npad * 4);
+        Fd = o;   o = align16(o + npad * 4);
+        diag = o; o = align16(o + npad * isz);
+        tgt = o;  o = align16(o + 2 * npad * 4);
+        dlt = o;  o = align16(o + 2 * npad * isz);
+        own = o;  o = align16(o + npad * 8);
+        pair = o; o = align16(o + 4 * npad * 4);
+        uni = o;  o = align16(o + npad * 4);
+        tld = xcol ? (cluster - 1) * rpc : 0;
+        const size_t tbytes = (size_t)rp * tld * isz;
+        T = o;
+        U = o;
+        V = align16(U + (size_t)pc * rp * isz);
+        U2 = align16(V + (size_t)pc * vld * isz);
+        V2 = align16(U2 + (sym ? 0 : (size_t)pc * rp * isz));
+        const size_t fend = align16(V2 + (sym ? 0 : (size_t)pc * vld * isz));
+        o = align16(fend > o + tbytes ? fend : o + tbytes);
+        part = o; o = align16(o + (size_t)(cluster + kMaxWarpsOs) * 8);
+        misc = o; o = align16(o + (kMaxWarpsOs + 8) * sizeof(int));
+        total = o;
+    }
+};
+
+size_t epoch_smem_bytes_os(int n, int rpc, int lds, int cluster, int bits, int chunk, bool sym, bool xcol) {
+    return OsLayout(n, rpc, lds, cluster, bits / 8, chunk, sym, xcol).total;
+}
+
+// Loads of this CTA's shared memory by 32-bit shared address.
+template <class IT> __device__ __forceinline__ IT lds_it(uint32_t a);
+template <> __device__ __forceinline__ int32_t lds_it<int32_t>(uint32_t a) {
+    int32_t v;
+    asm volatile("ld.shared.b32 %0, [%1];" : "=r"(v) : "r"(a));
+    return v;
+}
+template <> __device__ __forceinline__ int64_t lds_it<int64_t>(uint32_t a) {
+    long long v;
+    asm volatile("ld.shared.b64 %0, [%1];" : "=l"(v) : "r"(a));
+    return (int64_t)v;
+}
+
+// Loads / stores of another CTA's shared memory (shared::cluster addresses from mapa).
+__device__ __forceinline__ int32_t ld_cluster(uint32_t a, int32_t) {
+    int32_t v;
+    asm volatile("ld.shared::cluster.b32 %0, [%1];" : "=r"(v) : "r"(a));
+    return v;
+}
+__device__ __forceinline__ int64_t ld_cluster(uint32_t a, int64_t) {
+    long long v;
+    asm volatile("ld.shared::cluster.b64 %0, [%1];" : "=l"(v) : "r"(a));
+    return (int64_t)v;
+}
+__device__ __forceinline__ void st_cluster(uint32_t a, int32_t v) {
+    asm volatile("st.shared::cluster.b32 [%0], %1;" ::"r"(a), "r"(v) : "memory");
+}
+__device__ __forceinline__ void st_cluster(uint32_t a, int64_t v) {
+    asm volatile("st.shared::cluster.b64 [%0], %1;" ::"r"(a), "l"((long long)v) : "memory");
+}
+
+// Ballot word of a proposal (i -> partner with delta): the smaller word wins, i.e. the larger
+// delta, then the lower i (GPU-CUPIM qap.cu:1184-1198); deltas beyond int32 saturate.
+template <class IT> __device__ __forceinline__ unsigned long long oneshot_ballot(IT delta, int i) {
+    const long long d = (long long)delta;
+    const int32_t d32 = d > 2147483647ll ? 2147483647 : (d < -2147483648ll ? (int32_t)0x80000000 : (int32_t)d);
+    const uint32_t biased = ~((uint32_t)d32 ^ 0x80000000u);
+    return ((unsigned long long)biased << 32) | (uint32_t)i;
+}
+
+// Factors of cn accepted swaps for the one-shot force update, from 16-byte pieces of two rows
+// per swap: out[p][4 q + r] = M1[y_p][4 q + r] - M1[x_p][4 q + r] (q < nq), doubled when TWICE
+// (the row factors of a symmetric instance, whose two rank-1 terms per swap are equal), and for
+// asymmetric instances out2 from M2 likewise.  UNR pieces per thread are loaded before any is
+// used.
+template <class IT, bool SYM, bool TWICE, int UNR>
+__device__ __forceinline__ void stage_factors(int tid, int BT, int cn, int nq, const int32_t *M1,
+                                              const int32_t *M2, int ldm, const int32_t *x,
+                                              const int32_t *y, IT *out, IT *out2, int ld_out) {
+    using U = typename Unsigned<IT>::type;
+    const int total = cn * nq;
+    for (int base = tid; base < total; base += UNR * BT) {
+        int4 hi[UNR], lo[UNR], hi2[UNR], lo2[UNR];
+#pragma unroll
+        for (int m = 0; m < UNR; ++m) {
+            const int idx = base + m * BT;
+            if (idx < total) {
+                const int p = idx / nq, q = idx - p * nq;
+                const size_t ry = (size_t)y[p] * ldm + 4 * q, rx = (size_t)x[p] * ldm + 4 * q;
+                hi[m] = __ldg(reinterpret_cast<const int4 *>(M1 + ry));
+                lo[m] = __ldg(reinterpret_cast<const int4 *>(M1 + rx));
+                if constexpr (!SYM) {
+                    hi2[m] = __ldg(reinterpret_cast<const int4 *>(M2 + ry));
+                    lo2[m] = __ldg(reinterpret_cast<const int4 *>(M2 + rx));
+                }
+            }
+        }
+#pragma unroll
+        for (int m = 0; m < UNR; ++m) {
+            const int idx = base + m * BT;
+            if (idx < total) {
+                const int p = idx / nq, q = idx - p * nq;
+                IT *o = out + (size_t)p * ld_out + 4 * q;
+                const int32_t *h = &hi[m].x, *l = &lo[m].x;
+#pragma unroll
+                for (int r = 0; r < 4; ++r) {
+                    const U d = (U)(IT)h[r] - (U)(IT)l[r];
+                    o[r] = TWICE ? (IT)(2u * d) : (IT)d;
+                }
+                if constexpr (!SYM) {
+                    IT *o2 = out2 + (size_t)p * ld_out + 4 * q;
+                    const int32_t *h2 = &hi2[m].x, *l2 = &lo2[m].x;
+#pragma unroll
+                    for (int r = 0; r < 4; ++r) o2[r] = (IT)((U)(IT)h2[r] - (U)(IT)l2[r]);
+                }
+            }
+        }
+    }
+}
+
+// One epoch of replica rep under the one-shot parallel update of GPU-CUPIM (qap.cu:1038-1458):
+// spe steps, each of which lets every location propose a partner against the same snapshot,
+// resolves the collisions, applies the surviving (disjoint) swaps together and recomputes the
+// energy from the force matrix.  The replica's force matrix stays resident in shared memory,
+// split by rows over the cluster as in the sequential epoch.  Per step:
+//   1. proposals: one warp per location i of this CTA; lane t evaluates partners j = t + 32k
+//      (the reference's lane layout), reading column phi(i) of the other CTAs' rows through
+//      distributed shared memory; binary32 weights 2^(beta (d - max)) with the exact exp2f_neg,
+//      the reference's per-lane running sums and 32-lane scan, the threshold pick; the lane
+//      that owns location i stores the proposal into every CTA; cluster barrier;
+//   2. every CTA resolves all n proposals (shared-memory atomicMin on ballot words, same
+//      result everywhere) and compacts the accepted swaps in location order;
+//   3. the force update of this CTA's rows, sum over swaps p of U[p][k] V[p][c] (rank-2 per
+//      swap), in chunks of pc swaps with RT x 8 register tiles per lane;
+//   4. the new diagonal I[k][phi(k)] of this CTA's rows and its share of the energy go to
+//      every CTA; cluster barrier; E = -1/2 sum.  A step without swaps skips 3-4.
+template <class IT, int CL, bool SYM, bool GP>
+__device__ bool replica_epoch_os(const SolveDev &s, int rep, int rank, int e, const Grp &G,
+                                 unsigned char *smem) {
+    using U = typename Unsigned<IT>::type;
+    constexpr int VEC = Vec<IT>::kN;
+    constexpr int RT = sizeof(IT) == 4 ? 4 : 2;              // rows of a register tile
+    const int n = s.n;
+    const int tid = G.tid, BT = G.BT, lane = G.lane, warp = G.warp, nwarps = G.nwarps;
+    const int g = rep / s.R, l = rep - g * s.R;
+    const int rpc = s.rpc, lds = s.lds, ldm = s.ldm, pc = s.os_chunk;
+    const int row0 = rank * rpc;
+    const int rows = max(0, min(rpc, n - row0));
+    const int npad = (n + 3) & ~3, vld = 256;           // V rows: every lane's 8 columns
+    const int K = (n + 31) >> 5;                             // partners per lane (<= 8)
+    const bool xcol = CL > 1 && s.os_xcol != 0;
+    const OsLayout L(n, rpc, lds, CL, (int)sizeof(IT), pc, SYM, xcol);
+    const int tld = L.tld;
+    IT *sI = reinterpret_cast<IT *>(smem + L.I);
+    int32_t *s_phi = reinterpret_cast<int32_t *>(smem + L.phi);
+    int32_t *s_inv = reinterpret_cast<int32_t *>(smem + L.inv);
+    int32_t *s_bphi = reinterpret_cast<int32_t *>(smem + L.bphi);
+    int32_t *s_Dd = reinterpret_cast<int32_t *>(smem + L.Dd);
+    int32_t *s_Fd = reinterpret_cast<int32_t *>(smem + L.Fd);
+    float *s_uni = reinterpret_cast<float *>(smem + L.uni);
+    IT *s_T = reinterpret_cast<IT *>(smem + L.T);
+    IT *s_diag = reinterpret_cast<IT *>(smem + L.diag);
+    int32_t *s_tgt = reinterpret_cast<int32_t *>(smem + L.tgt);
+    IT *s_dlt = reinterpret_cast<IT *>(smem + L.dlt);
+    unsigned long long *s_own = reinterpret_cast<unsigned long long *>(smem + L.own);
+    int32_t *s_pi = reinterpret_cast<int32_t *>(smem + L.pair);
+    int32_t *s_pj = s_pi + npad, *s_pa = s_pj + npad, *s_pb = s_pa + npad;
+    IT *s_U = reinterpret_cast<IT *>(smem + L.U);
+    IT *s_V = reinterpret_cast<IT *>(smem + L.V);
+    IT *s_U2 = reinterpret_cast<IT *>(smem + L.U2);
+    IT *s_V2 = reinterpret_cast<IT *>(smem + L.V2);
+    long long *s_part = reinterpret_cast<long long *>(smem + L.part);
+    int *s_wcnt = reinterpret_cast<int *>(smem + L.misc);
+    int *s_flag = s_wcnt + kMaxWarpsOs;                     // [0] goal-print slot
+
+    // ---- load the replica
+    {
+        const IT *gI = reinterpret_cast<const IT *>(s.I) + ((size_t)rep * n + row0) * s.ldg;
+        const int nvg = s.ldg / VEC;
+        for (int idx = tid; idx < rows * nvg; idx += BT) {
+            const int k = idx / nvg, v = idx - k * nvg;
+            const int4 w4 = __ldcg(reinterpret_cast<const int4 *>(gI + (size_t)k * s.ldg + v * VEC));
+            Vec<IT> w;
+            memcpy(&w, &w4, 16);
+#pragma unroll
+            for (int q = 0; q < VEC; ++q) sI[(size_t)k * lds + v * VEC + q] = w.v[q];
+        }
+        const int32_t *gphi = s.phi + (size_t)rep * n;
+        for (int q = tid; q < npad; q += BT) {
+            int p = q < n ? __ldcg(gphi + q) : 0;
+            if ((unsigned)p >= (unsigned)n) {
+                atomicOr(s.error, kErrBadPerm);
+                p = 0;
+            }
+            s_phi[q] = p;
+            s_bphi[q] = p;
+            s_Dd[q] = q < n ? __ldcg(s.Ddiag + q) : 0;
+            s_Fd[q] = q < n ? __ldcg(s.Fdiag + q) : 0;
+        }
+    }
+    G.sync();
+    for (int q = tid; q < n; q += BT) s_inv[s_phi[q]] = q;
+
+    // shared::cluster addresses of every CTA's rows and cluster-wide arrays
+    uint32_t I_at[CL], diag_at[CL], tgt_at[CL], dlt_at[CL], part_at[CL], T_at[CL];
+#pragma unroll
+    for (int r = 0; r < CL; ++r) {
+        I_at[r] = CL > 1 ? cluster_addr(smem_u32(sI), r) : smem_u32(sI);
+        T_at[r] = CL > 1 ? cluster_addr(smem_u32(s_T), r) : smem_u32(s_T);
+        diag_at[r] = CL > 1 ? cluster_addr(smem_u32(s_diag), r) : smem_u32(s_diag);
+        tgt_at[r] = CL > 1 ? cluster_addr(smem_u32(s_tgt), r) : smem_u32(s_tgt);
+        dlt_at[r] = CL > 1 ? cluster_addr(smem_u32(s_dlt), r) : smem_u32(s_dlt);
+        part_at[r] = CL > 1 ? cluster_addr(smem_u32(s_part), r) : smem_u32(s_part);
+    }
+    const uint32_t k0 = (uint32_t)s.seed, k1 = (uint32_t)(s.seed >> 32);
+    // thresholds of this CTA's locations for step `step` (one Philox block each)
+    auto draw_thresholds = [&](uint32_t step) {
+        for (int q = tid; q < rows; q += BT) {
+            uint32_t w0, w1;
+            philox_2words((uint32_t)(row0 + q), step, (uint32_t)l, (uint32_t)g, k0, k1, w0, w1);
+            s_uni[q] = oneshot_uniform(w0);
+        }
+    };
+    // every other CTA q gets T_q[i - q.row0][slot of j] = I[j][phi(i)] for this CTA's rows j
+    // and q's locations i: one warp per location, 32 consecutive rows per store (128 bytes)
+    auto send_columns = [&]() {
+#pragma unroll
+        for (int q = 0; q < CL; ++q) {
+            if (q == rank) continue;
+            const int qrow0 = q * rpc, qrows = max(0, min(rpc, n - qrow0));
+            const int jr0 = row0 < qrow0 ? row0 : row0 - rpc;
+            for (int il = warp; il < qrows; il += nwarps) {
+                const int a = s_phi[qrow0 + il];
+                for (int jl = lane; jl < rows; jl += 32)
+                    st_cluster(T_at[q] + (uint32_t)(((size_t)il * tld + jr0 + jl) * sizeof(IT)),
+                               sI[(size_t)jl * lds + a]);
+            }
+        }
+    };
+    draw_thresholds((uint32_t)(e * s.spe));
+    cluster_sync<CL>(G);   // every CTA of the cluster is running before any remote access
+    // the diagonal of this CTA's rows into every CTA
+    for (int kk = tid; kk < rows; kk += BT) {
+        const int k = row0 + kk;
+        const IT dv = sI[(size_t)kk * lds + s_phi[k]];
+        if constexpr (CL == 1) s_diag[k] = dv;
+        else
+#pragma unroll
+            for (int r = 0; r < CL; ++r) st_cluster(diag_at[r] + (uint32_t)(k * sizeof(IT)), dv);
+    }
+    if (xcol) send_columns();
+    cluster_sync<CL>(G);
+
+    const float beta_f = __double2float_rn(__ldcg(s.beta + rep));
+    int64_t E = __ldcg((const long long *)s.E + rep), bestE = __ldcg((const long long *)s.bestE + rep);
+    unsigned long long accepts = 0;
+    bool improved = false;
+
+    for (int st = 0; st < s.spe; ++st) {
+        const uint32_t step = (uint32_t)(e * s.spe + st);
+        const int pb = st & 1;
+        int32_t *tgt = s_tgt + pb * npad;
+        IT *dlt = s_dlt + pb * npad;
+
+        // ---- 1. proposals of this CTA's locations
+        for (int il = warp; il < rows; il += nwarps) {
+            const int i = row0 + il;
+            const int a = s_phi[i];
+            const IT *Ii = sI + (size_t)il * lds;
+            const IT Iia = Ii[a];
+            const U Dii = (U)(IT)s_Dd[i], Faa = (U)(IT)s_Fd[a];
+            const int32_t *Di = s.D + (size_t)i * ldm, *DTi = s.DT + (size_t)i * ldm;
+            const int32_t *Fa = s.F + (size_t)a * ldm, *FTa = s.FT + (size_t)a * ldm;
+            IT d[8];
+            IT mx = (IT)((U)1 << (sizeof(IT) * 8 - 1));     // most negative
+#pragma unroll
+            for (int k = 0; k < 8; ++k) {
+                d[k] = 0;
+                const int j = lane + 32 * k;
+                if (k < K && j < n) {
+                    const int b = s_phi[j];
+                    IT Ija;
+                    if constexpr (CL == 1) {
+                        Ija = sI[j * lds + a];
+                    } else {
+                        if (j >= row0 && j < row0 + rpc) {
+                            Ija = sI[(j - row0) * lds + a];
+                        } else if (xcol) {
+                            Ija = s_T[il * tld + (j < row0 ? j : j - rpc)];
+                        } else {
+                            const int r = j / rpc;
+                            uint32_t base = I_at[0];
+#pragma unroll
+                            for (int q = 1; q < CL; ++q) base = (r == q) ? I_at[q] : base;
+                            Ija = ld_cluster(base + (uint32_t)(((size_t)(j - r * rpc) * lds + a) * sizeof(IT)), IT(0));
+                        }
+                    }
+                    const int32_t Dij = __ldg(Di + j), Fab = __ldg(Fa + b);
+                    const int32_t Dji = SYM ? Dij : __ldg(DTi + j), Fba = SYM ? Fab : __ldg(FTa + b);
+                    const U dd = Dii + (U)(IT)s_Dd[j] - (U)(IT)Dij - (U)(IT)Dji;
+                    const U ff = Faa + (U)(IT)s_Fd[b] - (U)(IT)Fab - (U)(IT)Fba;
+                    d[k] = (IT)((U)Ii[b] + (U)Ija - (U)Iia - (U)s_diag[j] - dd * ff);
+                    mx = d[k] > mx ? d[k] : mx;
+                }
+            }
+            mx = warp_max(mx);
+            // binary32 weights and the reference's lane-order sums (qap.cu:1069-1110)
+            float run = 0.0f, sacc[8];
+#pragma unroll
+            for (int k = 0; k < 8; ++k) {
+                sacc[k] = run;
+                if (k < K) {
+                    const int j = lane + 32 * k;
+                    float w = 0.0f;
+                    if (j < n) w = exp2f_neg(__fmul_rn(beta_f, __ll2float_rn((long long)d[k] - (long long)mx)));
+                    run = (k == 0) ? w : __fadd_rn(w, run);
+                    sacc[k] = run;
+                }
+            }
+            float x = run;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const float y = __shfl_up_sync(0xffffffffu, x, o);
+                if (lane >= o) x = __fadd_rn(x, y);
+            }
+            const float off = __fsub_rn(x, run);
+            const float total = __shfl_sync(0xffffffffu, __fadd_rn(off, run), 31);
+            const float thresh = __fmul_rn(s_uni[il], total);
+            int win = -1;
+            IT wd = 0, lastd = 0;
+#pragma unroll
+            for (int k = 0; k < 8; ++k) {
+                const int j = lane + 32 * k;
+                if (k < K && j < n) {
+                    const float cur = __fadd_rn(off, sacc[k]);
+                    const float prev = (k == 0) ? off : __fadd_rn(off, sacc[k - 1]);
+                    if (cur >= thresh && prev < thresh) {
+                        win = j;
+                        wd = d[k];
+                    }
+                    if (j == n - 1) lastd = d[k];
+                }
+            }
+            const unsigned fm = __ballot_sync(0xffffffffu, win >= 0);
+            const int src = fm ? __ffs(fm) - 1 : ((n - 1) & 31);   // fallback j = n-1 (:1136-1144)
+            const int tj = fm ? __shfl_sync(0xffffffffu, win, src) : n - 1;
+            const IT td = __shfl_sync(0xffffffffu, fm ? wd : lastd, src);
+            if (lane == 0) {
+                if constexpr (CL == 1) {
+                    tgt[i] = tj;
+                    dlt[i] = td;
+                } else {
+#pragma unroll
+                    for (int r = 0; r < CL; ++r) {
+                        st_cluster(tgt_at[r] + (uint32_t)((pb * npad + i) * 4), (int32_t)tj);
+                        st_cluster(dlt_at[r] + (uint32_t)((pb * npad + i) * sizeof(IT)), td);
+                    }
+                }
+            }
+        }
+        cluster_sync<CL>(G);   // every proposal of the replica is in every CTA
+
+        // ---- 2. collisions: a location goes to the best ballot touching it (qap.cu:1150-1225)
+        for (int q = tid; q < n; q += BT) s_own[q] = ~0ull;
+        draw_thresholds(step + 1u);   // phase 1 of this step has read them (cluster barrier above)
+        G.sync();
+        for (int q = tid; q < n; q += BT) {
+            const int t = tgt[q];
+            if (t != q && (unsigned)t < (unsigned)n) {
+                const unsigned long long w = oneshot_ballot(dlt[q], q);
+                atomicMin(&s_own[t], w);
+                atomicMin(&s_own[q], w);
+            }
+        }
+        G.sync();
+        int np = 0;
+        for (int q0 = 0; q0 < n; q0 += BT) {
+            const int q = q0 + tid;
+            bool acc = false;
+            int t = 0;
+            if (q < n) {
+                t = tgt[q];
+                acc = t != q && (unsigned)t < (unsigned)n && (uint32_t)s_own[q] == (uint32_t)q &&
+                      (uint32_t)s_own[t] == (uint32_t)q;
+            }
+            const unsigned m = __ballot_sync(0xffffffffu, acc);
+            if (lane == 0) s_wcnt[warp] = __popc(m);
+            G.sync();
+            int before = np, all = np;
+            for (int w = 0; w < nwarps; ++w) {
+                if (w == warp) before = all;
+                all += s_wcnt[w];
+            }
+            if (acc) {
+                const int pos = before + __popc(m & ((1u << lane) - 1u));
+                s_pi[pos] = q;
+                s_pj[pos] = t;
+                s_pa[pos] = s_phi[q];
+                s_pb[pos] = s_phi[t];
+            }
+            np = all;
+            G.sync();
+        }
+        // np is the same in every CTA of the cluster; a step without swaps changes nothing
+        if (np > 0) {
+            for (int p = tid; p < np; p += BT) {                  // qap.cu:1311-1332
+                const int i = s_pi[p], j = s_pj[p], a = s_pa[p], b = s_pb[p];
+                s_phi[i] = b;
+                s_phi[j] = a;
+                s_inv[a] = j;
+                s_inv[b] = i;
+            }
+
+            // ---- 3. force update of this CTA's rows (qap.cu:1337-1412), chunks of pc swaps
+            for (int c0 = 0; c0 < np; c0 += pc) {
+                const int cn = min(pc, np - c0);
+                // the chunk's factors from 16-byte row pieces of D^T, D, F^T, F, several pieces
+                // per thread in flight (rows are zero padded to ldm >= cl * rpc, npad)
+                constexpr int UNR = SYM ? 4 : 2;   // 512 threads: 128 registers each
+                stage_factors<IT, SYM, SYM, UNR>(tid, BT, cn, rpc / 4, s.DT + row0, s.D + row0, ldm, s_pi + c0, s_pj + c0,
+                                       s_U, s_U2, rpc);
+                stage_factors<IT, SYM, false, UNR>(tid, BT, cn, npad / 4, s.FT, s.F, ldm, s_pa + c0, s_pb + c0, s_V, s_V2,
+                                       vld);
+                for (int idx = tid; idx < cn * (vld - npad); idx += BT) {   // columns npad..vld-1
+                    const int p = idx / (vld - npad), c = npad + idx - p * (vld - npad);
+                    s_V[p * vld + c] = 0;
+                    if constexpr (!SYM) s_V2[p * vld + c] = 0;
+                }
+                G.sync();
+                for (int kq = warp * RT; kq < rows; kq += nwarps * RT) {
+                    U acc[RT][8];
+#pragma unroll
+                    for (int r = 0; r < RT; ++r)
+#pragma unroll
+                        for (int q = 0; q < 8; ++q) {
+                            const int c = lane + 32 * q;
+                            acc[r][q] = (q < K && c < n && kq + r < rows) ? (U)sI[(size_t)(kq + r) * lds + c] : (U)0;
+                        }
+                    {   // U / V rows are padded (rpc, 256 entries), so no load needs a guard
+                        const uint32_t ua = smem_u32(s_U) + (uint32_t)(kq * sizeof(IT));
+                        const uint32_t va = smem_u32(s_V) + (uint32_t)(lane * sizeof(IT));
+                        const uint32_t ua2 = smem_u32(s_U2) + (uint32_t)(kq * sizeof(IT));
+                        const uint32_t va2 = smem_u32(s_V2) + (uint32_t)(lane * sizeof(IT));
+                        for (int p = 0; p < cn; ++p) {
+                            U uu[RT], vv[8];
+#pragma unroll
+                            for (int r = 0; r < RT; ++r) uu[r] = (U)lds_it<IT>(ua + (uint32_t)((p * rpc + r) * sizeof(IT)));
+#pragma unroll
+                            for (int q = 0; q < 8; ++q) vv[q] = (U)lds_it<IT>(va + (uint32_t)((p * 256 + 32 * q) * sizeof(IT)));
+#pragma unroll
+                            for (int r = 0; r < RT; ++r)
+#pragma unroll
+                                for (int q = 0; q < 8; ++q) acc[r][q] += uu[r] * vv[q];
+                            if constexpr (!SYM) {
+#pragma unroll
+                                for (int r = 0; r < RT; ++r) uu[r] = (U)lds_it<IT>(ua2 + (uint32_t)((p * rpc + r) * sizeof(IT)));
+#pragma unroll
+                                for (int q = 0; q < 8; ++q) vv[q] = (U)lds_it<IT>(va2 + (uint32_t)((p * 256 + 32 * q) * sizeof(IT)));
+#pragma unroll
+                                for (int r = 0; r < RT; ++r)
+#pragma unroll
+                                    for (int q = 0; q < 8; ++q) acc[r][q] += uu[r] * vv[q];
+                            }
+                        }
+                    }
+#pragma unroll
+                    for (int r = 0; r < RT; ++r)
+#pragma unroll
+                        for (int q = 0; q < 8; ++q) {
+                            const int c = lane + 32 * q;
+                            if (q < K && c < n && kq + r < rows) sI[(size_t)(kq + r) * lds + c] = (IT)acc[r][q];
+                        }
+                }
+                G.sync();
+            }
+
+            // ---- 4. new diagonal and energy (qap.cu:1420-1458): E = -1/2 sum_k I[k][phi(k)]
+            long long mys = 0;
+            for (int kk = tid; kk < rows; kk += BT) {
+                const int k = row0 + kk;
+                const IT dv = sI[(size_t)kk * lds + s_phi[k]];
+                mys += (long long)dv;
+                if constexpr (CL == 1) s_diag[k] = dv;
+                else
+#pragma unroll
+                    for (int r = 0; r < CL; ++r) st_cluster(diag_at[r] + (uint32_t)(k * sizeof(IT)), dv);
+            }
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) mys += __shfl_xor_sync(0xffffffffu, mys, o);
+            if (lane == 0) s_part[CL + warp] = mys;
+            G.sync();
+            if (tid == 0) {
+                long long t = 0;
+                for (int w = 0; w < nwarps; ++w) t += s_part[CL + w];
+                if constexpr (CL == 1) s_part[0] = t;
+                else
+#pragma unroll
+                    for (int r = 0; r < CL; ++r) st_cluster(part_at[r] + (uint32_t)(rank * 8), (int64_t)t);
+            }
+            cluster_sync<CL>(G);   // new rows, diagonal and energy shares everywhere
+            long long tot = 0;
+#pragma unroll
+            for (int r = 0; r < CL; ++r) tot += s_part[r];
+            E = -tot / 2;
+            accepts += (unsigned long long)np;
+            if (xcol) {   // every CTA is past its force update: T (over U / V) may be written
+                send_columns();
+                cluster_sync<CL>(G);
+            }
+        }
+        if (E < bestE) {
+            bestE = E;
+            improved = true;
+            if (rank == 0) {
+                for (int q = tid; q < n; q += BT) s_bphi[q] = s_phi[q];
+                if constexpr (GP) {
+                    if (E < s.ev.goal_print) {
+                        if (tid == 0) s_flag[0] = goal_print_claim(s.ev, g, l, e, E);
+                        G.sync();
+                        const int slot = s_flag[0];
+                        if (slot >= 0)
+                            for (int q = tid; q < n; q += BT) s.ev.perm[(size_t)slot * n + q] = s_phi[q];
+                    }
+                }
+            }
+        }
+    }
+
+    // ---- store the replica
+    cluster_sync<CL>(G);   // no CTA reads another's shared memory any more
+    {
+        IT *gI = reinterpret_cast<IT *>(s.I) + ((size_t)rep * n + row0) * s.ldg;
+        const int nvg = s.ldg / VEC;
+        for (int idx = tid; idx < rows * nvg; idx += BT) {
+            const int k = idx / nvg, v = idx - k * nvg;
+            Vec<IT> w;
+#pragma unroll
+            for (int q = 0; q < VEC; ++q) w.v[q] = sI[(size_t)k * lds + v * VEC + q];
+            *reinterpret_cast<Vec<IT> *>(gI + (size_t)k * s.ldg + v * VEC) = w;
+        }
+    }
+    if (rank == 0) {
+        int32_t *gphi = s.phi + (size_t)rep * n;
+        for (int q = tid; q < n; q += BT) gphi[q] = s_phi[q];
+        if (improved) {
+            int32_t *gb = s.best_phi + (size_t)rep * n;
+            for (int q = tid; q < n; q += BT) gb[q] = s_bphi[q];
+        }
+        if (tid == 0) {
+            s.E[rep] = E;
+            s.bestE[rep] = bestE;
+            s.accepts[rep] = __ldcg(s.accepts + rep) + accepts;
+        }
+    }
+    __threadfence();
+    return true;
+}
+
 // Solve path: one launch = one epoch of every replica of the solve (grid = T*R*CL CTAs);
 // the last replica of each group to finish runs the group's tracking + exchange.
-template <class IT, int CL, bool SYM, bool GP, bool BIN = false>
-__global__ void __launch_bounds__(256, CL == 4 ? 2 : 1) epoch_kernel(SolveDev s) {
+// KIND: 0 the generic sequential epoch, 1 the binary-flow one, 2 the one-shot epoch (up to
+// 512 threads: its proposals are independent, so more warps hide more latency).
+template <class IT, int CL, bool SYM, bool GP, int KIND = 0>
+__global__ void __launch_bounds__(KIND == 2 ? 512 : 256, (CL == 4 && KIND != 2) ? 2 : 1) epoch_kernel(SolveDev s) {
     extern __shared__ __align__(16) unsigned char smem[];
     int rank = 0;
     if constexpr (CL > 1) rank = (int)cg::this_cluster().block_rank();
@@ -1259,7 +1849,8 @@ __global__ void __launch_bounds__(256, CL == 4 ? 2 : 1) epoch_kernel(SolveDev s)
     const Grp G{(int)threadIdx.x, (int)blockDim.x, (int)(threadIdx.x & 31), (int)(threadIdx.x >> 5),
                 (int)(blockDim.x >> 5), 0};
     bool ok;
-    if constexpr (BIN) ok = replica_epoch_bin<CL>(s, rep, rank, e, G, smem);
+    if constexpr (KIND == 1) ok = replica_epoch_bin<CL>(s, rep, rank, e, G, smem);
+    else if constexpr (KIND == 2) ok = replica_epoch_os<IT, CL, SYM, GP>(s, rep, rank, e, G, smem);
     else ok = replica_epoch<IT, CL, SYM, GP>(s, rep, rank, e, G, smem);
     __syncthreads();
     if (ok && rank == 0 && threadIdx.x == 0) {
@@ -1738,11 +2329,31 @@ static void *epoch_kernel_ptr(int bits, int cl, bool sym, bool gp) {
 // The binary-flow epoch (int32 forces, symmetric instance, no goal_print events).
 static void *epoch_bin_ptr(int cl) {
     switch (cl) {
-        case 1: return reinterpret_cast<void *>(&epoch_kernel<int32_t, 1, true, false, true>);
-        case 2: return reinterpret_cast<void *>(&epoch_kernel<int32_t, 2, true, false, true>);
-        case 4: return reinterpret_cast<void *>(&epoch_kernel<int32_t, 4, true, false, true>);
+        case 1: return reinterpret_cast<void *>(&epoch_kernel<int32_t, 1, true, false, 1>);
+        case 2: return reinterpret_cast<void *>(&epoch_kernel<int32_t, 2, true, false, 1>);
+        case 4: return reinterpret_cast<void *>(&epoch_kernel<int32_t, 4, true, false, 1>);
         default: return nullptr;
     }
+}
+
+template <class IT, int CL, bool SYM> static void *epoch_os_fn(bool gp) {
+    return gp ? reinterpret_cast<void *>(&epoch_kernel<IT, CL, SYM, true, 2>)
+              : reinterpret_cast<void *>(&epoch_kernel<IT, CL, SYM, false, 2>);
+}
+
+// The one-shot epoch.
+static void *epoch_os_ptr(int bits, int cl, bool sym, bool gp) {
+#define PIMQAP_PICK(IT)                                                                      \
+    switch (cl) {                                                                            \
+        case 1: return sym ? epoch_os_fn<IT, 1, true>(gp) : epoch_os_fn<IT, 1, false>(gp); \
+        case 2: return sym ? epoch_os_fn<IT, 2, true>(gp) : epoch_os_fn<IT, 2, false>(gp); \
+        case 4: return sym ? epoch_os_fn<IT, 4, true>(gp) : epoch_os_fn<IT, 4, false>(gp); \
+        default: return nullptr;                                                             \
+    }
+    if (bits == 32) { PIMQAP_PICK(int32_t) }
+    if (bits == 64) { PIMQAP_PICK(int64_t) }
+#undef PIMQAP_PICK
+    return nullptr;
 }
 
 static void *batch_fn(int bits, int cl) {
@@ -1816,6 +2427,9 @@ cudaError_t prepare_kernels() {
                     err = cudaFuncSetAttribute(epoch_kernel_ptr(bits, cl, sym != 0, gp != 0),
                                                cudaFuncAttributeMaxDynamicSharedMemorySize, maxsm);
                     if (err != cudaSuccess) return err;
+                    err = cudaFuncSetAttribute(epoch_os_ptr(bits, cl, sym != 0, gp != 0),
+                                               cudaFuncAttributeMaxDynamicSharedMemorySize, maxsm);
+                    if (err != cudaSuccess) return err;
                 }
     for (int bits : {32, 64})
         for (int cl : {1, 2, 4}) {
@@ -1847,8 +2461,9 @@ cudaError_t launch_epoch(const SolveDev &s, int bits, int cluster, bool sym, boo
                          size_t smem, cudaStream_t st) {
     const bool gp = s.ev.log != nullptr && s.ev.goal_print != 0;
     // clique-flow solves (s.act > 0) exist only in the binary-flow kernel
-    void *fn = (bin && bits == 32 && sym && (!gp || s.act > 0)) ? epoch_bin_ptr(cluster)
-                                                                 : epoch_kernel_ptr(bits, cluster, sym, gp);
+    void *fn = s.os_chunk > 0 ? epoch_os_ptr(bits, cluster, sym, gp)
+               : (bin && bits == 32 && sym && (!gp || s.act > 0)) ? epoch_bin_ptr(cluster)
+                                                                  : epoch_kernel_ptr(bits, cluster, sym, gp);
     if (!fn) return cudaErrorInvalidValue;
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3((unsigned)(s.T * s.R * cluster));

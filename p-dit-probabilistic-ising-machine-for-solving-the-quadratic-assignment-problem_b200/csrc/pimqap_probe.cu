@@ -10,6 +10,7 @@
 #include <string>
 
 #include "pimqap.h"
+#include "pimqap_weights.cuh"
 
 namespace {
 
@@ -36,7 +37,35 @@ __global__ void __launch_bounds__(kProbeThreads) smem_rmw_probe(int iters, int4 
     if (acc.x == 0x7fffffff) sink[blockIdx.x * blockDim.x + threadIdx.x] = acc;
 }
 
+__global__ void weight_exp2_kernel(const float *x, float *y, long long count) {
+    const long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (k < count) y[k] = pimqap::exp2f_neg(x[k]);
+}
+
 }  // namespace
+
+extern "C" pimqap_status pimqap_probe_weight_exp2(int32_t device, const float *x, float *y, int64_t count) {
+    if (!x || !y || count < 0) return PIMQAP_ERR_ARG;
+    if (count == 0) return PIMQAP_OK;
+    if (cudaSetDevice(device) != cudaSuccess) return PIMQAP_ERR_CUDA;
+    float *dx = nullptr, *dy = nullptr;
+    const size_t bytes = (size_t)count * sizeof(float);
+    if (cudaMalloc(&dx, bytes) != cudaSuccess) return PIMQAP_ERR_CUDA;
+    if (cudaMalloc(&dy, bytes) != cudaSuccess) {
+        cudaFree(dx);
+        return PIMQAP_ERR_CUDA;
+    }
+    cudaError_t err = cudaMemcpy(dx, x, bytes, cudaMemcpyHostToDevice);
+    if (err == cudaSuccess) {
+        const long long blocks = (count + 255) / 256;
+        weight_exp2_kernel<<<(unsigned)blocks, 256>>>(dx, dy, (long long)count);
+        err = cudaGetLastError();
+    }
+    if (err == cudaSuccess) err = cudaMemcpy(y, dy, bytes, cudaMemcpyDeviceToHost);
+    cudaFree(dx);
+    cudaFree(dy);
+    return err == cudaSuccess ? PIMQAP_OK : PIMQAP_ERR_CUDA;
+}
 
 extern "C" pimqap_status pimqap_probe_smem_bandwidth(int32_t device, double *gbs) {
     if (!gbs) return PIMQAP_ERR_ARG;

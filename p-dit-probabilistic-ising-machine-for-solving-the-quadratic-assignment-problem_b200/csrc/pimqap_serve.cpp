@@ -673,6 +673,8 @@ pimqap_status pimqap_server_submit(pimqap_server *h, const pimqap_instance *inst
     if (st != PIMQAP_OK) return st;
     if (params->active_facilities > 0)
         return fail(PIMQAP_ERR_ARG, "active_facilities is supported by pimqap_solve and solver handles only");
+    if (params->update_rule != PIMQAP_RULE_SEQUENTIAL)
+        return fail(PIMQAP_ERR_ARG, "the one-shot rule is supported by pimqap_solve and solver handles only");
     if (params->auto_beta) return fail(PIMQAP_ERR_ARG, "automatic beta selection needs pimqap_solve");
     if ((int64_t)params->groups * params->replicas > kServeMaxReplicas)
         return fail(PIMQAP_ERR_ARG, "a served request holds at most 1024 replicas (groups x replicas)");

@@ -194,6 +194,7 @@ extern "C" pimqap_status pimqap_solve_static(const pimqap_instance *inst,
         return fail(PIMQAP_ERR_ARG, "cluster_size must be 0, 1, 2 or 4");
     if (p->auto_beta) return fail(PIMQAP_ERR_ARG, "automatic beta selection needs pimqap_solve");
     if (p->active_facilities > 0) return fail(PIMQAP_ERR_ARG, "active_facilities needs pimqap_solve");
+    if (p->update_rule != PIMQAP_RULE_SEQUENTIAL) return fail(PIMQAP_ERR_ARG, "the one-shot rule needs pimqap_solve");
 
     // Instance analysis without heap buffers: symmetry and the per-row force bound.
     const int32_t *F = inst->flow, *D = inst->dist;

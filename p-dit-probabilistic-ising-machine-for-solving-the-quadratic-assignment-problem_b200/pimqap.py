@@ -48,7 +48,12 @@ class Params(C.Structure):
         ("auto_lower", C.c_double), ("auto_higher", C.c_double), ("goal_print", C.c_int64),
         ("event_capacity", C.c_int32), ("event_perm_capacity", C.c_int32),
         ("compact_instance", C.c_int32), ("active_facilities", C.c_int32),
+        ("update_rule", C.c_int32),
     ]
+
+
+RULE_SEQUENTIAL = 0
+RULE_ONE_SHOT = 1
 
 
 EVENT_GROUP_BEST = 0
@@ -163,6 +168,8 @@ def lib() -> C.CDLL:
     L.pimqap_solve_static.restype = st
     L.pimqap_probe_smem_bandwidth.argtypes = [C.c_int32, C.POINTER(C.c_double)]
     L.pimqap_probe_smem_bandwidth.restype = st
+    L.pimqap_probe_weight_exp2.argtypes = [C.c_int32, C.POINTER(C.c_float), C.POINTER(C.c_float), C.c_int64]
+    L.pimqap_probe_weight_exp2.restype = st
     _lib = L
     return L
 
@@ -292,6 +299,15 @@ def batch_solve(instances: Sequence, params: Sequence[Params]) -> List[dict]:
         r.final_energies = e.ctypes.data_as(C.POINTER(C.c_int64))
     _check(lib().pimqap_batch_solve(insts, ps, count, rs))
     return [_result_dict(r, p, e) for r, p, e in zip(rs, perms, energies)]
+
+
+def probe_weight_exp2(x: np.ndarray, device: int = 0) -> np.ndarray:
+    """The one-shot rule's binary32 weight function 2^x (x <= 0), evaluated by the device code."""
+    xs = np.ascontiguousarray(x, np.float32)
+    ys = np.zeros_like(xs)
+    fp = C.POINTER(C.c_float)
+    _check(lib().pimqap_probe_weight_exp2(device, xs.ctypes.data_as(fp), ys.ctypes.data_as(fp), xs.size))
+    return ys
 
 
 def probe_smem_bandwidth(device: int = 0) -> float:

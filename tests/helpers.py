@@ -4,12 +4,15 @@ import numpy as np
 LN2_INV = 1.44269504089
 
 
-def oracle_after(oracle, F, D, *, T, R, spe, beta_max, beta_ratio, seed, cap, megaiters, active=0):
+def oracle_after(oracle, F, D, *, T, R, spe, beta_max, beta_ratio, seed, cap, megaiters, active=0,
+                 rule=0, goal=0):
     """Oracle state after `megaiters` mega-iterations followed by each group's tracking /
     exchange step of the next mega-iteration (the solver runs that step at the end of every
-    epoch, on the device, before the next launch).  active > 0: clique-flow moves."""
-    st = oracle.setup(D, F, T, R, spe, beta_max * LN2_INV, beta_ratio, seed, cap=cap, active=active)
-    oracle.run(st, D, F, megaiters)
+    epoch, on the device, before the next launch).  active > 0: clique-flow moves; rule = 1:
+    one-shot steps."""
+    st = oracle.setup(D, F, T, R, spe, beta_max * LN2_INV, beta_ratio, seed, cap=cap, active=active,
+                      rule=rule)
+    oracle.run(st, D, F, megaiters, goal)
     oracle.track_exchange_all(st)
     return st
 
