@@ -299,6 +299,11 @@ def run_ours(args):
                                max_megaiters=args.steps * MEGAITERS_PER_STEP,
                                cluster_size=args.cluster_size, threads_per_block=args.threads,
                                active_facilities=act, update_rule=rule)
+    # one untimed call of the same API (one mega-iteration) takes any first-call cost of the
+    # process (module loading, first graph of this shape) out of the timed call
+    pw = pimqap.Params.from_buffer_copy(p2)
+    pw.max_megaiters = 1
+    pimqap.solve(Fp.numpy(), Dp.numpy(), pw)
     barrier()
     e0 = time.perf_counter()
     res = pimqap.solve(Fp.numpy(), Dp.numpy(), p2)

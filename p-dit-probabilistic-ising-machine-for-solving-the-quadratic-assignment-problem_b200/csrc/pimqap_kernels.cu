@@ -861,8 +861,10 @@ __device__ bool replica_epoch(const SolveDev &s, int rep, int rank, int e, const
 // Shared-memory layout of the binary-flow epoch (replica_epoch_bin): the instance itself is
 // resident next to the force-matrix rows, D as int16 columns of this CTA's rows and F as bit
 // rows, so no update waits for a row from L2.
+constexpr int kBinLog = 16;   // accepted swaps the binary-flow epoch keeps before rewriting its rows
+
 struct BinLayout {
-    size_t I, phi, inv, bphi, Dd, A, B, Ds, Fb, red, wsum, r, misc, bar, total;
+    size_t I, phi, inv, bphi, Dd, A, B, Ds, Fb, LU, V8, red, wsum, r, misc, bar, total;
     __host__ __device__ BinLayout(int n, int rpc, int lds, int cluster) {
         const size_t npad = (size_t)((n + 3) & ~3), rp = (size_t)rpc, nw = (size_t)((n + 31) / 32);
         size_t o = 0;
@@ -875,6 +877,8 @@ struct BinLayout {
         B = o;     o = align16(o + (cluster > 1 ? 2 * npad * 4 : 0));
         Ds = o;    o = align16(o + (size_t)n * rp * 2);   // Ds[r][k] = D[r][row0 + k]
         Fb = o;    o = align16(o + (size_t)n * nw * 4);   // bit b % 32 of Fb[a][b / 32] = F[a][b]
+        LU = o;    o = align16(o + (size_t)kBinLog * rp * 4);   // LU[p][k] = 2 (D[k][j_p] - D[k][i_p])
+        V8 = o;    o = align16(o + (size_t)kBinLog * npad);     // V8[p][c] = F[b_p][c] - F[a_p][c]
         red = o;   o = align16(o + kMaxWarps * 8);
         wsum = o;  o = align16(o + kMaxWarps * sizeof(double));
         r = o;     o = align16(o + 2 * sizeof(double));
@@ -917,6 +921,8 @@ __device__ bool replica_epoch_bin(const SolveDev &s, int rep, int rank, int e, c
     IT *s_B = reinterpret_cast<IT *>(smem + L.B);
     int16_t *s_Ds = reinterpret_cast<int16_t *>(smem + L.Ds);
     uint32_t *s_Fb = reinterpret_cast<uint32_t *>(smem + L.Fb);
+    IT *s_LU = reinterpret_cast<IT *>(smem + L.LU);
+    int8_t *s_V8 = reinterpret_cast<int8_t *>(smem + L.V8);
     IT *s_red = reinterpret_cast<IT *>(smem + L.red);
     double *s_wsum = reinterpret_cast<double *>(smem + L.wsum);
     double *s_r = reinterpret_cast<double *>(smem + L.r);
@@ -991,6 +997,54 @@ __device__ bool replica_epoch_bin(const SolveDev &s, int rep, int rank, int e, c
     const int act = s.act;
     bool failed = false;
     int upd = 0;
+    // Deferred force updates (not for clique flows): an accepted swap p is logged as the row
+    // factors LU[p][k] = 2 (D[k][j_p] - D[k][i_p]) of this CTA's rows and the column factors
+    // V8[p][c] = F[b_p][c] - F[a_p][c] (int8); a force entry is then
+    // I[k][c] + sum_p LU[p][k] V8[p][c].  Each
+    // update corrects the entries it reads; every kBinLog swaps (and at the end of the epoch)
+    // the rows are rewritten once for all of them.  Integer sums in any order: exact.
+    const bool lazy = act == 0;
+    int m = 0;                                               // pending swaps (same in all CTAs)
+    auto flush = [&]() {
+        // rows in blocks of 8 consecutive rows x 4 columns per thread
+        constexpr int RT = 8;
+        const int ngroups = max(1, BT / nvec);               // row-block groups in flight
+        for (int cv = tid % nvec, grp = tid / nvec; cv < nvec; cv += (BT >= nvec ? nvec : BT)) {
+            if (BT >= nvec && grp >= ngroups) break;
+            const int c0 = cv * VEC;
+            const int gfirst = (BT >= nvec) ? grp : 0, ginc = (BT >= nvec) ? ngroups : 1;
+            for (int kb = gfirst * RT; kb < rows; kb += ginc * RT) {
+                U acc[RT][VEC];
+#pragma unroll
+                for (int r = 0; r < RT; ++r) {
+                    Vec<IT> xv = {};
+                    if (kb + r < rows) xv = *reinterpret_cast<const Vec<IT> *>(sI + (size_t)(kb + r) * lds + c0);
+#pragma unroll
+                    for (int q = 0; q < VEC; ++q) acc[r][q] = (U)xv.v[q];
+                }
+                for (int p = 0; p < m; ++p) {
+                    const char4 v4 = *reinterpret_cast<const char4 *>(s_V8 + (size_t)p * npad + c0);
+                    const U v[VEC] = {(U)(int)v4.x, (U)(int)v4.y, (U)(int)v4.z, (U)(int)v4.w};
+                    const IT *lu = s_LU + (size_t)p * rpc + kb;
+#pragma unroll
+                    for (int r = 0; r < RT; ++r) {
+                        const U u = (kb + r < rows) ? (U)lu[r] : 0u;
+#pragma unroll
+                        for (int q = 0; q < VEC; ++q) acc[r][q] += u * v[q];
+                    }
+                }
+#pragma unroll
+                for (int r = 0; r < RT; ++r) {
+                    if (kb + r < rows) {
+                        Vec<IT> xv;
+#pragma unroll
+                        for (int q = 0; q < VEC; ++q) xv.v[q] = (IT)acc[r][q];
+                        *reinterpret_cast<Vec<IT> *>(sI + (size_t)(kb + r) * lds + c0) = xv;
+                    }
+                }
+            }
+        }
+    };
 
     for (int sw = 0; sw < s.spe && !failed; ++sw) {
         const uint32_t sweep = (uint32_t)(e * s.spe + sw);
@@ -1019,7 +1073,15 @@ __device__ bool replica_epoch_bin(const SolveDev &s, int rep, int rank, int e, c
                 const IT *Ij = sI + (size_t)jj * lds;
                 const U dd = (U)Dii + (U)s_Dd[j] - 2u * (U)(IT)Di[jj];
                 const U ff = (U)Faa + (U)fbit(b, b) - 2u * (U)fbit(a, b);
-                const U Bv = (U)Ij[a] - (U)Ij[b] - dd * ff;
+                U Bv = (U)Ij[a] - (U)Ij[b] - dd * ff;
+                // pending swaps: I[j][a] - I[j][b] (and, with one CTA, I[i][b] - I[i][a]) as corrected
+#pragma unroll 4
+                for (int q = 0; q < m; ++q) {
+                    const int8_t *v8 = s_V8 + (size_t)q * npad;
+                    const int w = (int)v8[a] - (int)v8[b];
+                    const U lu = (CL == 1) ? (U)s_LU[q * rpc + jj] - (U)s_LU[q * rpc + i] : (U)s_LU[q * rpc + jj];
+                    Bv += lu * (U)w;
+                }
                 if constexpr (CL == 1) {
                     s_A[p * npad + b] = (IT)(Bv + (U)Ii[b] - (U)Iia);
                 } else {
@@ -1030,10 +1092,26 @@ __device__ bool replica_epoch_bin(const SolveDev &s, int rep, int rank, int e, c
             }
             if constexpr (CL > 1) {
                 if (owner == rank) {
-                    for (int c4 = tid; c4 < nvec; c4 += BT) {
+                    const int il = i - row0;
+                    // on the threads after the B-half's when both fit, so the halves run side by side
+                    const int aoff = (rows + nvec <= BT) ? rows : 0;
+                    for (int c4 = tid - aoff; c4 >= 0 && c4 < nvec; c4 += BT) {
                         Vec<IT> v = *reinterpret_cast<const Vec<IT> *>(Ii + c4 * VEC);
 #pragma unroll
                         for (int q = 0; q < VEC; ++q) v.v[q] = (IT)((U)v.v[q] - (U)Iia);
+                        // pending swaps: I[i][c] - I[i][a] as corrected
+                        const int c0 = c4 * VEC;
+#pragma unroll 4
+                        for (int q2 = 0; q2 < m; ++q2) {
+                            const int8_t *v8 = s_V8 + (size_t)q2 * npad;
+                            const char4 v4 = *reinterpret_cast<const char4 *>(v8 + c0);
+                            const int va = (int)v8[a];
+                            const U lu = (U)s_LU[q2 * rpc + il];
+                            v.v[0] = (IT)((U)v.v[0] + lu * (U)((int)v4.x - va));
+                            v.v[1] = (IT)((U)v.v[1] + lu * (U)((int)v4.y - va));
+                            v.v[2] = (IT)((U)v.v[2] + lu * (U)((int)v4.z - va));
+                            v.v[3] = (IT)((U)v.v[3] + lu * (U)((int)v4.w - va));
+                        }
 #pragma unroll
                         for (int r = 0; r < CL; ++r)
                             st_async16(A_at[r] + (uint32_t)((p * npad + c4 * VEC) * sizeof(IT)), v,
@@ -1148,6 +1226,22 @@ __device__ bool replica_epoch_bin(const SolveDev &s, int rep, int rank, int e, c
                 if (tid == 0) s_misc[1] = upd;
             }
             const int16_t *Dj = s_Ds + (size_t)j * rpc;
+            if (lazy) {   // log the swap; rewrite the rows once kBinLog swaps are pending
+                for (int k = tid; k < rows; k += BT) s_LU[m * rpc + k] = (IT)(2u * ((U)(IT)Dj[k] - (U)(IT)Di[k]));
+                for (int c = tid; c < npad; c += BT)
+                    s_V8[(size_t)m * npad + c] = (int8_t)(c < n ? fbit(bs, c) - fbit(a, c) : 0);
+                ++m;
+                if (m == kBinLog) {
+                    G.sync();
+                    flush();
+                    m = 0;
+                }
+                G.sync();                                    // log, rows and phi visible
+                if (s_misc[1] == upd) {
+                    for (int q = tid; q < n; q += BT) s_bphi[q] = s_phi[q];
+                }
+                continue;
+            }
             // I[k][c] += 2 (D[j][k] - D[i][k]) (F[bs][c] - F[a][c]).  With clique flows only
             // columns a and bs change when both facilities are active, and only the active
             // columns when one is (CPU_PIM_tai256c.cpp:286-302): the other differences are 0.
@@ -1210,6 +1304,12 @@ __device__ bool replica_epoch_bin(const SolveDev &s, int rep, int rank, int e, c
         }
     }
 
+    if (m > 0) {   // the swaps still pending (m is the same in every thread)
+        G.sync();
+        flush();
+        m = 0;
+        G.sync();
+    }
     cluster_sync<CL>(G);
     if constexpr (CL > 1) {
         if (tid == 0) {
