@@ -921,7 +921,7 @@ __device__ bool replica_epoch_bin(const SolveDev &s, int rep, int rank, int e, c
     IT *s_B = reinterpret_cast<IT *>(smem + L.B);
     int16_t *s_Ds = reinterpret_cast<int16_t *>(smem + L.Ds);
     uint32_t *s_Fb = reinterpret_cast<uint32_t *>(smem + L.Fb);
-    IT *s_LU = reinterpret_cast<IT *>(smem + L.LU);
+    float *s_LU = reinterpret_cast<float *>(smem + L.LU);
     int8_t *s_V8 = reinterpret_cast<int8_t *>(smem + L.V8);
     IT *s_red = reinterpret_cast<IT *>(smem + L.red);
     double *s_wsum = reinterpret_cast<double *>(smem + L.wsum);
@@ -1000,7 +1000,9 @@ __device__ bool replica_epoch_bin(const SolveDev &s, int rep, int rank, int e, c
     // Deferred force updates (not for clique flows): an accepted swap p is logged as the row
     // factors LU[p][k] = 2 (D[k][j_p] - D[k][i_p]) of this CTA's rows and the column factors
     // V8[p][c] = F[b_p][c] - F[a_p][c] (int8); a force entry is then
-    // I[k][c] + sum_p LU[p][k] V8[p][c].  Each
+    // I[k][c] + sum_p LU[p][k] V8[p][c].  The sums are formed in binary32, which is exact here:
+    // |LU| <= 2^17 (int16 distances), |V8| <= 1, at most kBinLog = 16 terms, so every partial
+    // sum (also of the corrections below, |weight| <= 2) stays below 2^24.  Each
     // update corrects the entries it reads; every kBinLog swaps (and at the end of the epoch)
     // the rows are rewritten once for all of them.  Integer sums in any order: exact.
     const bool lazy = act == 0;
@@ -1014,32 +1016,33 @@ __device__ bool replica_epoch_bin(const SolveDev &s, int rep, int rank, int e, c
             const int c0 = cv * VEC;
             const int gfirst = (BT >= nvec) ? grp : 0, ginc = (BT >= nvec) ? ngroups : 1;
             for (int kb = gfirst * RT; kb < rows; kb += ginc * RT) {
-                U acc[RT][VEC];
+                float acc[RT][VEC];
 #pragma unroll
-                for (int r = 0; r < RT; ++r) {
-                    Vec<IT> xv = {};
-                    if (kb + r < rows) xv = *reinterpret_cast<const Vec<IT> *>(sI + (size_t)(kb + r) * lds + c0);
+                for (int r = 0; r < RT; ++r)
 #pragma unroll
-                    for (int q = 0; q < VEC; ++q) acc[r][q] = (U)xv.v[q];
-                }
+                    for (int q = 0; q < VEC; ++q) acc[r][q] = 0.0f;
                 for (int p = 0; p < m; ++p) {
                     const char4 v4 = *reinterpret_cast<const char4 *>(s_V8 + (size_t)p * npad + c0);
-                    const U v[VEC] = {(U)(int)v4.x, (U)(int)v4.y, (U)(int)v4.z, (U)(int)v4.w};
-                    const IT *lu = s_LU + (size_t)p * rpc + kb;
+                    const float v[VEC] = {(float)v4.x, (float)v4.y, (float)v4.z, (float)v4.w};
+                    // LU rows are rpc long (a multiple of 4) and 16-byte aligned; rows past `rows`
+                    // hold zeros and are never written back
+                    const float4 l0 = *reinterpret_cast<const float4 *>(s_LU + (size_t)p * rpc + kb);
+                    const float4 l1 = (kb + 4 < rpc) ? *reinterpret_cast<const float4 *>(s_LU + (size_t)p * rpc + kb + 4)
+                                                     : make_float4(0.f, 0.f, 0.f, 0.f);
+                    const float u[RT] = {l0.x, l0.y, l0.z, l0.w, l1.x, l1.y, l1.z, l1.w};
 #pragma unroll
-                    for (int r = 0; r < RT; ++r) {
-                        const U u = (kb + r < rows) ? (U)lu[r] : 0u;
+                    for (int r = 0; r < RT; ++r)
 #pragma unroll
-                        for (int q = 0; q < VEC; ++q) acc[r][q] += u * v[q];
-                    }
+                        for (int q = 0; q < VEC; ++q) acc[r][q] = fmaf(u[r], v[q], acc[r][q]);
                 }
 #pragma unroll
                 for (int r = 0; r < RT; ++r) {
                     if (kb + r < rows) {
-                        Vec<IT> xv;
+                        Vec<IT> *dst = reinterpret_cast<Vec<IT> *>(sI + (size_t)(kb + r) * lds + c0);
+                        Vec<IT> xv = *dst;
 #pragma unroll
-                        for (int q = 0; q < VEC; ++q) xv.v[q] = (IT)acc[r][q];
-                        *reinterpret_cast<Vec<IT> *>(sI + (size_t)(kb + r) * lds + c0) = xv;
+                        for (int q = 0; q < VEC; ++q) xv.v[q] = (IT)((U)xv.v[q] + (U)(int)acc[r][q]);
+                        *dst = xv;
                     }
                 }
             }
@@ -1075,13 +1078,15 @@ __device__ bool replica_epoch_bin(const SolveDev &s, int rep, int rank, int e, c
                 const U ff = (U)Faa + (U)fbit(b, b) - 2u * (U)fbit(a, b);
                 U Bv = (U)Ij[a] - (U)Ij[b] - dd * ff;
                 // pending swaps: I[j][a] - I[j][b] (and, with one CTA, I[i][b] - I[i][a]) as corrected
+                float cf = 0.0f;
 #pragma unroll 4
                 for (int q = 0; q < m; ++q) {
                     const int8_t *v8 = s_V8 + (size_t)q * npad;
-                    const int w = (int)v8[a] - (int)v8[b];
-                    const U lu = (CL == 1) ? (U)s_LU[q * rpc + jj] - (U)s_LU[q * rpc + i] : (U)s_LU[q * rpc + jj];
-                    Bv += lu * (U)w;
+                    const float w = (float)((int)v8[a] - (int)v8[b]);
+                    const float lu = (CL == 1) ? s_LU[q * rpc + jj] - s_LU[q * rpc + i] : s_LU[q * rpc + jj];
+                    cf = fmaf(lu, w, cf);
                 }
+                Bv += (U)(int)cf;
                 if constexpr (CL == 1) {
                     s_A[p * npad + b] = (IT)(Bv + (U)Ii[b] - (U)Iia);
                 } else {
@@ -1101,17 +1106,20 @@ __device__ bool replica_epoch_bin(const SolveDev &s, int rep, int rank, int e, c
                         for (int q = 0; q < VEC; ++q) v.v[q] = (IT)((U)v.v[q] - (U)Iia);
                         // pending swaps: I[i][c] - I[i][a] as corrected
                         const int c0 = c4 * VEC;
+                        float cf[VEC] = {0.0f, 0.0f, 0.0f, 0.0f};
 #pragma unroll 4
                         for (int q2 = 0; q2 < m; ++q2) {
                             const int8_t *v8 = s_V8 + (size_t)q2 * npad;
                             const char4 v4 = *reinterpret_cast<const char4 *>(v8 + c0);
                             const int va = (int)v8[a];
-                            const U lu = (U)s_LU[q2 * rpc + il];
-                            v.v[0] = (IT)((U)v.v[0] + lu * (U)((int)v4.x - va));
-                            v.v[1] = (IT)((U)v.v[1] + lu * (U)((int)v4.y - va));
-                            v.v[2] = (IT)((U)v.v[2] + lu * (U)((int)v4.z - va));
-                            v.v[3] = (IT)((U)v.v[3] + lu * (U)((int)v4.w - va));
+                            const float lu = s_LU[q2 * rpc + il];
+                            cf[0] = fmaf(lu, (float)((int)v4.x - va), cf[0]);
+                            cf[1] = fmaf(lu, (float)((int)v4.y - va), cf[1]);
+                            cf[2] = fmaf(lu, (float)((int)v4.z - va), cf[2]);
+                            cf[3] = fmaf(lu, (float)((int)v4.w - va), cf[3]);
                         }
+#pragma unroll
+                        for (int q = 0; q < VEC; ++q) v.v[q] = (IT)((U)v.v[q] + (U)(int)cf[q]);
 #pragma unroll
                         for (int r = 0; r < CL; ++r)
                             st_async16(A_at[r] + (uint32_t)((p * npad + c4 * VEC) * sizeof(IT)), v,
@@ -1227,7 +1235,8 @@ __device__ bool replica_epoch_bin(const SolveDev &s, int rep, int rank, int e, c
             }
             const int16_t *Dj = s_Ds + (size_t)j * rpc;
             if (lazy) {   // log the swap; rewrite the rows once kBinLog swaps are pending
-                for (int k = tid; k < rows; k += BT) s_LU[m * rpc + k] = (IT)(2u * ((U)(IT)Dj[k] - (U)(IT)Di[k]));
+                for (int k = tid; k < rpc; k += BT)
+                    s_LU[m * rpc + k] = k < rows ? (float)(2 * ((int)Dj[k] - (int)Di[k])) : 0.0f;
                 for (int c = tid; c < npad; c += BT)
                     s_V8[(size_t)m * npad + c] = (int8_t)(c < n ? fbit(bs, c) - fbit(a, c) : 0);
                 ++m;
