@@ -53,7 +53,7 @@ __host__ __device__ inline size_t align16(size_t x) { return (x + 15) & ~size_t(
 //   Drow, DTrow  [2][rpc]  D[i][own rows], D[own rows][i] for the current / next location i
 //   Frow, FTrow  [2][npad] F[a][*], F[*][a] for a = phi(i), current / next
 //   Dj, DTj, Fb, FTb        the same rows for the partner j / facility b of an accepted swap
-//   red, wsum, r, misc, bar  reductions, random number, pick, mbarriers
+//   red, wsum, r, misc, bar  reductions, the random numbers of a sweep, pick, mbarriers
 struct SmemLayout {
     size_t I, phi, inv, bphi, Dd, Fd, A, B, Drow, DTrow, Frow, FTrow, Dj, DTj, Fb, FTb;
     size_t u1, u2, red, wsum, r, misc, bar, total;
@@ -81,7 +81,7 @@ struct SmemLayout {
         u2 = o;    o = align16(o + rp * isz);
         red = o;   o = align16(o + kMaxWarps * 8);
         wsum = o;  o = align16(o + kMaxWarps * sizeof(double));
-        r = o;     o = align16(o + 2 * sizeof(double));
+        r = o;     o = align16(o + npad * sizeof(double));   // r of each update of a sweep
         misc = o;  o = align16(o + 4 * sizeof(int));
         bar = o;   o = align16(o + 2 * sizeof(unsigned long long));
         total = o;
@@ -576,13 +576,18 @@ __device__ bool replica_epoch(const SolveDev &s, int rep, int rank, int e, const
 
     for (int sw = 0; sw < s.spe && !failed; ++sw) {
         const uint32_t sweep = (uint32_t)(e * s.spe + sw);
+        // r of every update of this sweep (:212), one Philox block each, drawn by all threads up
+        // front; the picks read them after their barriers (the last pick of the previous sweep
+        // read its r before its final barrier)
+        for (int q = tid; q < n; q += BT) {
+            uint32_t w0, w1;
+            philox_2words((uint32_t)q, sweep, (uint32_t)l, (uint32_t)g, k0, k1, w0, w1);
+            s_r[q] = canonical53(w0, w1);
+        }
         for (int i = 0; i < n; ++i, ++upd) {
             const int p = upd & 1;
-            if (tid == 0) {
-                uint32_t w0, w1;
-                philox_2words((uint32_t)i, sweep, (uint32_t)l, (uint32_t)g, k0, k1, w0, w1);
-                s_r[p] = canonical53(w0, w1);
-                if constexpr (CL > 1) mbar_arrive_expect_tx(smem_u32(&s_bar[p]), tx_bytes);
+            if constexpr (CL > 1) {
+                if (tid == 0) mbar_arrive_expect_tx(smem_u32(&s_bar[p]), tx_bytes);
             }
             const int a = s_phi[i];
             const int inext = (i + 1 == n) ? 0 : i + 1;
@@ -691,7 +696,7 @@ __device__ bool replica_epoch(const SolveDev &s, int rep, int rank, int e, const
                 if (w == warp) base = total;
                 total = __dadd_rn(total, s_wsum[w]);
             }
-            const double target = __dmul_rn(s_r[p], total);     // :247
+            const double target = __dmul_rn(s_r[i], total);     // :247
             const double X = __dadd_rn(base, excl);
 #pragma unroll
             for (int k = 0; k < 4; ++k) {
@@ -881,7 +886,7 @@ struct BinLayout {
         V8 = o;    o = align16(o + (size_t)kBinLog * npad);     // V8[p][c] = F[b_p][c] - F[a_p][c]
         red = o;   o = align16(o + kMaxWarps * 8);
         wsum = o;  o = align16(o + kMaxWarps * sizeof(double));
-        r = o;     o = align16(o + 2 * sizeof(double));
+        r = o;     o = align16(o + npad * sizeof(double));   // r of each update of a sweep
         misc = o;  o = align16(o + 4 * sizeof(int));
         bar = o;   o = align16(o + 2 * sizeof(unsigned long long));
         total = o;
@@ -1051,13 +1056,18 @@ __device__ bool replica_epoch_bin(const SolveDev &s, int rep, int rank, int e, c
 
     for (int sw = 0; sw < s.spe && !failed; ++sw) {
         const uint32_t sweep = (uint32_t)(e * s.spe + sw);
+        // r of every update of this sweep (:212), one Philox block each, drawn by all threads up
+        // front; the picks read them after their barriers (the last pick of the previous sweep
+        // read its r before its final barrier)
+        for (int q = tid; q < n; q += BT) {
+            uint32_t w0, w1;
+            philox_2words((uint32_t)q, sweep, (uint32_t)l, (uint32_t)g, k0, k1, w0, w1);
+            s_r[q] = canonical53(w0, w1);
+        }
         for (int i = 0; i < n; ++i, ++upd) {
             const int p = upd & 1;
-            if (tid == 0) {
-                uint32_t w0, w1;
-                philox_2words((uint32_t)i, sweep, (uint32_t)l, (uint32_t)g, k0, k1, w0, w1);
-                s_r[p] = canonical53(w0, w1);
-                if constexpr (CL > 1) mbar_arrive_expect_tx(smem_u32(&s_bar[p]), tx_bytes);
+            if constexpr (CL > 1) {
+                if (tid == 0) mbar_arrive_expect_tx(smem_u32(&s_bar[p]), tx_bytes);
             }
             const int a = s_phi[i];
             // clique flows (act > 0): an inactive facility weighs the actives and one lumped
@@ -1185,7 +1195,7 @@ __device__ bool replica_epoch_bin(const SolveDev &s, int rep, int rank, int e, c
                 if (w == warp) base = total;
                 total = __dadd_rn(total, s_wsum[w]);
             }
-            const double target = __dmul_rn(s_r[p], total);     // :247
+            const double target = __dmul_rn(s_r[i], total);     // :247
             const double X = __dadd_rn(base, excl);
 #pragma unroll
             for (int k = 0; k < 4; ++k) {
