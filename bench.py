@@ -253,6 +253,30 @@ def run_ours(args):
         if world > 1:
             dist.barrier()
 
+    # e2e first: the same work through the C ABI (pimqap_solve) from pinned host buffers,
+    # before the clock sampler's process runs
+    Fp = torch.from_numpy(inst.F).pin_memory()
+    Dp = torch.from_numpy(inst.D).pin_memory()
+    p2 = pimqap.default_params(replicas=REPLICAS, groups=GROUPS, sweeps_per_exchange=SWEEPS_PER_EXCHANGE,
+                               beta_max=BETA_MAX, beta_ratio=BETA_RATIO, beta_internal=1, seed=1 + rank,
+                               device=local,
+                               megaiters_per_launch=4 * MEGAITERS_PER_STEP,   # fewer host round trips
+                               max_megaiters=args.steps * MEGAITERS_PER_STEP,
+                               cluster_size=args.cluster_size, threads_per_block=args.threads,
+                               active_facilities=act, update_rule=rule)
+    # one untimed call of the same API (one mega-iteration) takes any first-call cost of the
+    # process (module loading, first graph of this shape) out of the timed call
+    pw = pimqap.Params.from_buffer_copy(p2)
+    pw.max_megaiters = 1
+    pimqap.solve(Fp.numpy(), Dp.numpy(), pw)
+    barrier()
+    e0 = time.perf_counter()
+    res = pimqap.solve(Fp.numpy(), Dp.numpy(), p2)
+    e_wall = time.perf_counter() - e0
+    e2e_sweeps = args.steps * MEGAITERS_PER_STEP * SWEEPS_PER_EXCHANGE
+    e2e_value = whole_job_rate(proposals(REPLICAS * GROUPS, e2e_sweeps), world,
+                               max_over_ranks(e_wall, world, f"cuda:{local}"))
+
     ms_total = 0.0
     with ClockSampler(local) as clocks:
         barrier()
@@ -288,27 +312,6 @@ def run_ours(args):
     achieved = alg_bytes / (ms_total * 1e-3) / 1e9
     smem_peak = pimqap.probe_smem_bandwidth(local)
     traffic = read_traffic("epoch_kernel_oneshot_grid256.md" if rule else "epoch_kernel_grid256.md")
-
-    # e2e through the C ABI from pinned host buffers
-    Fp = torch.from_numpy(inst.F).pin_memory()
-    Dp = torch.from_numpy(inst.D).pin_memory()
-    p2 = pimqap.default_params(replicas=REPLICAS, groups=GROUPS, sweeps_per_exchange=SWEEPS_PER_EXCHANGE,
-                               beta_max=BETA_MAX, beta_ratio=BETA_RATIO, beta_internal=1, seed=1 + rank,
-                               device=local,
-                               megaiters_per_launch=MEGAITERS_PER_STEP,
-                               max_megaiters=args.steps * MEGAITERS_PER_STEP,
-                               cluster_size=args.cluster_size, threads_per_block=args.threads,
-                               active_facilities=act, update_rule=rule)
-    # one untimed call of the same API (one mega-iteration) takes any first-call cost of the
-    # process (module loading, first graph of this shape) out of the timed call
-    pw = pimqap.Params.from_buffer_copy(p2)
-    pw.max_megaiters = 1
-    pimqap.solve(Fp.numpy(), Dp.numpy(), pw)
-    barrier()
-    e0 = time.perf_counter()
-    res = pimqap.solve(Fp.numpy(), Dp.numpy(), p2)
-    e_wall = time.perf_counter() - e0
-    e2e_value = whole_job_rate(proposals(reps, sweeps), world, max_over_ranks(e_wall, world, f"cuda:{local}"))
 
     line = None
     if rank == 0:
