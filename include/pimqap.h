@@ -146,6 +146,11 @@ typedef struct pimqap_result {
 pimqap_status pimqap_read_problem(const char *path, int32_t max_n, int32_t *n,
                                   int32_t *flow, int32_t *dist);
 
+/* The same reader into arrays it allocates (the survey's pimqap_load_file): inst->flow and
+   inst->dist hold n*n entries each until pimqap_free_instance releases them. */
+pimqap_status pimqap_load_file(const char *path, pimqap_instance *inst);
+void pimqap_free_instance(pimqap_instance *inst);
+
 /* ---------------------------------------------------------------- one-shot solve */
 
 /* The whole CPU_PIM run with fixed beta parameters (replaces setup() + the threadToRun
@@ -238,6 +243,19 @@ pimqap_status pimqap_solver_event_perm(pimqap_solver *s, int32_t perm_index, int
 
 void pimqap_solver_destroy(pimqap_solver *s);
 
+/* Parity tool: nsweeps sweeps of ONE replica (doMegaItera, CPU_PIM.cpp:195-290, with NUMITERA
+   sweeps and no exchange partner) from the caller's permutation phi_in (facility at each
+   location), at beta = params->beta_max (natural units unless params->beta_internal), with the
+   uniform r of every update given by the caller (r[s * n + i] for sweep s, location i, each in
+   [0, 1); the reference draws it with generate_canonical, :212) instead of the Philox stream.
+   The force matrix is set up from phi_in on the device (:164-192).  Outputs (any may be NULL):
+   the final permutation (n), force matrix (n*n, widened to int64), energy, best energy and
+   accepted moves.  Force width and launch shape follow params; the sequential rule only. */
+pimqap_status pimqap_sweep_replay(const pimqap_instance *inst, const pimqap_params *params,
+                                  const int32_t *phi_in, int32_t nsweeps, const double *r,
+                                  int32_t *phi_out, int64_t *force, int64_t *energy,
+                                  int64_t *best_energy, int64_t *accepts);
+
 /* ---------------------------------------------------------------- batched solve */
 
 /* Many independent instances of uneven n, each with its own replica set and parameters,
@@ -246,6 +264,18 @@ void pimqap_solver_destroy(pimqap_solver *s);
    Each result equals what pimqap_solve returns for that instance alone. */
 pimqap_status pimqap_batch_solve(const pimqap_instance *insts, const pimqap_params *params,
                                  int32_t count, pimqap_result *results);
+
+/* The same batch without blocking: pimqap_batch_submit copies the instances and parameters and
+   returns at once; the batch runs on a host thread of its own.  The caller's results array
+   (with its best_perm / final_energies buffers) is written when the batch finishes and must
+   stay alive until pimqap_batch_poll returns PIMQAP_OK (PIMQAP_ERR_NOT_READY before) or
+   pimqap_batch_wait (up to timeout_s seconds, < 0 = no limit) does; then release the handle. */
+typedef struct pimqap_batch pimqap_batch;
+pimqap_status pimqap_batch_submit(const pimqap_instance *insts, const pimqap_params *params,
+                                  int32_t count, pimqap_result *results, pimqap_batch **out);
+pimqap_status pimqap_batch_poll(pimqap_batch *b);
+pimqap_status pimqap_batch_wait(pimqap_batch *b, double timeout_s);
+void pimqap_batch_release(pimqap_batch *b);
 
 /* ---------------------------------------------------------------- serving */
 

@@ -104,6 +104,9 @@ class Oracle:
         L.orc_setup.argtypes = [C.POINTER(_RunState), _i32p, _i32p, C.c_double, C.c_double]
         L.orc_run.argtypes = [C.POINTER(_RunState), _i32p, _i32p, C.c_int64, C.c_int64]
         L.orc_run.restype = C.c_int
+        L.orc_replay_sweeps.argtypes = [C.c_int, _i32p, _i32p, _i64p, _i32p, _i32p, _i64p, _i64p,
+                                        C.c_double, C.c_int, _f64p, C.c_void_p]
+        L.orc_replay_sweeps.restype = C.c_int64
         L.orc_exp2f_neg.argtypes = [C.c_float]
         L.orc_exp2f_neg.restype = C.c_float
         L.orc_oneshot_uniform.argtypes = [C.c_uint32]
@@ -177,6 +180,20 @@ class Oracle:
             st.time_since_swap[t] = tss[0]
             st.thread_best[t] = tb[0]
         st.c.single_best = int(sb[0])
+
+    def replay_sweeps(self, D, F, phi, beta, r):
+        """Sweeps of one replica from permutation phi with the uniforms r ([nsweeps, n]).
+        Returns (phi, I, E, bestE, accepts)."""
+        D = np.ascontiguousarray(D, np.int32)
+        F = np.ascontiguousarray(F, np.int32)
+        phi = np.ascontiguousarray(phi, np.int32).copy()
+        inv = np.argsort(phi).astype(np.int32)
+        I, E0 = self.force_init(D, F, phi)
+        E = np.array([E0], np.int64)
+        bestE = np.array([NO_BEST], np.int64)
+        r = np.ascontiguousarray(r, np.float64)
+        acc = self.lib.orc_replay_sweeps(D.shape[0], D, F, I, phi, inv, E, bestE, beta, r.shape[0], r.ravel(), None)
+        return phi, I, int(E[0]), int(bestE[0]), int(acc)
 
     def exp2f_neg(self, x: float) -> float:
         return float(self.lib.orc_exp2f_neg(x))

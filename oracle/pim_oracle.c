@@ -138,10 +138,16 @@ static int64_t trunc_cutoff(double x) {
 int orc_update(int n, const int32_t *D, const int32_t *F, int64_t *I, int32_t *phi,
                int32_t *phiinv, int64_t *E, int64_t *bestE, double beta, int i,
                uint32_t w0, uint32_t w1, int64_t *dE_out) {
+    return orc_update_r(n, D, F, I, phi, phiinv, E, bestE, beta, i,
+                        orc_canonical(w0, w1), dE_out);   /* r, :212 */
+}
+
+int orc_update_r(int n, const int32_t *D, const int32_t *F, int64_t *I, int32_t *phi,
+                 int32_t *phiinv, int64_t *E, int64_t *bestE, double beta, int i, double r,
+                 int64_t *dE_out) {
     long double probs[256];
     int64_t dEs[256];
     int64_t maxDeltaE = 0;                              /* :208, starts at 0 */
-    const double r = orc_canonical(w0, w1);             /* :212 */
     double probSum = 0.0;
     const int a = phi[i];                               /* :215 */
     const int64_t *Ii = I + (size_t)i * n;
@@ -302,6 +308,22 @@ int64_t orc_replica_sweeps(int n, const int32_t *D, const int32_t *F, int64_t *I
             uint32_t w1 = orc_sweep_word(seed, group, replica, sw, (uint32_t)i, 1);
             int a = phi[i];
             int b = orc_update(n, D, F, I, phi, phiinv, E, bestE, beta, i, w0, w1, 0);
+            if (b >= 0 && b != a) ++accepts;
+            if (picks) picks[(size_t)s * n + i] = b;
+        }
+    }
+    return accepts;
+}
+
+int64_t orc_replay_sweeps(int n, const int32_t *D, const int32_t *F, int64_t *I, int32_t *phi,
+                          int32_t *phiinv, int64_t *E, int64_t *bestE, double beta, int nsweeps,
+                          const double *r, int32_t *picks) {
+    int64_t accepts = 0;
+    for (int s = 0; s < nsweeps; ++s) {
+        for (int i = 0; i < n; ++i) {
+            const int a = phi[i];
+            const int b = orc_update_r(n, D, F, I, phi, phiinv, E, bestE, beta, i,
+                                       r[(size_t)s * n + i], 0);
             if (b >= 0 && b != a) ++accepts;
             if (picks) picks[(size_t)s * n + i] = b;
         }

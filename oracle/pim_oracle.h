@@ -74,6 +74,16 @@ int orc_update(int n, const int32_t *D, const int32_t *F, int64_t *I, int32_t *p
                int32_t *phiinv, int64_t *E, int64_t *bestE, double beta, int i,
                uint32_t w0, uint32_t w1, int64_t *dE_out);
 
+/* orc_update with the uniform r given directly instead of two engine words. */
+int orc_update_r(int n, const int32_t *D, const int32_t *F, int64_t *I, int32_t *phi,
+                 int32_t *phiinv, int64_t *E, int64_t *bestE, double beta, int i, double r,
+                 int64_t *dE_out);
+/* nsweeps sweeps of one replica with the uniforms r[s * n + i] of update (sweep s, location i);
+   picks (optional) as orc_replica_sweeps.  Returns the accepted moves. */
+int64_t orc_replay_sweeps(int n, const int32_t *D, const int32_t *F, int64_t *I, int32_t *phi,
+                          int32_t *phiinv, int64_t *E, int64_t *bestE, double beta, int nsweeps,
+                          const double *r, int32_t *picks);
+
 /* nsweeps sweeps of one replica (doMegaItera with NUMITERA = nsweeps).  picks (optional,
    nsweeps*n) records orc_update's return per update.  Returns the number of accepted moves. */
 int64_t orc_replica_sweeps(int n, const int32_t *D, const int32_t *F, int64_t *I,

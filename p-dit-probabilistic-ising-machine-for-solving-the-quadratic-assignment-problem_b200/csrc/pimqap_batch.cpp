@@ -10,6 +10,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <chrono>
 #include <cmath>
 #include <cstdio>
@@ -18,6 +19,7 @@
 #include <limits>
 #include <memory>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "pimqap.h"
@@ -409,6 +411,77 @@ uint64_t splitmix64(uint64_t x) {
 // the reference's, in the same double arithmetic.  Because the reference's trials run in order
 // and its best energy carries over between them, the first trial (in that order) whose tracked
 // best reaches the goal ends automatic mode (:419-422); the trials after it are ignored.
+// ------------------------------------------------------------------ asynchronous batches
+
+// A batch solved on its own host thread: the instances and parameters are copied at submit,
+// the caller's result array (and its best_perm / final_energies buffers) is written when the
+// batch finishes and must stay alive until pimqap_batch_poll / pimqap_batch_wait reports it.
+struct pimqap_batch {
+    std::vector<std::vector<int32_t>> flows, dists;
+    std::vector<pimqap_instance> insts;
+    std::vector<pimqap_params> params;
+    pimqap_result *results = nullptr;
+    std::thread worker;
+    std::atomic<int> done{0};
+    pimqap_status status = PIMQAP_OK;
+    std::string error;
+};
+
+extern "C" pimqap_status pimqap_batch_submit(const pimqap_instance *insts, const pimqap_params *params,
+                                             int32_t count, pimqap_result *results, pimqap_batch **out) {
+    if (!out) return fail(PIMQAP_ERR_ARG, "null batch handle");
+    *out = nullptr;
+    if (!insts || !params || !results || count < 1) return fail(PIMQAP_ERR_ARG, "empty batch");
+    std::unique_ptr<pimqap_batch> b(new pimqap_batch());
+    b->flows.resize(count);
+    b->dists.resize(count);
+    b->insts.resize(count);
+    for (int k = 0; k < count; ++k) {
+        const int n = insts[k].n;
+        if (n < 1 || n > PIMQAP_MAX_N || !insts[k].flow || !insts[k].dist)
+            return fail(PIMQAP_ERR_ARG, "instance " + std::to_string(k) + " is malformed");
+        b->flows[k].assign(insts[k].flow, insts[k].flow + (size_t)n * n);
+        b->dists[k].assign(insts[k].dist, insts[k].dist + (size_t)n * n);
+        b->insts[k] = pimqap_instance{n, b->flows[k].data(), b->dists[k].data()};
+    }
+    b->params.assign(params, params + count);
+    b->results = results;
+    pimqap_batch *raw = b.get();
+    raw->worker = std::thread([raw, count] {
+        raw->status = pimqap_batch_solve(raw->insts.data(), raw->params.data(), count, raw->results);
+        if (raw->status != PIMQAP_OK) raw->error = pimqap_last_error();
+        raw->done.store(1, std::memory_order_release);
+    });
+    *out = b.release();
+    return PIMQAP_OK;
+}
+
+extern "C" pimqap_status pimqap_batch_poll(pimqap_batch *b) {
+    if (!b) return fail(PIMQAP_ERR_ARG, "null batch handle");
+    if (!b->done.load(std::memory_order_acquire)) return PIMQAP_ERR_NOT_READY;
+    if (b->worker.joinable()) b->worker.join();
+    if (b->status != PIMQAP_OK) return fail(b->status, b->error);
+    return PIMQAP_OK;
+}
+
+extern "C" pimqap_status pimqap_batch_wait(pimqap_batch *b, double timeout_s) {
+    if (!b) return fail(PIMQAP_ERR_ARG, "null batch handle");
+    const auto t0 = std::chrono::steady_clock::now();
+    while (!b->done.load(std::memory_order_acquire)) {
+        if (timeout_s >= 0 &&
+            std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count() >= timeout_s)
+            return PIMQAP_ERR_NOT_READY;
+        std::this_thread::sleep_for(std::chrono::microseconds(200));
+    }
+    return pimqap_batch_poll(b);
+}
+
+extern "C" void pimqap_batch_release(pimqap_batch *b) {
+    if (!b) return;
+    if (b->worker.joinable()) b->worker.join();
+    delete b;
+}
+
 extern "C" pimqap_status pimqap_auto_beta_report(const pimqap_instance *inst, const pimqap_params *params,
                                                  pimqap_auto_report *rep) {
     if (!inst || !params || !rep) return fail(PIMQAP_ERR_ARG, "null argument");

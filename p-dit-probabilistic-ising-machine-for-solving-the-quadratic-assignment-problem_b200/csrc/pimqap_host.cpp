@@ -537,6 +537,94 @@ pimqap_status pimqap_read_problem(const char *path, int32_t max_n, int32_t *n_ou
     return PIMQAP_OK;
 }
 
+pimqap_status pimqap_load_file(const char *path, pimqap_instance *inst) {
+    if (!inst) return fail(PIMQAP_ERR_ARG, "null instance");
+    *inst = pimqap_instance{0, nullptr, nullptr};
+    int32_t n = 0;
+    pimqap_status st = pimqap_read_problem(path, PIMQAP_MAX_N, &n, nullptr, nullptr);
+    if (st != PIMQAP_OK) return st;
+    int32_t *F = static_cast<int32_t *>(std::malloc(sizeof(int32_t) * (size_t)n * n));
+    int32_t *D = static_cast<int32_t *>(std::malloc(sizeof(int32_t) * (size_t)n * n));
+    if (!F || !D) {
+        std::free(F);
+        std::free(D);
+        return fail(PIMQAP_ERR_ARG, "out of host memory");
+    }
+    st = pimqap_read_problem(path, PIMQAP_MAX_N, &n, F, D);
+    if (st != PIMQAP_OK) {
+        std::free(F);
+        std::free(D);
+        return st;
+    }
+    *inst = pimqap_instance{n, F, D};
+    return PIMQAP_OK;
+}
+
+void pimqap_free_instance(pimqap_instance *inst) {
+    if (!inst) return;
+    std::free(const_cast<int32_t *>(inst->flow));
+    std::free(const_cast<int32_t *>(inst->dist));
+    *inst = pimqap_instance{0, nullptr, nullptr};
+}
+
+pimqap_status pimqap_sweep_replay(const pimqap_instance *inst, const pimqap_params *params,
+                                  const int32_t *phi_in, int32_t nsweeps, const double *r,
+                                  int32_t *phi_out, int64_t *force, int64_t *energy,
+                                  int64_t *best_energy, int64_t *accepts) {
+    if (!inst || !params || !phi_in || !r || nsweeps < 0) return fail(PIMQAP_ERR_ARG, "bad replay arguments");
+    if (params->update_rule != PIMQAP_RULE_SEQUENTIAL || params->active_facilities != 0)
+        return fail(PIMQAP_ERR_ARG, "the replay runs CPU_PIM's sequential rule only");
+    const int n = inst->n;
+    if (n < 1 || n > PIMQAP_MAX_N) return fail(PIMQAP_ERR_ARG, "bad n");
+    std::vector<char> seen((size_t)n, 0);
+    for (int q = 0; q < n; ++q) {
+        if (phi_in[q] < 0 || phi_in[q] >= n || seen[(size_t)phi_in[q]]) return fail(PIMQAP_ERR_ARG, "phi is not a permutation");
+        seen[(size_t)phi_in[q]] = 1;
+    }
+    for (int64_t k = 0; k < (int64_t)nsweeps * n; ++k)
+        if (!(r[k] >= 0.0 && r[k] < 1.0)) return fail(PIMQAP_ERR_ARG, "every r must be in [0, 1)");
+    // one replica, one sweep per mega-iteration, no goal, no events: exactly nsweeps sweeps
+    pimqap_params p = *params;
+    p.replicas = 1;
+    p.groups = 1;
+    p.sweeps_per_exchange = 1;
+    p.rank_slots = 0;
+    p.auto_beta = 0;
+    p.max_megaiters = nsweeps;
+    p.goal = std::numeric_limits<int64_t>::min();
+    p.timeout_s = 0;
+    p.goal_print = 0;
+    p.event_capacity = 0;
+    pimqap_solver *s = nullptr;
+    pimqap_status st = pimqap_solver_create(inst, &p, &s);
+    if (st != PIMQAP_OK) return st;
+    std::unique_ptr<pimqap_solver, void (*)(pimqap_solver *)> guard(s, pimqap_solver_destroy);
+    double *dr = nullptr;
+    struct FreeDev { void operator()(double *q) const { if (q) cudaFree(q); } };
+    // the caller's permutation replaces the shuffle, then set-up runs again on it
+    PQ_CUDA(cudaMemcpy(s->dev.phi, phi_in, sizeof(int32_t) * n, cudaMemcpyHostToDevice));
+    PQ_CUDA(pimqap::launch_setup(s->dev, s->bits, s->stream));
+    if (nsweeps > 0) {
+        PQ_CUDA(cudaMalloc(&dr, sizeof(double) * (size_t)nsweeps * n));
+    }
+    std::unique_ptr<double, FreeDev> rguard(dr);
+    if (nsweeps > 0) {
+        PQ_CUDA(cudaMemcpy(dr, r, sizeof(double) * (size_t)nsweeps * n, cudaMemcpyHostToDevice));
+        s->dev.replay_r = dr;
+        st = pimqap_solver_run(s, nsweeps, nullptr);
+        if (st != PIMQAP_OK) return st;
+    }
+    PQ_CUDA(cudaStreamSynchronize(s->stream));
+    st = pimqap_solver_replica(s, 0, 0, phi_out, force, energy, best_energy, nullptr);
+    if (st != PIMQAP_OK) return st;
+    if (accepts) {
+        unsigned long long a = 0;
+        PQ_CUDA(cudaMemcpy(&a, s->dev.accepts, 8, cudaMemcpyDeviceToHost));
+        *accepts = (int64_t)a;
+    }
+    return PIMQAP_OK;
+}
+
 pimqap_status pimqap_solver_create(const pimqap_instance *inst, const pimqap_params *params,
                                    pimqap_solver **out) {
     if (!out) return fail(PIMQAP_ERR_ARG, "null output handle");

@@ -85,6 +85,8 @@ struct SolveDev {
     int32_t os_xcol;           // one-shot with a cluster: peers push the force-matrix columns
                                //      the proposals need (0: the proposals read them remotely)
     int32_t pad_os;
+    const double *replay_r;    // [sweeps][n] the uniform r of every update, given by the caller
+                               //      (pimqap_sweep_replay); nullptr: drawn from the Philox stream
 };
 
 // Compact per-instance result of a batch.

@@ -580,6 +580,10 @@ __device__ bool replica_epoch(const SolveDev &s, int rep, int rank, int e, const
         // front; the picks read them after their barriers (the last pick of the previous sweep
         // read its r before its final barrier)
         for (int q = tid; q < n; q += BT) {
+            if (s.replay_r) {   // a replay with the caller's uniforms
+                s_r[q] = __ldcg(s.replay_r + (size_t)sweep * n + q);
+                continue;
+            }
             uint32_t w0, w1;
             philox_2words((uint32_t)q, sweep, (uint32_t)l, (uint32_t)g, k0, k1, w0, w1);
             s_r[q] = canonical53(w0, w1);
@@ -1060,6 +1064,10 @@ __device__ bool replica_epoch_bin(const SolveDev &s, int rep, int rank, int e, c
         // front; the picks read them after their barriers (the last pick of the previous sweep
         // read its r before its final barrier)
         for (int q = tid; q < n; q += BT) {
+            if (s.replay_r) {   // a replay with the caller's uniforms
+                s_r[q] = __ldcg(s.replay_r + (size_t)sweep * n + q);
+                continue;
+            }
             uint32_t w0, w1;
             philox_2words((uint32_t)q, sweep, (uint32_t)l, (uint32_t)g, k0, k1, w0, w1);
             s_r[q] = canonical53(w0, w1);

@@ -19,6 +19,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "csrc", "libpimqap.so")
 
 OK = 0
+NOT_READY = 8
 STATUS = {0: "OK", 1: "ERR_ARG", 2: "ERR_IO", 3: "ERR_CUDA", 4: "ERR_NO_DEVICE", 5: "ERR_RANGE",
           6: "ERR_DEVICE", 7: "ERR_BUSY", 8: "ERR_NOT_READY"}
 NO_BEST = 2147483647
@@ -170,6 +171,22 @@ def lib() -> C.CDLL:
     L.pimqap_probe_smem_bandwidth.restype = st
     L.pimqap_probe_weight_exp2.argtypes = [C.c_int32, C.POINTER(C.c_float), C.POINTER(C.c_float), C.c_int64]
     L.pimqap_probe_weight_exp2.restype = st
+    L.pimqap_load_file.argtypes = [C.c_char_p, C.POINTER(Instance)]
+    L.pimqap_load_file.restype = st
+    L.pimqap_free_instance.argtypes = [C.POINTER(Instance)]
+    L.pimqap_free_instance.restype = None
+    L.pimqap_sweep_replay.argtypes = [C.POINTER(Instance), C.POINTER(Params), C.c_void_p, C.c_int32,
+                                      C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
+    L.pimqap_sweep_replay.restype = st
+    L.pimqap_batch_submit.argtypes = [C.POINTER(Instance), C.POINTER(Params), C.c_int32, C.POINTER(Result),
+                                      C.POINTER(C.c_void_p)]
+    L.pimqap_batch_submit.restype = st
+    L.pimqap_batch_poll.argtypes = [C.c_void_p]
+    L.pimqap_batch_poll.restype = st
+    L.pimqap_batch_wait.argtypes = [C.c_void_p, C.c_double]
+    L.pimqap_batch_wait.restype = st
+    L.pimqap_batch_release.argtypes = [C.c_void_p]
+    L.pimqap_batch_release.restype = None
     _lib = L
     return L
 
@@ -200,6 +217,80 @@ class _Inst:
             raise ValueError("flow and dist must be n x n")
         self.c = Instance(n, self.F.ctypes.data_as(C.POINTER(C.c_int32)),
                           self.D.ctypes.data_as(C.POINTER(C.c_int32)))
+
+
+def load_file(path: str):
+    """pimqap_load_file: (F, D) as int32 arrays, read into library-allocated memory and copied."""
+    inst = Instance()
+    _check(lib().pimqap_load_file(path.encode(), C.byref(inst)))
+    try:
+        n = inst.n
+        F = np.ctypeslib.as_array(inst.flow, shape=(n, n)).copy()
+        D = np.ctypeslib.as_array(inst.dist, shape=(n, n)).copy()
+    finally:
+        lib().pimqap_free_instance(C.byref(inst))
+    return F, D
+
+
+def sweep_replay(F: np.ndarray, D: np.ndarray, params: Params, phi: np.ndarray, r: np.ndarray) -> dict:
+    """nsweeps sweeps of one replica from phi with the uniforms r ([nsweeps, n])."""
+    inst = _Inst(F, D)
+    n = inst.F.shape[0]
+    r = np.ascontiguousarray(r, np.float64).reshape(-1, n)
+    phi = np.ascontiguousarray(phi, np.int32)
+    out_phi = np.zeros(n, np.int32)
+    force = np.zeros((n, n), np.int64)
+    E = np.zeros(1, np.int64)
+    bE = np.zeros(1, np.int64)
+    acc = np.zeros(1, np.int64)
+    _check(lib().pimqap_sweep_replay(C.byref(inst.c), C.byref(params), phi.ctypes.data, r.shape[0],
+                                     r.ctypes.data, out_phi.ctypes.data, force.ctypes.data, E.ctypes.data,
+                                     bE.ctypes.data, acc.ctypes.data))
+    return dict(phi=out_phi, I=force, E=int(E[0]), bestE=int(bE[0]), accepts=int(acc[0]))
+
+
+class Batch:
+    """pimqap_batch_submit / poll / wait / release: a batch that runs while the caller goes on."""
+
+    def __init__(self, instances: Sequence, params: Sequence[Params]):
+        self._keep = [_Inst(F, D) for F, D in instances]
+        count = len(self._keep)
+        insts = (Instance * count)(*[k.c for k in self._keep])
+        ps = (Params * count)(*params)
+        self._perms = [np.zeros(k.F.shape[0], np.int32) for k in self._keep]
+        self._energies = [np.zeros(max(1, p.groups * p.replicas), np.int64) for p in params]
+        self._rs = (Result * count)()
+        for r, p, e in zip(self._rs, self._perms, self._energies):
+            r.best_perm = p.ctypes.data_as(C.POINTER(C.c_int32))
+            r.final_energies = e.ctypes.data_as(C.POINTER(C.c_int64))
+        self._h = C.c_void_p()
+        _check(lib().pimqap_batch_submit(insts, ps, count, self._rs, C.byref(self._h)))
+
+    def poll(self) -> bool:
+        st = lib().pimqap_batch_poll(self._h)
+        if st == NOT_READY:
+            return False
+        _check(st)
+        return True
+
+    def wait(self, timeout: float = -1.0) -> Optional[List[dict]]:
+        """The results, or None when timeout (s) ran out first (< 0: no limit)."""
+        st = lib().pimqap_batch_wait(self._h, timeout)
+        if st == NOT_READY:
+            return None
+        _check(st)
+        return [_result_dict(r, p, e) for r, p, e in zip(self._rs, self._perms, self._energies)]
+
+    def close(self) -> None:
+        if self._h:
+            lib().pimqap_batch_release(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 def read_problem(path: str, max_n: int = MAX_N):

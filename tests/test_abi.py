@@ -48,6 +48,37 @@ def test_read_problem_round_trip(tmp_path):
     assert np.array_equal(F, inst.F) and np.array_equal(D, inst.D)
 
 
+def test_load_file_allocates_and_frees(tmp_path):
+    inst = instances.uniform(29, 4)
+    path = str(tmp_path / "u29.dat")
+    instances.write_instance(path, inst)
+    F, D = pimqap.load_file(path)
+    assert np.array_equal(F, inst.F) and np.array_equal(D, inst.D)
+    with pytest.raises(pimqap.PimqapError) as e:
+        pimqap.load_file(str(tmp_path / "missing.dat"))
+    assert e.value.status == 2
+    empty = pimqap.Instance()
+    pimqap.lib().pimqap_free_instance(C.byref(empty))     # freeing an empty instance is a no-op
+    assert empty.n == 0
+
+
+def test_replay_and_batch_arguments_are_checked():
+    inst = instances.uniform(6, 1)
+    p = pimqap.default_params(replicas=1, groups=1, beta_max=0.1)
+    with pytest.raises(pimqap.PimqapError) as e:             # not a permutation
+        pimqap.sweep_replay(inst.F, inst.D, p, np.array([0, 0, 1, 2, 3, 4]), np.full((1, 6), 0.5))
+    assert e.value.status == 1
+    with pytest.raises(pimqap.PimqapError) as e:             # r outside [0, 1)
+        pimqap.sweep_replay(inst.F, inst.D, p, np.arange(6), np.full((1, 6), 1.0))
+    assert e.value.status == 1
+    p.update_rule = pimqap.RULE_ONE_SHOT
+    with pytest.raises(pimqap.PimqapError):
+        pimqap.sweep_replay(inst.F, inst.D, p, np.arange(6), np.full((1, 6), 0.5))
+    h = C.c_void_p()
+    assert pimqap.lib().pimqap_batch_submit(None, None, 0, None, C.byref(h)) == 1
+    assert pimqap.lib().pimqap_batch_poll(None) == 1
+
+
 def test_read_problem_errors(tmp_path):
     with pytest.raises(pimqap.PimqapError) as e:
         pimqap.read_problem(str(tmp_path / "missing.dat"))
