@@ -136,6 +136,8 @@ typedef struct pimqap_result {
     double beta_ratio_used;     /* deltaBeta of the run */
     double admit_ms;            /* serving: submit -> admitted to the device (host clock) */
     double latency_ms;          /* serving: submit -> result available (host clock) */
+    int64_t sweeps;             /* replica-sweeps over all replicas (updates / n) */
+    int64_t proposals;          /* swap proposals, n (n - 1) / 2 per replica-sweep */
 } pimqap_result;
 
 /* ---------------------------------------------------------------- instance I/O */

@@ -292,6 +292,8 @@ pimqap_status ClassRun::finish(const std::vector<Plan> &plans, pimqap_result *re
                                   : (R.target_megaiter >= 0 ? 0.0 : -1.0);
         R.megaiters_done = o.epoch;
         R.updates = (int64_t)o.epoch * P.spe * P.n * (int64_t)P.T * P.R;
+        R.sweeps = R.updates / P.n;
+        R.proposals = R.sweeps * ((int64_t)P.n * (P.n - 1) / 2);
         R.accepts = (int64_t)o.accepts;
         R.device_ms = ms;
         R.force_bits = P.bits;

@@ -785,6 +785,8 @@ pimqap_status pimqap_solver_result(pimqap_solver *s, pimqap_result *r) {
     r->time_to_target_ms = (r->target_megaiter >= 0 && tns != ~0ull && tns >= sns) ? (double)(tns - sns) * 1e-6 : -1.0;
     r->megaiters_done = s->megaiters_done;
     r->updates = s->megaiters_done * (int64_t)s->spe * s->n * (int64_t)reps;
+    r->sweeps = r->updates / s->n;
+    r->proposals = r->sweeps * ((int64_t)s->n * (s->n - 1) / 2);
     int64_t a = 0;
     for (auto v : acc) a += (int64_t)v;
     r->accepts = a;

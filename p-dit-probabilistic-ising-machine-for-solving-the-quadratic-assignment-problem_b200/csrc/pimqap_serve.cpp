@@ -361,6 +361,8 @@ void read_result(Server &S, Request &R) {
     res.target_megaiter = (o.target_epoch == std::numeric_limits<long long>::max()) ? -1 : o.target_epoch;
     res.megaiters_done = o.epoch;
     res.updates = (int64_t)o.epoch * P.spe * P.n * (int64_t)reps;
+    res.sweeps = res.updates / P.n;
+    res.proposals = res.sweeps * ((int64_t)P.n * (P.n - 1) / 2);
     res.accepts = (int64_t)o.accepts;
     res.force_bits = P.bits;
     res.cluster_size = P.cl;

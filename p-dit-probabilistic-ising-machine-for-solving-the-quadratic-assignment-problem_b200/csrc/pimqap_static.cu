@@ -410,6 +410,8 @@ extern "C" pimqap_status pimqap_solve_static(const pimqap_instance *inst,
     result->time_to_target_ms = (result->target_megaiter >= 0 && tns != ~0ull && tns >= sns) ? (double)(tns - sns) * 1e-6 : -1.0;
     result->megaiters_done = epoch0;
     result->updates = (int64_t)epoch0 * p->sweeps_per_exchange * n * (int64_t)reps;
+    result->sweeps = result->updates / n;
+    result->proposals = result->sweeps * ((int64_t)n * (n - 1) / 2);
     result->accepts = (int64_t)sum.accepts;
     result->device_ms = std::chrono::duration<double, std::milli>(wall1 - run0).count();
     result->wall_ms = std::chrono::duration<double, std::milli>(wall1 - wall0).count();

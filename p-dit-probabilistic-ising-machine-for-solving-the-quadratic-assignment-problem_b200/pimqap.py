@@ -91,6 +91,7 @@ class Result(C.Structure):
         ("h2d_bytes", C.c_int64), ("d2h_bytes", C.c_int64),
         ("final_energies", C.POINTER(C.c_int64)), ("beta_max_used", C.c_double),
         ("beta_ratio_used", C.c_double), ("admit_ms", C.c_double), ("latency_ms", C.c_double),
+        ("sweeps", C.c_int64), ("proposals", C.c_int64),
     ]
 
 

@@ -19,7 +19,8 @@ def asym(n, seed):
 
 
 def same(a, b):
-    keys = ("best_energy", "megaiters_done", "updates", "accepts", "target_megaiter", "stopped_by")
+    keys = ("best_energy", "megaiters_done", "updates", "sweeps", "proposals", "accepts", "target_megaiter",
+            "stopped_by")
     return all(a[k] == b[k] for k in keys) and np.array_equal(a["best_perm"], b["best_perm"])
 
 

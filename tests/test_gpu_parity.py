@@ -104,6 +104,9 @@ def test_trajectory_matches_oracle(gpu, oracle, name):
     inst, st, bad, res = run_case(gpu, oracle, name)
     assert not bad, bad[:10]
     assert res["megaiters_done"] == CASES[name][6]
+    _, T, R, spe, _, _, M, _ = CASES[name]
+    assert res["sweeps"] == M * spe * T * R and res["updates"] == res["sweeps"] * inst.n
+    assert res["proposals"] == res["sweeps"] * (inst.n * (inst.n - 1) // 2)
     assert res["accepts"] == st.accepts
     assert res["best_energy"] == min(int(st.bestE.min()), st.single_best)
 

@@ -15,7 +15,8 @@ pytestmark = pytest.mark.gpu
 
 
 def same(a, b):
-    keys = ("best_energy", "megaiters_done", "updates", "accepts", "target_megaiter", "stopped_by")
+    keys = ("best_energy", "megaiters_done", "updates", "sweeps", "proposals", "accepts", "target_megaiter",
+            "stopped_by")
     return all(a[k] == b[k] for k in keys) and np.array_equal(a["best_perm"], b["best_perm"]) \
         and np.array_equal(a["final_energies"], b["final_energies"])
 
