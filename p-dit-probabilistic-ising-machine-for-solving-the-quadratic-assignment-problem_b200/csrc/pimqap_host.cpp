@@ -125,9 +125,15 @@ InstanceInfo analyse(int n, const int32_t *F, const int32_t *D) {
     info.symmetric = sym;
     info.binary_flow = true;
     info.dist16 = true;
+    info.dmin = info.dmax = D[0];
+    info.fmin = info.fmax = F[0];
     for (int k = 0; k < n * n; ++k) {
         if (F[k] != 0 && F[k] != 1) info.binary_flow = false;
         if (D[k] < -32768 || D[k] > 32767) info.dist16 = false;
+        info.dmin = std::min<int64_t>(info.dmin, D[k]);
+        info.dmax = std::max<int64_t>(info.dmax, D[k]);
+        info.fmin = std::min<int64_t>(info.fmin, F[k]);
+        info.fmax = std::max<int64_t>(info.fmax, F[k]);
     }
     if (info.binary_flow) {   // clique of unit flows on a prefix of the facilities?
         int A = 0;
@@ -321,12 +327,19 @@ pimqap_status plan_instance(const pimqap_instance *inst, const pimqap_params *pa
         // preferring the layout whose peers push the columns the proposals need
         P.lds = P.npad + 1;
         P.cl = 0;
+        // the force update on the tensor cores when fp16 holds every factor exactly (at most 2048
+        // in magnitude: 2 dD for symmetric instances, dD otherwise, and dF) and no fp32 sum can
+        // reach 2^24 (n / 2 swaps x 2 terms x |dD| |dF|)
+        const int64_t dr = info.dmax - info.dmin, fr = info.fmax - info.fmin;
+        const bool mma = (info.symmetric ? 2 * dr : dr) <= 2048 && fr <= 2048 &&
+                         (int64_t)n * dr * fr < (int64_t)1 << 24 && params->compact_instance == 0;
+        P.os_mma = mma;
         for (int cl : {1, 2, 4}) {
             if (want_cluster && cl != want_cluster) continue;
             for (int xcol = (cl > 1 ? 1 : 0); xcol >= 0 && !P.cl; --xcol)
                 for (int pc : {32, 16, 8, 4}) {
                     const size_t sm = pimqap::epoch_smem_bytes_os(n, rows_per_cta(cl), P.lds, cl, P.bits, pc,
-                                                                  P.sym, xcol != 0);
+                                                                  P.sym, xcol != 0, mma);
                     if (sm <= maxsm) {
                         P.cl = cl;
                         P.os_chunk = pc;
@@ -394,6 +407,7 @@ void carve_instance(const Plan &P, char *head, char *tail, SolveDev *out) {
     d.act = P.act;
     d.os_chunk = P.os_chunk;
     d.os_xcol = P.os_xcol;
+    d.os_mma = P.os_mma;
     d.ldg = P.npad; d.lds = P.lds; d.ldm = P.ldm; d.rpc = P.rpc;
     char *cur = head;
     d.D = carve<int32_t>(cur, nn);

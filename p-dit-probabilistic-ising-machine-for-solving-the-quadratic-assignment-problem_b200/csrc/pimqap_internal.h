@@ -84,7 +84,8 @@ struct SolveDev {
                                //      many swaps (0: sequential sweeps)
     int32_t os_xcol;           // one-shot with a cluster: peers push the force-matrix columns
                                //      the proposals need (0: the proposals read them remotely)
-    int32_t pad_os;
+    int32_t os_mma;            // one-shot: the force update on the tensor cores (exact for this
+                               //      instance: small factors, sums below 2^24)
     const double *replay_r;    // [sweeps][n] the uniform r of every update, given by the caller
                                //      (pimqap_sweep_replay); nullptr: drawn from the Philox stream
 };
@@ -187,7 +188,8 @@ size_t epoch_smem_bytes(int n, int rpc, int lds, int cluster, int bits);
 // Shared memory of the binary-flow epoch kernel (0 / 1 flows and int16 distances resident).
 size_t epoch_smem_bytes_bin(int n, int rpc, int lds, int cluster);
 // Shared memory of the one-shot epoch kernel (force update in chunks of `chunk` swaps).
-size_t epoch_smem_bytes_os(int n, int rpc, int lds, int cluster, int bits, int chunk, bool sym, bool xcol);
+size_t epoch_smem_bytes_os(int n, int rpc, int lds, int cluster, int bits, int chunk, bool sym, bool xcol,
+                           bool mma);
 
 // One-time kernel attributes (dynamic shared memory, non-portable cluster size).
 cudaError_t prepare_kernels();

@@ -22,6 +22,7 @@
 //      cluster barrier publishes the new rows.
 // Rejected updates cost one barrier; double-buffered delta / maxima slots make that safe.
 #include <cooperative_groups.h>
+#include <cuda_fp16.h>
 #include <cuda_runtime.h>
 
 #include <cstdint>
@@ -1373,6 +1374,12 @@ __device__ bool replica_epoch_bin(const SolveDev &s, int rep, int rank, int e, c
 
 // ------------------------------------------------------------------ the one-shot epoch
 
+// The tensor-core force update of the one-shot epoch stages 64 factor columns at a time, as
+// fp16 rows of kMmaLd halves (144 bytes: the 8 rows and 4 column pairs one fragment load
+// touches fall in 32 different banks).
+constexpr int kMmaK = 64;
+constexpr int kMmaLd = 72;
+
 // Shared-memory layout of the one-shot epoch (replica_epoch_os).
 //   I       rpc rows of the force matrix; odd row stride lds, so 32 lanes reading one column
 //           of 32 rows hit 32 banks
@@ -1396,7 +1403,8 @@ __device__ bool replica_epoch_bin(const SolveDev &s, int rep, int rank, int e, c
 struct OsLayout {
     size_t I, phi, inv, bphi, Dd, Fd, diag, tgt, dlt, own, pair, uni, T, U, V, U2, V2, part, misc, total;
     int tld;   // row stride of T (elements)
-    __host__ __device__ OsLayout(int n, int rpc, int lds, int cluster, int isz, int pc, bool sym, bool xcol) {
+    __host__ __device__ OsLayout(int n, int rpc, int lds, int cluster, int isz, int pc, bool sym, bool xcol,
+                                 bool mma = false) {
         const size_t npad = (size_t)((n + 3) & ~3), rp = (size_t)rpc, vld = 256;
         size_t o = 0;
         I = o;    o = align16(o + rp * lds * isz);
@@ -1418,7 +1426,11 @@ struct OsLayout {
         V = align16(U + (size_t)pc * rp * isz);
         U2 = align16(V + (size_t)pc * vld * isz);
         V2 = align16(U2 + (sym ? 0 : (size_t)pc * rp * isz));
-        const size_t fend = align16(V2 + (sym ? 0 : (size_t)pc * vld * isz));
+        size_t fend = align16(V2 + (sym ? 0 : (size_t)pc * vld * isz));
+        if (mma) {   // the tensor-core factors (fp16) share the same space
+            const size_t mend = align16(U + (size_t)((rpc + 15) & ~15) * kMmaLd * 2 + (size_t)((n + 7) & ~7) * kMmaLd * 2);
+            fend = mend > fend ? mend : fend;
+        }
         o = align16(fend > o + tbytes ? fend : o + tbytes);
         part = o; o = align16(o + (size_t)(cluster + kMaxWarpsOs) * 8);
         misc = o; o = align16(o + (kMaxWarpsOs + 8) * sizeof(int));
@@ -1426,8 +1438,18 @@ struct OsLayout {
     }
 };
 
-size_t epoch_smem_bytes_os(int n, int rpc, int lds, int cluster, int bits, int chunk, bool sym, bool xcol) {
-    return OsLayout(n, rpc, lds, cluster, bits / 8, chunk, sym, xcol).total;
+size_t epoch_smem_bytes_os(int n, int rpc, int lds, int cluster, int bits, int chunk, bool sym, bool xcol,
+                           bool mma) {
+    return OsLayout(n, rpc, lds, cluster, bits / 8, chunk, sym, xcol, mma).total;
+}
+
+// One m16n8k16 tensor-core product with fp16 inputs and fp32 accumulation: d += a b.
+__device__ __forceinline__ void mma_16816(float d[4], const uint32_t a[4], const uint32_t b[2]) {
+    asm volatile(
+        "mma.sync.aligned.m16n8k16.row.col.f32.f16.f16.f32 {%0, %1, %2, %3}, {%4, %5, %6, %7}, "
+        "{%8, %9}, {%0, %1, %2, %3};"
+        : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
+        : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b[0]), "r"(b[1]));
 }
 
 // Loads of this CTA's shared memory by 32-bit shared address.
@@ -1551,7 +1573,8 @@ __device__ bool replica_epoch_os(const SolveDev &s, int rep, int rank, int e, co
     const int npad = (n + 3) & ~3, vld = 256;           // V rows: every lane's 8 columns
     const int K = (n + 31) >> 5;                             // partners per lane (<= 8)
     const bool xcol = CL > 1 && s.os_xcol != 0;
-    const OsLayout L(n, rpc, lds, CL, (int)sizeof(IT), pc, SYM, xcol);
+    const bool mma = s.os_mma != 0;
+    const OsLayout L(n, rpc, lds, CL, (int)sizeof(IT), pc, SYM, xcol, mma);
     const int tld = L.tld;
     IT *sI = reinterpret_cast<IT *>(smem + L.I);
     int32_t *s_phi = reinterpret_cast<int32_t *>(smem + L.phi);
@@ -1813,67 +1836,178 @@ __device__ bool replica_epoch_os(const SolveDev &s, int rep, int rank, int e, co
                 s_inv[b] = i;
             }
 
-            // ---- 3. force update of this CTA's rows (qap.cu:1337-1412), chunks of pc swaps
-            for (int c0 = 0; c0 < np; c0 += pc) {
-                const int cn = min(pc, np - c0);
-                // the chunk's factors from 16-byte row pieces of D^T, D, F^T, F, several pieces
-                // per thread in flight (rows are zero padded to ldm >= cl * rpc, npad)
-                constexpr int UNR = SYM ? 4 : 2;   // 512 threads: 128 registers each
-                stage_factors<IT, SYM, SYM, UNR>(tid, BT, cn, rpc / 4, s.DT + row0, s.D + row0, ldm, s_pi + c0, s_pj + c0,
-                                       s_U, s_U2, rpc);
-                stage_factors<IT, SYM, false, UNR>(tid, BT, cn, npad / 4, s.FT, s.F, ldm, s_pa + c0, s_pb + c0, s_V, s_V2,
-                                       vld);
-                for (int idx = tid; idx < cn * (vld - npad); idx += BT) {   // columns npad..vld-1
-                    const int p = idx / (vld - npad), c = npad + idx - p * (vld - npad);
-                    s_V[p * vld + c] = 0;
-                    if constexpr (!SYM) s_V2[p * vld + c] = 0;
+            // ---- 3. force update of this CTA's rows (qap.cu:1337-1412)
+            if (mma) {
+                // dI = U^T V on the tensor cores (m16n8k16, fp16 in, fp32 sums): the factors are
+                // integers of at most 2048 in magnitude and every sum stays below 2^24 (the host
+                // checks both), so the products and sums are exact; added to the rows once
+                __half *hU = reinterpret_cast<__half *>(smem + L.U);
+                const int rb16 = (rpc + 15) & ~15, nc8 = (n + 7) & ~7;
+                __half *hV = hU + (size_t)rb16 * kMmaLd;
+                const int kpp = SYM ? 1 : 2;                 // factor columns per swap
+                const int spc = kMmaK / kpp;                 // swaps per staged chunk
+                const int nrb = (rows + 15) >> 4, nct = (n + 7) >> 3;
+                const int ngroups = nrb * ((nct + 7) >> 3);  // 16 x 64 output blocks
+                const int g8 = lane >> 2, t4 = lane & 3;
+                // chunk by chunk: stage the factors once, then every warp runs its 16 x 64 output
+                // blocks and adds each block's sums (below 2^24, exact) to the rows
+                for (int c0 = 0; c0 < np; c0 += spc) {
+                    const int cn = min(spc, np - c0), kc = cn * kpp;
+                    // U[k][col]: 2 (D[k][j] - D[k][i]) (symmetric) or D[k][j] - D[k][i] and
+                    // D[j][k] - D[i][k]; V[c][col]: F[c][b] - F[c][a] (and F[b][c] - F[a][c])
+                    // consecutive threads take consecutive swaps of one row group, so their
+                    // 2-byte stores into a factor row are conflict-free
+#pragma unroll 2
+                    for (int idx = tid; idx < cn * (rpc >> 2); idx += BT) {
+                        const int q4 = idx / cn, p = idx - q4 * cn;
+                        const int i = s_pi[c0 + p], j = s_pj[c0 + p];
+                        const int4 hi = __ldg(reinterpret_cast<const int4 *>(s.DT + (size_t)j * ldm + row0) + q4);
+                        const int4 lo = __ldg(reinterpret_cast<const int4 *>(s.DT + (size_t)i * ldm + row0) + q4);
+                        const int h4[4] = {hi.x - lo.x, hi.y - lo.y, hi.z - lo.z, hi.w - lo.w};
+#pragma unroll
+                        for (int r = 0; r < 4; ++r)
+                            hU[(size_t)(4 * q4 + r) * kMmaLd + p * kpp] = __int2half_rn(SYM ? 2 * h4[r] : h4[r]);
+                        if constexpr (!SYM) {
+                            const int4 hi2 = __ldg(reinterpret_cast<const int4 *>(s.D + (size_t)j * ldm + row0) + q4);
+                            const int4 lo2 = __ldg(reinterpret_cast<const int4 *>(s.D + (size_t)i * ldm + row0) + q4);
+                            const int d4[4] = {hi2.x - lo2.x, hi2.y - lo2.y, hi2.z - lo2.z, hi2.w - lo2.w};
+#pragma unroll
+                            for (int r = 0; r < 4; ++r)
+                                hU[(size_t)(4 * q4 + r) * kMmaLd + p * kpp + 1] = __int2half_rn(d4[r]);
+                        }
+                    }
+#pragma unroll 2
+                    for (int idx = tid; idx < cn * (npad >> 2); idx += BT) {
+                        const int q4 = idx / cn, p = idx - q4 * cn;
+                        const int a = s_pa[c0 + p], b = s_pb[c0 + p];
+                        const int4 hi = __ldg(reinterpret_cast<const int4 *>(s.FT + (size_t)b * ldm) + q4);
+                        const int4 lo = __ldg(reinterpret_cast<const int4 *>(s.FT + (size_t)a * ldm) + q4);
+                        const int h4[4] = {hi.x - lo.x, hi.y - lo.y, hi.z - lo.z, hi.w - lo.w};
+#pragma unroll
+                        for (int r = 0; r < 4; ++r) hV[(size_t)(4 * q4 + r) * kMmaLd + p * kpp] = __int2half_rn(h4[r]);
+                        if constexpr (!SYM) {
+                            const int4 hi2 = __ldg(reinterpret_cast<const int4 *>(s.F + (size_t)b * ldm) + q4);
+                            const int4 lo2 = __ldg(reinterpret_cast<const int4 *>(s.F + (size_t)a * ldm) + q4);
+                            const int d4[4] = {hi2.x - lo2.x, hi2.y - lo2.y, hi2.z - lo2.z, hi2.w - lo2.w};
+#pragma unroll
+                            for (int r = 0; r < 4; ++r) hV[(size_t)(4 * q4 + r) * kMmaLd + p * kpp + 1] = __int2half_rn(d4[r]);
+                        }
+                    }
+                    // zeros in the factor columns kc..(kc rounded up to 16)-1 that the last
+                    // k-step reads (the space held other data); padded rows and columns
+                    // only reach output entries that are never written back
+                    const int kz = ((kc + 15) & ~15) - kc;
+                    for (int idx = tid; idx < (rpc + npad) * kz; idx += BT) {
+                        const int row = idx / kz, kk = kc + idx - row * kz;
+                        if (row < rpc) hU[(size_t)row * kMmaLd + kk] = __int2half_rn(0);
+                        else hV[(size_t)(row - rpc) * kMmaLd + kk] = __int2half_rn(0);
+                    }
+                    G.sync();
+                    for (int blk = warp; blk < ngroups; blk += nwarps) {
+                        const int rb = blk % nrb, cg = blk / nrb;
+                        float acc[8][4];
+#pragma unroll
+                        for (int t8 = 0; t8 < 8; ++t8)
+#pragma unroll
+                            for (int q = 0; q < 4; ++q) acc[t8][q] = 0.0f;
+                        for (int ks = 0; ks * 16 < kc; ++ks) {
+                            const __half *ar = hU + (size_t)(rb * 16 + g8) * kMmaLd + ks * 16 + 2 * t4;
+                            uint32_t af[4];
+                            af[0] = *reinterpret_cast<const uint32_t *>(ar);
+                            af[1] = *reinterpret_cast<const uint32_t *>(ar + 8 * kMmaLd);
+                            af[2] = *reinterpret_cast<const uint32_t *>(ar + 8);
+                            af[3] = *reinterpret_cast<const uint32_t *>(ar + 8 * kMmaLd + 8);
+#pragma unroll
+                            for (int t8 = 0; t8 < 8; ++t8) {
+                                const int ct = cg * 8 + t8;
+                                if (ct < nct) {
+                                    const __half *br = hV + (size_t)(ct * 8 + g8) * kMmaLd + ks * 16 + 2 * t4;
+                                    uint32_t bf[2];
+                                    bf[0] = *reinterpret_cast<const uint32_t *>(br);
+                                    bf[1] = *reinterpret_cast<const uint32_t *>(br + 8);
+                                    mma_16816(acc[t8], af, bf);
+                                }
+                            }
+                        }
+#pragma unroll
+                        for (int t8 = 0; t8 < 8; ++t8) {
+                            const int c = (cg * 8 + t8) * 8 + 2 * t4;
+#pragma unroll
+                            for (int q = 0; q < 4; ++q) {
+                                const int r = rb * 16 + g8 + (q >> 1) * 8, cc = c + (q & 1);
+                                if (r < rows && cc < n) {
+                                    IT *dst = sI + (size_t)r * lds + cc;
+                                    *dst = (IT)((U)*dst + (U)(IT)(long long)acc[t8][q]);
+                                }
+                            }
+                        }
+                    }
+                    G.sync();                                // before the next chunk is staged
                 }
                 G.sync();
-                for (int kq = warp * RT; kq < rows; kq += nwarps * RT) {
-                    U acc[RT][8];
+            } else {
+                for (int c0 = 0; c0 < np; c0 += pc) {
+                    const int cn = min(pc, np - c0);
+                    // the chunk's factors from 16-byte row pieces of D^T, D, F^T, F, several pieces
+                    // per thread in flight (rows are zero padded to ldm >= cl * rpc, npad)
+                    constexpr int UNR = SYM ? 4 : 2;   // 512 threads: 128 registers each
+                    stage_factors<IT, SYM, SYM, UNR>(tid, BT, cn, rpc / 4, s.DT + row0, s.D + row0, ldm, s_pi + c0, s_pj + c0,
+                                           s_U, s_U2, rpc);
+                    stage_factors<IT, SYM, false, UNR>(tid, BT, cn, npad / 4, s.FT, s.F, ldm, s_pa + c0, s_pb + c0, s_V, s_V2,
+                                           vld);
+                    for (int idx = tid; idx < cn * (vld - npad); idx += BT) {   // columns npad..vld-1
+                        const int p = idx / (vld - npad), c = npad + idx - p * (vld - npad);
+                        s_V[p * vld + c] = 0;
+                        if constexpr (!SYM) s_V2[p * vld + c] = 0;
+                    }
+                    G.sync();
+                    for (int kq = warp * RT; kq < rows; kq += nwarps * RT) {
+                        U acc[RT][8];
 #pragma unroll
-                    for (int r = 0; r < RT; ++r)
+                        for (int r = 0; r < RT; ++r)
 #pragma unroll
-                        for (int q = 0; q < 8; ++q) {
-                            const int c = lane + 32 * q;
-                            acc[r][q] = (q < K && c < n && kq + r < rows) ? (U)sI[(size_t)(kq + r) * lds + c] : (U)0;
-                        }
-                    {   // U / V rows are padded (rpc, 256 entries), so no load needs a guard
-                        const uint32_t ua = smem_u32(s_U) + (uint32_t)(kq * sizeof(IT));
-                        const uint32_t va = smem_u32(s_V) + (uint32_t)(lane * sizeof(IT));
-                        const uint32_t ua2 = smem_u32(s_U2) + (uint32_t)(kq * sizeof(IT));
-                        const uint32_t va2 = smem_u32(s_V2) + (uint32_t)(lane * sizeof(IT));
-                        for (int p = 0; p < cn; ++p) {
-                            U uu[RT], vv[8];
+                            for (int q = 0; q < 8; ++q) {
+                                const int c = lane + 32 * q;
+                                acc[r][q] = (q < K && c < n && kq + r < rows) ? (U)sI[(size_t)(kq + r) * lds + c] : (U)0;
+                            }
+                        {   // U / V rows are padded (rpc, 256 entries), so no load needs a guard
+                            const uint32_t ua = smem_u32(s_U) + (uint32_t)(kq * sizeof(IT));
+                            const uint32_t va = smem_u32(s_V) + (uint32_t)(lane * sizeof(IT));
+                            const uint32_t ua2 = smem_u32(s_U2) + (uint32_t)(kq * sizeof(IT));
+                            const uint32_t va2 = smem_u32(s_V2) + (uint32_t)(lane * sizeof(IT));
+                            for (int p = 0; p < cn; ++p) {
+                                U uu[RT], vv[8];
 #pragma unroll
-                            for (int r = 0; r < RT; ++r) uu[r] = (U)lds_it<IT>(ua + (uint32_t)((p * rpc + r) * sizeof(IT)));
+                                for (int r = 0; r < RT; ++r) uu[r] = (U)lds_it<IT>(ua + (uint32_t)((p * rpc + r) * sizeof(IT)));
 #pragma unroll
-                            for (int q = 0; q < 8; ++q) vv[q] = (U)lds_it<IT>(va + (uint32_t)((p * 256 + 32 * q) * sizeof(IT)));
-#pragma unroll
-                            for (int r = 0; r < RT; ++r)
-#pragma unroll
-                                for (int q = 0; q < 8; ++q) acc[r][q] += uu[r] * vv[q];
-                            if constexpr (!SYM) {
-#pragma unroll
-                                for (int r = 0; r < RT; ++r) uu[r] = (U)lds_it<IT>(ua2 + (uint32_t)((p * rpc + r) * sizeof(IT)));
-#pragma unroll
-                                for (int q = 0; q < 8; ++q) vv[q] = (U)lds_it<IT>(va2 + (uint32_t)((p * 256 + 32 * q) * sizeof(IT)));
+                                for (int q = 0; q < 8; ++q) vv[q] = (U)lds_it<IT>(va + (uint32_t)((p * 256 + 32 * q) * sizeof(IT)));
 #pragma unroll
                                 for (int r = 0; r < RT; ++r)
 #pragma unroll
                                     for (int q = 0; q < 8; ++q) acc[r][q] += uu[r] * vv[q];
+                                if constexpr (!SYM) {
+#pragma unroll
+                                    for (int r = 0; r < RT; ++r) uu[r] = (U)lds_it<IT>(ua2 + (uint32_t)((p * rpc + r) * sizeof(IT)));
+#pragma unroll
+                                    for (int q = 0; q < 8; ++q) vv[q] = (U)lds_it<IT>(va2 + (uint32_t)((p * 256 + 32 * q) * sizeof(IT)));
+#pragma unroll
+                                    for (int r = 0; r < RT; ++r)
+#pragma unroll
+                                        for (int q = 0; q < 8; ++q) acc[r][q] += uu[r] * vv[q];
+                                }
                             }
                         }
+#pragma unroll
+                        for (int r = 0; r < RT; ++r)
+#pragma unroll
+                            for (int q = 0; q < 8; ++q) {
+                                const int c = lane + 32 * q;
+                                if (q < K && c < n && kq + r < rows) sI[(size_t)(kq + r) * lds + c] = (IT)acc[r][q];
+                            }
                     }
-#pragma unroll
-                    for (int r = 0; r < RT; ++r)
-#pragma unroll
-                        for (int q = 0; q < 8; ++q) {
-                            const int c = lane + 32 * q;
-                            if (q < K && c < n && kq + r < rows) sI[(size_t)(kq + r) * lds + c] = (IT)acc[r][q];
-                        }
+                    G.sync();
                 }
-                G.sync();
+
             }
 
             // ---- 4. new diagonal and energy (qap.cu:1420-1458): E = -1/2 sum_k I[k][phi(k)]

@@ -55,6 +55,7 @@ struct Plan {
     int act = 0;           // clique-flow moves with facilities 0..act-1 active (0 = off)
     int os_chunk = 0;      // > 0: the one-shot rule (swaps per force-update chunk)
     int os_xcol = 0;       // one-shot: peers push the force-matrix columns of the proposals
+    int os_mma = 0;        // one-shot: force update on the tensor cores
     size_t head = 0, tail = 0, total = 0;
     int64_t h2d_bytes = 0;
 };
@@ -67,6 +68,7 @@ struct InstanceInfo {
     bool binary_flow = false;   // every flow is 0 or 1
     bool dist16 = false;        // every distance fits in int16
     int clique = 0;             // A > 0: F[a][b] = 1 exactly for a != b < A, and diag(D) = 0
+    int64_t dmin = 0, dmax = 0, fmin = 0, fmax = 0;   // value ranges of D and F
 };
 InstanceInfo analyse(int n, const int32_t *F, const int32_t *D);
 
