@@ -57,6 +57,7 @@ LADDER_HEAVY = (2.0 ** -13, 1.0787607977571199)     # heavy-tailed n = 180, 64 r
 METRIC = "swap proposals/sec"
 UNIT = "proposals/s"
 L2_FLUSH_BYTES = 256 << 20
+E2E_SOLVES = 3                  # end-to-end solves timed; the median wall is reported
 
 
 def proposals(replicas: int, sweeps: int, n: int = N) -> float:
@@ -269,10 +270,16 @@ def run_ours(args):
     pw = pimqap.Params.from_buffer_copy(p2)
     pw.max_megaiters = 1
     pimqap.solve(Fp.numpy(), Dp.numpy(), pw)
-    barrier()
-    e0 = time.perf_counter()
-    res = pimqap.solve(Fp.numpy(), Dp.numpy(), p2)
-    e_wall = time.perf_counter() - e0
+    # three timed solves, the median wall reported (a single solve of under a second saw the
+    # host's scheduling noise: 0.70 to 1.48 s for the same device time)
+    e_runs = []
+    for _ in range(E2E_SOLVES):
+        barrier()
+        e0 = time.perf_counter()
+        res = pimqap.solve(Fp.numpy(), Dp.numpy(), p2)
+        e_runs.append((time.perf_counter() - e0, res))
+    e_walls = [w for w, _ in e_runs]
+    e_wall, res = sorted(e_runs, key=lambda x: x[0])[len(e_runs) // 2]
     e2e_sweeps = args.steps * MEGAITERS_PER_STEP * SWEEPS_PER_EXCHANGE
     e2e_value = whole_job_rate(proposals(REPLICAS * GROUPS, e2e_sweeps), world,
                                max_over_ranks(e_wall, world, f"cuda:{local}"))
@@ -355,7 +362,9 @@ def run_ours(args):
                          "bytes_model": bytes_model},
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": res["h2d_bytes"],
                     "d2h_bytes_per_step": res["d2h_bytes"], "wall_s": e_wall,
-                    "note": "one step = one pimqap_solve of the whole workload (upload, set-up, sweeps, result)"},
+                    "wall_s_each": e_walls, "library_wall_ms": res["wall_ms"], "device_ms": res["device_ms"],
+                    "note": f"one step = one pimqap_solve of the whole workload (upload, set-up, sweeps, "
+                            f"result); median wall of {E2E_SOLVES} solves"},
             "clocks": clocks.summary(),
             "cpu_baseline": cpu,
         }
