@@ -148,14 +148,35 @@ def ref_cpu_throughput(F, D, budget_s: float, replicas: int = REPLICAS):
     return val, cores, "reference", sample
 
 
+def workload_config(workload, update_rule, world):
+    """The workload part of the line's config, the same in both arms."""
+    return {"workload": ("grid256: n=256 Bernoulli(0.36) flow, 16x16 grid sq. distance + U[0,3]; "
+                         if workload == "grid256" else
+                         "clique92: n=256, unit flows among facilities 0..91, 16x16 grid sq. "
+                         "distance + U[0,3]; the tai256c program's moves; ") +
+                        "64 replicas, geometric beta ladder, exchange every 4 sweeps, "
+                        "10^4 sweeps = 100 steps" +
+                        ("; GPU-CUPIM's one-shot rule (a sweep = one parallel step)"
+                         if update_rule == "one-shot" else ""),
+            "update_rule": update_rule,
+            "n": N, "replicas": REPLICAS * GROUPS, "sweeps_per_step": MEGAITERS_PER_STEP * SWEEPS_PER_EXCHANGE,
+            "beta0_internal": BETA_MAX, "beta_ratio": BETA_RATIO,
+            "ladder": "reference automatic mode on this instance (pimqap_auto_beta, seed 1), then fixed",
+            "parallelism": f"instances x{world}"}
+
+
 def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     from oracle import RefHarness, ref_available
-    cfg = {"workload": "grid256 n=256, 64 replicas, exchange every 4 sweeps", "n": N,
-           "replicas": REPLICAS, "sweeps_per_exchange": SWEEPS_PER_EXCHANGE}
+    if args.workload != "grid256" or args.update_rule != "sequential":
+        print(json.dumps({"impl": "reference", "unavailable": "the reference arm times the grid256 workload "
+                                                              "with the sequential rule (CPU_PIM.cpp) only"}))
+        return
+    cfg = dict(workload_config(args.workload, args.update_rule, 1),
+               parallelism="host threads (the reference's CPU program; no GPU)")
     if not ref_available("big_mt"):
         print(json.dumps({"impl": "reference", "unavailable": "reference CPU_PIM.cpp not built (oracle/_ref missing)"}))
         return
@@ -177,12 +198,13 @@ def run_reference(args):
     val = proposals(cores * REPLICAS, sweeps) / total
     sample = (f"each step {m} mega-iterations (4 sweeps each) of {cores} groups x {REPLICAS} replicas "
               f"of the n=256 instance; one group per host thread")
-    line = {"impl": "reference", "metric": METRIC, "value": val, "unit": UNIT, "n_gpus": 0,
+    line = {"impl": "reference", "metric": METRIC, "value": val, "unit": UNIT, "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * total / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int32",
             "data": "synthetic (seeded grid256 instance)", "config": cfg,
             "cpu_baseline": {"value": val, "unit": UNIT, "cores": cores, "kind": "reference", "sample": sample},
-            "e2e": {"value": val, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+            "e2e": {"value": val, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+            "note": "the reference's CPU program on this host's cores; no GPU is used at any n_gpus"}
     print(json.dumps(line))
 
 
@@ -333,21 +355,9 @@ def run_ours(args):
             "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": f"int{8 * s}",
             "data": "synthetic (seeded grid256 instance per GPU)",
-            "config": {"workload": ("grid256: n=256 Bernoulli(0.36) flow, 16x16 grid sq. distance + U[0,3]; "
-                                    if args.workload == "grid256" else
-                                    "clique92: n=256, unit flows among facilities 0..91, 16x16 grid sq. "
-                                    "distance + U[0,3]; the tai256c program's moves; ") +
-                                   "64 replicas, geometric beta ladder, exchange every 4 sweeps, "
-                                   "10^4 sweeps = 100 steps" +
-                                   ("; GPU-CUPIM's one-shot rule (a sweep = one parallel step)"
-                                    if rule else ""),
-                       "update_rule": args.update_rule,
-                       "n": N, "replicas": reps, "sweeps_per_step": MEGAITERS_PER_STEP * SWEEPS_PER_EXCHANGE,
-                       "beta0_internal": BETA_MAX, "beta_ratio": BETA_RATIO,
-                       "ladder": "reference automatic mode on this instance (pimqap_auto_beta, seed 1), then fixed",
-                       "parallelism": f"instances x{world}",
-                       "cluster_size": r1["cluster_size"], "force_bits": r1["force_bits"],
-                       "l2": "flushed between steps (256 MiB write)"},
+            "config": dict(workload_config(args.workload, args.update_rule, world),
+                           cluster_size=r1["cluster_size"], force_bits=r1["force_bits"],
+                           l2="flushed between steps (256 MiB write)"),
             "candidate_deltas_per_s": cand * world / (ms_max * 1e-3),
             "accept_rate": accepts / (reps * sweeps * N),
             "best_energy": r1["best_energy"],
