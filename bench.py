@@ -373,6 +373,8 @@ def run_ours(args):
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": res["h2d_bytes"],
                     "d2h_bytes_per_step": res["d2h_bytes"], "wall_s": e_wall,
                     "wall_s_each": e_walls, "library_wall_ms": res["wall_ms"], "device_ms": res["device_ms"],
+                    "library_wall_ms_each": [r["wall_ms"] for _, r in e_runs],
+                    "device_ms_each": [r["device_ms"] for _, r in e_runs],
                     "note": f"one step = one pimqap_solve of the whole workload (upload, set-up, sweeps, "
                             f"result); median wall of {E2E_SOLVES} solves"},
             "clocks": clocks.summary(),
