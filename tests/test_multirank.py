@@ -58,3 +58,31 @@ def test_reference_arm_prints_only_on_rank_zero():
     r = subprocess.run([sys.executable, os.path.join(ROOT, "bench.py"), "--impl", "reference", "--gpus", "2",
                         "--steps", "3", "--warmup", "3"], capture_output=True, text=True, env=env, timeout=120)
     assert r.returncode == 0 and r.stdout.strip() == ""
+
+
+def test_reference_arm_names_the_solver_arms_workload():
+    """Rank 0 times the reference's CPU program on the workload the solver's arm names (the same
+    config keys but the parallelism), and reports what it cannot time instead of timing
+    something else."""
+    import json
+    sys.path.insert(0, ROOT)
+    import bench
+    env = dict(os.environ, RANK="0", WORLD_SIZE="1", LOCAL_RANK="0")
+    r = subprocess.run([sys.executable, os.path.join(ROOT, "bench.py"), "--impl", "reference",
+                        "--update-rule", "one-shot", "--steps", "3", "--warmup", "3"],
+                       capture_output=True, text=True, env=env, timeout=120)
+    assert r.returncode == 0
+    line = json.loads(r.stdout.strip().splitlines()[-1])
+    assert line["impl"] == "reference" and "unavailable" in line
+    r = subprocess.run([sys.executable, os.path.join(ROOT, "bench.py"), "--impl", "reference",
+                        "--steps", "1", "--warmup", "3"], capture_output=True, text=True, env=env, timeout=300)
+    assert r.returncode == 0
+    line = json.loads(r.stdout.strip().splitlines()[-1])
+    if "unavailable" in line:                         # oracle/_ref not built here
+        return
+    want = bench.workload_config("grid256", "sequential", 1)
+    got = dict(line["config"])
+    assert got.pop("parallelism") != want.pop("parallelism")
+    assert got == want
+    assert line["metric"] == bench.METRIC and line["unit"] == bench.UNIT and line["higher_is_better"]
+    assert line["e2e"]["value"] == line["value"] == line["cpu_baseline"]["value"] > 0
