@@ -16,6 +16,7 @@
 #include <fstream>
 #include <limits>
 #include <memory>
+#include <mutex>
 #include <random>
 #include <string>
 #include <vector>
@@ -209,6 +210,63 @@ int round_up(int x, int m) { return (x + m - 1) / m * m; }
 
 using namespace pimqap::detail;
 
+// ------------------------------------------------------------------ device block reuse
+
+namespace {
+
+// A finished handle's device block (up to kKeepBytes) is kept for the next handle on the same
+// device, so back-to-back solves make no cudaMalloc / cudaFree: both take the driver's
+// allocation locks and cudaFree waits for the whole device, which on a busy host has cost up
+// to 0.6 s in a solve of 0.36 s.  One block per device; larger blocks are freed as before.
+// Every byte of a block is rewritten by the next solve's set-up (head uploaded, tail cleared).
+constexpr size_t kKeepBytes = 256ull << 20;
+constexpr int kKeepDevices = 64;
+struct KeptBlock {
+    void *p = nullptr;
+    size_t bytes = 0;
+};
+std::mutex g_keep_mu;
+KeptBlock g_keep[kKeepDevices];
+
+// A block of at least `bytes` on the current device (`device`): the kept one when it is big
+// enough, else a new allocation.  *got is the block's real size.
+cudaError_t block_acquire(int device, size_t bytes, void **p, size_t *got) {
+    if (device >= 0 && device < kKeepDevices) {
+        std::lock_guard<std::mutex> lk(g_keep_mu);
+        KeptBlock &k = g_keep[device];
+        if (k.p && k.bytes >= bytes) {
+            *p = k.p;
+            *got = k.bytes;
+            k = KeptBlock{};
+            return cudaSuccess;
+        }
+    }
+    *got = bytes;
+    return cudaMalloc(p, bytes);
+}
+
+// Returns a block no work is pending on: kept when it is small enough and larger than the
+// block kept now (which is freed instead), else freed.
+void block_release(int device, void *p, size_t bytes) {
+    if (!p) return;
+    if (bytes <= kKeepBytes && device >= 0 && device < kKeepDevices) {
+        void *drop = p;
+        {
+            std::lock_guard<std::mutex> lk(g_keep_mu);
+            KeptBlock &k = g_keep[device];
+            if (!k.p || k.bytes < bytes) {
+                drop = k.p;
+                k = KeptBlock{p, bytes};
+            }
+        }
+        if (drop) cudaFree(drop);
+        return;
+    }
+    cudaFree(p);
+}
+
+}  // namespace
+
 // ------------------------------------------------------------------ solver object
 
 struct pimqap_solver {
@@ -238,8 +296,11 @@ struct pimqap_solver {
         if (graph) cudaGraphExecDestroy(graph);
         if (ev0) cudaEventDestroy(ev0);
         if (ev1) cudaEventDestroy(ev1);
-        if (stream) cudaStreamDestroy(stream);
-        if (dmem) cudaFree(dmem);
+        if (stream) {
+            cudaStreamSynchronize(stream);   // nothing in flight on the block it gives back
+            cudaStreamDestroy(stream);
+        }
+        block_release(device, dmem, dbytes);
     }
 };
 
@@ -666,8 +727,7 @@ pimqap_status pimqap_solver_create(const pimqap_instance *inst, const pimqap_par
     s->cl = plan.cl;
     s->threads = plan.threads;
     s->smem = plan.bin ? plan.smem_bin : plan.smem;
-    PQ_CUDA(cudaMalloc(&s->dmem, plan.total));
-    s->dbytes = plan.total;
+    PQ_CUDA(block_acquire(s->device, plan.total, &s->dmem, &s->dbytes));
     PQ_CUDA(cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking));
     PQ_CUDA(cudaEventCreate(&s->ev0));
     PQ_CUDA(cudaEventCreate(&s->ev1));
