@@ -11,7 +11,9 @@
  *   - Every function returns a pimqap_status (0 = OK).  No exception crosses the ABI.
  *     pimqap_last_error() gives the message of the calling thread's last failure.
  *   - All pointers are caller-owned host memory unless stated otherwise; the solver copies
- *     what it needs.  Device memory is owned by the solver / server handles.
+ *     what it needs.  Device memory is owned by the solver / server handles.  A destroyed
+ *     solver handle's device block of up to 256 MiB is kept (one per GPU, until the process
+ *     exits) for the next handle on that GPU, so repeated solves skip cudaMalloc / cudaFree.
  *   - A solver handle is used by one host thread at a time.  A server handle is locked
  *     internally and may be used from several threads.
  *   - Energies and costs are exact int64.  The force matrix is int32 when a bound computed
