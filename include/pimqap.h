@@ -247,6 +247,13 @@ pimqap_status pimqap_solver_event_perm(pimqap_solver *s, int32_t perm_index, int
 
 void pimqap_solver_destroy(pimqap_solver *s);
 
+/* No counterpart in the reference (its memory is static arrays).  Frees the device blocks that
+   destroyed solver handles left for reuse (one per GPU, up to 256 MiB each).  Call it before
+   cudaDeviceReset or before handing the memory to other code; the next solve allocates anew.
+   Returns the first cudaFree error as PIMQAP_ERR_CUDA; with nothing kept it makes no CUDA
+   call. */
+pimqap_status pimqap_release_kept_memory(void);
+
 /* Parity tool: nsweeps sweeps of ONE replica (doMegaItera, CPU_PIM.cpp:195-290, with NUMITERA
    sweeps and no exchange partner) from the caller's permutation phi_in (facility at each
    location), at beta = params->beta_max (natural units unless params->beta_internal), with the

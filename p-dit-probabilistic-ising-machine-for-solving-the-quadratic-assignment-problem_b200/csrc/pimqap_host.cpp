@@ -942,6 +942,25 @@ pimqap_status pimqap_solver_event_perm(pimqap_solver *s, int32_t perm_index, int
 
 void pimqap_solver_destroy(pimqap_solver *s) { delete s; }
 
+pimqap_status pimqap_release_kept_memory(void) {
+    KeptBlock take[kKeepDevices];
+    {
+        std::lock_guard<std::mutex> lk(g_keep_mu);
+        for (int d = 0; d < kKeepDevices; ++d) {
+            take[d] = g_keep[d];
+            g_keep[d] = KeptBlock{};
+        }
+    }
+    pimqap_status st = PIMQAP_OK;
+    for (int d = 0; d < kKeepDevices; ++d) {
+        if (!take[d].p) continue;
+        const cudaError_t e = cudaFree(take[d].p);
+        if (e != cudaSuccess && st == PIMQAP_OK)
+            st = fail(PIMQAP_ERR_CUDA, std::string("cudaFree of a kept block: ") + cudaGetErrorString(e));
+    }
+    return st;
+}
+
 pimqap_status pimqap_solve(const pimqap_instance *inst, const pimqap_params *params,
                            pimqap_result *result) {
     if (!result) return fail(PIMQAP_ERR_ARG, "null result");

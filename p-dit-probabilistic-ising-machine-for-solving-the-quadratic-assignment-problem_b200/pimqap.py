@@ -140,6 +140,8 @@ def lib() -> C.CDLL:
     L.pimqap_solver_group.restype = st
     L.pimqap_solver_destroy.argtypes = [C.c_void_p]
     L.pimqap_solver_destroy.restype = None
+    L.pimqap_release_kept_memory.argtypes = []
+    L.pimqap_release_kept_memory.restype = st
     L.pimqap_batch_solve.argtypes = [C.POINTER(Instance), C.POINTER(Params), C.c_int32, C.POINTER(Result)]
     L.pimqap_batch_solve.restype = st
     L.pimqap_server_create.argtypes = [C.POINTER(ServerConfig), C.POINTER(C.c_void_p)]
@@ -325,6 +327,11 @@ def solve(F: np.ndarray, D: np.ndarray, params: Params) -> dict:
     r, perm, energies = _new_result(inst.F.shape[0], params.groups * params.replicas)
     _check(lib().pimqap_solve(C.byref(inst.c), C.byref(params), C.byref(r)))
     return _result_dict(r, perm, energies)
+
+
+def release_kept_memory() -> None:
+    """pimqap_release_kept_memory: frees the device blocks finished solves left for reuse."""
+    _check(lib().pimqap_release_kept_memory())
 
 
 def auto_beta(F: np.ndarray, D: np.ndarray, params: Params) -> dict:

@@ -114,3 +114,8 @@ def test_n_out_of_range_rejected():
     with pytest.raises(pimqap.PimqapError) as e:
         pimqap.Solver(F, F, pimqap.default_params())
     assert e.value.status == 1
+
+
+def test_release_kept_memory_with_nothing_kept_makes_no_cuda_call():
+    # no solve has run in this process, so nothing is kept and no GPU is needed
+    pimqap.release_kept_memory()
