@@ -26,6 +26,9 @@ CASES = [
     ("big", 40, 2, 8, 2, 0.05, 1.3, 6, 17, "uniform"),
     ("big", 256, 1, 2, 1, 0.002, 1.5, 1, 19, "grid"),                      # n = 256
     ("big", 100, 1, 3, 1, 0.0005, 2.0, 2, 23, "heavy_small"),
+    ("stock", 1, 1, 2, 1, 1.0, 1.2, 5, 29, "uniform"),                    # n = 1: only the self move
+    ("stock", 2, 2, 3, 2, 0.3, 1.3, 12, 31, "uniform"),                   # n = 2
+    ("big", 64, 1, 4, 2, 0.05, 1.25, 4, 37, "binary"),                    # 0/1 flows (binary-flow kernel's domain)
 ]
 
 
@@ -34,6 +37,11 @@ def make(gen, n, seed):
         return instances.uniform(n, seed)
     if gen == "grid":
         return instances.grid256(seed)
+    if gen == "binary":
+        rng = np.random.default_rng(seed)
+        up = np.triu((rng.random((n, n)) < 0.36).astype(np.int64), 1)
+        D = instances.uniform(n, seed + 1).D
+        return instances.Instance(n, up + up.T, D)
     if gen == "heavy_small":
         # heavy-tailed shape with flows scaled down so every int32 intermediate of the
         # reference stays exact
