@@ -150,7 +150,7 @@ typedef struct pimqap_result {
 pimqap_status pimqap_read_problem(const char *path, int32_t max_n, int32_t *n,
                                   int32_t *flow, int32_t *dist);
 
-/* The same reader into arrays it allocates (the survey's pimqap_load_file): inst->flow and
+/* The same reader (readProblem, CPU_PIM.cpp:79-107) into arrays it allocates: inst->flow and
    inst->dist hold n*n entries each until pimqap_free_instance releases them. */
 pimqap_status pimqap_load_file(const char *path, pimqap_instance *inst);
 void pimqap_free_instance(pimqap_instance *inst);

@@ -71,7 +71,7 @@ void usage(const char *argv0) {   // :486-503
     cout << "If -b is not set, then automatic mode is used." << endl;
     cout << "In automatic mode, a series of short trials at different betas are used to try and choose the best parameters." << endl;
     cout << endl;
-    cout << "Options of this build:" << endl;
+    cout << "Additional options:" << endl;
     cout << "--seed S        key of the counter-based random stream (default 1)" << endl;
     cout << "--json PATH     write the best cost, permutation and time to target as JSON" << endl;
     cout << "--device D      CUDA device ordinal (default 0)" << endl;
