@@ -328,7 +328,7 @@ pimqap_status check_params(const pimqap_instance *inst, const pimqap_params *p) 
         return fail(PIMQAP_ERR_ARG, "event capacities must be >= 0");
     if (p->compact_instance != 0 && p->compact_instance != 1)
         return fail(PIMQAP_ERR_ARG, "compact_instance must be 0 or 1");
-    if (p->active_facilities < 0 || p->active_facilities >= inst->n && p->active_facilities != 0)
+    if (p->active_facilities != 0 && (p->active_facilities < 2 || p->active_facilities >= inst->n))
         return fail(PIMQAP_ERR_ARG, "active_facilities must be 0 or in [2, n)");
     if (p->update_rule != PIMQAP_RULE_SEQUENTIAL && p->update_rule != PIMQAP_RULE_ONE_SHOT)
         return fail(PIMQAP_ERR_ARG, "update_rule must be 0 (sequential) or 1 (one-shot)");

@@ -109,6 +109,32 @@ def test_invalid_params_rejected_before_device(field, value):
     assert e.value.status == 1
 
 
+@pytest.mark.parametrize("fields", [{"update_rule": 2}, {"cluster_size": 3}, {"compact_instance": 2},
+                                    {"active_facilities": 1}, {"active_facilities": 8},
+                                    {"max_megaiters": -1}, {"event_capacity": -1},
+                                    {"threads_per_block": 512},
+                                    {"update_rule": 1, "active_facilities": 4}])
+def test_invalid_combinations_rejected_before_device(fields):
+    inst = instances.uniform(8, 1)
+    p = pimqap.default_params(replicas=4, groups=1, max_megaiters=1)
+    for k, v in fields.items():
+        setattr(p, k, v)
+    with pytest.raises(pimqap.PimqapError) as e:
+        pimqap.Solver(inst.F, inst.D, p)
+    assert e.value.status == 1
+
+
+def test_valid_solve_without_a_gpu_fails_loudly():
+    """No CPU fallback: with no sm_100 device a valid solve reports PIMQAP_ERR_NO_DEVICE."""
+    from conftest import _has_gpu
+    if _has_gpu():
+        pytest.skip("a GPU is visible")
+    inst = instances.uniform(8, 1)
+    with pytest.raises(pimqap.PimqapError) as e:
+        pimqap.solve(inst.F, inst.D, pimqap.default_params(replicas=2, groups=1, max_megaiters=1))
+    assert e.value.status == 4
+
+
 def test_n_out_of_range_rejected():
     F = np.zeros((257, 257), np.int32)
     with pytest.raises(pimqap.PimqapError) as e:
