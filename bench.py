@@ -26,7 +26,6 @@ from __future__ import annotations
 import argparse
 import json
 import os
-import re
 import statistics
 import subprocess
 import sys
@@ -148,20 +147,23 @@ def ref_cpu_throughput(F, D, budget_s: float, replicas: int = REPLICAS):
     return val, cores, "reference", sample
 
 
-def workload_config(workload, update_rule, world):
-    """The workload part of the line's config, the same in both arms."""
+def workload_config(workload, update_rule, world, steps):
+    """The workload part of the line's config, the same in both arms; it names the sweeps the
+    timed region actually runs (the published configuration's 10^4 sweeps are --steps 100)."""
+    sweeps = steps * MEGAITERS_PER_STEP * SWEEPS_PER_EXCHANGE
     return {"workload": ("grid256: n=256 Bernoulli(0.36) flow, 16x16 grid sq. distance + U[0,3]; "
                          if workload == "grid256" else
                          "clique92: n=256, unit flows among facilities 0..91, 16x16 grid sq. "
                          "distance + U[0,3]; the tai256c program's moves; ") +
                         "64 replicas, geometric beta ladder, exchange every 4 sweeps, "
-                        "10^4 sweeps = 100 steps" +
+                        f"{sweeps} sweeps timed ({steps} steps of 100)" +
                         ("; GPU-CUPIM's one-shot rule (a sweep = one parallel step)"
                          if update_rule == "one-shot" else ""),
             "update_rule": update_rule,
             "n": N, "replicas": REPLICAS * GROUPS, "sweeps_per_step": MEGAITERS_PER_STEP * SWEEPS_PER_EXCHANGE,
             "beta0_internal": BETA_MAX, "beta_ratio": BETA_RATIO,
             "ladder": "reference automatic mode on this instance (pimqap_auto_beta, seed 1), then fixed",
+            "sweeps_timed": sweeps,
             "parallelism": f"instances x{world}"}
 
 
@@ -175,7 +177,7 @@ def run_reference(args):
         print(json.dumps({"impl": "reference", "unavailable": "the reference arm times the grid256 workload "
                                                               "with the sequential rule (CPU_PIM.cpp) only"}))
         return
-    cfg = dict(workload_config(args.workload, args.update_rule, 1),
+    cfg = dict(workload_config(args.workload, args.update_rule, 1, args.steps),
                parallelism="host threads (the reference's CPU program; no GPU)")
     if not ref_available("big_mt"):
         print(json.dumps({"impl": "reference", "unavailable": "reference CPU_PIM.cpp not built (oracle/_ref missing)"}))
@@ -209,15 +211,6 @@ def run_reference(args):
 
 
 # ------------------------------------------------------------------ our arm
-
-def read_traffic(summary="epoch_kernel_grid256.md"):
-    """dram bytes per launch of the sweep kernel from the committed ncu summary, or None."""
-    path = os.path.join(ROOT, "profiles", summary)
-    if not os.path.exists(path):
-        return None
-    m = re.search(r"dram_bytes_per_launch:\s*([0-9.eE+]+)", open(path).read())
-    return float(m.group(1)) if m else None
-
 
 def rank_instance(rank, workload="grid256"):
     """The instance rank `rank` solves: one instance per GPU (the work is sharded by
@@ -340,7 +333,14 @@ def run_ours(args):
     launches = args.steps * MEGAITERS_PER_STEP
     achieved = alg_bytes / (ms_total * 1e-3) / 1e9
     smem_peak = pimqap.probe_smem_bandwidth(local)
-    traffic = read_traffic("epoch_kernel_oneshot_grid256.md" if rule else "epoch_kernel_grid256.md")
+    # HBM bytes every launch moves by construction: each replica's state is loaded into shared
+    # memory and stored back (force rows, permutation, best permutation; the scalars are noise),
+    # and every CTA stages the instance (the binary-flow kernel: D rows and F as bits, read as
+    # int32 rows).  Measured DRAM bytes come from ncu captures, not from this run.
+    cl = r1["cluster_size"]
+    npad = (N + 3) & ~3
+    state_bytes = reps * (2 * N * npad * s + 3 * N * 4)
+    stage_bytes = reps * cl * 2 * N * npad * 4
 
     line = None
     if rank == 0:
@@ -355,7 +355,7 @@ def run_ours(args):
             "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": f"int{8 * s}",
             "data": "synthetic (seeded grid256 instance per GPU)",
-            "config": dict(workload_config(args.workload, args.update_rule, world),
+            "config": dict(workload_config(args.workload, args.update_rule, world, args.steps),
                            cluster_size=r1["cluster_size"], force_bits=r1["force_bits"],
                            l2="flushed between steps (256 MiB write)"),
             "candidate_deltas_per_s": cand * world / (ms_max * 1e-3),
@@ -367,7 +367,10 @@ def run_ours(args):
                          "frac": achieved / smem_peak,
                          "peak_source": "measured on this GPU by pimqap_probe_smem_bandwidth (shared-memory "
                                         "read-modify-write, 128-bit, 2 CTAs/SM)",
-                         "traffic": traffic,
+                         "traffic": None,
+                         "traffic_note": "not measured in this run (no profiler in the timed region); "
+                                         "ncu DRAM bytes per launch are in the committed profile summary",
+                         "hbm_bytes_per_launch_by_construction": state_bytes + stage_bytes,
                          "alg_bytes_per_launch": alg_bytes / launches,
                          "bytes_model": bytes_model},
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": res["h2d_bytes"],

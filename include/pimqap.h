@@ -174,7 +174,9 @@ pimqap_status pimqap_solve(const pimqap_instance *inst, const pimqap_params *par
    needs more is rejected with PIMQAP_ERR_ARG.  The first call on a device looks the array's
    address up (make it before any stream capture).  Calls share the array: this library
    serialises its own calls per device, and calls that overlap on one GPU from elsewhere race.
-   Work runs on the legacy default stream; no stream, event or graph is created. */
+   Work runs on the legacy default stream; no stream, event or graph is created, so
+   result->device_ms is the host wall time of the launch loop here, not an event-timed
+   device figure like pimqap_solve's. */
 #define PIMQAP_STATIC_SCRATCH_BYTES ((size_t)8 << 20)
 pimqap_status pimqap_solve_static(const pimqap_instance *inst, const pimqap_params *params,
                                   pimqap_result *result);

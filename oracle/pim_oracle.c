@@ -183,13 +183,18 @@ int orc_update_r(int n, const int32_t *D, const int32_t *F, int64_t *I, int32_t 
                 phiinv[b] = i;
                 phi[j] = a;
                 phiinv[a] = j;
-                for (int k = 0; k < n; ++k) {            /* :263-269 */
-                    int64_t d1 = (int64_t)D[k * n + j] - D[k * n + i];
-                    int64_t d2 = (int64_t)D[j * n + k] - D[i * n + k];
+                /* :263-269, I[k][c] += d1(k) (F[c][b] - F[c][a]) + d2(k) (F[b][c] - F[a][c]),
+                   with the two flow differences taken once per swap (integers: same sums) */
+                int64_t colf[256], rowf[256];
+                for (int c = 0; c < n; ++c) {
+                    colf[c] = (int64_t)F[c * n + b] - F[c * n + a];
+                    rowf[c] = (int64_t)F[b * n + c] - F[a * n + c];
+                }
+                for (int k = 0; k < n; ++k) {
+                    const int64_t d1 = (int64_t)D[k * n + j] - D[k * n + i];
+                    const int64_t d2 = (int64_t)D[j * n + k] - D[i * n + k];
                     int64_t *Ik = I + (size_t)k * n;
-                    for (int c = 0; c < n; ++c)
-                        Ik[c] += d1 * ((int64_t)F[c * n + b] - F[c * n + a]) +
-                                 d2 * ((int64_t)F[b * n + c] - F[a * n + c]);
+                    for (int c = 0; c < n; ++c) Ik[c] += d1 * colf[c] + d2 * rowf[c];
                 }
                 if (*E < *bestE) *bestE = *E;            /* :271-272 */
             }
@@ -573,12 +578,18 @@ int orc_run(orc_run_state *st, const int32_t *D, const int32_t *F, int64_t megai
             return 1;
         }
         uint32_t sweep0 = (uint32_t)(st->megaiters_done * st->numitera);
-        for (int t = 0; t < T; ++t) {
-            for (int l = 0; l < R; ++l) {                /* :360-362 */
-                size_t rep = (size_t)t * R + l;
+        /* :360-362.  The replicas' sweeps between two exchanges touch only their own state,
+           so they run in parallel (the reference runs its groups on threads too); the
+           results do not depend on the schedule. */
+        int64_t acc = 0;
+#pragma omp parallel for schedule(dynamic, 1) reduction(+ : acc)
+        for (int q = 0; q < T * R; ++q) {
+            {
+                const int t = q / R, l = q % R;
+                size_t rep = (size_t)q;
                 if (st->rule == 1) {
                     for (int s2 = 0; s2 < st->numitera; ++s2)
-                        st->accepts += orc_oneshot_step(
+                        acc += orc_oneshot_step(
                             n, D, F, st->I + rep * (size_t)n * n, st->phi + rep * n, st->phiinv + rep * n,
                             &st->E[rep], &st->bestE[rep], st->beta[rep], st->seed, (uint32_t)t,
                             (uint32_t)l, sweep0 + (uint32_t)s2, 0);
@@ -595,16 +606,17 @@ int orc_run(orc_run_state *st, const int32_t *D, const int32_t *F, int64_t megai
                                 orc_sweep_word(st->seed, (uint32_t)t, (uint32_t)l, sw, (uint32_t)i, 0),
                                 orc_sweep_word(st->seed, (uint32_t)t, (uint32_t)l, sw, (uint32_t)i, 1),
                                 st->seed, (uint32_t)t, (uint32_t)l, sw);
-                            if (b >= 0 && b != a) st->accepts++;
+                            if (b >= 0 && b != a) acc++;
                         }
                     continue;
                 }
-                st->accepts += orc_replica_sweeps(
+                acc += orc_replica_sweeps(
                     n, D, F, st->I + rep * (size_t)n * n, st->phi + rep * n,
                     st->phiinv + rep * n, &st->E[rep], &st->bestE[rep], st->beta[rep],
                     st->seed, (uint32_t)t, (uint32_t)l, sweep0, st->numitera, 0);
             }
         }
+        st->accepts += acc;
         st->megaiters_done++;
     }
     return 0;

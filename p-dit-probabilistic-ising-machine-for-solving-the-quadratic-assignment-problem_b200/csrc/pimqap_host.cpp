@@ -54,56 +54,24 @@ void trace(const char *phase) {
 
 
 
-// ------------------------------------------------------------------ random words (host)
+// ------------------------------------------------------------------ initial permutations
 
-// Philox4x32-10 (Salmon et al., SC'11).
-void philox4x32_10(uint32_t c[4], uint32_t k0, uint32_t k1) {
-    for (int r = 0; r < 10; ++r) {
-        const uint64_t p0 = (uint64_t)0xD2511F53u * c[0];
-        const uint64_t p1 = (uint64_t)0xCD9E8D57u * c[2];
-        const uint32_t n0 = (uint32_t)(p1 >> 32) ^ c[1] ^ k0;
-        const uint32_t n2 = (uint32_t)(p0 >> 32) ^ c[3] ^ k1;
-        c[0] = n0;
-        c[1] = (uint32_t)p1;
-        c[2] = n2;
-        c[3] = (uint32_t)p0;
-        k0 += 0x9E3779B9u;
-        k1 += 0xBB67AE85u;
+void shuffle_group(ShuffleEngine &eng, int n, int32_t *perm) {
+    for (int i = 0; i < n; ++i) perm[i] = i;
+    for (int i = 0; i < n; ++i) {
+        std::uniform_int_distribution<ShuffleEngine::result_type> distN(0, n - 1);
+        const int j = (int)distN(eng);
+        if (i != j) std::swap(perm[i], perm[j]);
     }
 }
 
-// The shuffle stream as a C++ uniform random bit generator with the reference engine's
-// interface (32-bit words, result_type uint_fast32_t), so std::uniform_int_distribution
-// draws from it exactly as the reference's distN(rng[0]) draws from std::mt19937
-// (CPU_PIM.cpp:147-148).  Word k is Philox({k/4, k>>34, 0, ~0}, seed)[k%4].
-struct ShuffleEngine {
-    typedef uint_fast32_t result_type;
-    static constexpr result_type min() { return 0; }
-    static constexpr result_type max() { return 0xFFFFFFFFu; }
-    uint64_t seed = 0;
-    uint64_t k = 0;
-    result_type operator()() {
-        uint32_t c[4] = {(uint32_t)(k >> 2), (uint32_t)(k >> 34), 0u, 0xFFFFFFFFu};
-        philox4x32_10(c, (uint32_t)seed, (uint32_t)(seed >> 32));
-        return c[(k++) & 3];
-    }
-};
-
-// Initial permutations of all groups (CPU_PIM.cpp:134-162): identity, then per group and
-// location one draw j in [0, n) and the transposition (i j); all replicas of a group share it.
+// Initial permutations of all groups (CPU_PIM.cpp:134-162); all replicas of a group share
+// their group's permutation.
 std::vector<int32_t> initial_perms(int n, int T, uint64_t seed) {
     std::vector<int32_t> perms((size_t)T * n);
     ShuffleEngine eng;
     eng.seed = seed;
-    for (int t = 0; t < T; ++t) {
-        int32_t *p = perms.data() + (size_t)t * n;
-        for (int i = 0; i < n; ++i) p[i] = i;
-        for (int i = 0; i < n; ++i) {
-            std::uniform_int_distribution<ShuffleEngine::result_type> distN(0, n - 1);
-            const int j = (int)distN(eng);
-            if (i != j) std::swap(p[i], p[j]);
-        }
-    }
+    for (int t = 0; t < T; ++t) shuffle_group(eng, n, perms.data() + (size_t)t * n);
     return perms;
 }
 
@@ -324,6 +292,8 @@ pimqap_status check_params(const pimqap_instance *inst, const pimqap_params *p) 
     if (!(p->beta_ratio > 0) || !std::isfinite(p->beta_ratio))
         return fail(PIMQAP_ERR_ARG, "beta_ratio must be a positive finite number");
     if (p->max_megaiters < 0) return fail(PIMQAP_ERR_ARG, "max_megaiters must be >= 0");
+    if (!(p->timeout_s >= 0) || !std::isfinite(p->timeout_s))   // -s (CPU_PIM.cpp:350-357)
+        return fail(PIMQAP_ERR_ARG, "timeout_s must be a finite number >= 0 (0 = no timeout)");
     if (p->event_capacity < 0 || p->event_perm_capacity < 0)
         return fail(PIMQAP_ERR_ARG, "event capacities must be >= 0");
     if (p->compact_instance != 0 && p->compact_instance != 1)

@@ -37,6 +37,45 @@ template <class T> T *carve(char *&cur, size_t count) {
     return p;
 }
 
+// Philox4x32-10 (Salmon et al., SC'11) on the host: the ten rounds applied to counter c in
+// place, key (k0, k1).
+inline void philox4x32_10(uint32_t c[4], uint32_t k0, uint32_t k1) {
+    for (int r = 0; r < 10; ++r) {
+        const uint64_t p0 = (uint64_t)0xD2511F53u * c[0];
+        const uint64_t p1 = (uint64_t)0xCD9E8D57u * c[2];
+        const uint32_t n0 = (uint32_t)(p1 >> 32) ^ c[1] ^ k0;
+        const uint32_t n2 = (uint32_t)(p0 >> 32) ^ c[3] ^ k1;
+        c[0] = n0;
+        c[1] = (uint32_t)p1;
+        c[2] = n2;
+        c[3] = (uint32_t)p0;
+        k0 += 0x9E3779B9u;
+        k1 += 0xBB67AE85u;
+    }
+}
+
+// The shuffle stream as a C++ uniform random bit generator with the reference engine's
+// interface (32-bit words, result_type uint_fast32_t), so std::uniform_int_distribution
+// draws from it exactly as the reference's distN(rng[0]) draws from std::mt19937
+// (CPU_PIM.cpp:147-148).  Word k is Philox({k/4, k>>34, 0, ~0}, seed)[k%4].
+struct ShuffleEngine {
+    typedef uint_fast32_t result_type;
+    static constexpr result_type min() { return 0; }
+    static constexpr result_type max() { return 0xFFFFFFFFu; }
+    uint64_t seed = 0;
+    uint64_t k = 0;
+    result_type operator()() {
+        uint32_t c[4] = {(uint32_t)(k >> 2), (uint32_t)(k >> 34), 0u, 0xFFFFFFFFu};
+        philox4x32_10(c, (uint32_t)seed, (uint32_t)(seed >> 32));
+        return c[(k++) & 3];
+    }
+};
+
+// The initial permutation of the next group (CPU_PIM.cpp:143-162): identity, then for each
+// location i one draw j in [0, n) from the shared stream and the transposition (i j).
+// Groups draw one after another from the same engine.
+void shuffle_group(ShuffleEngine &eng, int n, int32_t *perm);
+
 // Initial permutations of T groups (CPU_PIM.cpp:134-162) from the shuffle stream of `seed`.
 std::vector<int32_t> initial_perms(int n, int T, uint64_t seed);
 

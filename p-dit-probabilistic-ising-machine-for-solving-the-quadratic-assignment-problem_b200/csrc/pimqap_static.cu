@@ -25,6 +25,9 @@
 //   - No cudaMalloc, cudaFree, cudaMallocHost, stream, event or graph creation, and no host heap
 //     allocation on the success path (small fixed-size host buffers live on the stack).  A
 //     failure records its message in the library's last-error slot.
+//   - result->device_ms is the host wall time of the launch loop (this entry point creates no
+//     CUDA event), so it includes launch and stop-test round trips that pimqap_solve's
+//     event-timed figure leaves out.
 //   - The force-matrix width is chosen from the cheap per-row bound only (the tighter sorted
 //     bound of pimqap_solve needs heap buffers); int64 is used when that bound exceeds int32.
 //     Widths do not change results, only memory.
@@ -41,6 +44,7 @@
 
 #include "pimqap.h"
 #include "pimqap_internal.h"
+#include "pimqap_plan.h"
 
 using pimqap::SolveDev;
 
@@ -59,42 +63,8 @@ pimqap_status fail(pimqap_status st, const char *msg) {
     return st;
 }
 
-// Philox4x32-10 (Salmon et al., SC'11) and the shuffle-stream engine, as in pimqap_solve.
-void philox4x32_10(uint32_t c[4], uint32_t k0, uint32_t k1) {
-    for (int r = 0; r < 10; ++r) {
-        const uint64_t p0 = (uint64_t)0xD2511F53u * c[0];
-        const uint64_t p1 = (uint64_t)0xCD9E8D57u * c[2];
-        const uint32_t n0 = (uint32_t)(p1 >> 32) ^ c[1] ^ k0;
-        const uint32_t n2 = (uint32_t)(p0 >> 32) ^ c[3] ^ k1;
-        c[0] = n0;
-        c[1] = (uint32_t)p1;
-        c[2] = n2;
-        c[3] = (uint32_t)p0;
-        k0 += 0x9E3779B9u;
-        k1 += 0xBB67AE85u;
-    }
-}
-
-struct ShuffleEngine {
-    typedef uint_fast32_t result_type;
-    static constexpr result_type min() { return 0; }
-    static constexpr result_type max() { return 0xFFFFFFFFu; }
-    uint64_t seed = 0;
-    uint64_t k = 0;
-    result_type operator()() {
-        uint32_t c[4] = {(uint32_t)(k >> 2), (uint32_t)(k >> 34), 0u, 0xFFFFFFFFu};
-        philox4x32_10(c, (uint32_t)seed, (uint32_t)(seed >> 32));
-        return c[(k++) & 3];
-    }
-};
-
-size_t carve_size(size_t bytes) { return (bytes + 255) & ~size_t(255); }
-
-template <class T> T *carve(char *&cur, size_t count) {
-    T *p = reinterpret_cast<T *>(cur);
-    cur += carve_size(count * sizeof(T));
-    return p;
-}
+using pimqap::detail::carve;
+using pimqap::detail::carve_size;
 
 // Small per-call results reduced on the device (no host array of T*R entries is needed).
 struct StaticSummary {
@@ -130,6 +100,26 @@ __global__ void static_prepare_kernel(SolveDev d, const int32_t *Draw, const int
         *d.stop_epoch = pimqap::kNoStop;
         *d.target_epoch = 0x7fffffffffffffffll;
         *d.target_ns = ~0ull;
+    }
+}
+
+// Replica set-up from one copy per group: every replica of group t starts from the group's
+// permutation (CPU_PIM.cpp:143-162), every group has the same beta ladder (:111-119), and rank
+// slot l holds replica l (slots past R hold 0, as the reference's zeroed array does).
+__global__ void static_replicate_kernel(SolveDev d, const int32_t *group_perms, const double *ladder) {
+    const int n = d.n, R = d.R, T = d.T, cap = d.cap;
+    const int tid = blockIdx.x * blockDim.x + threadIdx.x;
+    const int stride = gridDim.x * blockDim.x;
+    const long long reps = (long long)T * R;
+    for (long long q = tid; q < reps * n; q += stride) {
+        const long long rep = q / n;
+        const int i = (int)(q - rep * n);
+        d.phi[q] = group_perms[(rep / R) * n + i];
+    }
+    for (long long q = tid; q < reps; q += stride) d.beta[q] = ladder[q % R];
+    for (long long q = tid; q < (long long)T * cap; q += stride) {
+        const int l = (int)(q % cap);
+        d.order[q] = l < R ? l : 0;
     }
 }
 
@@ -174,27 +164,15 @@ __global__ void static_summary_kernel(SolveDev d, StaticSummary *out) {
 extern "C" pimqap_status pimqap_solve_static(const pimqap_instance *inst,
                                               const pimqap_params *p, pimqap_result *result) {
     const auto wall0 = std::chrono::steady_clock::now();
-    if (!inst || !p || !result) return fail(PIMQAP_ERR_ARG, "null instance, params or result");
-    const int n = inst->n;
-    if (n < 1 || n > PIMQAP_MAX_N) return fail(PIMQAP_ERR_ARG, "n must be in [1, 256]");
-    if (!inst->flow || !inst->dist) return fail(PIMQAP_ERR_ARG, "null flow or dist");
-    if (p->replicas < 1 || p->replicas > PIMQAP_MAX_REPLICAS) return fail(PIMQAP_ERR_ARG, "replicas must be in [1, 64]");
-    if (p->groups < 1 || p->groups > PIMQAP_MAX_GROUPS) return fail(PIMQAP_ERR_ARG, "groups must be in [1, 1024]");
-    if (p->sweeps_per_exchange < 1) return fail(PIMQAP_ERR_ARG, "sweeps_per_exchange must be >= 1");
-    if (p->rank_slots != 0 && (p->rank_slots < p->replicas || p->rank_slots > 4096))
-        return fail(PIMQAP_ERR_ARG, "rank_slots must be 0 or in [replicas, 4096]");
-    if (!(p->beta_max > 0) || !std::isfinite(p->beta_max)) return fail(PIMQAP_ERR_ARG, "beta_max must be a positive finite number");
-    if (!(p->beta_ratio > 0) || !std::isfinite(p->beta_ratio)) return fail(PIMQAP_ERR_ARG, "beta_ratio must be a positive finite number");
-    if (p->max_megaiters < 0) return fail(PIMQAP_ERR_ARG, "max_megaiters must be >= 0");
-    if (p->force_bits != 0 && p->force_bits != 32 && p->force_bits != 64) return fail(PIMQAP_ERR_ARG, "force_bits must be 0, 32 or 64");
-    if (p->threads_per_block != 0 && p->threads_per_block != 64 && p->threads_per_block != 128 &&
-        p->threads_per_block != 256)
-        return fail(PIMQAP_ERR_ARG, "threads_per_block must be 0, 64, 128 or 256");
-    if (p->cluster_size != 0 && p->cluster_size != 1 && p->cluster_size != 2 && p->cluster_size != 4)
-        return fail(PIMQAP_ERR_ARG, "cluster_size must be 0, 1, 2 or 4");
+    if (!result) return fail(PIMQAP_ERR_ARG, "null result");
+    // The checks of pimqap_solve (they build a message only when they fail, so a valid call
+    // still allocates nothing), then what this entry point does not run.
+    const pimqap_status chk = pimqap::detail::check_params(inst, p);
+    if (chk != PIMQAP_OK) return chk;
     if (p->auto_beta) return fail(PIMQAP_ERR_ARG, "automatic beta selection needs pimqap_solve");
-    if (p->active_facilities > 0) return fail(PIMQAP_ERR_ARG, "active_facilities needs pimqap_solve");
-    if (p->update_rule != PIMQAP_RULE_SEQUENTIAL) return fail(PIMQAP_ERR_ARG, "the one-shot rule needs pimqap_solve");
+    if (p->active_facilities != 0) return fail(PIMQAP_ERR_ARG, "active_facilities needs pimqap_solve");
+    if (p->update_rule == PIMQAP_RULE_ONE_SHOT) return fail(PIMQAP_ERR_ARG, "the one-shot rule needs pimqap_solve");
+    const int n = inst->n;
 
     // Instance analysis without heap buffers: symmetry and the per-row force bound.
     const int32_t *F = inst->flow, *D = inst->dist;
@@ -274,7 +252,8 @@ extern "C" pimqap_status pimqap_solve_static(const pimqap_instance *inst,
                         2 * carve_size(nraw * 4) +
                         2 * carve_size((size_t)n * 4) + 2 * carve_size(reps * n * 4) +
                         4 * carve_size(reps * 8) + carve_size((size_t)T * cap * 4) +
-                        4 * carve_size((size_t)T * 8) + 8 * carve_size(8) + carve_size(sizeof(StaticSummary));
+                        4 * carve_size((size_t)T * 8) + 8 * carve_size(8) + carve_size(sizeof(StaticSummary)) +
+                        carve_size((size_t)T * n * 4) + carve_size((size_t)R * 8);
     if (need > kStaticScratchBytes) {
         char msg[160];
         std::snprintf(msg, sizeof msg,
@@ -314,6 +293,8 @@ extern "C" pimqap_status pimqap_solve_static(const pimqap_instance *inst,
     d.error = carve<int32_t>(cur, 1);
     StaticSummary *dsum = carve<StaticSummary>(cur, 1);
     int32_t *rawD = carve<int32_t>(cur, nraw), *rawF = carve<int32_t>(cur, nraw);
+    int32_t *group_perms = carve<int32_t>(cur, (size_t)T * n);
+    double *dladder = carve<double>(cur, R);
 
     const cudaStream_t q = 0;   // the legacy default stream: nothing is created per call
 #define PQS_CUDA(x)                                                     \
@@ -326,43 +307,38 @@ extern "C" pimqap_status pimqap_solve_static(const pimqap_instance *inst,
     static_prepare_kernel<<<64, 256, 0, q>>>(d, rawD, rawF, dD, dF, dDT, dFT, dDd, dFd);
     PQS_CUDA(cudaGetLastError());
 
-    // Host set-up with fixed-size stack buffers: shuffle, beta ladder, rank slots per group.
+    // Host set-up with fixed-size stack buffers: each group's shuffle (drawn group after group
+    // from one stream), uploaded a chunk of groups per copy, and the beta ladder once; a kernel
+    // gives every replica its group's permutation and ladder slot.
     const double beta0 = p->beta_internal ? p->beta_max : p->beta_max * 1.44269504089;
-    ShuffleEngine eng;
+    pimqap::detail::ShuffleEngine eng;
     eng.seed = p->seed;
-    int32_t perm[PIMQAP_MAX_N];
-    double ladder[PIMQAP_MAX_REPLICAS];
-    int32_t order[64];
-    for (int t = 0; t < T; ++t) {
-        for (int i = 0; i < n; ++i) perm[i] = i;
-        for (int i = 0; i < n; ++i) {
-            std::uniform_int_distribution<ShuffleEngine::result_type> distN(0, n - 1);
-            const int j = (int)distN(eng);
-            if (i != j) std::swap(perm[i], perm[j]);
-        }
-        for (int l = 0; l < R; ++l)
-            PQS_CUDA(cudaMemcpy(d.phi + ((size_t)t * R + l) * n, perm, (size_t)n * 4, cudaMemcpyHostToDevice));
-        double running = beta0;
-        for (int l = R - 1; l >= 0; --l) {
-            ladder[l] = running;
-            running /= p->beta_ratio;
-        }
-        PQS_CUDA(cudaMemcpy(d.beta + (size_t)t * R, ladder, (size_t)R * 8, cudaMemcpyHostToDevice));
-        for (int c0 = 0; c0 < cap; c0 += 64) {   // slots past R start at 0 (cleared above)
-            const int cnt = std::min(64, R - c0);
-            if (cnt <= 0) break;
-            for (int k = 0; k < cnt; ++k) order[k] = c0 + k;
-            PQS_CUDA(cudaMemcpy(d.order + (size_t)t * cap + c0, order, (size_t)cnt * 4, cudaMemcpyHostToDevice));
-        }
+    constexpr int kStageInts = 4096;                  // 16 KB of permutations per copy
+    int32_t stage[kStageInts];
+    const int per_copy = kStageInts / n;             // >= 16 groups, since n <= 256
+    for (int t0 = 0; t0 < T; t0 += per_copy) {
+        const int cnt = std::min(per_copy, T - t0);
+        for (int k = 0; k < cnt; ++k) pimqap::detail::shuffle_group(eng, n, stage + (size_t)k * n);
+        PQS_CUDA(cudaMemcpy(group_perms + (size_t)t0 * n, stage, (size_t)cnt * n * 4, cudaMemcpyHostToDevice));
     }
+    double ladder[PIMQAP_MAX_REPLICAS];
+    double running = beta0;
+    for (int l = R - 1; l >= 0; --l) {
+        ladder[l] = running;
+        running /= p->beta_ratio;
+    }
+    PQS_CUDA(cudaMemcpy(dladder, ladder, (size_t)R * 8, cudaMemcpyHostToDevice));
+    static_replicate_kernel<<<64, 256, 0, q>>>(d, group_perms, dladder);
+    PQS_CUDA(cudaGetLastError());
     PQS_CUDA(pimqap::launch_setup(d, bits, q));
     PQS_CUDA(cudaStreamSynchronize(q));
 
-    // Mega-iterations, one epoch launch each; goal and timeout are checked every few launches.
+    // Mega-iterations, one epoch launch each; goal and timeout are checked every few launches,
+    // the timeout counted from here as pimqap_solve counts it from the start of its run loop.
     const auto run0 = std::chrono::steady_clock::now();
     const int check_every = p->megaiters_per_launch > 0 ? p->megaiters_per_launch : 50;
     int64_t left = p->max_megaiters;
-    bool stopped_goal = false, timed_out = false;
+    bool stopped_goal = false;
     while (left > 0) {
         const int g = (int)std::min<int64_t>(left, check_every);
         for (int k = 0; k < g; ++k) PQS_CUDA(pimqap::launch_epoch(d, bits, cl, sym, false, threads, smem, q));
@@ -374,10 +350,8 @@ extern "C" pimqap_status pimqap_solve_static(const pimqap_instance *inst,
             break;
         }
         if (p->timeout_s > 0 &&
-            std::chrono::duration<double>(std::chrono::steady_clock::now() - wall0).count() >= p->timeout_s) {
-            timed_out = true;
+            std::chrono::duration<double>(std::chrono::steady_clock::now() - run0).count() >= p->timeout_s)
             break;
-        }
     }
     static_summary_kernel<<<1, 256, 0, q>>>(d, dsum);
     PQS_CUDA(cudaGetLastError());
@@ -413,12 +387,14 @@ extern "C" pimqap_status pimqap_solve_static(const pimqap_instance *inst,
     result->sweeps = result->updates / n;
     result->proposals = result->sweeps * ((int64_t)n * (n - 1) / 2);
     result->accepts = (int64_t)sum.accepts;
+    // host wall time of the launch loop: this entry point creates no CUDA events
     result->device_ms = std::chrono::duration<double, std::milli>(wall1 - run0).count();
     result->wall_ms = std::chrono::duration<double, std::milli>(wall1 - wall0).count();
     result->force_bits = bits;
     result->cluster_size = cl;
-    result->stopped_by = stopped_goal ? 1 : (timed_out ? 2 : 0);
-    result->h2d_bytes = (int64_t)(2 * nraw * 4 + reps * n * 4 + reps * 8 + (size_t)T * std::min(cap, R) * 4);
+    // pimqap_solve's rule: a timeout is the stop only when mega-iterations were left to run
+    result->stopped_by = stopped_goal ? 1 : ((p->timeout_s > 0 && epoch0 < p->max_megaiters) ? 2 : 0);
+    result->h2d_bytes = (int64_t)(2 * nraw * 4 + (size_t)T * n * 4 + (size_t)R * 8);
     result->d2h_bytes = (int64_t)(sizeof sum + 4 + 4 + 8 + 8 + 8 + 8 + (perm_dst ? (size_t)n * 4 : 0));
     return PIMQAP_OK;
 }

@@ -96,32 +96,62 @@ def test_read_problem_errors(tmp_path):
     assert e.value.status == 2
 
 
+# Both solve entry points take the same parameters and reject the same invalid ones before
+# touching a device: the solver handle (pimqap_solver_create, behind pimqap_solve) and the
+# allocation-free pimqap_solve_static.
+ENTRY_POINTS = {
+    "solver": lambda inst, p: pimqap.Solver(inst.F, inst.D, p),
+    "solve_static": lambda inst, p: pimqap.solve_static(inst.F, inst.D, p),
+}
+
+
+@pytest.mark.parametrize("entry", sorted(ENTRY_POINTS))
 @pytest.mark.parametrize("field,value", [("replicas", 0), ("replicas", 65), ("groups", 0),
                                          ("sweeps_per_exchange", 0), ("beta_max", 0.0),
                                          ("beta_ratio", -1.0), ("force_bits", 16),
-                                         ("threads_per_block", 96), ("rank_slots", 2)])
-def test_invalid_params_rejected_before_device(field, value):
+                                         ("threads_per_block", 96), ("rank_slots", 2),
+                                         ("timeout_s", -1.0), ("timeout_s", float("nan")),
+                                         ("timeout_s", float("inf"))])
+def test_invalid_params_rejected_before_device(entry, field, value):
     inst = instances.uniform(8, 1)
     p = pimqap.default_params(replicas=4, groups=1, max_megaiters=1)
     setattr(p, field, value)
     with pytest.raises(pimqap.PimqapError) as e:
-        pimqap.Solver(inst.F, inst.D, p)
+        ENTRY_POINTS[entry](inst, p)
     assert e.value.status == 1
 
 
+@pytest.mark.parametrize("entry", sorted(ENTRY_POINTS))
 @pytest.mark.parametrize("fields", [{"update_rule": 2}, {"cluster_size": 3}, {"compact_instance": 2},
-                                    {"active_facilities": 1}, {"active_facilities": 8},
+                                    {"active_facilities": 1}, {"active_facilities": -3},
+                                    {"active_facilities": 8},
                                     {"max_megaiters": -1}, {"event_capacity": -1},
                                     {"threads_per_block": 512},
                                     {"update_rule": 1, "active_facilities": 4}])
-def test_invalid_combinations_rejected_before_device(fields):
+def test_invalid_combinations_rejected_before_device(entry, fields):
     inst = instances.uniform(8, 1)
     p = pimqap.default_params(replicas=4, groups=1, max_megaiters=1)
     for k, v in fields.items():
         setattr(p, k, v)
     with pytest.raises(pimqap.PimqapError) as e:
-        pimqap.Solver(inst.F, inst.D, p)
+        ENTRY_POINTS[entry](inst, p)
     assert e.value.status == 1
+    if fields == {"update_rule": 2}:
+        assert "update_rule must be" in str(e.value)
+
+
+@pytest.mark.parametrize("fields,msg", [({"auto_beta": 1}, "automatic beta"),
+                                        ({"active_facilities": 4}, "active_facilities"),
+                                        ({"update_rule": 1}, "one-shot")])
+def test_static_solve_rejects_what_it_does_not_run(fields, msg):
+    """Valid for pimqap_solve, but not run by the allocation-free entry point."""
+    inst = instances.uniform(8, 1)
+    p = pimqap.default_params(replicas=4, groups=1, max_megaiters=1)
+    for k, v in fields.items():
+        setattr(p, k, v)
+    with pytest.raises(pimqap.PimqapError) as e:
+        pimqap.solve_static(inst.F, inst.D, p)
+    assert e.value.status == 1 and msg in str(e.value) and "pimqap_solve" in str(e.value)
 
 
 def test_valid_solve_without_a_gpu_fails_loudly():

@@ -96,3 +96,26 @@ def test_same_result_alone_and_in_a_mix(gpu):
     ps[3] = p
     got = gpu.batch_solve(mix, ps)[3]
     assert same(got, alone)
+
+
+def test_heavy_batch_matches_solo_and_oracle(gpu, oracle):
+    """Eight instances of the heavy-tailed 128-instance batch (n ~ U[100, 256], lognormal flows
+    with 70 % zeros, Euclidean distances) in one launch on the heavy ladder: each equals its
+    solo solve, and its complete replica state equals the oracle's."""
+    from helpers import compare_solver_to_oracle
+    batch = instances.heavy_batch(8)
+    b0 = 2.0 ** -13 / 1.44269504089
+    params = [gpu.default_params(replicas=4, groups=1, sweeps_per_exchange=4, beta_max=b0, beta_ratio=1.5,
+                                 seed=500 + k, max_megaiters=2) for k in range(len(batch))]
+    got = gpu.batch_solve([(b.F, b.D) for b in batch], params)
+    for k, (inst, p) in enumerate(zip(batch, params)):
+        alone = gpu.solve(inst.F, inst.D, p)
+        assert same(got[k], alone), (k, inst.n)
+        st = oracle_after(oracle, inst.F, inst.D, T=1, R=4, spe=4, beta_max=b0, beta_ratio=1.5,
+                          seed=500 + k, cap=10, megaiters=2)
+        assert got[k]["accepts"] == st.accepts
+        assert got[k]["best_energy"] == min(int(st.bestE.min()), st.single_best)
+        with gpu.Solver(inst.F, inst.D, p) as s:   # the full state, through the solver handle
+            s.run(2)
+            bad = compare_solver_to_oracle(s, st, 10)
+        assert not bad, (k, bad[:5])

@@ -42,6 +42,8 @@ def heavy_small(n, seed):
     return instances.Instance(n, np.minimum(inst.F, 60), inst.D // 4)
 
 
+HEAVY_B = 2.0 ** -13 / 1.44269504089   # the heavy ladder's coldest beta, in natural units
+
 # name: (instance factory, T, R, spe, beta_max (natural), beta_ratio, megaiters, extra params)
 CASES = {
     "plain_n32_R16": (lambda: instances.uniform(32, 11), 1, 16, 1, 10.0, 1.5849, 25, {}),
@@ -79,6 +81,16 @@ CASES = {
                                 {"active_facilities": 20}),
     "clique9_n36_t64": (lambda: instances.clique_flow(37, side=6, active=9), 1, 5, 3, 0.05, 1.2, 20,
                         {"active_facilities": 9, "threads_per_block": 64}),
+    # the heavy-tailed workload unscaled (lognormal flows, 70 % zeros, Euclidean distances),
+    # full 4-sweep epochs at n = 100, 180 and 256 on the heavy ladder (2^-13 internal), int32 and
+    # int64 force matrices, clusters of 1, 2 and 4
+    "heavy_n100_i4": (lambda: instances.heavy(100, 81), 1, 4, 4, HEAVY_B, 1.5, 3, {}),
+    "heavy_n180_cluster2_i4": (lambda: instances.heavy(180, 82), 2, 2, 4, HEAVY_B, 1.3, 2, {"cluster_size": 2}),
+    "heavy_n256_i4": (lambda: instances.heavy(256, 83), 1, 3, 4, HEAVY_B, 1.5, 2, {}),
+    "heavy_n256_cluster4_i4": (lambda: instances.heavy(256, 84), 1, 2, 4, HEAVY_B, 1.5, 2, {"cluster_size": 4}),
+    "heavy_n256_int64_i4": (lambda: instances.heavy(256, 85), 1, 2, 4, HEAVY_B, 1.5, 2, {"force_bits": 64}),
+    "heavy_n213_int64_cluster4_i4": (lambda: instances.heavy(213, 86), 1, 2, 4, HEAVY_B, 1.5, 2,
+                                     {"force_bits": 64, "cluster_size": 4}),
 }
 
 
@@ -99,10 +111,18 @@ def run_case(gpu, oracle, name, seed=7):
     return inst, st, bad, res
 
 
+# (force width, cluster size) that a case is meant to cover
+SHAPES = {"heavy_n100_i4": (32, 1), "heavy_n180_cluster2_i4": (32, 2), "heavy_n256_i4": (32, 2),
+          "heavy_n256_cluster4_i4": (32, 4), "heavy_n256_int64_i4": (64, 4),
+          "heavy_n213_int64_cluster4_i4": (64, 4)}
+
+
 @pytest.mark.parametrize("name", list(CASES))
 def test_trajectory_matches_oracle(gpu, oracle, name):
     inst, st, bad, res = run_case(gpu, oracle, name)
     assert not bad, bad[:10]
+    if name in SHAPES:
+        assert (res["force_bits"], res["cluster_size"]) == SHAPES[name]
     assert res["megaiters_done"] == CASES[name][6]
     _, T, R, spe, _, _, M, _ = CASES[name]
     assert res["sweeps"] == M * spe * T * R and res["updates"] == res["sweeps"] * inst.n
@@ -196,3 +216,32 @@ def test_chunking_does_not_change_the_trajectory(gpu):
             s.run(7)
             out.append((s.result()["accepts"], s.replica(1, 3)["E"], s.replica(0, 0)["phi"].tobytes()))
     assert out[0] == out[1] == out[2]
+
+
+# The headline configuration exactly as the benchmark runs it: the n = 256 grid instance, 64
+# replicas on the automatic-mode ladder (beta0 = 2^-5 internal, deltaBeta = 64^(1/64)), exchange
+# every 4 sweeps, 25 mega-iterations per graph launch, the binary-flow kernel on 2-CTA clusters.
+# The complete state is compared with the oracle after two launches (200 sweeps of every
+# replica, about 3.1 M updates at a 95 % accept rate: thousands of deferred-log rewrite cycles).
+HEADLINE_B0 = 2.0 ** -5
+HEADLINE_RATIO = 1.0671404006768237
+
+
+def test_headline_configuration_matches_oracle(gpu, oracle):
+    inst = instances.grid256(1000)
+    M = 50
+    p = gpu.default_params(replicas=64, groups=1, sweeps_per_exchange=4, beta_max=HEADLINE_B0,
+                           beta_ratio=HEADLINE_RATIO, beta_internal=1, seed=1, max_megaiters=2 ** 31 - 1,
+                           megaiters_per_launch=25)
+    with gpu.Solver(inst.F, inst.D, p) as s:
+        s.run(25)
+        s.run(25)
+        st = oracle.setup(inst.D, inst.F, 1, 64, 4, HEADLINE_B0, HEADLINE_RATIO, 1, cap=64)
+        oracle.run(st, inst.D, inst.F, M, -(1 << 62))
+        oracle.track_exchange_all(st)
+        bad = compare_solver_to_oracle(s, st, 64)
+        res = s.result()
+    assert (res["force_bits"], res["cluster_size"]) == (32, 2)
+    assert not bad, bad[:10]
+    assert res["accepts"] == st.accepts
+    assert res["accepts"] > 0.9 * 64 * 4 * M * 256

@@ -80,7 +80,7 @@ def test_reference_arm_names_the_solver_arms_workload():
     line = json.loads(r.stdout.strip().splitlines()[-1])
     if "unavailable" in line:                         # oracle/_ref not built here
         return
-    want = bench.workload_config("grid256", "sequential", 1)
+    want = bench.workload_config("grid256", "sequential", 1, 1)
     got = dict(line["config"])
     assert got.pop("parallelism") != want.pop("parallelism")
     assert got == want

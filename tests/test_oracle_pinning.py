@@ -29,7 +29,24 @@ CASES = [
     ("stock", 1, 1, 2, 1, 1.0, 1.2, 5, 29, "uniform"),                    # n = 1: only the self move
     ("stock", 2, 2, 3, 2, 0.3, 1.3, 12, 31, "uniform"),                   # n = 2
     ("big", 64, 1, 4, 2, 0.05, 1.25, 4, 37, "binary"),                    # 0/1 flows (binary-flow kernel's domain)
+    # the heavy-tailed workload unscaled (lognormal flows, 70 % zeros, Euclidean distances):
+    # a full 4-sweep epoch at n = 180 and n = 256, the reference's own delta function on it
+    ("big", 180, 1, 2, 4, 1.2e-4, 1.08, 2, 41, "heavy"),
+    ("big", 256, 1, 2, 4, 1.2e-4, 1.5, 2, 43, "heavy"),
 ]
+
+
+def int32_exact(inst):
+    """True when every force entry, delta and energy the reference computes in int32
+    (CPU_PIM.cpp:54, :62, :164-192, :225) fits.  |I[i][a]| <= B[i][a], the rearrangement
+    bound of the sorted rows of D and F; a delta is at most 4 max|I| + 16 max|D| max|F|; and
+    since sum_i I[i][phi(i)] = -2E, |E| <= 1/2 sum_i max_a B[i][a]."""
+    D = np.abs(inst.D.astype(np.float64))
+    F = np.abs(inst.F.astype(np.float64))
+    srt = lambda M: -np.sort(-M, axis=1)
+    B = srt(D) @ srt(F).T + srt(D.T) @ srt(F.T).T
+    lim = 2 ** 31 - 1
+    return 4 * B.max() + 16 * D.max() * F.max() < lim and 0.5 * B.max(axis=1).sum() < lim
 
 
 def make(gen, n, seed):
@@ -42,6 +59,8 @@ def make(gen, n, seed):
         up = np.triu((rng.random((n, n)) < 0.36).astype(np.int64), 1)
         D = instances.uniform(n, seed + 1).D
         return instances.Instance(n, up + up.T, D)
+    if gen == "heavy":
+        return instances.heavy(n, seed)
     if gen == "heavy_small":
         # heavy-tailed shape with flows scaled down so every int32 intermediate of the
         # reference stays exact
@@ -56,6 +75,7 @@ def test_restatement_matches_reference(oracle, case):
     variant, n, T, R, it, b0, db, M, seed, gen = case
     ref = RefHarness(variant)
     inst = make(gen, n, seed)
+    assert int32_exact(inst), "the reference's int32 arithmetic would not be exact on this instance"
     ref.load(inst.F, inst.D)
     ref.setup(T, R, it, b0, db, seed)
     st = oracle.setup(inst.D, inst.F, T, R, it, b0, db, seed, cap=ref.maxr)

@@ -55,6 +55,50 @@ def test_static_solve_goal_stop_matches(gpu):
         assert same(gpu.solve_static(inst.F, inst.D, p), ref)
 
 
+def test_static_solve_timeout_stop_matches(gpu):
+    """The -s stop (CPU_PIM.cpp:350-357) on this entry point: stopped_by = 2 only when
+    mega-iterations were left when the time ran out, as pimqap_solve reports it."""
+    import time
+    inst = instances.uniform(48, 314)
+    base = dict(replicas=8, groups=4, sweeps_per_exchange=4, beta_max=0.05, beta_ratio=1.3,
+                megaiters_per_launch=8, seed=9)
+    p = gpu.default_params(timeout_s=0.3, max_megaiters=2 ** 40, **base)
+    for _ in range(2):
+        t0 = time.perf_counter()
+        got = gpu.solve_static(inst.F, inst.D, p)
+        assert time.perf_counter() - t0 < 0.3 + 10.0
+        assert got["stopped_by"] == 2 and 0 < got["megaiters_done"] < p.max_megaiters
+        perm = got["best_perm"]
+        assert int((inst.D.astype(np.int64) * inst.F[np.ix_(perm, perm)]).sum()) == got["best_energy"]
+    assert gpu.solve(inst.F, inst.D, p)["stopped_by"] == 2
+    # every mega-iteration ran before the time ran out: no timeout stop, on both entry points
+    q = gpu.default_params(timeout_s=600.0, max_megaiters=6, **base)
+    ref = gpu.solve(inst.F, inst.D, q)
+    assert ref["stopped_by"] == 0
+    assert same(gpu.solve_static(inst.F, inst.D, q), ref)
+
+
+def test_static_solve_leaves_free_device_memory_unchanged(gpu):
+    """The entry point's defining claim: a call allocates no device memory.  Free device memory
+    is read after warm-up calls of every shape used below (the first launch of a kernel may load
+    its module) and after the blocks that solver handles keep are released."""
+    import torch
+    shapes = [(instances.uniform(32, 321), dict(replicas=8, groups=2, max_megaiters=6, beta_max=0.05)),
+              (instances.heavy(90, 322), dict(replicas=6, groups=2, max_megaiters=3, beta_max=1e-5)),
+              (instances.grid256(323), dict(replicas=4, groups=1, max_megaiters=2, beta_max=0.002))]
+    for inst, kw in shapes:
+        gpu.solve_static(inst.F, inst.D, gpu.default_params(seed=1, **kw))
+    gpu.release_kept_memory()
+    torch.cuda.synchronize(0)
+    free0, _ = torch.cuda.mem_get_info(0)
+    for rep in range(2):
+        for inst, kw in shapes:
+            gpu.solve_static(inst.F, inst.D, gpu.default_params(seed=2 + rep, **kw))
+    torch.cuda.synchronize(0)
+    free1, _ = torch.cuda.mem_get_info(0)
+    assert free1 == free0, f"free device memory changed by {free0 - free1} bytes"
+
+
 def test_static_solve_rejects_oversized(gpu):
     inst = instances.grid256(312)
     p = gpu.default_params(replicas=64, groups=1, max_megaiters=1)   # 64 x 256 KiB of force matrices
