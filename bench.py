@@ -258,7 +258,8 @@ def run_ours(args):
                                    beta_max=BETA_MAX, beta_ratio=BETA_RATIO, beta_internal=1, seed=1 + rank,
                                    device=local, megaiters_per_launch=MEGAITERS_PER_STEP,
                                    max_megaiters=2 ** 31 - 1, cluster_size=args.cluster_size,
-                                   threads_per_block=args.threads, active_facilities=act, update_rule=rule)
+                                   threads_per_block=args.threads, active_facilities=act, update_rule=rule,
+                                   replica_pairing=args.pairing)
     flush = torch.empty(L2_FLUSH_BYTES, dtype=torch.uint8, device=f"cuda:{local}")
     solver = pimqap.Solver(inst.F, inst.D, params)
     for _ in range(args.warmup):
@@ -279,7 +280,7 @@ def run_ours(args):
                                megaiters_per_launch=4 * MEGAITERS_PER_STEP,   # fewer host round trips
                                max_megaiters=args.steps * MEGAITERS_PER_STEP,
                                cluster_size=args.cluster_size, threads_per_block=args.threads,
-                               active_facilities=act, update_rule=rule)
+                               active_facilities=act, update_rule=rule, replica_pairing=args.pairing)
     # one untimed call of the same API (one mega-iteration) takes any first-call cost of the
     # process (module loading, first graph of this shape) out of the timed call
     pw = pimqap.Params.from_buffer_copy(p2)
@@ -357,6 +358,7 @@ def run_ours(args):
             "data": "synthetic (seeded grid256 instance per GPU)",
             "config": dict(workload_config(args.workload, args.update_rule, world, args.steps),
                            cluster_size=r1["cluster_size"], force_bits=r1["force_bits"],
+                           replica_pairing=args.pairing,
                            l2="flushed between steps (256 MiB write)"),
             "candidate_deltas_per_s": cand * world / (ms_max * 1e-3),
             "accept_rate": accepts / (reps * sweeps * N),
@@ -519,7 +521,9 @@ def main():
     ap.add_argument("--update-rule", choices=["sequential", "one-shot"], default="sequential",
                     help="sequential: CPU_PIM's sweeps (the headline); one-shot: GPU-CUPIM's parallel step")
     ap.add_argument("--cluster-size", type=int, default=0, help="CTAs per replica (0 = automatic)")
-    ap.add_argument("--threads", type=int, default=0, help="threads per CTA (0 = automatic)")
+    ap.add_argument("--threads", type=int, default=0, help="threads per replica and CTA (0 = automatic)")
+    ap.add_argument("--pairing", type=int, default=0, choices=[0, 1, 2],
+                    help="replicas per CTA set of the binary-flow kernel: 0 = automatic, 1, 2")
     ap.add_argument("--suite", choices=["headline", "batch", "serve"], default="headline",
                     help="headline: the n=256 workload (the driver's line); batch / serve: the other workloads")
     ap.add_argument("--batch-instances", type=int, default=512, help="batch suite: instances")

@@ -107,6 +107,13 @@ typedef struct pimqap_params {
                                     larger delta and the surviving swaps apply together; a
                                     "sweep" is then one such step.  pimqap_solve / solver
                                     handles only */
+    int32_t replica_pairing;     /* binary-flow instances (symmetric 0/1 flows, int16 distances):
+                                    0 = automatic (one replica per CTA set: measured faster),
+                                    1 = one replica per CTA (or cluster), 2 = two replicas of
+                                    the instance per CTA (or cluster), each on half of its warps
+                                    over one shared copy of the instance, so their update chains
+                                    interleave.  Same results either way.  pimqap_solve / solver
+                                    handles only */
 } pimqap_params;
 
 #define PIMQAP_RULE_SEQUENTIAL 0

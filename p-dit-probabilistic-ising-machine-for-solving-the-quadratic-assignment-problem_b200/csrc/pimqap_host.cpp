@@ -241,7 +241,7 @@ struct pimqap_solver {
     pimqap_params p{};
     int n = 0, T = 0, R = 0, cap = 0, spe = 0;
     int bits = 32, cl = 1, threads = 256;
-    bool sym = false, bin = false;
+    bool sym = false, bin = false, pair = false;
     size_t smem = 0;
     int device = 0;
     cudaStream_t stream = nullptr;
@@ -311,6 +311,8 @@ pimqap_status check_params(const pimqap_instance *inst, const pimqap_params *p) 
         return fail(PIMQAP_ERR_ARG, "threads_per_block must be 0, 64, 128 or 256 (or 512 with the one-shot rule)");
     if (p->cluster_size != 0 && p->cluster_size != 1 && p->cluster_size != 2 && p->cluster_size != 4)
         return fail(PIMQAP_ERR_ARG, "cluster_size must be 0, 1, 2 or 4");
+    if (p->replica_pairing < 0 || p->replica_pairing > 2)
+        return fail(PIMQAP_ERR_ARG, "replica_pairing must be 0 (automatic), 1 (off) or 2 (on)");
     return PIMQAP_OK;
 }
 
@@ -428,6 +430,32 @@ pimqap_status plan_instance(const pimqap_instance *inst, const pimqap_params *pa
     P.h2d_bytes = (int64_t)P.head;
     *out = P;
     return PIMQAP_OK;
+}
+
+pimqap_status plan_pairing(const pimqap_instance *inst, const pimqap_params *params, size_t maxsm,
+                           Plan *P) {
+    // Automatic mode does not pair: with one replica per update chain the throughput is set by
+    // the chain's latency, and on the n = 256 workload two chains per 4-CTA cluster measured
+    // 2.64e9 proposals/s against 2.95e9 for one chain per 2-CTA cluster.
+    if (params->replica_pairing != 2) return PIMQAP_OK;
+    // the unpaired plan may use the generic kernel where the binary-flow layout needs a larger
+    // cluster than the generic one: every cluster size is tried for the pair
+    if (!P->os_chunk && (int64_t)P->T * P->R >= 2) {
+        for (int cl : {1, 2, 4}) {
+            if (cl < P->cl || (params->cluster_size && cl != params->cluster_size)) continue;
+            Plan Q;
+            if (plan_instance(inst, params, maxsm, cl, &Q) != PIMQAP_OK || !Q.bin) continue;
+            const size_t sp = pimqap::epoch_smem_bytes_bin_pair(Q.n, Q.rpc, Q.lds, cl);
+            if (sp > maxsm) continue;
+            Q.pair = true;
+            Q.smem_bin = sp;
+            *P = Q;
+            return PIMQAP_OK;
+        }
+    }
+    return fail(PIMQAP_ERR_ARG, "replica_pairing = 2 needs the binary-flow kernel (symmetric 0/1 flows, "
+                                "int16 distances, int32 forces, sequential rule, at least two replicas) "
+                                "and a paired layout that fits the cluster size");
 }
 
 void carve_instance(const Plan &P, char *head, char *tail, SolveDev *out) {
@@ -686,6 +714,9 @@ pimqap_status pimqap_solver_create(const pimqap_instance *inst, const pimqap_par
     Plan plan;
     st = plan_instance(inst, params, (size_t)maxsm, params->cluster_size, &plan);
     if (st != PIMQAP_OK) return st;
+    st = plan_pairing(inst, params, (size_t)maxsm, &plan);
+    if (st != PIMQAP_OK) return st;
+    s->pair = plan.pair;
     s->n = plan.n;
     s->T = plan.T;
     s->R = plan.R;
@@ -753,7 +784,7 @@ pimqap_status pimqap_solver_run(pimqap_solver *s, int64_t megaiters, double *dev
             PQ_CUDA(cudaStreamBeginCapture(s->stream, cudaStreamCaptureModeThreadLocal));
             for (int k = 0; k < g; ++k) {
                 cudaError_t e = pimqap::launch_epoch(s->dev, s->bits, s->cl, s->sym, s->bin, s->threads,
-                                                     s->smem, s->stream);
+                                                     s->smem, s->stream, s->pair);
                 if (e != cudaSuccess) {
                     cudaStreamEndCapture(s->stream, &graph);
                     return fail(PIMQAP_ERR_CUDA, std::string("epoch launch: ") + cudaGetErrorString(e));

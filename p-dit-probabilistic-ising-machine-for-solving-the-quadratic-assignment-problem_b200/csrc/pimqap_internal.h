@@ -187,9 +187,14 @@ void set_last_error(const char *msg);
 size_t epoch_smem_bytes(int n, int rpc, int lds, int cluster, int bits);
 // Shared memory of the binary-flow epoch kernel (0 / 1 flows and int16 distances resident).
 size_t epoch_smem_bytes_bin(int n, int rpc, int lds, int cluster);
+// Shared memory of the paired binary-flow epoch kernel (two replicas per CTA set).
+size_t epoch_smem_bytes_bin_pair(int n, int rpc, int lds, int cluster);
 // Shared memory of the one-shot epoch kernel (force update in chunks of `chunk` swaps).
 size_t epoch_smem_bytes_os(int n, int rpc, int lds, int cluster, int bits, int chunk, bool sym, bool xcol,
                            bool mma);
+
+// Resident clusters (CTAs for cl == 1) of the paired binary-flow epoch on the whole device.
+cudaError_t pair_occupancy(int cl, int threads, size_t smem, int *clusters);
 
 // One-time kernel attributes (dynamic shared memory, non-portable cluster size).
 cudaError_t prepare_kernels();
@@ -198,8 +203,9 @@ cudaError_t prepare_kernels();
 // exchange step of mega-iteration 0 (which also records start_ns).
 cudaError_t launch_setup(const SolveDev &s, int bits, cudaStream_t st);
 
-// One epoch: spe sweeps of every replica, then each group's tracking + exchange.
+// One epoch: spe sweeps of every replica, then each group's tracking + exchange.  pair: the
+// binary-flow kernel with two replicas per CTA set (threads per replica; smem of the pair).
 cudaError_t launch_epoch(const SolveDev &s, int bits, int cluster, bool sym, bool bin, int threads,
-                         size_t smem, cudaStream_t st);
+                         size_t smem, cudaStream_t st, bool pair = false);
 
 }  // namespace pimqap

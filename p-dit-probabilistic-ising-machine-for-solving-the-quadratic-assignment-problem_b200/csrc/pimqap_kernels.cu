@@ -873,10 +873,13 @@ __device__ bool replica_epoch(const SolveDev &s, int rep, int rank, int e, const
 // rows, so no update waits for a row from L2.
 constexpr int kBinLog = 16;   // accepted swaps the binary-flow epoch keeps before rewriting its rows
 
+//   inst = false: the replica's own section only (no Ds / Fb), for two replicas of one
+//   instance that share one copy of the instance tables (BinPairLayout).
 struct BinLayout {
     size_t I, phi, inv, bphi, Dd, A, B, Ds, Fb, LU, V8, red, wsum, r, misc, bar, total;
-    __host__ __device__ BinLayout(int n, int rpc, int lds, int cluster) {
+    __host__ __device__ BinLayout(int n, int rpc, int lds, int cluster, bool inst = true) {
         const size_t npad = (size_t)((n + 3) & ~3), rp = (size_t)rpc, nw = (size_t)((n + 31) / 32);
+        const size_t ni = inst ? (size_t)n : 0;
         size_t o = 0;
         I = o;     o = align16(o + rp * lds * 4);
         phi = o;   o = align16(o + npad * 4);
@@ -885,8 +888,8 @@ struct BinLayout {
         Dd = o;    o = align16(o + npad * 4);
         A = o;     o = align16(o + 2 * npad * 4);
         B = o;     o = align16(o + (cluster > 1 ? 2 * npad * 4 : 0));
-        Ds = o;    o = align16(o + (size_t)n * rp * 2);   // Ds[r][k] = D[r][row0 + k]
-        Fb = o;    o = align16(o + (size_t)n * nw * 4);   // bit b % 32 of Fb[a][b / 32] = F[a][b]
+        Ds = o;    o = align16(o + ni * rp * 2);   // Ds[r][k] = D[r][row0 + k]
+        Fb = o;    o = align16(o + ni * nw * 4);   // bit b % 32 of Fb[a][b / 32] = F[a][b]
         LU = o;    o = align16(o + (size_t)kBinLog * rp * 4);   // LU[p][k] = 2 (D[k][j_p] - D[k][i_p])
         V8 = o;    o = align16(o + (size_t)kBinLog * npad);     // V8[p][c] = F[b_p][c] - F[a_p][c]
         red = o;   o = align16(o + kMaxWarps * 8);
@@ -898,8 +901,49 @@ struct BinLayout {
     }
 };
 
+// Two replicas of one instance per CTA (the paired binary-flow epoch): the instance tables
+// Ds / Fb once, then one replica section per replica.  Each replica is run by half of the CTA's
+// warps with its own named barrier, so the two update chains interleave on the SM and each
+// hides the other's barrier and shared-memory latency.
+struct BinPairLayout {
+    size_t Ds, Fb, rep[2], total;
+    __host__ __device__ BinPairLayout(int n, int rpc, int lds, int cluster) {
+        const size_t rp = (size_t)rpc, nw = (size_t)((n + 31) / 32);
+        const size_t slice = BinLayout(n, rpc, lds, cluster, false).total;
+        size_t o = 0;
+        Ds = o;     o = align16(o + (size_t)n * rp * 2);
+        Fb = o;     o = align16(o + (size_t)n * nw * 4);
+        rep[0] = o; o += slice;
+        rep[1] = o; o += slice;
+        total = o;
+    }
+};
+
 size_t epoch_smem_bytes_bin(int n, int rpc, int lds, int cluster) {
     return BinLayout(n, rpc, lds, cluster).total;
+}
+
+size_t epoch_smem_bytes_bin_pair(int n, int rpc, int lds, int cluster) {
+    return BinPairLayout(n, rpc, lds, cluster).total;
+}
+
+// The binary-flow instance tables of cluster rank `rank` in shared memory: Ds[r][k] =
+// D[r][row0 + k] for the CTA's rows (int16) and F as bit rows.  Run by threads tid = 0..BT-1.
+__device__ __forceinline__ void load_bin_instance(const SolveDev &s, int rank, int tid, int BT, int lane,
+                                                  int warp, int nwarps, int16_t *s_Ds, uint32_t *s_Fb) {
+    const int n = s.n, rpc = s.rpc, ldm = s.ldm, nw = (n + 31) / 32;
+    const int row0 = rank * rpc;
+    const int rows = max(0, min(rpc, n - row0));
+    for (int idx = tid; idx < n * rows; idx += BT) {
+        const int r = idx / rows, k = idx - r * rows;
+        s_Ds[(size_t)r * rpc + k] = (int16_t)__ldcg(s.D + (size_t)r * ldm + row0 + k);
+    }
+    for (int widx = warp; widx < n * nw; widx += nwarps) {
+        const int r = widx / nw, w = widx - r * nw, b = 32 * w + lane;
+        const bool one = b < n && __ldcg(s.F + (size_t)r * ldm + b) != 0;
+        const unsigned bits = __ballot_sync(0xffffffffu, one);
+        if (lane == 0) s_Fb[widx] = bits;
+    }
 }
 
 // One epoch of replica rep for a symmetric instance whose flows are 0 / 1 and whose distances
@@ -907,9 +951,13 @@ size_t epoch_smem_bytes_bin(int n, int rpc, int lds, int cluster) {
 // Every delta, weight and update is the same integer / fp64 computation as replica_epoch's:
 // dd = Dii + Djj - 2 Dij, ff = Faa + Fbb - 2 Fab, and the rank-2 update
 // I[k][c] += 2 (Djk - Dik)(Fbc - Fac) (CPU_PIM.cpp:220-232, :262-268 with D = Dᵀ, F = Fᵀ).
+//   Ds_shared / Fb_shared (both or neither): the instance tables, already loaded by the caller
+//   into shared memory that another replica of the same instance uses too; smem then holds
+//   only this replica's section (BinLayout with inst = false).
 template <int CL>
 __device__ bool replica_epoch_bin(const SolveDev &s, int rep, int rank, int e, const Grp &G,
-                                  unsigned char *smem) {
+                                  unsigned char *smem, int16_t *Ds_shared = nullptr,
+                                  uint32_t *Fb_shared = nullptr) {
     using IT = int32_t;
     using U = uint32_t;
     constexpr int VEC = 4;
@@ -921,7 +969,8 @@ __device__ bool replica_epoch_bin(const SolveDev &s, int rep, int rank, int e, c
     const int rows = max(0, min(rpc, n - row0));
     const int npad = (n + 3) & ~3;
     const int nw = (n + 31) / 32;
-    const BinLayout L(n, rpc, lds, CL);
+    const bool own_inst = Ds_shared == nullptr;
+    const BinLayout L(n, rpc, lds, CL, own_inst);
     IT *sI = reinterpret_cast<IT *>(smem + L.I);
     int32_t *s_phi = reinterpret_cast<int32_t *>(smem + L.phi);
     int32_t *s_inv = reinterpret_cast<int32_t *>(smem + L.inv);
@@ -929,8 +978,8 @@ __device__ bool replica_epoch_bin(const SolveDev &s, int rep, int rank, int e, c
     int32_t *s_Dd = reinterpret_cast<int32_t *>(smem + L.Dd);
     IT *s_A = reinterpret_cast<IT *>(smem + L.A);
     IT *s_B = reinterpret_cast<IT *>(smem + L.B);
-    int16_t *s_Ds = reinterpret_cast<int16_t *>(smem + L.Ds);
-    uint32_t *s_Fb = reinterpret_cast<uint32_t *>(smem + L.Fb);
+    int16_t *s_Ds = own_inst ? reinterpret_cast<int16_t *>(smem + L.Ds) : Ds_shared;
+    uint32_t *s_Fb = own_inst ? reinterpret_cast<uint32_t *>(smem + L.Fb) : Fb_shared;
     float *s_LU = reinterpret_cast<float *>(smem + L.LU);
     int8_t *s_V8 = reinterpret_cast<int8_t *>(smem + L.V8);
     IT *s_red = reinterpret_cast<IT *>(smem + L.red);
@@ -961,16 +1010,7 @@ __device__ bool replica_epoch_bin(const SolveDev &s, int rep, int rank, int e, c
             s_inv[q] = 0;
             s_Dd[q] = q < n ? __ldcg(s.Ddiag + q) : 0;
         }
-        for (int idx = tid; idx < n * rows; idx += BT) {
-            const int r = idx / rows, k = idx - r * rows;
-            s_Ds[(size_t)r * rpc + k] = (int16_t)__ldcg(s.D + (size_t)r * ldm + row0 + k);
-        }
-        for (int widx = warp; widx < n * nw; widx += nwarps) {
-            const int r = widx / nw, w = widx - r * nw, b = 32 * w + lane;
-            const bool one = b < n && __ldcg(s.F + (size_t)r * ldm + b) != 0;
-            const unsigned bits = __ballot_sync(0xffffffffu, one);
-            if (lane == 0) s_Fb[widx] = bits;
-        }
+        if (own_inst) load_bin_instance(s, rank, tid, BT, lane, warp, nwarps, s_Ds, s_Fb);
         if (tid == 0) {
             s_misc[0] = 0x7fffffff;
             s_misc[1] = -1;
@@ -2126,6 +2166,52 @@ __global__ void __launch_bounds__(KIND == 2 ? 512 : 256, (CL == 4 && KIND != 2) 
     }
 }
 
+// The paired binary-flow epoch: cluster c of CL CTAs runs replicas 2c and 2c + 1, each on half
+// of every CTA's warps (named barriers 1 and 2) over one shared copy of the instance tables.
+// Both halves take part in the two cluster barriers of an epoch whether or not their replica
+// runs (an odd replica count leaves the last half idle; a group past its stop epoch idles).
+template <int CL>
+__global__ void __launch_bounds__(512, 1) epoch_pair_kernel(SolveDev s) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    int rank = 0;
+    if constexpr (CL > 1) rank = (int)cg::this_cluster().block_rank();
+    const BinPairLayout P(s.n, s.rpc, s.lds, CL);
+    int16_t *Ds = reinterpret_cast<int16_t *>(smem + P.Ds);
+    uint32_t *Fb = reinterpret_cast<uint32_t *>(smem + P.Fb);
+    load_bin_instance(s, rank, (int)threadIdx.x, (int)blockDim.x, (int)(threadIdx.x & 31),
+                      (int)(threadIdx.x >> 5), (int)(blockDim.x >> 5), Ds, Fb);
+    __syncthreads();
+    const int half_threads = (int)blockDim.x / 2;
+    const int h = (int)threadIdx.x / half_threads;
+    const int tid = (int)threadIdx.x - h * half_threads;
+    const Grp G{tid, half_threads, tid & 31, tid >> 5, half_threads >> 5, 1 + h};
+    const int rep = 2 * ((int)blockIdx.x / CL) + h;
+    bool run = rep < s.T * s.R;
+    int g = 0, e = 0;
+    if (run) {
+        g = rep / s.R;
+        e = *((volatile int32_t *)s.epoch + g);
+        run = e < *(volatile int32_t *)s.stop_epoch;
+    }
+    if (!run) {   // the cluster barriers of an epoch, without a replica
+        cluster_sync<CL>(G);
+        cluster_sync<CL>(G);
+        return;
+    }
+    const bool ok = replica_epoch_bin<CL>(s, rep, rank, e, G, smem + P.rep[h], Ds, Fb);
+    G.sync();
+    if (ok && rank == 0 && tid == 0) {
+        const unsigned prev = atomicAdd(s.finish + g, 1u);
+        if (prev == (unsigned)s.R - 1u) {
+            __threadfence();
+            track_exchange(s, g, e + 1);
+            s.finish[g] = 0u;
+            s.epoch[g] = e + 1;
+            __threadfence();
+        }
+    }
+}
+
 // ------------------------------------------------------------------ the batch kernel
 
 constexpr unsigned long long kQueueWaitNs = 30000000000ull;   // 30 s without any progress
@@ -2587,6 +2673,16 @@ static void *epoch_kernel_ptr(int bits, int cl, bool sym, bool gp) {
     return nullptr;
 }
 
+// The paired binary-flow epoch (two replicas per CTA set).
+static void *epoch_pair_ptr(int cl) {
+    switch (cl) {
+        case 1: return reinterpret_cast<void *>(&epoch_pair_kernel<1>);
+        case 2: return reinterpret_cast<void *>(&epoch_pair_kernel<2>);
+        case 4: return reinterpret_cast<void *>(&epoch_pair_kernel<4>);
+        default: return nullptr;
+    }
+}
+
 // The binary-flow epoch (int32 forces, symmetric instance, no goal_print events).
 static void *epoch_bin_ptr(int cl) {
     switch (cl) {
@@ -2674,6 +2770,31 @@ cudaError_t batch_occupancy(int bits, int cl, int threads, size_t smem, int *cta
     return e;
 }
 
+cudaError_t pair_occupancy(int cl, int threads, size_t smem, int *clusters) {
+    void *fn = epoch_pair_ptr(cl);
+    if (!fn) return cudaErrorInvalidValue;
+    if (cl == 1) {
+        int dev = 0, sms = 0, per = 0;
+        cudaError_t e = cudaGetDevice(&dev);
+        if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, fn, 2 * threads, smem);
+        *clusters = per * sms;
+        return e;
+    }
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3((unsigned)cl);
+    cfg.blockDim = dim3((unsigned)(2 * threads));
+    cfg.dynamicSmemBytes = smem;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = (unsigned)cl;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    return cudaOccupancyMaxActiveClusters(clusters, fn, &cfg);
+}
+
 cudaError_t prepare_kernels() {
     int dev = 0;
     cudaError_t err = cudaGetDevice(&dev);
@@ -2700,6 +2821,8 @@ cudaError_t prepare_kernels() {
     for (int cl : {1, 2, 4}) {
         err = cudaFuncSetAttribute(epoch_bin_ptr(cl), cudaFuncAttributeMaxDynamicSharedMemorySize, maxsm);
         if (err != cudaSuccess) return err;
+        err = cudaFuncSetAttribute(epoch_pair_ptr(cl), cudaFuncAttributeMaxDynamicSharedMemorySize, maxsm);
+        if (err != cudaSuccess) return err;
     }
     return cudaSuccess;
 }
@@ -2719,16 +2842,20 @@ cudaError_t launch_setup(const SolveDev &s, int bits, cudaStream_t st) {
 }
 
 cudaError_t launch_epoch(const SolveDev &s, int bits, int cluster, bool sym, bool bin, int threads,
-                         size_t smem, cudaStream_t st) {
+                         size_t smem, cudaStream_t st, bool pair) {
     const bool gp = s.ev.log != nullptr && s.ev.goal_print != 0;
-    // clique-flow solves (s.act > 0) exist only in the binary-flow kernel
+    const bool binary = bin && bits == 32 && sym && (!gp || s.act > 0);
+    pair = pair && binary;
+    // clique-flow solves (s.act > 0) exist only in the binary-flow kernels
     void *fn = s.os_chunk > 0 ? epoch_os_ptr(bits, cluster, sym, gp)
-               : (bin && bits == 32 && sym && (!gp || s.act > 0)) ? epoch_bin_ptr(cluster)
-                                                                  : epoch_kernel_ptr(bits, cluster, sym, gp);
+               : pair         ? epoch_pair_ptr(cluster)
+               : binary       ? epoch_bin_ptr(cluster)
+                              : epoch_kernel_ptr(bits, cluster, sym, gp);
     if (!fn) return cudaErrorInvalidValue;
+    const int reps = s.T * s.R;
     cudaLaunchConfig_t cfg = {};
-    cfg.gridDim = dim3((unsigned)(s.T * s.R * cluster));
-    cfg.blockDim = dim3((unsigned)threads);
+    cfg.gridDim = dim3((unsigned)((pair ? (reps + 1) / 2 : reps) * cluster));
+    cfg.blockDim = dim3((unsigned)(pair ? 2 * threads : threads));
     cfg.dynamicSmemBytes = smem;
     cfg.stream = st;
     cudaLaunchAttribute attr[1];

@@ -90,7 +90,8 @@ struct Plan {
     bool sym = false;
     bool bin = false;      // the solve path may run the binary-flow epoch kernel
     size_t smem = 0;       // epoch kernel shared memory per CTA (the generic kernel)
-    size_t smem_bin = 0;   // the binary-flow kernel's (when bin)
+    size_t smem_bin = 0;   // the binary-flow kernel's (when bin; of the pair when pair)
+    bool pair = false;     // the solve path runs two replicas per CTA set (binary-flow kernel)
     int act = 0;           // clique-flow moves with facilities 0..act-1 active (0 = off)
     int os_chunk = 0;      // > 0: the one-shot rule (swaps per force-update chunk)
     int os_xcol = 0;       // one-shot: peers push the force-matrix columns of the proposals
@@ -118,6 +119,12 @@ pimqap_status open_device(int device, int *maxsm);
 // of the force matrix fits one CTA, or want_cluster), strides and device footprint.
 pimqap_status plan_instance(const pimqap_instance *inst, const pimqap_params *params, size_t maxsm,
                             int want_cluster, Plan *out, const InstanceInfo *known = nullptr);
+
+// Solver path only: replaces *P by the paired binary-flow layout (two replicas per CTA set,
+// on the smallest cluster of at least P->cl CTAs that holds it) when params->replica_pairing
+// is 2; 0 and 1 keep one replica per CTA set.
+pimqap_status plan_pairing(const pimqap_instance *inst, const pimqap_params *params, size_t maxsm,
+                           Plan *P);
 
 // Device pointers of one instance carved from its head and tail regions.
 void carve_instance(const Plan &P, char *head, char *tail, SolveDev *out);

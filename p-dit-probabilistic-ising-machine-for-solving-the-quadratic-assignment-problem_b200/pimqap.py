@@ -50,6 +50,7 @@ class Params(C.Structure):
         ("event_capacity", C.c_int32), ("event_perm_capacity", C.c_int32),
         ("compact_instance", C.c_int32), ("active_facilities", C.c_int32),
         ("update_rule", C.c_int32),
+        ("replica_pairing", C.c_int32),
     ]
 
 

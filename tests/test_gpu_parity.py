@@ -53,7 +53,7 @@ CASES = {
     "heavy_n60": (lambda: heavy_small(60, 15), 1, 3, 1, 0.0005, 2.0, 4, {}),
     "heavy_n48": (lambda: instances.heavy(48, 16), 1, 3, 1, 1e-5, 2.0, 4, {}),
     "wide_int64_n32": (lambda: wide(32, 26), 2, 3, 2, 1e-9, 1.5, 6, {}),
-    "grid_n256_cluster": (lambda: instances.grid256(17), 1, 2, 1, 0.0015, 1.5, 2, {}),
+    "grid_n256_cluster": (lambda: instances.grid256(17), 1, 2, 1, 0.0015, 1.5, 2, {"replica_pairing": 1}),
     "grid_n256_int64_cluster4": (lambda: instances.grid256(18), 1, 1, 1, 0.0015, 1.5, 1, {"force_bits": 64}),
     "n200_single_cta": (lambda: instances.uniform(200, 19), 1, 2, 1, 0.0005, 1.5, 1, {}),
     "cold_forced_swaps": (lambda: instances.uniform(12, 20), 2, 10, 1, 40.0, 1.2, 150, {}),
@@ -81,6 +81,18 @@ CASES = {
                                 {"active_facilities": 20}),
     "clique9_n36_t64": (lambda: instances.clique_flow(37, side=6, active=9), 1, 5, 3, 0.05, 1.2, 20,
                         {"active_facilities": 9, "threads_per_block": 64}),
+    # two replicas per CTA set (replica_pairing = 2): the binary-flow epoch on half of the warps
+    # each, over one shared copy of the instance; odd replica counts leave a half idle, and pairs
+    # may span two groups
+    "grid_n256_pair": (lambda: instances.grid256(17), 1, 4, 2, 0.0015, 1.5, 2, {"replica_pairing": 2}),
+    "grid_n256_pair_odd": (lambda: instances.grid256(27), 1, 3, 1, 0.002, 1.4, 3, {"replica_pairing": 2}),
+    "binary_n90_pair_groups": (lambda: binary(90, 32), 2, 3, 2, 0.01, 1.4, 4, {"replica_pairing": 2}),
+    "binary_n200_pair_t128": (lambda: binary(200, 34, 30000), 1, 4, 1, 0.0001, 1.5, 2,
+                              {"replica_pairing": 2, "threads_per_block": 128}),
+    "binary_n64_pair_t64": (lambda: binary(64, 39), 1, 5, 3, 0.02, 1.3, 5,
+                            {"replica_pairing": 2, "threads_per_block": 64}),
+    "clique92_n256_pair": (lambda: instances.clique_flow(35), 2, 3, 1, 0.002, 1.5, 3,
+                           {"active_facilities": 92, "replica_pairing": 2}),
     # the heavy-tailed workload unscaled (lognormal flows, 70 % zeros, Euclidean distances),
     # full 4-sweep epochs at n = 100, 180 and 256 on the heavy ladder (2^-13 internal), int32 and
     # int64 force matrices, clusters of 1, 2 and 4
@@ -114,7 +126,8 @@ def run_case(gpu, oracle, name, seed=7):
 # (force width, cluster size) that a case is meant to cover
 SHAPES = {"heavy_n100_i4": (32, 1), "heavy_n180_cluster2_i4": (32, 2), "heavy_n256_i4": (32, 2),
           "heavy_n256_cluster4_i4": (32, 4), "heavy_n256_int64_i4": (64, 4),
-          "heavy_n213_int64_cluster4_i4": (64, 4)}
+          "heavy_n213_int64_cluster4_i4": (64, 4), "grid_n256_pair": (32, 4), "grid_n256_pair_odd": (32, 4),
+          "binary_n90_pair_groups": (32, 1), "clique92_n256_pair": (32, 4)}
 
 
 @pytest.mark.parametrize("name", list(CASES))
@@ -227,12 +240,14 @@ HEADLINE_B0 = 2.0 ** -5
 HEADLINE_RATIO = 1.0671404006768237
 
 
-def test_headline_configuration_matches_oracle(gpu, oracle):
+@pytest.mark.parametrize("pairing", [1, 2])
+def test_headline_configuration_matches_oracle(gpu, oracle, pairing):
+    """pairing 1: one replica per 2-CTA cluster; 2: two replicas per 4-CTA cluster."""
     inst = instances.grid256(1000)
     M = 50
     p = gpu.default_params(replicas=64, groups=1, sweeps_per_exchange=4, beta_max=HEADLINE_B0,
                            beta_ratio=HEADLINE_RATIO, beta_internal=1, seed=1, max_megaiters=2 ** 31 - 1,
-                           megaiters_per_launch=25)
+                           megaiters_per_launch=25, replica_pairing=pairing)
     with gpu.Solver(inst.F, inst.D, p) as s:
         s.run(25)
         s.run(25)
@@ -241,7 +256,31 @@ def test_headline_configuration_matches_oracle(gpu, oracle):
         oracle.track_exchange_all(st)
         bad = compare_solver_to_oracle(s, st, 64)
         res = s.result()
-    assert (res["force_bits"], res["cluster_size"]) == (32, 2)
+    assert (res["force_bits"], res["cluster_size"]) == (32, 2 * pairing)
     assert not bad, bad[:10]
     assert res["accepts"] == st.accepts
     assert res["accepts"] > 0.9 * 64 * 4 * M * 256
+
+
+def test_pairing_takes_the_same_trajectory(gpu):
+    """replica_pairing changes the launch shape only (0 = automatic, which does not pair)."""
+    inst = instances.grid256(77)
+    out = []
+    for pairing in (0, 1, 2):
+        p = gpu.default_params(replicas=8, groups=1, sweeps_per_exchange=2, beta_max=0.002, beta_ratio=1.3,
+                               seed=4, max_megaiters=3, replica_pairing=pairing)
+        r = gpu.solve(inst.F, inst.D, p)
+        out.append((r["best_energy"], r["accepts"], r["best_perm"].tobytes()))
+    assert out[0] == out[1] == out[2]
+
+
+def test_pairing_is_rejected_where_it_cannot_run(gpu):
+    inst = instances.uniform(40, 78)                 # not 0/1 flows: no binary-flow kernel
+    p = gpu.default_params(replicas=4, groups=1, beta_max=0.02, max_megaiters=1, replica_pairing=2)
+    with pytest.raises(gpu.PimqapError) as e:
+        gpu.solve(inst.F, inst.D, p)
+    assert e.value.status == 1 and "replica_pairing" in str(e.value)
+    g = instances.grid256(79)
+    p = gpu.default_params(replicas=1, groups=1, beta_max=0.002, max_megaiters=1, replica_pairing=2)
+    with pytest.raises(gpu.PimqapError):             # one replica: nothing to pair
+        gpu.solve(g.F, g.D, p)
