@@ -8,7 +8,9 @@ single-instance workload), 64 replicas on one geometric beta ladder, replica exc
 4 sweeps (the reference's NUMITERA default), 10^4 sweeps = 100 steps of 100 sweeps.
 
 A "step" is 25 mega-iterations = 100 sweeps of all 64 replicas.  Proposals are counted as
-the published metric defines them: n (n - 1) / 2 per sweep per replica.
+the published metric defines them: n (n - 1) / 2 per sweep per replica.  --workload cfg1 runs
+the reference's CPU-sized case instead (n = 32, 16 replicas, exchange every sweep; a step is
+100 sweeps, so --steps 10 is its 1000 sweeps); --workload clique92 the tai256c structure.
 
   value       device-timed throughput with the instance resident in HBM (CUDA events on
               the solver's stream, L2 flushed between steps, max over ranks)
@@ -42,7 +44,6 @@ import instances  # noqa: E402
 
 N = 256
 REPLICAS = 64
-GROUPS = 1
 SWEEPS_PER_EXCHANGE = 4
 MEGAITERS_PER_STEP = 25
 # Geometric ladder chosen by the reference's automatic mode (pimqap_auto_beta on this
@@ -57,6 +58,32 @@ METRIC = "swap proposals/sec"
 UNIT = "proposals/s"
 L2_FLUSH_BYTES = 256 << 20
 E2E_SOLVES = 3                  # end-to-end solves timed; the median wall is reported
+
+
+# Workloads of the headline line.  grid256 is the driver's default (the published single-GPU
+# configuration); clique92 is the structure the reference's tai256c program is written for;
+# cfg1 is the reference's own CPU-sized case (n = 32, 16 replicas, beta 0.01 .. 10 natural,
+# exchange every sweep, 1000 sweeps).
+WORKLOADS = {
+    "grid256": dict(n=N, replicas=REPLICAS, spe=SWEEPS_PER_EXCHANGE, megaiters_per_step=MEGAITERS_PER_STEP,
+                    beta0=BETA_MAX, ratio=BETA_RATIO, act=0,
+                    instance=lambda rank: instances.grid256(1000 + rank),
+                    ladder="reference automatic mode on this instance (pimqap_auto_beta, seed 1), then fixed",
+                    desc="grid256: n=256 Bernoulli(0.36) flow, 16x16 grid sq. distance + U[0,3]; 64 replicas, "
+                         "geometric beta ladder, exchange every 4 sweeps"),
+    "clique92": dict(n=N, replicas=REPLICAS, spe=SWEEPS_PER_EXCHANGE, megaiters_per_step=MEGAITERS_PER_STEP,
+                     beta0=BETA_MAX, ratio=BETA_RATIO, act=92,
+                     instance=lambda rank: instances.clique_flow(1000 + rank),
+                     ladder="the grid256 ladder",
+                     desc="clique92: n=256, unit flows among facilities 0..91, 16x16 grid sq. distance + U[0,3]; "
+                          "the tai256c program's moves; 64 replicas, geometric beta ladder, exchange every 4 sweeps"),
+    "cfg1": dict(n=32, replicas=16, spe=1, megaiters_per_step=100,
+                 beta0=10.0 * 1.44269504089, ratio=1.5849, act=0,
+                 instance=lambda rank: instances.uniform(32, 1000 + rank),
+                 ladder="geometric 0.01 .. 10 in natural units (-b 10 -m 1.5849)",
+                 desc="cfg1: n=32, symmetric uniform [0,99] flow and distance, zero diagonal; 16 replicas, "
+                      "beta 0.01 .. 10 natural, exchange every sweep; the published 1000 sweeps are --steps 10"),
+}
 
 
 def proposals(replicas: int, sweeps: int, n: int = N) -> float:
@@ -126,7 +153,7 @@ class ClockSampler:
 
 # ------------------------------------------------------------------ reference CPU timing
 
-def ref_cpu_throughput(F, D, budget_s: float, replicas: int = REPLICAS):
+def ref_cpu_throughput(F, D, budget_s: float, W: dict):
     """The reference's threadToRun on one thread per host core for ~budget_s seconds.
     Returns (proposals/s, cores, kind, sample description) or None."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
@@ -136,33 +163,32 @@ def ref_cpu_throughput(F, D, budget_s: float, replicas: int = REPLICAS):
     ref = RefHarness("big_mt")
     cores = max(1, min(os.cpu_count() or 1, ref.maxt))
     ref.load(F, D)
-    ref.setup_replicated(cores, replicas, SWEEPS_PER_EXCHANGE, BETA_MAX, BETA_RATIO, 1)
+    ref.setup_replicated(cores, W["replicas"], W["spe"], W["beta0"], W["ratio"], 1)
     t1 = ref.run(1)
     m = max(1, int(budget_s / max(t1, 1e-3)))
     el = ref.run(m)
-    sweeps = m * SWEEPS_PER_EXCHANGE
-    val = proposals(cores * replicas, sweeps) / el
-    sample = (f"{cores} threads x {replicas} replicas of the n=256 instance, {sweeps} sweeps each "
-              f"({m} mega-iterations of 4 sweeps), {el:.1f} s")
+    sweeps = m * W["spe"]
+    val = proposals(cores * W["replicas"], sweeps, W["n"]) / el
+    sample = (f"{cores} threads x {W['replicas']} replicas of the n={W['n']} instance, {sweeps} sweeps each "
+              f"({m} mega-iterations of {W['spe']} sweeps), {el:.1f} s")
     return val, cores, "reference", sample
 
 
-def workload_config(workload, update_rule, world, steps):
+def workload_config(workload, update_rule, world, steps, groups=1):
     """The workload part of the line's config, the same in both arms; it names the sweeps the
-    timed region actually runs (the published configuration's 10^4 sweeps are --steps 100)."""
-    sweeps = steps * MEGAITERS_PER_STEP * SWEEPS_PER_EXCHANGE
-    return {"workload": ("grid256: n=256 Bernoulli(0.36) flow, 16x16 grid sq. distance + U[0,3]; "
-                         if workload == "grid256" else
-                         "clique92: n=256, unit flows among facilities 0..91, 16x16 grid sq. "
-                         "distance + U[0,3]; the tai256c program's moves; ") +
-                        "64 replicas, geometric beta ladder, exchange every 4 sweeps, "
-                        f"{sweeps} sweeps timed ({steps} steps of 100)" +
+    timed region actually runs.  groups > 1: that many independent parallel-tempering groups of
+    the workload's replicas (the reference's -t threads) on each GPU."""
+    W = WORKLOADS[workload]
+    sweeps = steps * W["megaiters_per_step"] * W["spe"]
+    return {"workload": W["desc"] + f"; {sweeps} sweeps timed ({steps} steps of "
+                                     f"{W['megaiters_per_step'] * W['spe']})" +
                         ("; GPU-CUPIM's one-shot rule (a sweep = one parallel step)"
                          if update_rule == "one-shot" else ""),
             "update_rule": update_rule,
-            "n": N, "replicas": REPLICAS * GROUPS, "sweeps_per_step": MEGAITERS_PER_STEP * SWEEPS_PER_EXCHANGE,
-            "beta0_internal": BETA_MAX, "beta_ratio": BETA_RATIO,
-            "ladder": "reference automatic mode on this instance (pimqap_auto_beta, seed 1), then fixed",
+            "n": W["n"], "replicas": W["replicas"] * groups, "groups": groups,
+            "sweeps_per_step": W["megaiters_per_step"] * W["spe"], "sweeps_per_exchange": W["spe"],
+            "beta0_internal": W["beta0"], "beta_ratio": W["ratio"],
+            "ladder": W["ladder"],
             "sweeps_timed": sweeps,
             "parallelism": f"instances x{world}"}
 
@@ -173,20 +199,21 @@ def run_reference(args):
         return
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     from oracle import RefHarness, ref_available
-    if args.workload != "grid256" or args.update_rule != "sequential":
-        print(json.dumps({"impl": "reference", "unavailable": "the reference arm times the grid256 workload "
-                                                              "with the sequential rule (CPU_PIM.cpp) only"}))
+    if args.workload == "clique92" or args.update_rule != "sequential":
+        print(json.dumps({"impl": "reference", "unavailable": "the reference arm times the grid256 and cfg1 "
+                                                              "workloads with the sequential rule (CPU_PIM.cpp) only"}))
         return
-    cfg = dict(workload_config(args.workload, args.update_rule, 1, args.steps),
+    W = WORKLOADS[args.workload]
+    cfg = dict(workload_config(args.workload, args.update_rule, 1, args.steps, args.groups),
                parallelism="host threads (the reference's CPU program; no GPU)")
     if not ref_available("big_mt"):
         print(json.dumps({"impl": "reference", "unavailable": "reference CPU_PIM.cpp not built (oracle/_ref missing)"}))
         return
-    inst = instances.grid256(1000)
+    inst = W["instance"](0)
     ref = RefHarness("big_mt")
     cores = max(1, min(os.cpu_count() or 1, ref.maxt))
     ref.load(inst.F, inst.D)
-    ref.setup_replicated(cores, REPLICAS, SWEEPS_PER_EXCHANGE, BETA_MAX, BETA_RATIO, 1)
+    ref.setup_replicated(cores, W["replicas"], W["spe"], W["beta0"], W["ratio"], 1)
     t1 = ref.run(1)
     # each step a bounded sample: the whole run stays within ~3 minutes
     per_step = min(2.0, 180.0 / max(1, args.steps + args.warmup))
@@ -196,14 +223,14 @@ def run_reference(args):
     total = 0.0
     for _ in range(args.steps):
         total += ref.run(m)
-    sweeps = args.steps * m * SWEEPS_PER_EXCHANGE
-    val = proposals(cores * REPLICAS, sweeps) / total
-    sample = (f"each step {m} mega-iterations (4 sweeps each) of {cores} groups x {REPLICAS} replicas "
-              f"of the n=256 instance; one group per host thread")
+    sweeps = args.steps * m * W["spe"]
+    val = proposals(cores * W["replicas"], sweeps, W["n"]) / total
+    sample = (f"each step {m} mega-iterations ({W['spe']} sweeps each) of {cores} groups x {W['replicas']} "
+              f"replicas of the n={W['n']} instance; one group per host thread")
     line = {"impl": "reference", "metric": METRIC, "value": val, "unit": UNIT, "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * total / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int32",
-            "data": "synthetic (seeded grid256 instance)", "config": cfg,
+            "data": f"synthetic (seeded {args.workload} instance)", "config": cfg,
             "cpu_baseline": {"value": val, "unit": UNIT, "cores": cores, "kind": "reference", "sample": sample},
             "e2e": {"value": val, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
             "note": "the reference's CPU program on this host's cores; no GPU is used at any n_gpus"}
@@ -214,11 +241,8 @@ def run_reference(args):
 
 def rank_instance(rank, workload="grid256"):
     """The instance rank `rank` solves: one instance per GPU (the work is sharded by
-    instance; ranks never exchange data).  clique92: the structure of the reference's tai256c
-    program (unit flows among 92 of 256 facilities), solved with its moves."""
-    if workload == "clique92":
-        return instances.clique_flow(1000 + rank)
-    return instances.grid256(1000 + rank)
+    instance; ranks never exchange data)."""
+    return WORKLOADS[workload]["instance"](rank)
 
 
 def max_over_ranks(x, world, device):
@@ -251,19 +275,20 @@ def run_ours(args):
         import datetime
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
 
+    W = WORKLOADS[args.workload]
+    n, reps, spe, MPS = W["n"], W["replicas"] * args.groups, W["spe"], W["megaiters_per_step"]
     inst = rank_instance(rank, args.workload)
-    act = 92 if args.workload == "clique92" else 0
     rule = pimqap.RULE_ONE_SHOT if args.update_rule == "one-shot" else pimqap.RULE_SEQUENTIAL
-    params = pimqap.default_params(replicas=REPLICAS, groups=GROUPS, sweeps_per_exchange=SWEEPS_PER_EXCHANGE,
-                                   beta_max=BETA_MAX, beta_ratio=BETA_RATIO, beta_internal=1, seed=1 + rank,
-                                   device=local, megaiters_per_launch=MEGAITERS_PER_STEP,
-                                   max_megaiters=2 ** 31 - 1, cluster_size=args.cluster_size,
-                                   threads_per_block=args.threads, active_facilities=act, update_rule=rule,
-                                   replica_pairing=args.pairing)
+    common = dict(replicas=W["replicas"], groups=args.groups, sweeps_per_exchange=spe, beta_max=W["beta0"],
+                  beta_ratio=W["ratio"], beta_internal=1, seed=1 + rank, device=local,
+                  cluster_size=args.cluster_size, threads_per_block=args.threads,
+                  active_facilities=W["act"], update_rule=rule, replica_pairing=args.pairing,
+                  launch_mode=args.launch_mode)
+    params = pimqap.default_params(megaiters_per_launch=MPS, max_megaiters=2 ** 31 - 1, **common)
     flush = torch.empty(L2_FLUSH_BYTES, dtype=torch.uint8, device=f"cuda:{local}")
     solver = pimqap.Solver(inst.F, inst.D, params)
     for _ in range(args.warmup):
-        solver.run(MEGAITERS_PER_STEP)
+        solver.run(MPS)
     r0 = solver.result()
 
     def barrier():
@@ -274,13 +299,8 @@ def run_ours(args):
     # before the clock sampler's process runs
     Fp = torch.from_numpy(inst.F).pin_memory()
     Dp = torch.from_numpy(inst.D).pin_memory()
-    p2 = pimqap.default_params(replicas=REPLICAS, groups=GROUPS, sweeps_per_exchange=SWEEPS_PER_EXCHANGE,
-                               beta_max=BETA_MAX, beta_ratio=BETA_RATIO, beta_internal=1, seed=1 + rank,
-                               device=local,
-                               megaiters_per_launch=4 * MEGAITERS_PER_STEP,   # fewer host round trips
-                               max_megaiters=args.steps * MEGAITERS_PER_STEP,
-                               cluster_size=args.cluster_size, threads_per_block=args.threads,
-                               active_facilities=act, update_rule=rule, replica_pairing=args.pairing)
+    p2 = pimqap.default_params(megaiters_per_launch=4 * MPS,   # fewer host round trips
+                               max_megaiters=args.steps * MPS, **common)
     # one untimed call of the same API (one mega-iteration) takes any first-call cost of the
     # process (module loading, first graph of this shape) out of the timed call
     pw = pimqap.Params.from_buffer_copy(p2)
@@ -296,8 +316,8 @@ def run_ours(args):
         e_runs.append((time.perf_counter() - e0, res))
     e_walls = [w for w, _ in e_runs]
     e_wall, res = sorted(e_runs, key=lambda x: x[0])[len(e_runs) // 2]
-    e2e_sweeps = args.steps * MEGAITERS_PER_STEP * SWEEPS_PER_EXCHANGE
-    e2e_value = whole_job_rate(proposals(REPLICAS * GROUPS, e2e_sweeps), world,
+    e2e_sweeps = args.steps * MPS * spe
+    e2e_value = whole_job_rate(proposals(reps, e2e_sweeps, n), world,
                                max_over_ranks(e_wall, world, f"cuda:{local}"))
 
     ms_total = 0.0
@@ -308,46 +328,46 @@ def run_ours(args):
         for _ in range(args.steps):
             flush.zero_()
             torch.cuda.synchronize()
-            ms_total += solver.run(MEGAITERS_PER_STEP)
+            ms_total += solver.run(MPS)
         torch.cuda.synchronize()
         barrier()
         wall = time.perf_counter() - w0
     r1 = solver.result()
     solver.close()
     ms_max = max_over_ranks(ms_total, world, f"cuda:{local}")
-    sweeps = args.steps * MEGAITERS_PER_STEP * SWEEPS_PER_EXCHANGE
-    reps = REPLICAS * GROUPS
-    value = whole_job_rate(proposals(reps, sweeps), world, ms_max * 1e-3)
+    sweeps = args.steps * MPS * spe
+    value = whole_job_rate(proposals(reps, sweeps, n), world, ms_max * 1e-3)
 
     # roofline of the sweep kernel (every timed launch is that kernel)
     accepts = r1["accepts"] - r0["accepts"]
-    cand = float(reps) * sweeps * N * N
+    cand = float(reps) * sweeps * n * n
     s = r1["force_bits"] // 8
     if rule == pimqap.RULE_ONE_SHOT:
         # one read-modify-write of the force matrix per replica step, whatever the number of
         # swaps it applies, plus the swaps' D / F rows
-        alg_bytes = (3 * s + 20) * cand + 2 * N * N * s * float(reps) * sweeps + 32 * N * float(accepts)
+        alg_bytes = (3 * s + 20) * cand + 2 * n * n * s * float(reps) * sweeps + 32 * n * float(accepts)
         bytes_model = f"({3 * s}+20) B per candidate delta + 2 n^2 {s} B per replica step + 32 n B per accept"
     else:
-        alg_bytes = (3 * s + 20) * cand + (2 * N * N * s + 32 * N) * float(accepts)
+        alg_bytes = (3 * s + 20) * cand + (2 * n * n * s + 32 * n) * float(accepts)
         bytes_model = f"({3 * s}+20) B per candidate delta + (2 n^2 {s} + 32 n) B per accept"
-    launches = args.steps * MEGAITERS_PER_STEP
+    launches = r1["launches"] - r0["launches"]
+    persistent = launches == args.steps
     achieved = alg_bytes / (ms_total * 1e-3) / 1e9
     smem_peak = pimqap.probe_smem_bandwidth(local)
-    # HBM bytes every launch moves by construction: each replica's state is loaded into shared
-    # memory and stored back (force rows, permutation, best permutation; the scalars are noise),
-    # and every CTA stages the instance (the binary-flow kernel: D rows and F as bits, read as
-    # int32 rows).  Measured DRAM bytes come from ncu captures, not from this run.
+    # HBM bytes every mega-iteration moves by construction: each replica's state is loaded into
+    # shared memory and stored back (force rows, permutation, best permutation; the scalars are
+    # noise), and every CTA stages the instance (D and F rows read as int32).  Measured DRAM bytes
+    # come from ncu captures, not from this run.
     cl = r1["cluster_size"]
-    npad = (N + 3) & ~3
-    state_bytes = reps * (2 * N * npad * s + 3 * N * 4)
-    stage_bytes = reps * cl * 2 * N * npad * 4
+    npad = (n + 3) & ~3
+    state_bytes = reps * (2 * n * npad * s + 3 * n * 4)
+    stage_bytes = reps * cl * 2 * n * npad * 4
 
     line = None
     if rank == 0:
         cpu = None
-        if world == 1 and not args.no_cpu_baseline and args.workload == "grid256" and rule == 0:
-            got = ref_cpu_throughput(inst.F, inst.D, budget_s=12.0)
+        if world == 1 and not args.no_cpu_baseline and args.workload != "clique92" and rule == 0:
+            got = ref_cpu_throughput(inst.F, inst.D, 12.0, W)
             if got:
                 v, cores, kind, sample = got
                 cpu = {"value": v, "unit": UNIT, "cores": cores, "kind": kind, "sample": sample}
@@ -355,13 +375,15 @@ def run_ours(args):
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": f"int{8 * s}",
-            "data": "synthetic (seeded grid256 instance per GPU)",
-            "config": dict(workload_config(args.workload, args.update_rule, world, args.steps),
+            "data": f"synthetic (seeded {args.workload} instance per GPU)",
+            "config": dict(workload_config(args.workload, args.update_rule, world, args.steps, args.groups),
                            cluster_size=r1["cluster_size"], force_bits=r1["force_bits"],
                            replica_pairing=args.pairing,
+                           launch="one persistent launch per step" if persistent else
+                                  "a CUDA graph of one launch per mega-iteration",
                            l2="flushed between steps (256 MiB write)"),
             "candidate_deltas_per_s": cand * world / (ms_max * 1e-3),
-            "accept_rate": accepts / (reps * sweeps * N),
+            "accept_rate": accepts / (reps * sweeps * n),
             "best_energy": r1["best_energy"],
             "gpu_launches": launches,
             "wall_s_timed_region": wall,
@@ -372,8 +394,8 @@ def run_ours(args):
                          "traffic": None,
                          "traffic_note": "not measured in this run (no profiler in the timed region); "
                                          "ncu DRAM bytes per launch are in the committed profile summary",
-                         "hbm_bytes_per_launch_by_construction": state_bytes + stage_bytes,
-                         "alg_bytes_per_launch": alg_bytes / launches,
+                         "hbm_bytes_per_megaiter_by_construction": state_bytes + stage_bytes,
+                         "alg_bytes_per_launch": alg_bytes / max(1, launches),
                          "bytes_model": bytes_model},
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": res["h2d_bytes"],
                     "d2h_bytes_per_step": res["d2h_bytes"], "wall_s": e_wall,
@@ -509,6 +531,62 @@ def run_serve_suite(args):
     print(json.dumps(line))
 
 
+def run_divergence_suite(args):
+    """Decision divergence between the GPU kernel (fp64 exp2 weights, tree-ordered fp64 sums) and
+    the reference's arithmetic (x87 exp2l weights, sequential long-double sums rounded to double,
+    CPU_PIM.cpp:236-251) as restated by the oracle, on the headline workload (n = 256 grid
+    instance, 64 replicas, exchange every 4 sweeps) at the benchmark's ladder and at a hot
+    ladder.  Both sides run the same Philox stream in lock step; every --div-chunk
+    mega-iterations the permutation, energy and best energy of every replica are compared.  Any differing decision changes a permutation at once, so the first mismatching
+    chunk bounds the first divergence; a run then ends and the next starts from a new seed.
+    Reports the updates compared and the divergences seen."""
+    import pimqap
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    from oracle import Oracle
+    orc = Oracle()
+    inst = instances.grid256(1000)
+    ladders = {"bench": (BETA_MAX, BETA_RATIO), "hot": (2.0 ** -10, BETA_RATIO)}
+    per_ladder = args.div_updates
+    out = {"suite": "divergence", "workload": "grid256 n=256, 64 replicas, exchange every 4 sweeps",
+           "chunk_megaiters": args.div_chunk, "ladders": {}}
+    t_start = time.perf_counter()
+    for name, (b0, ratio) in ladders.items():
+        done, divergences, runs, first = 0, 0, 0, []
+        seed = 1
+        while done < per_ladder:
+            runs += 1
+            p = pimqap.default_params(replicas=REPLICAS, groups=1, sweeps_per_exchange=SWEEPS_PER_EXCHANGE,
+                                      beta_max=b0, beta_ratio=ratio, beta_internal=1, seed=seed,
+                                      max_megaiters=2 ** 31 - 1, megaiters_per_launch=args.div_chunk)
+            st = orc.setup(inst.D, inst.F, 1, REPLICAS, SWEEPS_PER_EXCHANGE, b0, ratio, seed, cap=REPLICAS)
+            with pimqap.Solver(inst.F, inst.D, p) as s:
+                m = 0
+                while done < per_ladder:
+                    s.run(args.div_chunk)
+                    orc.run(st, inst.D, inst.F, args.div_chunk, -(1 << 62))
+                    m += args.div_chunk
+                    # permutation, energy and best of every replica slot (the exchange the solver
+                    # runs at the end of a launch moves betas, not these)
+                    bad = False
+                    for l in range(REPLICAS):
+                        r = s.replica(0, l, force=False)
+                        if (not np.array_equal(r["phi"], st.phi[0, l]) or r["E"] != st.E[0, l]
+                                or r["bestE"] != st.bestE[0, l]):
+                            bad = True
+                            break
+                    if bad:
+                        divergences += 1
+                        first.append({"seed": seed, "megaiter_chunk_end": m})
+                        break
+                    done += REPLICAS * SWEEPS_PER_EXCHANGE * args.div_chunk * N
+            seed += 1
+        out["ladders"][name] = {"beta0_internal": b0, "beta_ratio": ratio, "updates_compared": done,
+                                "divergences": divergences, "runs": runs, "divergent_chunks": first,
+                                "rate_upper_95": 3.0 / done if divergences == 0 else None}
+    out["wall_s"] = time.perf_counter() - t_start
+    print(json.dumps(out))
+
+
 def main():
     ap = argparse.ArgumentParser(description=__doc__.split("\n")[0])
     ap.add_argument("--gpus", type=int, default=1)
@@ -516,16 +594,26 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--workload", choices=["grid256", "clique92"], default="grid256",
-                    help="headline instance (clique92: the tai256c program's structure and moves)")
+    ap.add_argument("--workload", choices=sorted(WORKLOADS), default="grid256",
+                    help="headline instance (clique92: the tai256c program's structure and moves; "
+                         "cfg1: n=32, 16 replicas, exchange every sweep)")
+    ap.add_argument("--groups", type=int, default=1,
+                    help="independent parallel-tempering groups of the workload's replicas per GPU (the "
+                         "reference's -t; its CPU arm runs one group per host thread)")
+    ap.add_argument("--launch-mode", type=int, default=0, choices=[0, 1, 2],
+                    help="0 = automatic (persistent when resident), 1 = a launch per mega-iteration, 2 = persistent")
     ap.add_argument("--update-rule", choices=["sequential", "one-shot"], default="sequential",
                     help="sequential: CPU_PIM's sweeps (the headline); one-shot: GPU-CUPIM's parallel step")
     ap.add_argument("--cluster-size", type=int, default=0, help="CTAs per replica (0 = automatic)")
     ap.add_argument("--threads", type=int, default=0, help="threads per replica and CTA (0 = automatic)")
     ap.add_argument("--pairing", type=int, default=0, choices=[0, 1, 2],
                     help="replicas per CTA set of the binary-flow kernel: 0 = automatic, 1, 2")
-    ap.add_argument("--suite", choices=["headline", "batch", "serve"], default="headline",
-                    help="headline: the n=256 workload (the driver's line); batch / serve: the other workloads")
+    ap.add_argument("--suite", choices=["headline", "batch", "serve", "divergence"], default="headline",
+                    help="headline: the n=256 workload (the driver's line); batch / serve: the other "
+                         "workloads; divergence: GPU vs oracle decisions over a long stream")
+    ap.add_argument("--div-updates", type=int, default=10_000_000,
+                    help="divergence suite: updates compared per ladder")
+    ap.add_argument("--div-chunk", type=int, default=10, help="divergence suite: mega-iterations per comparison")
     ap.add_argument("--batch-instances", type=int, default=512, help="batch suite: instances")
     ap.add_argument("--batch-sweeps", type=int, default=2000, help="batch suite: sweeps per instance")
     ap.add_argument("--batch-fixed-only", action="store_true",
@@ -541,6 +629,9 @@ def main():
         return
     if args.suite == "serve":
         run_serve_suite(args)
+        return
+    if args.suite == "divergence":
+        run_divergence_suite(args)
         return
     if args.impl == "reference":
         run_reference(args)

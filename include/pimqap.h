@@ -76,7 +76,9 @@ typedef struct pimqap_params {
     int32_t force_bits;          /* 0 = choose from the instance bound, 32 or 64 = force */
     int32_t device;              /* CUDA device ordinal */
     int32_t megaiters_per_launch;/* mega-iterations per CUDA-graph launch (0 = automatic) */
-    int32_t threads_per_block;   /* 0 = automatic, else 64, 128 or 256 */
+    int32_t threads_per_block;   /* 0 = automatic, else 64, 128 or 256 (also 32 for n <= 128
+                                    with the sequential rule, 512 with the one-shot rule): the
+                                    threads of one replica's CTA */
     int32_t cluster_size;        /* CTAs per replica: 0 = smallest that fits, else 1, 2 or 4 */
     int32_t beta_internal;       /* nonzero: beta_max is already in the reference's internal
                                     (log2) units, as automatic mode sets beta0 = 2^k (:397) */
@@ -114,6 +116,12 @@ typedef struct pimqap_params {
                                     over one shared copy of the instance, so their update chains
                                     interleave.  Same results either way.  pimqap_solve / solver
                                     handles only */
+    int32_t launch_mode;         /* 0 = automatic: one persistent launch per run call when every
+                                    replica can be resident at once and no event log is kept,
+                                    else a launch per mega-iteration; 1 = a launch per
+                                    mega-iteration (CUDA graphs of megaiters_per_launch);
+                                    2 = persistent (rejected when it cannot run).  Same results
+                                    either way.  pimqap_solve / solver handles only */
 } pimqap_params;
 
 #define PIMQAP_RULE_SEQUENTIAL 0
@@ -137,6 +145,8 @@ typedef struct pimqap_result {
     int32_t force_bits;         /* 32 or 64: the force-matrix width used */
     int32_t cluster_size;       /* CTAs per replica (1, 2 or 4) */
     int32_t stopped_by;         /* 0 = max_megaiters, 1 = goal, 2 = timeout */
+    int32_t launches;           /* kernel launches of the sweeps (solver path): one per
+                                   mega-iteration, or one per run call when persistent */
     int64_t h2d_bytes;          /* host-to-device bytes copied by the solver so far */
     int64_t d2h_bytes;          /* device-to-host bytes copied by the solver so far */
     int64_t *final_energies;    /* caller-provided, groups * replicas entries (may be NULL):

@@ -77,7 +77,8 @@ std::vector<BatchClass> plan_classes(const std::vector<Plan> &plans, const std::
         for (int k : c.members) {
             const Plan &P = plans[k];
             nmax = std::max(nmax, P.n);
-            slice = std::max(slice, c.cl == 1 ? pimqap::batch_slice_bytes(P.n, c.bits) : 16 + P.smem);
+            slice = std::max(slice, c.cl == 1 ? pimqap::batch_slice_bytes(P.n, c.bits)
+                                               : 16 + std::max(P.smem, pimqap::exchange_scratch_bytes()));
         }
         c.slice = (slice + 15) & ~size_t(15);
         if (c.cl == 1) {

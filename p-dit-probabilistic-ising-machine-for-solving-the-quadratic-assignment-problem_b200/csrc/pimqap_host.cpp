@@ -19,6 +19,7 @@
 #include <mutex>
 #include <random>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "pimqap.h"
@@ -242,8 +243,12 @@ struct pimqap_solver {
     int n = 0, T = 0, R = 0, cap = 0, spe = 0;
     int bits = 32, cl = 1, threads = 256;
     bool sym = false, bin = false, pair = false;
+    bool persistent = false;   // one persistent launch per run call (solve_kernel)
     size_t smem = 0;
     int device = 0;
+    volatile int32_t *kill = nullptr;   // mapped host word of the persistent launch (timeout)
+    int64_t launches = 0;               // sweep-kernel launches so far
+    cudaGraphExec_t solve_graph = nullptr;
     cudaStream_t stream = nullptr;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     void *dmem = nullptr;
@@ -262,6 +267,7 @@ struct pimqap_solver {
     ~pimqap_solver() {
         events.reset();
         if (graph) cudaGraphExecDestroy(graph);
+        if (solve_graph) cudaGraphExecDestroy(solve_graph);
         if (ev0) cudaEventDestroy(ev0);
         if (ev1) cudaEventDestroy(ev1);
         if (stream) {
@@ -269,6 +275,7 @@ struct pimqap_solver {
             cudaStreamDestroy(stream);
         }
         block_release(device, dmem, dbytes);
+        if (kill) cudaFreeHost(const_cast<int32_t *>(kill));
     }
 };
 
@@ -307,12 +314,17 @@ pimqap_status check_params(const pimqap_instance *inst, const pimqap_params *p) 
     if (p->force_bits != 0 && p->force_bits != 32 && p->force_bits != 64)
         return fail(PIMQAP_ERR_ARG, "force_bits must be 0, 32 or 64");
     if (p->threads_per_block != 0 && p->threads_per_block != 64 && p->threads_per_block != 128 &&
-        p->threads_per_block != 256 && !(p->threads_per_block == 512 && p->update_rule == PIMQAP_RULE_ONE_SHOT))
-        return fail(PIMQAP_ERR_ARG, "threads_per_block must be 0, 64, 128 or 256 (or 512 with the one-shot rule)");
+        p->threads_per_block != 256 && !(p->threads_per_block == 512 && p->update_rule == PIMQAP_RULE_ONE_SHOT) &&
+        !(p->threads_per_block == 32 && inst->n <= 128 && p->update_rule == PIMQAP_RULE_SEQUENTIAL))
+        return fail(PIMQAP_ERR_ARG, "threads_per_block must be 0, 64, 128 or 256 (512 with the one-shot rule, "
+                                    "32 with the sequential rule for n <= 128)");
     if (p->cluster_size != 0 && p->cluster_size != 1 && p->cluster_size != 2 && p->cluster_size != 4)
         return fail(PIMQAP_ERR_ARG, "cluster_size must be 0, 1, 2 or 4");
     if (p->replica_pairing < 0 || p->replica_pairing > 2)
         return fail(PIMQAP_ERR_ARG, "replica_pairing must be 0 (automatic), 1 (off) or 2 (on)");
+    if (p->launch_mode < 0 || p->launch_mode > 2)
+        return fail(PIMQAP_ERR_ARG, "launch_mode must be 0 (automatic), 1 (a launch per mega-iteration) or "
+                                    "2 (one persistent launch)");
     return PIMQAP_OK;
 }
 
@@ -425,7 +437,7 @@ pimqap_status plan_instance(const pimqap_instance *inst, const pimqap_params *pa
              carve_size(reps * 8) + carve_size((size_t)P.T * P.cap * 4) + carve_size((size_t)P.T * 8) +
              4 * carve_size(8);
     P.tail = carve_size(reps * (size_t)n * P.npad * isz) + carve_size(reps * n * 4) + 3 * carve_size(reps * 8) +
-             3 * carve_size((size_t)P.T * 8) + 2 * carve_size(8);
+             3 * carve_size((size_t)P.T * 8) + 5 * carve_size(8);
     P.total = P.head + P.tail;
     P.h2d_bytes = (int64_t)P.head;
     *out = P;
@@ -494,6 +506,10 @@ void carve_instance(const Plan &P, char *head, char *tail, SolveDev *out) {
     d.epoch = carve<int32_t>(cur, T);
     d.start_ns = carve<unsigned long long>(cur, 1);
     d.error = carve<int32_t>(cur, 1);
+    d.epoch_all = carve<int32_t>(cur, 1);
+    d.finish_all = carve<unsigned int>(cur, 1);
+    d.run_end = carve<int32_t>(cur, 1);
+    d.kill = nullptr;
     *out = d;
 }
 
@@ -761,7 +777,109 @@ pimqap_status pimqap_solver_create(const pimqap_instance *inst, const pimqap_par
         st = s->events->drain(q, s->start_ns, true);
         if (st != PIMQAP_OK) return st;
     }
+    // The whole run as one persistent launch per run call when every replica can be resident
+    // at once.  Solves with an event log keep a launch per mega-iteration chunk: their log is
+    // drained between chunks.
+    if (params->launch_mode == 2 && s->pair)
+        return fail(PIMQAP_ERR_ARG, "launch_mode = 2 needs every replica resident at once, no event log and "
+                                    "one replica per CTA set");
+    if (params->launch_mode != 1 && !s->pair) {
+        bool fits = false;
+        PQ_CUDA(pimqap::solve_fits(d, s->bits, s->cl, s->sym, s->bin, s->threads, s->smem, &fits));
+        const bool able = fits && !s->events;
+        if (params->launch_mode == 2 && !able)
+            return fail(PIMQAP_ERR_ARG, "launch_mode = 2 needs every replica resident at once, no event log and "
+                                        "one replica per CTA set");
+        if (able) {
+            int32_t *k = nullptr;
+            PQ_CUDA(cudaHostAlloc(reinterpret_cast<void **>(&k), sizeof(int32_t), cudaHostAllocMapped));
+            *k = 0;
+            s->kill = k;
+            int32_t *kd = nullptr;
+            PQ_CUDA(cudaHostGetDevicePointer(reinterpret_cast<void **>(&kd), k, 0));
+            d.kill = kd;
+            s->persistent = true;
+        }
+    }
     *out = guard.release();
+    return PIMQAP_OK;
+}
+
+// pimqap_solver_run as one persistent launch: the launch runs mega-iterations up to
+// run_end on the device; the host only waits, and on a timeout sets the kill word, which stops
+// the launch at the next mega-iteration boundary.
+static pimqap_status run_persistent(pimqap_solver *s, int64_t megaiters, double *device_ms) {
+    const auto wall0 = std::chrono::steady_clock::now();
+    int32_t done = 0;
+    PQ_CUDA(cudaMemcpy(&done, s->dev.epoch_all, 4, cudaMemcpyDeviceToHost));
+    s->d2h += 4;
+    const int32_t end = (int32_t)std::min<int64_t>((int64_t)done + megaiters, (int64_t)pimqap::kNoStop - 1);
+    double ms_total = 0;
+    if (end > done && !s->stopped_goal) {
+        if (!s->solve_graph) {
+            cudaGraph_t graph;
+            PQ_CUDA(cudaStreamBeginCapture(s->stream, cudaStreamCaptureModeThreadLocal));
+            cudaError_t e = pimqap::launch_solve(s->dev, s->bits, s->cl, s->sym, s->bin, s->threads, s->smem,
+                                                 s->stream);
+            if (e != cudaSuccess) {
+                cudaStreamEndCapture(s->stream, &graph);
+                return fail(PIMQAP_ERR_CUDA, std::string("persistent launch: ") + cudaGetErrorString(e));
+            }
+            PQ_CUDA(cudaStreamEndCapture(s->stream, &graph));
+            cudaError_t ie = cudaGraphInstantiate(&s->solve_graph, graph, 0);
+            cudaGraphDestroy(graph);
+            PQ_CUDA(ie);
+        }
+        *s->kill = 0;
+        PQ_CUDA(cudaMemcpyAsync(const_cast<int32_t *>(s->dev.run_end), &end, 4, cudaMemcpyHostToDevice, s->stream));
+        s->h2d += 4;
+        PQ_CUDA(cudaEventRecord(s->ev0, s->stream));
+        PQ_CUDA(cudaGraphLaunch(s->solve_graph, s->stream));
+        ++s->launches;
+        PQ_CUDA(cudaEventRecord(s->ev1, s->stream));
+        if (s->p.timeout_s > 0) {
+            // the -s stop (CPU_PIM.cpp:350-357): at the first boundary after the time is up
+            for (;;) {
+                const cudaError_t q = cudaEventQuery(s->ev1);
+                if (q == cudaSuccess) break;
+                if (q != cudaErrorNotReady) PQ_CUDA(q);
+                const double el = std::chrono::duration<double>(std::chrono::steady_clock::now() - wall0).count();
+                if (el >= s->p.timeout_s) {
+                    *s->kill = 1;
+                    break;
+                }
+                std::this_thread::sleep_for(std::chrono::microseconds(200));
+            }
+        }
+        PQ_CUDA(cudaStreamSynchronize(s->stream));
+        float ms = 0;
+        PQ_CUDA(cudaEventElapsedTime(&ms, s->ev0, s->ev1));
+        ms_total = ms;
+    }
+    int32_t epoch0 = 0, err = 0, stop = 0;
+    PQ_CUDA(cudaMemcpy(&epoch0, s->dev.epoch, 4, cudaMemcpyDeviceToHost));
+    PQ_CUDA(cudaMemcpy(&err, s->dev.error, 4, cudaMemcpyDeviceToHost));
+    PQ_CUDA(cudaMemcpy(&stop, s->dev.stop_epoch, 4, cudaMemcpyDeviceToHost));
+    s->d2h += 12;
+    s->megaiters_done = epoch0;
+    // a stop word set by the goal (not by the kill word) ends the solve for good
+    if (stop != pimqap::kNoStop && !*s->kill) s->stopped_goal = true;
+    if (*s->kill && stop != pimqap::kNoStop) {
+        // the kill word moved the stop: clear it for a later run call unless the goal set it
+        int64_t tepoch = 0;
+        PQ_CUDA(cudaMemcpy(&tepoch, s->dev.target_epoch, 8, cudaMemcpyDeviceToHost));
+        s->d2h += 8;
+        if (tepoch != std::numeric_limits<int64_t>::max()) {
+            s->stopped_goal = true;
+        } else {
+            const int32_t none = pimqap::kNoStop;
+            PQ_CUDA(cudaMemcpy(s->dev.stop_epoch, &none, 4, cudaMemcpyHostToDevice));
+            s->h2d += 4;
+        }
+    }
+    s->device_ms += ms_total;
+    if (device_ms) *device_ms = ms_total;
+    if (err) return fail(PIMQAP_ERR_DEVICE, "device check failed (error word " + std::to_string(err) + ")");
     return PIMQAP_OK;
 }
 
@@ -769,6 +887,7 @@ pimqap_status pimqap_solver_run(pimqap_solver *s, int64_t megaiters, double *dev
     if (!s) return fail(PIMQAP_ERR_ARG, "null solver");
     if (megaiters < 0) return fail(PIMQAP_ERR_ARG, "megaiters must be >= 0");
     PQ_CUDA(cudaSetDevice(s->device));
+    if (s->persistent) return run_persistent(s, megaiters, device_ms);
     const auto wall0 = std::chrono::steady_clock::now();
     const int per = s->p.megaiters_per_launch > 0 ? s->p.megaiters_per_launch : 50;
     double ms_total = 0;
@@ -798,6 +917,7 @@ pimqap_status pimqap_solver_run(pimqap_solver *s, int64_t megaiters, double *dev
         }
         PQ_CUDA(cudaEventRecord(s->ev0, s->stream));
         PQ_CUDA(cudaGraphLaunch(s->graph, s->stream));
+        s->launches += g;
         PQ_CUDA(cudaEventRecord(s->ev1, s->stream));
         int32_t stop = 0;
         PQ_CUDA(cudaMemcpyAsync(&stop, s->dev.stop_epoch, 4, cudaMemcpyDeviceToHost, s->stream));
@@ -869,6 +989,7 @@ pimqap_status pimqap_solver_result(pimqap_solver *s, pimqap_result *r) {
     r->force_bits = s->bits;
     r->cluster_size = s->cl;
     r->stopped_by = s->stopped_goal ? 1 : 0;
+    r->launches = (int32_t)std::min<int64_t>(s->launches, 0x7fffffff);
     s->d2h += (int64_t)(reps * 16 + 8 * 4 + (perm_dst ? (size_t)s->n * 4 : 0));
     r->h2d_bytes = s->h2d;
     r->d2h_bytes = s->d2h;

@@ -88,6 +88,12 @@ struct SolveDev {
                                //      instance: small factors, sums below 2^24)
     const double *replay_r;    // [sweeps][n] the uniform r of every update, given by the caller
                                //      (pimqap_sweep_replay); nullptr: drawn from the Philox stream
+    // The persistent solve (one launch runs many mega-iterations; solve_kernel):
+    int32_t *epoch_all;        // [1] mega-iterations every group has completed (the release word)
+    unsigned int *finish_all;  // [1] groups done with the current mega-iteration
+    const int32_t *run_end;    // [1] the launch stops before this mega-iteration
+    const volatile int32_t *kill;  // [1] mapped host word: nonzero stops the launch at the next
+                                   //     mega-iteration boundary (the host's timeout); may be null
 };
 
 // Compact per-instance result of a batch.
@@ -183,6 +189,10 @@ cudaError_t launch_collect(const SolveDev *inst, int count, BatchResultDev *out,
 // Records msg as the calling thread's pimqap_last_error() text.
 void set_last_error(const char *msg);
 
+// Shared memory the tracking / exchange step needs once an epoch is over (the sweep kernels are
+// launched with at least this much).
+size_t exchange_scratch_bytes();
+
 // Shared memory of one CTA of the epoch kernel.
 size_t epoch_smem_bytes(int n, int rpc, int lds, int cluster, int bits);
 // Shared memory of the binary-flow epoch kernel (0 / 1 flows and int16 distances resident).
@@ -195,6 +205,15 @@ size_t epoch_smem_bytes_os(int n, int rpc, int lds, int cluster, int bits, int c
 
 // Resident clusters (CTAs for cl == 1) of the paired binary-flow epoch on the whole device.
 cudaError_t pair_occupancy(int cl, int threads, size_t smem, int *clusters);
+
+// The persistent solve: every replica (CTA or cluster) resident for the whole launch, which runs
+// mega-iterations from *epoch_all up to *run_end (or the goal / kill stop) with a bounded
+// device-side barrier between them.  Returns cudaErrorInvalidValue for shapes it lacks.
+cudaError_t launch_solve(const SolveDev &s, int bits, int cluster, bool sym, bool bin, int threads,
+                         size_t smem, cudaStream_t st);
+// Whether every replica of the solve can be resident at once for launch_solve's kernel.
+cudaError_t solve_fits(const SolveDev &s, int bits, int cluster, bool sym, bool bin, int threads,
+                       size_t smem, bool *fits);
 
 // One-time kernel attributes (dynamic shared memory, non-portable cluster size).
 cudaError_t prepare_kernels();

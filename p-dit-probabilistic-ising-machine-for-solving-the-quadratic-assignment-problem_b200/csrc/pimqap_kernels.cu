@@ -25,6 +25,7 @@
 #include <cuda_fp16.h>
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cstdint>
 
 #include "pimqap_internal.h"
@@ -46,6 +47,11 @@ template <class IT> struct alignas(16) Vec {
 };
 
 __host__ __device__ inline size_t align16(size_t x) { return (x + 15) & ~size_t(15); }
+
+// Shared memory the tracking / exchange step stages a group in (track_exchange): energies,
+// bests and betas of up to kMaxReplicas replicas and their rank slots (+ slot cap-1).
+constexpr int kMaxReplicas = 64;
+constexpr size_t kExchangeScratchBytes = (size_t)kMaxReplicas * (8 + 8 + 8) + (kMaxReplicas + 1) * 4;
 
 // Offsets (bytes) of the epoch kernel's shared-memory sections.
 //   I       rpc rows of the replica's force matrix (row stride lds)
@@ -92,6 +98,8 @@ struct SmemLayout {
 size_t epoch_smem_bytes(int n, int rpc, int lds, int cluster, int bits) {
     return SmemLayout(n, rpc, lds, cluster, bits / 8).total;
 }
+
+size_t exchange_scratch_bytes() { return 16 + kExchangeScratchBytes; }
 
 // Philox4x32-10 (Salmon et al., SC'11): words 0 and 1 of the block for counter c, key k.
 __device__ __forceinline__ void philox_2words(uint32_t c0, uint32_t c1, uint32_t c2, uint32_t c3,
@@ -296,13 +304,40 @@ __device__ __forceinline__ void prefetch_rows(int tid, int BT, int nD, const int
 
 // Best tracking, replica exchange and goal test of group g at the start of mega-iteration
 // e_next (CPU_PIM.cpp:295-348).  Runs on one thread after every replica of the group has
-// finished its sweeps; reads their energies through L2.
-__device__ void track_exchange(const SolveDev &s, int g, int e_next) {
+// finished its sweeps.  With `scratch` (kExchangeScratchBytes of shared memory that nothing
+// else uses meanwhile) the group's energies, bests, betas and rank order are first read
+// through L2 with independent loads and the bubble pass runs on those copies, so its chain of
+// rank-slot reads and writes stays in shared memory; without it, it works on global memory.
+__device__ void track_exchange(const SolveDev &s, int g, int e_next, unsigned char *scratch = nullptr) {
     const int R = s.R, cap = s.cap;
-    volatile int64_t *E = s.E + (size_t)g * R;
-    volatile int64_t *bestE = s.bestE + (size_t)g * R;
-    volatile double *beta = s.beta + (size_t)g * R;
-    volatile int32_t *order = s.order + (size_t)g * cap;
+    int64_t *gE = s.E + (size_t)g * R;
+    int64_t *gbestE = s.bestE + (size_t)g * R;
+    double *gbeta = s.beta + (size_t)g * R;
+    int32_t *gorder = s.order + (size_t)g * cap;
+    const bool staged = scratch != nullptr && R <= kMaxReplicas;
+    volatile int64_t *E, *bestE;
+    volatile double *beta;
+    volatile int32_t *order;
+    int hi;                                                  // index of rank slot cap-1
+    if (staged) {
+        int64_t *sE = reinterpret_cast<int64_t *>(scratch);
+        int64_t *sB = sE + kMaxReplicas;
+        double *sb = reinterpret_cast<double *>(sB + kMaxReplicas);
+        int32_t *so = reinterpret_cast<int32_t *>(sb + kMaxReplicas);
+#pragma unroll 8
+        for (int l = 0; l < R; ++l) {
+            sE[l] = __ldcg((const long long *)gE + l);
+            sB[l] = __ldcg((const long long *)gbestE + l);
+            sb[l] = __ldcg(gbeta + l);
+            so[l] = __ldcg(gorder + l);
+        }
+        hi = cap - 1 < R ? cap - 1 : R;                      // slots R .. cap-2 are never read
+        if (hi == R) so[R] = __ldcg(gorder + cap - 1);
+        E = sE; bestE = sB; beta = sb; order = so;
+    } else {
+        E = gE; bestE = gbestE; beta = gbeta; order = gorder;
+        hi = cap - 1;
+    }
     int tss = *((volatile int32_t *)s.tss + g) + 1;          // :295
     int64_t gb = *((volatile int64_t *)s.group_best + g);
     bool found = false;
@@ -319,11 +354,12 @@ __device__ void track_exchange(const SolveDev &s, int g, int e_next) {
         }
     }
     if (found) atomicMin((long long *)s.single_best, (long long)gb);
+    bool ok = true;
     for (int l = 0; l < R - 1; ++l) {                        // :324-337
         const int i1 = order[l], i2 = order[l + 1];
         if ((unsigned)i1 >= (unsigned)R || (unsigned)i2 >= (unsigned)R) {   // never in a valid state
-            atomicOr(s.error, kErrShape);
-            return;
+            ok = false;
+            break;
         }
         const double e1 = (double)E[i1], e2 = (double)E[i2];
         if (e1 < e2) {
@@ -335,17 +371,28 @@ __device__ void track_exchange(const SolveDev &s, int g, int e_next) {
             if (i2 == R - 1) tss = 0;                        // replica index, as :333
         }
     }
-    if (tss > 100) {                                         // :339-344, slot cap-1
-        const int i1 = order[cap - 1], i2 = order[0];
+    if (ok && tss > 100) {                                   // :339-344, slot cap-1
+        const int i1 = order[hi], i2 = order[0];
         if ((unsigned)i1 >= (unsigned)R || (unsigned)i2 >= (unsigned)R) {
-            atomicOr(s.error, kErrShape);
-            return;
+            ok = false;
+        } else {
+            order[hi] = i2;
+            order[0] = i1;
+            const double tb = beta[i1];
+            beta[i1] = beta[i2];
+            beta[i2] = tb;
         }
-        order[cap - 1] = i2;
-        order[0] = i1;
-        const double tb = beta[i1];
-        beta[i1] = beta[i2];
-        beta[i2] = tb;
+    }
+    if (staged) {   // the copies back (also after a failed check: nothing else has changed)
+        for (int l = 0; l < R; ++l) {
+            gbeta[l] = beta[l];
+            gorder[l] = order[l];
+        }
+        if (hi == R) gorder[cap - 1] = order[R];
+    }
+    if (!ok) {
+        atomicOr(s.error, kErrShape);
+        return;
     }
     s.tss[g] = tss;
     s.group_best[g] = gb;
@@ -909,7 +956,8 @@ struct BinPairLayout {
     size_t Ds, Fb, rep[2], total;
     __host__ __device__ BinPairLayout(int n, int rpc, int lds, int cluster) {
         const size_t rp = (size_t)rpc, nw = (size_t)((n + 31) / 32);
-        const size_t slice = BinLayout(n, rpc, lds, cluster, false).total;
+        // each section also holds the exchange scratch once its replica's epoch is done
+        const size_t slice = align16(max(BinLayout(n, rpc, lds, cluster, false).total, kExchangeScratchBytes));
         size_t o = 0;
         Ds = o;     o = align16(o + (size_t)n * rp * 2);
         Fb = o;     o = align16(o + (size_t)n * nw * 4);
@@ -2158,7 +2206,7 @@ __global__ void __launch_bounds__(KIND == 2 ? 512 : 256, (CL == 4 && KIND != 2) 
         const unsigned prev = atomicAdd(s.finish + g, 1u);
         if (prev == (unsigned)s.R - 1u) {
             __threadfence();
-            track_exchange(s, g, e + 1);
+            track_exchange(s, g, e + 1, smem);   // the epoch's shared memory is dead now
             s.finish[g] = 0u;
             s.epoch[g] = e + 1;
             __threadfence();
@@ -2204,10 +2252,95 @@ __global__ void __launch_bounds__(512, 1) epoch_pair_kernel(SolveDev s) {
         const unsigned prev = atomicAdd(s.finish + g, 1u);
         if (prev == (unsigned)s.R - 1u) {
             __threadfence();
-            track_exchange(s, g, e + 1);
+            track_exchange(s, g, e + 1, smem + P.rep[h]);   // this half's section is dead now
             s.finish[g] = 0u;
             s.epoch[g] = e + 1;
             __threadfence();
+        }
+    }
+}
+
+// The persistent solve: CTA (cluster) rep / CL runs replica rep for every mega-iteration of the
+// launch, from *epoch_all up to *run_end.  After each epoch the last replica of a group runs the
+// group's tracking + exchange, the last group releases the next mega-iteration (*epoch_all) and,
+// when the host's kill word is set, moves the stop to the next boundary.  Thread 0 of the
+// cluster's rank 0 waits for the release (bounded) and decides whether the cluster goes on; the
+// decision reaches the cluster's other CTAs through rank 0's shared memory between two cluster
+// barriers, so a cluster never splits.  A kernel boundary of the per-epoch launches and this
+// barrier order the same steps, so both take the same trajectory.  Needs every CTA resident.
+template <class IT, int CL, bool SYM, bool GP, int KIND>
+__global__ void __launch_bounds__(KIND == 2 ? 512 : 256, (CL == 4 && KIND != 2) ? 2 : 1) solve_kernel(SolveDev s) {
+    // Between epochs no shared memory is live: the first word carries the cluster's decision.
+    extern __shared__ __align__(16) unsigned char smem[];
+    volatile int32_t *s_go = reinterpret_cast<volatile int32_t *>(smem);
+    int rank = 0;
+    if constexpr (CL > 1) rank = (int)cg::this_cluster().block_rank();
+    const int rep = blockIdx.x / CL;
+    const int g = rep / s.R;
+    const Grp G{(int)threadIdx.x, (int)blockDim.x, (int)(threadIdx.x & 31), (int)(threadIdx.x >> 5),
+                (int)(blockDim.x >> 5), 0};
+    volatile int32_t *epoch_all = s.epoch_all;
+    int e = -1;                                   // the epoch just run (-1: none yet)
+    unsigned long long spent = 0;                 // its duration
+    for (;;) {
+        if (rank == 0 && threadIdx.x == 0) {
+            bool released = true;
+            if (e >= 0) {
+                // the slowest replica takes about as long as this one: a healthy wait is a fraction
+                // of an epoch, so the limit is eight epochs of this replica and at least two seconds
+                const unsigned long long limit = max(2000000000ull, 8ull * spent);
+                const unsigned long long w0 = globaltimer_ns();
+                while (*epoch_all <= e) {
+                    if (*(volatile int32_t *)s.error != 0) {
+                        released = false;
+                        break;
+                    }
+                    if (globaltimer_ns() - w0 > limit) {
+                        atomicOr(s.error, kErrTimeout);
+                        released = false;
+                        break;
+                    }
+                }
+                __threadfence();
+            }
+            const int en = *epoch_all;
+            const int stop = min(*(volatile int32_t *)s.stop_epoch, *(volatile const int32_t *)s.run_end);
+            *s_go = (released && en < stop && *(volatile int32_t *)s.error == 0) ? en : -1;
+        }
+        if constexpr (CL > 1) {
+            cluster_barrier<CL>();
+            int go;
+            asm volatile("ld.shared::cluster.s32 %0, [%1];" : "=r"(go) : "r"(cluster_addr(smem_u32(smem), 0)) : "memory");
+            e = go;
+            cluster_barrier<CL>();                // every CTA has read it before rank 0 reuses the word
+        } else {
+            __syncthreads();
+            e = *s_go;
+            __syncthreads();
+        }
+        if (e < 0) break;
+        const unsigned long long t0 = globaltimer_ns();
+        bool ok;
+        if constexpr (KIND == 1) ok = replica_epoch_bin<CL>(s, rep, rank, e, G, smem);
+        else if constexpr (KIND == 2) ok = replica_epoch_os<IT, CL, SYM, GP>(s, rep, rank, e, G, smem);
+        else ok = replica_epoch<IT, CL, SYM, GP>(s, rep, rank, e, G, smem);
+        __syncthreads();
+        spent = globaltimer_ns() - t0;
+        // a failed epoch has set the error word; rank 0 sees it while it waits and stops the cluster
+        if (ok && rank == 0 && threadIdx.x == 0 && atomicAdd(s.finish + g, 1u) == (unsigned)s.R - 1u) {
+            __threadfence();
+            // the epoch's shared memory is dead; the decision word at offset 0 is written only
+            // after the release, past the scratch's use
+            track_exchange(s, g, e + 1, smem + 16);
+            s.finish[g] = 0u;
+            s.epoch[g] = e + 1;
+            __threadfence();
+            if (atomicAdd(s.finish_all, 1u) == (unsigned)s.T - 1u) {
+                *s.finish_all = 0u;
+                if (s.kill && *s.kill) atomicMin(s.stop_epoch, e + 1);
+                __threadfence();
+                *epoch_all = e + 1;               // release mega-iteration e + 1
+            }
         }
     }
 }
@@ -2434,7 +2567,8 @@ __device__ void replica_setup(const SolveDev &s, int rep, const Grp &G, int32_t 
 
 // The last replica of an instance to finish its set-up: mega-iteration 0's tracking, then the
 // first epoch, or the end when nothing is to run.
-__device__ void setup_done(const BatchDev &B, int k) {
+// `scratch`: the worker's shared memory, dead by now (the exchange stages a group in it).
+__device__ void setup_done(const BatchDev &B, int k, unsigned char *scratch) {
     SolveDev s;
     load_desc(s, B.inst + k);
     const int replicas = s.T * s.R;
@@ -2443,7 +2577,7 @@ __device__ void setup_done(const BatchDev &B, int k) {
     __threadfence();
     B.finish_inst[k] = 0u;
     *s.start_ns = globaltimer_ns();
-    for (int g = 0; g < s.T; ++g) track_exchange(s, g, 0);
+    for (int g = 0; g < s.T; ++g) track_exchange(s, g, 0, scratch);
     __threadfence();
     const int stop = *(volatile int32_t *)s.stop_epoch;
     if (0 < stop && 0 < __ldcg(B.max_megaiters + k)) {
@@ -2459,14 +2593,14 @@ __device__ void setup_done(const BatchDev &B, int k) {
 // After replica-epoch `e` of instance k: the last replica to finish runs every group's
 // tracking + exchange (lock step across groups, as one launch per epoch gives), then the next
 // epoch or the end of the instance.
-__device__ void epoch_done(const BatchDev &B, int k, int e) {
+__device__ void epoch_done(const BatchDev &B, int k, int e, unsigned char *scratch) {
     SolveDev s;
     load_desc(s, B.inst + k);
     const int replicas = s.T * s.R;
     const unsigned prev = atomicAdd(B.finish_inst + k, 1u);
     if (prev != (unsigned)replicas - 1u) return;
     __threadfence();
-    for (int g = 0; g < s.T; ++g) track_exchange(s, g, e + 1);
+    for (int g = 0; g < s.T; ++g) track_exchange(s, g, e + 1, scratch);
     B.finish_inst[k] = 0u;
     for (int g = 0; g < s.T; ++g) s.epoch[g] = e + 1;
     __threadfence();
@@ -2488,7 +2622,7 @@ size_t batch_slice_bytes(int n, int bits) {
     const int npad = (n + 3) & ~3;
     int lds = npad;
     if ((lds / vec) % 2 == 0) lds += vec;
-    return align16(16 + SmemLayout(n, npad, lds, 1, isz).total);
+    return align16(16 + std::max(SmemLayout(n, npad, lds, 1, isz).total, kExchangeScratchBytes));
 }
 
 template <class IT>
@@ -2522,15 +2656,15 @@ __global__ void __launch_bounds__(256) batch_kernel(BatchDev B) {
         load_desc(s, B.inst + k);
         if (item & kSetupItem) {
             replica_setup<IT>(s, rep, G, reinterpret_cast<int32_t *>(work),
-                              reinterpret_cast<long long *>(work + 16 * kMaxN));
-            if (G.tid == 0) setup_done(B, k);
+                              reinterpret_cast<long long *>(work + align16(4 * (size_t)s.n)));
+            if (G.tid == 0) setup_done(B, k, work);
             continue;
         }
         const int e = *((volatile int32_t *)s.epoch);
         if (__ldcg(B.sym + k)) replica_epoch<IT, 1, true>(s, rep, 0, e, G, work);
         else replica_epoch<IT, 1, false>(s, rep, 0, e, G, work);
         G.sync();
-        if (G.tid == 0) epoch_done(B, k, e);
+        if (G.tid == 0) epoch_done(B, k, e, work);
     }
 }
 
@@ -2569,8 +2703,8 @@ __global__ void __launch_bounds__(256, 1) batch_cluster_kernel(BatchDev B) {
                 SolveDev s;
                 load_desc(s, B.inst + k);
                 replica_setup<IT>(s, (int)(item & 0x7fffffffull), G, reinterpret_cast<int32_t *>(work),
-                                  reinterpret_cast<long long *>(work + 16 * kMaxN));
-                if (threadIdx.x == 0) setup_done(B, k);
+                                  reinterpret_cast<long long *>(work + align16(4 * (size_t)s.n)));
+                if (threadIdx.x == 0) setup_done(B, k, work);
             }
         } else {
             const int k = (int)(item >> 32), rep = (int)(item & 0x7fffffffull);
@@ -2587,7 +2721,7 @@ __global__ void __launch_bounds__(256, 1) batch_cluster_kernel(BatchDev B) {
             if (!ok) {
                 if (threadIdx.x == 0) set_error(B, kErrTimeout);
             } else if (rank == 0 && threadIdx.x == 0) {
-                epoch_done(B, k, e);
+                epoch_done(B, k, e, work);
             }
         }
         // the header is rewritten only after every rank has read it; this barrier also orders
@@ -2667,6 +2801,31 @@ static void *epoch_kernel_ptr(int bits, int cl, bool sym, bool gp) {
         case 4: return sym ? epoch_fn<IT, 4, true>(gp) : epoch_fn<IT, 4, false>(gp); \
         default: return nullptr;                                                     \
     }
+    if (bits == 32) { PIMQAP_PICK(int32_t) }
+    if (bits == 64) { PIMQAP_PICK(int64_t) }
+#undef PIMQAP_PICK
+    return nullptr;
+}
+
+template <class IT, int CL, bool SYM> static void *solve_fn(bool gp, int kind) {
+    if (kind == 1) return reinterpret_cast<void *>(&solve_kernel<int32_t, CL, true, false, 1>);
+    if (kind == 2)
+        return gp ? reinterpret_cast<void *>(&solve_kernel<IT, CL, SYM, true, 2>)
+                  : reinterpret_cast<void *>(&solve_kernel<IT, CL, SYM, false, 2>);
+    return gp ? reinterpret_cast<void *>(&solve_kernel<IT, CL, SYM, true, 0>)
+              : reinterpret_cast<void *>(&solve_kernel<IT, CL, SYM, false, 0>);
+}
+
+// The persistent solve kernel of a shape (kind: 0 generic, 1 binary-flow, 2 one-shot).
+static void *solve_kernel_ptr(int bits, int cl, bool sym, bool gp, int kind) {
+#define PIMQAP_PICK(IT)                                                                          \
+    switch (cl) {                                                                                \
+        case 1: return sym ? solve_fn<IT, 1, true>(gp, kind) : solve_fn<IT, 1, false>(gp, kind); \
+        case 2: return sym ? solve_fn<IT, 2, true>(gp, kind) : solve_fn<IT, 2, false>(gp, kind); \
+        case 4: return sym ? solve_fn<IT, 4, true>(gp, kind) : solve_fn<IT, 4, false>(gp, kind); \
+        default: return nullptr;                                                                 \
+    }
+    if (kind == 1 && (bits != 32 || !sym)) return nullptr;
     if (bits == 32) { PIMQAP_PICK(int32_t) }
     if (bits == 64) { PIMQAP_PICK(int64_t) }
 #undef PIMQAP_PICK
@@ -2818,6 +2977,16 @@ cudaError_t prepare_kernels() {
             err = cudaFuncSetAttribute(batch_fn(bits, cl), cudaFuncAttributeMaxDynamicSharedMemorySize, maxsm);
             if (err != cudaSuccess) return err;
         }
+    for (int bits : {32, 64})
+        for (int cl : {1, 2, 4})
+            for (int sym = 0; sym < 2; ++sym)
+                for (int gp = 0; gp < 2; ++gp)
+                    for (int kind = 0; kind < 3; ++kind) {
+                        void *fn = solve_kernel_ptr(bits, cl, sym != 0, gp != 0, kind);
+                        if (!fn) continue;
+                        err = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, maxsm);
+                        if (err != cudaSuccess) return err;
+                    }
     for (int cl : {1, 2, 4}) {
         err = cudaFuncSetAttribute(epoch_bin_ptr(cl), cudaFuncAttributeMaxDynamicSharedMemorySize, maxsm);
         if (err != cudaSuccess) return err;
@@ -2841,6 +3010,66 @@ cudaError_t launch_setup(const SolveDev &s, int bits, cudaStream_t st) {
     return cudaGetLastError();
 }
 
+// The kernel the persistent solve runs for a solve's shape (the kind launch_epoch picks).
+static void *solve_ptr_for(const SolveDev &s, int bits, int cluster, bool sym, bool bin) {
+    const bool gp = s.ev.log != nullptr && s.ev.goal_print != 0;
+    const int kind = s.os_chunk > 0 ? 2 : ((bin && bits == 32 && sym && (!gp || s.act > 0)) ? 1 : 0);
+    return solve_kernel_ptr(bits, cluster, sym, gp, kind);
+}
+
+static cudaLaunchConfig_t solve_config(const SolveDev &s, int cluster, int threads, size_t smem,
+                                       cudaStream_t st, cudaLaunchAttribute *attr) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3((unsigned)(s.T * s.R * cluster));
+    cfg.blockDim = dim3((unsigned)threads);
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = st;
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = (unsigned)cluster;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    return cfg;
+}
+
+cudaError_t solve_fits(const SolveDev &s, int bits, int cluster, bool sym, bool bin, int threads,
+                       size_t smem, bool *fits) {
+    *fits = false;
+    void *fn = solve_ptr_for(s, bits, cluster, sym, bin);
+    if (!fn) return cudaSuccess;
+    smem = std::max(smem, exchange_scratch_bytes());
+    const long long ctas = (long long)s.T * s.R * cluster;
+    if (cluster == 1) {
+        int dev = 0, sms = 0, per = 0;
+        cudaError_t e = cudaGetDevice(&dev);
+        if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, fn, threads, smem);
+        if (e != cudaSuccess) return e;
+        *fits = (long long)per * sms >= ctas;
+        return cudaSuccess;
+    }
+    cudaLaunchAttribute attr[1];
+    cudaLaunchConfig_t cfg = solve_config(s, cluster, threads, smem, nullptr, attr);
+    cfg.gridDim = dim3((unsigned)cluster);
+    int clusters = 0;
+    cudaError_t e = cudaOccupancyMaxActiveClusters(&clusters, fn, &cfg);
+    if (e != cudaSuccess) return e;
+    *fits = (long long)clusters * cluster >= ctas;
+    return cudaSuccess;
+}
+
+cudaError_t launch_solve(const SolveDev &s, int bits, int cluster, bool sym, bool bin, int threads,
+                         size_t smem, cudaStream_t st) {
+    void *fn = solve_ptr_for(s, bits, cluster, sym, bin);
+    if (!fn) return cudaErrorInvalidValue;
+    smem = std::max(smem, exchange_scratch_bytes());
+    cudaLaunchAttribute attr[1];
+    cudaLaunchConfig_t cfg = solve_config(s, cluster, threads, smem, st, attr);
+    void *args[] = {const_cast<SolveDev *>(&s)};
+    return cudaLaunchKernelExC(&cfg, fn, args);
+}
+
 cudaError_t launch_epoch(const SolveDev &s, int bits, int cluster, bool sym, bool bin, int threads,
                          size_t smem, cudaStream_t st, bool pair) {
     const bool gp = s.ev.log != nullptr && s.ev.goal_print != 0;
@@ -2853,6 +3082,7 @@ cudaError_t launch_epoch(const SolveDev &s, int bits, int cluster, bool sym, boo
                               : epoch_kernel_ptr(bits, cluster, sym, gp);
     if (!fn) return cudaErrorInvalidValue;
     const int reps = s.T * s.R;
+    if (!pair) smem = std::max(smem, exchange_scratch_bytes());   // the pair's sections hold it
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3((unsigned)((pair ? (reps + 1) / 2 : reps) * cluster));
     cfg.blockDim = dim3((unsigned)(pair ? 2 * threads : threads));

@@ -302,7 +302,8 @@ bool class_fits(const BatchClass &sh, const pimqap_instance &inst, const pimqap_
     p.force_bits = sh.bits;
     Plan P;
     if (plan_instance(&inst, &p, (size_t)maxsm, sh.cl, &P, &info) != PIMQAP_OK) return false;
-    const size_t need = sh.cl == 1 ? pimqap::batch_slice_bytes(P.n, sh.bits) : 16 + P.smem;
+    const size_t need = sh.cl == 1 ? pimqap::batch_slice_bytes(P.n, sh.bits)
+                                    : 16 + std::max(P.smem, pimqap::exchange_scratch_bytes());
     if (need > sh.slice) return false;
     if (out) *out = P;
     return true;

@@ -51,6 +51,7 @@ class Params(C.Structure):
         ("compact_instance", C.c_int32), ("active_facilities", C.c_int32),
         ("update_rule", C.c_int32),
         ("replica_pairing", C.c_int32),
+        ("launch_mode", C.c_int32),
     ]
 
 
@@ -88,7 +89,7 @@ class Result(C.Structure):
         ("target_megaiter", C.c_int64), ("time_to_target_ms", C.c_double),
         ("megaiters_done", C.c_int64), ("updates", C.c_int64), ("accepts", C.c_int64),
         ("device_ms", C.c_double), ("wall_ms", C.c_double), ("force_bits", C.c_int32),
-        ("cluster_size", C.c_int32), ("stopped_by", C.c_int32),
+        ("cluster_size", C.c_int32), ("stopped_by", C.c_int32), ("launches", C.c_int32),
         ("h2d_bytes", C.c_int64), ("d2h_bytes", C.c_int64),
         ("final_energies", C.POINTER(C.c_int64)), ("beta_max_used", C.c_double),
         ("beta_ratio_used", C.c_double), ("admit_ms", C.c_double), ("latency_ms", C.c_double),
@@ -439,14 +440,15 @@ class Solver:
         _check(lib().pimqap_solver_result(self.h, C.byref(r)))
         return _result_dict(r, perm, energies)
 
-    def replica(self, t: int, l: int) -> dict:
+    def replica(self, t: int, l: int, force: bool = True) -> dict:
+        """State of replica l of group t; force=False skips the force matrix (I is None)."""
         n = self.n
         phi = np.zeros(n, np.int32)
-        I = np.zeros((n, n), np.int64)
+        I = np.zeros((n, n), np.int64) if force else None
         E = np.zeros(1, np.int64)
         bE = np.zeros(1, np.int64)
         b = np.zeros(1, np.float64)
-        _check(lib().pimqap_solver_replica(self.h, t, l, phi.ctypes.data, I.ctypes.data,
+        _check(lib().pimqap_solver_replica(self.h, t, l, phi.ctypes.data, I.ctypes.data if force else None,
                                            E.ctypes.data, bE.ctypes.data, b.ctypes.data))
         return dict(phi=phi, I=I, E=int(E[0]), bestE=int(bE[0]), beta=float(b[0]))
 

@@ -61,6 +61,10 @@ CASES = {
     "hot_cutoff_min": (lambda: instances.uniform(16, 22), 1, 5, 2, 1e-6, 1.1, 10, {}),
     "threads64_n40": (lambda: instances.uniform(40, 23), 1, 4, 2, 0.02, 1.3, 6, {"threads_per_block": 64}),
     "threads256_n40": (lambda: instances.uniform(40, 23), 1, 4, 2, 0.02, 1.3, 6, {"threads_per_block": 256}),
+    # one warp per replica (32 threads, up to 4 candidates per lane)
+    "threads32_n32_groups": (lambda: instances.uniform(32, 42), 3, 4, 1, 10.0, 1.5849, 12, {"threads_per_block": 32}),
+    "threads32_n120_asym": (lambda: asym(120, 43), 1, 3, 2, 0.002, 1.5, 3, {"threads_per_block": 32}),
+    "binary_n64_t32": (lambda: binary(64, 44), 2, 3, 2, 0.02, 1.3, 5, {"threads_per_block": 32}),
     "n1_trivial": (lambda: instances.uniform(1, 24), 1, 2, 1, 1.0, 1.2, 3, {}),
     "n5_tiny": (lambda: instances.uniform(5, 25), 2, 3, 2, 0.05, 1.3, 6, {}),
     "grid_n256_cluster4": (lambda: instances.grid256(27), 1, 2, 1, 0.0015, 1.5, 2, {"cluster_size": 4}),
@@ -106,8 +110,9 @@ CASES = {
 }
 
 
-def run_case(gpu, oracle, name, seed=7):
+def run_case(gpu, oracle, name, seed=7, **override):
     make, T, R, spe, bmax, ratio, M, extra = CASES[name]
+    extra = dict(extra, **override)
     inst = make()
     cap = max(R, 10)
     p = gpu.default_params(replicas=R, groups=T, sweeps_per_exchange=spe, beta_max=bmax,
@@ -284,3 +289,56 @@ def test_pairing_is_rejected_where_it_cannot_run(gpu):
     p = gpu.default_params(replicas=1, groups=1, beta_max=0.002, max_megaiters=1, replica_pairing=2)
     with pytest.raises(gpu.PimqapError):             # one replica: nothing to pair
         gpu.solve(g.F, g.D, p)
+
+
+# Both launch modes on shapes of every kernel: 1 = a launch per mega-iteration (CUDA graphs of
+# chunks), 2 = one persistent launch per run call with the device-side barrier between
+# mega-iterations.  Each must leave exactly the oracle's state.
+LAUNCH_CASES = ["plain_n32_R16", "groups_T3_R5_i4", "threads32_n32_groups", "asym_n37_cluster4_t64", "int64_forced_n24",
+                "grid_n256_cluster", "binary_n90_single_cta", "clique20_n64_single_cta",
+                "heavy_n256_cluster4_i4", "cold_forced_swaps", "n1_trivial"]
+
+
+@pytest.mark.parametrize("mode", [1, 2])
+@pytest.mark.parametrize("name", LAUNCH_CASES)
+def test_launch_modes_match_oracle(gpu, oracle, name, mode):
+    inst, st, bad, res = run_case(gpu, oracle, name, launch_mode=mode)
+    assert not bad, bad[:10]
+    assert res["megaiters_done"] == CASES[name][6]
+
+
+def test_persistent_runs_in_several_calls_and_stops_on_the_goal(gpu, oracle):
+    """Run calls continue where the last one stopped, and the goal stops the persistent launch
+    at the oracle's mega-iteration."""
+    inst = instances.uniform(24, 51)
+    kw = dict(T=2, R=6, spe=1, beta_max=0.05, beta_ratio=1.3, seed=9, cap=10)
+    st = oracle_after(oracle, inst.F, inst.D, megaiters=30, **kw)
+    goal = int(st.single_best) + 500
+    st2 = oracle.setup(inst.D, inst.F, 2, 6, 1, 0.05 * 1.44269504089, 1.3, 9, cap=10)
+    assert oracle.run(st2, inst.D, inst.F, 100, goal) == 1
+    p = gpu.default_params(replicas=6, groups=2, sweeps_per_exchange=1, beta_max=0.05, beta_ratio=1.3,
+                           seed=9, max_megaiters=100, goal=goal, launch_mode=2)
+    with gpu.Solver(inst.F, inst.D, p) as s:
+        for _ in range(10):
+            s.run(3)
+        r = s.result()
+    assert r["stopped_by"] == 1 and r["target_megaiter"] == st2.target_megaiter
+    assert r["megaiters_done"] == st2.megaiters_done
+    inst = instances.uniform(20, 52)
+    p = gpu.default_params(replicas=4, groups=3, sweeps_per_exchange=2, beta_max=0.04, beta_ratio=1.3,
+                           seed=3, launch_mode=2)
+    with gpu.Solver(inst.F, inst.D, p) as s:
+        for m in (1, 4, 2, 7):
+            s.run(m)
+        st = oracle_after(oracle, inst.F, inst.D, T=3, R=4, spe=2, beta_max=0.04, beta_ratio=1.3, seed=3,
+                          cap=10, megaiters=14)
+        assert not compare_solver_to_oracle(s, st, 10)
+
+
+def test_persistent_mode_is_rejected_where_it_cannot_run(gpu):
+    inst = instances.uniform(20, 53)
+    p = gpu.default_params(replicas=4, groups=1, beta_max=0.04, max_megaiters=2, launch_mode=2,
+                           event_capacity=16)
+    with pytest.raises(gpu.PimqapError) as e:        # an event log is drained between launches
+        gpu.solve(inst.F, inst.D, p)
+    assert e.value.status == 1 and "launch_mode" in str(e.value)
