@@ -420,61 +420,128 @@ def _sweeps_proposals(n: int, replicas: int, sweeps: int) -> float:
     return float(replicas) * sweeps * n * (n - 1) / 2.0
 
 
-def run_batch_suite(args):
-    """512 instances, n ~ U[20, 150], uniform [0, 99] flows and distances, 32 replicas each,
-    2000 sweeps (500 mega-iterations of 4), in persistent launches.  Reports throughput of the
-    fixed-work batch and time-to-target against per-instance targets from a run twice as long
-    (gap <= 0.1 %), for the batch and for the plain form (one pimqap_solve per instance, one
-    instance per launch), the latter timed on every 16th instance and scaled to 512."""
+def _ref_best(F, D, replicas, sweeps, b0, ratio, seconds_cap=120.0):
+    """Best energy the reference's own CPU code (oracle/_ref, its std::mt19937 seeded from
+    random_device) reaches on one instance: one parallel-tempering group per host thread, each
+    `sweeps` sweeps (fewer when that would pass seconds_cap).  None when it is not built."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    from oracle import RefHarness, ref_available
+    if not ref_available("big_mt"):
+        return None
+    ref = RefHarness("big_mt")
+    cores = max(1, min(os.cpu_count() or 1, ref.maxt))
+    ref.load(F, D)
+    ref.setup_replicated(cores, replicas, 4, b0, ratio, 1)
+    t1 = ref.run(1)
+    m = max(1, min(sweeps // 4, int(seconds_cap / max(t1, 1e-4))))
+    el = ref.run(m - 1) if m > 1 else 0.0
+    best = min(min(ref.replica(t, l)["bestE"] for l in range(replicas)) for t in range(cores))
+    best = min(best, ref.single_best())
+    return {"best": int(best), "groups": cores, "sweeps": 4 * m, "seconds": t1 + el}
+
+
+def run_ttt_suite(args, name, batch, replicas, ladder, budget, plain_every, xcheck):
+    """One batch of `batch` instances, `replicas` replicas each on `ladder`, `budget` sweeps:
+
+    - the autotuner's choice per class (pimqap_batch_tune) and the fixed-work batch with the
+      tuned shapes and with the fixed rules' shapes (PIMQAP_AUTOTUNE=0): proposals/s of each;
+    - targets: the best energy of a run four times as long (other seeds), cross-checked on
+      `xcheck` instances against the reference's own CPU code (best over one group per host
+      thread) - a target above the reference's best is reported;
+    - time to target (gap <= 0.1 %) of the batch and of the plain form (one pimqap_solve per
+      instance, one instance per launch, every `plain_every`-th instance timed and scaled), both
+      with the long run's budget; instances that miss it within the budget are counted as
+      censored, not as reached."""
     import pimqap
-    batch = instances.uniform_batch(args.batch_instances)
-    M = max(1, args.batch_sweeps // 4)
-    b0, ratio = LADDER_UNIFORM
+    b0, ratio = ladder
+    M = max(1, budget // 4)
 
     def params(seed, **kw):
-        return pimqap.default_params(replicas=32, groups=1, sweeps_per_exchange=4, beta_max=b0,
+        return pimqap.default_params(replicas=replicas, groups=1, sweeps_per_exchange=4, beta_max=b0,
                                      beta_ratio=ratio, beta_internal=1, seed=seed, **kw)
 
     pairs = [(b.F, b.D) for b in batch]
+    props = sum(_sweeps_proposals(b.n, replicas, 4 * M) for b in batch)
     pimqap.batch_solve(pairs[:2], [params(1, max_megaiters=2), params(2, max_megaiters=2)])   # warm-up
     t0 = time.perf_counter()
-    fixed = pimqap.batch_solve(pairs, [params(k + 1, max_megaiters=M) for k in range(len(batch))])
-    fixed_wall = time.perf_counter() - t0
-    props = sum(_sweeps_proposals(b.n, 32, 4 * M) for b in batch)
+    tuning = pimqap.batch_tune(pairs, [params(k + 1, max_megaiters=M) for k in range(len(batch))])
+    tune_wall = time.perf_counter() - t0
+
+    def fixed_work(autotune):
+        os.environ["PIMQAP_AUTOTUNE"] = "1" if autotune else "0"
+        try:
+            t0 = time.perf_counter()
+            res = pimqap.batch_solve(pairs, [params(k + 1, max_megaiters=M) for k in range(len(batch))])
+            return time.perf_counter() - t0, res
+        finally:
+            os.environ.pop("PIMQAP_AUTOTUNE", None)
+
+    rules_wall, _ = fixed_work(False)
+    fixed_wall, fixed = fixed_work(True)
     if args.batch_fixed_only:   # the fixed-work batch alone (profiling)
-        print(json.dumps({"suite": "batch", "instances": len(batch), "sweeps": 4 * M, "wall_s": fixed_wall,
-                          "proposals_per_s_wall": props / fixed_wall}))
+        print(json.dumps({"suite": name, "instances": len(batch), "sweeps": 4 * M, "wall_s": fixed_wall,
+                          "proposals_per_s_wall": props / fixed_wall, "fixed_rules_wall_s": rules_wall}))
         return
     t0 = time.perf_counter()
-    longrun = pimqap.batch_solve(pairs, [params(10 ** 6 + k, max_megaiters=2 * M) for k in range(len(batch))])
+    longrun = pimqap.batch_solve(pairs, [params(10 ** 6 + k, max_megaiters=4 * M) for k in range(len(batch))])
     long_wall = time.perf_counter() - t0
     targets = [min(l["best_energy"], f["best_energy"]) for l, f in zip(longrun, fixed)]
-    goals = [int(t * 1.001) for t in targets]
+    goals = [int(t + abs(t) // 1000) for t in targets]          # gap <= 0.1 %
+    checks = []
+    for k in range(0, len(batch), max(1, len(batch) // max(1, xcheck)))[:xcheck]:
+        got = _ref_best(batch[k].F, batch[k].D, replicas, args.xcheck_sweeps, b0, ratio)
+        if got:
+            got.update(instance=k, n=batch[k].n, target=targets[k],
+                       target_at_or_below_reference=targets[k] <= got["best"])
+            checks.append(got)
     t0 = time.perf_counter()
-    res = pimqap.batch_solve(pairs, [params(k + 1, max_megaiters=M, goal=goals[k]) for k in range(len(batch))])
+    res = pimqap.batch_solve(pairs, [params(k + 1, max_megaiters=4 * M, goal=goals[k]) for k in range(len(batch))])
     batch_ttt = time.perf_counter() - t0
     reached = sum(1 for r in res if r["stopped_by"] == 1)
-    sample = list(range(0, len(batch), 16))
+    ttt_each = sorted(r["time_to_target_ms"] for r in res if r["stopped_by"] == 1)
+    sample = list(range(0, len(batch), plain_every))
     t0 = time.perf_counter()
     plain_reached = 0
     for k in sample:
-        r = pimqap.solve(batch[k].F, batch[k].D, params(k + 1, max_megaiters=M, goal=goals[k]))
+        r = pimqap.solve(batch[k].F, batch[k].D, params(k + 1, max_megaiters=4 * M, goal=goals[k]))
         plain_reached += r["stopped_by"] == 1
     plain_sample = time.perf_counter() - t0
     plain_total = plain_sample * len(batch) / len(sample)
-    line = {"suite": "batch", "metric": "time-to-target (<=0.1% gap) and swap proposals/sec",
-            "instances": len(batch), "n_range": [20, 150], "replicas": 32, "sweeps": 4 * M,
+    line = {"suite": name, "metric": "time-to-target (<=0.1% gap) and swap proposals/sec",
+            "instances": len(batch), "n_range": [min(b.n for b in batch), max(b.n for b in batch)],
+            "replicas": replicas, "sweeps": 4 * M,
             "ladder": {"beta0_internal": b0, "beta_ratio": ratio},
-            "fixed_work": {"wall_s": fixed_wall, "device_ms_first_class": fixed[0]["device_ms"],
-                           "proposals_per_s_wall": props / fixed_wall,
+            "autotuner": {"wall_s": tune_wall, "classes": tuning},
+            "fixed_work": {"wall_s": fixed_wall, "proposals_per_s_wall": props / fixed_wall,
+                           "fixed_rules_wall_s": rules_wall, "fixed_rules_proposals_per_s_wall": props / rules_wall,
                            "accept_rate": sum(r["accepts"] for r in fixed) / sum(r["updates"] for r in fixed)},
-            "targets": "best of a 4000-sweep batch run (other seeds) and the 2000-sweep run; goal = target * 1.001",
+            "targets": f"best of a {16 * M}-sweep batch run (other seeds) and the {4 * M}-sweep run; "
+                       f"goal = target + |target| // 1000",
             "long_run_wall_s": long_wall,
+            "reference_cross_check": checks,
+            "ttt_budget_sweeps": 16 * M,
             "batch_time_to_target_s": batch_ttt, "batch_reached": reached,
+            "batch_censored": len(batch) - reached,
+            "batch_ttt_ms_p50_p90_of_reached": [ttt_each[len(ttt_each) // 2], ttt_each[int(0.9 * len(ttt_each))]]
+            if ttt_each else None,
             "plain_time_to_target_s_est": plain_total, "plain_sampled": len(sample),
             "plain_reached_in_sample": plain_reached,
             "speedup_vs_plain": plain_total / batch_ttt}
     print(json.dumps(line))
+
+
+def run_batch_suite(args):
+    """512 instances, n ~ U[20, 150], uniform [0, 99] flows and distances, 32 replicas each,
+    2000 sweeps, in persistent launches (run_ttt_suite)."""
+    batch = instances.uniform_batch(args.batch_instances)
+    run_ttt_suite(args, "batch", batch, 32, LADDER_UNIFORM, args.batch_sweeps, 16, args.xcheck)
+
+
+def run_heavy_suite(args):
+    """128 heavy-tailed instances, n ~ U[100, 256] (lognormal flows with 70 % zeros, Euclidean
+    distances), 64 replicas each, int64 energies (run_ttt_suite)."""
+    batch = instances.heavy_batch(args.heavy_instances)
+    run_ttt_suite(args, "heavy", batch, 64, LADDER_HEAVY, args.heavy_sweeps, 8, args.xcheck)
 
 
 def run_serve_suite(args):
@@ -608,7 +675,7 @@ def main():
     ap.add_argument("--threads", type=int, default=0, help="threads per replica and CTA (0 = automatic)")
     ap.add_argument("--pairing", type=int, default=0, choices=[0, 1, 2],
                     help="replicas per CTA set of the binary-flow kernel: 0 = automatic, 1, 2")
-    ap.add_argument("--suite", choices=["headline", "batch", "serve", "divergence"], default="headline",
+    ap.add_argument("--suite", choices=["headline", "batch", "heavy", "serve", "divergence"], default="headline",
                     help="headline: the n=256 workload (the driver's line); batch / serve: the other "
                          "workloads; divergence: GPU vs oracle decisions over a long stream")
     ap.add_argument("--div-updates", type=int, default=10_000_000,
@@ -617,7 +684,13 @@ def main():
     ap.add_argument("--batch-instances", type=int, default=512, help="batch suite: instances")
     ap.add_argument("--batch-sweeps", type=int, default=2000, help="batch suite: sweeps per instance")
     ap.add_argument("--batch-fixed-only", action="store_true",
-                    help="batch suite: run only the fixed-work batch (profiling)")
+                    help="batch / heavy suites: run only the fixed-work batch (profiling)")
+    ap.add_argument("--heavy-instances", type=int, default=128, help="heavy suite: instances")
+    ap.add_argument("--heavy-sweeps", type=int, default=1000, help="heavy suite: sweeps per instance")
+    ap.add_argument("--xcheck", type=int, default=4,
+                    help="batch / heavy suites: instances whose targets are checked against the reference's CPU code")
+    ap.add_argument("--xcheck-sweeps", type=int, default=2000,
+                    help="batch / heavy suites: sweeps of each reference group in that check (capped at 120 s)")
     ap.add_argument("--rate", type=float, default=200.0, help="serve suite: arrivals per second")
     ap.add_argument("--duration", type=float, default=5.0, help="serve suite: seconds of arrivals")
     ap.add_argument("--drain", type=float, default=180.0, help="serve suite: seconds allowed after arrivals end")
@@ -626,6 +699,9 @@ def main():
         ap.error("--warmup must be >= 3")
     if args.suite == "batch":
         run_batch_suite(args)
+        return
+    if args.suite == "heavy":
+        run_heavy_suite(args)
         return
     if args.suite == "serve":
         run_serve_suite(args)

@@ -116,12 +116,13 @@ typedef struct pimqap_params {
                                     over one shared copy of the instance, so their update chains
                                     interleave.  Same results either way.  pimqap_solve / solver
                                     handles only */
-    int32_t launch_mode;         /* 0 = automatic: one persistent launch per run call when every
-                                    replica can be resident at once and no event log is kept,
-                                    else a launch per mega-iteration; 1 = a launch per
-                                    mega-iteration (CUDA graphs of megaiters_per_launch);
-                                    2 = persistent (rejected when it cannot run).  Same results
-                                    either way.  pimqap_solve / solver handles only */
+    int32_t launch_mode;         /* 0 = automatic (= 1, measured as fast or faster);
+                                    1 = a launch per mega-iteration (CUDA graphs of
+                                    megaiters_per_launch); 2 = one persistent launch per run
+                                    call with a device-side barrier between mega-iterations
+                                    (every replica resident at once, no event log; rejected
+                                    otherwise).  Same results either way.  pimqap_solve /
+                                    solver handles only */
 } pimqap_params;
 
 #define PIMQAP_RULE_SEQUENTIAL 0
@@ -306,6 +307,28 @@ pimqap_status pimqap_batch_submit(const pimqap_instance *insts, const pimqap_par
 pimqap_status pimqap_batch_poll(pimqap_batch *b);
 pimqap_status pimqap_batch_wait(pimqap_batch *b, double timeout_s);
 void pimqap_batch_release(pimqap_batch *b);
+
+/* The autotuner of the batched solve (no reference counterpart): a batch's instances fall into
+   classes (force width x CTAs per replica x band of n), each run by one persistent launch.  For
+   each class shape it has not seen yet in this process, the tuner times one mega-iteration of
+   the class's instances under every candidate worker shape (threads per replica 32-256 x
+   replicas per CTA) and keeps the fastest; pimqap_batch_solve then uses the cached choice.
+   Shapes never change results.  pimqap_batch_tune runs the tuner on a batch without solving it
+   and reports each class; with PIMQAP_AUTOTUNE=0 in the environment the batch keeps the fixed
+   rules' shapes (the report then has tried = 0). */
+typedef struct pimqap_class_tuning {
+    int32_t force_bits, cluster_size, band, n_max, members;
+    int32_t threads, workers, grid;              /* the shape in use: threads per replica,
+                                                    replicas per CTA, CTAs of the launch */
+    int32_t fixed_threads, fixed_workers;        /* the fixed rules' shape */
+    int32_t tried;                               /* shapes timed when the class was tuned */
+    int32_t pad;
+    double fixed_ms, tuned_ms;                   /* device time of one mega-iteration of the
+                                                    class's instances under each shape */
+} pimqap_class_tuning;
+pimqap_status pimqap_batch_tune(const pimqap_instance *insts, const pimqap_params *params,
+                                int32_t count, pimqap_class_tuning *classes, int32_t capacity,
+                                int32_t *class_count);
 
 /* ---------------------------------------------------------------- serving */
 

@@ -1,12 +1,15 @@
 // pimqap_batch.cpp - batched solve: many independent instances of uneven n in persistent
 // launches (no reference counterpart: the reference solves one instance per process).
 //
-// The autotuner partitions a batch into classes: force-matrix width x CTAs per replica
-// (1, 2 or 4) x, for single-CTA replicas, a band of n.  Each class is one persistent launch
-// whose workers (a group of warps with its own named barrier and shared-memory slice, or a
-// whole cluster) pop replica-epochs from a device queue.  The classes run concurrently on
-// separate streams, their grids split the SMs in proportion to estimated work.  Results are
-// gathered on the device and read back in one copy per class.
+// A batch is partitioned into classes: force-matrix width x CTAs per replica (1, 2 or 4) x,
+// for single-CTA replicas, a band of n.  Each class is one persistent launch whose workers (a
+// group of warps with its own named barrier and shared-memory slice, or a whole cluster) pop
+// replica-epochs from a device queue.  The classes run concurrently on separate streams, each
+// with a grid that fills the GPU, largest class first.  The autotuner (tune_classes) times one
+// mega-iteration of a class's instances under each candidate worker shape - threads per
+// replica and replicas (workers) per CTA - and keeps the fastest; the choice is cached per
+// class shape for the rest of the process.  Results are gathered on the device and read back
+// in one copy per class.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -17,7 +20,10 @@
 #include <cstdlib>
 #include <cstring>
 #include <limits>
+#include <map>
 #include <memory>
+#include <mutex>
+#include <tuple>
 #include <string>
 #include <thread>
 #include <vector>
@@ -72,6 +78,8 @@ std::vector<BatchClass> plan_classes(const std::vector<Plan> &plans, const std::
     double total = 0;
     for (auto &c : classes) total += c.work;
     for (auto &c : classes) {
+        c.nmax = 0;
+        for (int k : c.members) c.nmax = std::max(c.nmax, plans[k].n);
         int nmax = 0;
         size_t slice = 0;
         for (int k : c.members) {
@@ -96,11 +104,149 @@ std::vector<BatchClass> plan_classes(const std::vector<Plan> &plans, const std::
         // their own streams, and a class's CTAs start on the SMs the previous classes' workers
         // release when their work runs out.
         c.grid = (c.cl == 1) ? sms * occ : occ * c.cl;   // occ: resident clusters for cl > 1
-        (void)total;
     }
+    (void)total;
     std::stable_sort(classes.begin(), classes.end(),
                      [](const BatchClass &a, const BatchClass &b) { return a.work > b.work; });
     return classes;
+}
+
+// ------------------------------------------------------------------ the autotuner
+
+namespace {
+
+struct TuneKey {
+    int bits, cl, band, nmax16, spe;
+    bool operator<(const TuneKey &o) const {
+        return std::tie(bits, cl, band, nmax16, spe) < std::tie(o.bits, o.cl, o.band, o.nmax16, o.spe);
+    }
+};
+std::mutex g_tune_mu;
+std::map<TuneKey, ClassTuning> g_tune;
+
+TuneKey key_of(const BatchClass &c, const std::vector<Plan> &plans) {
+    int spe = 0;
+    for (int k : c.members) spe = std::max(spe, plans[k].spe);
+    return TuneKey{c.bits, c.cl, c.band, (c.nmax + 15) / 16, spe};
+}
+
+// Worker shapes a class can run: threads per replica from 32 to 256 (every lane holds at most
+// four candidates, the launch at most 256 threads), as many workers per CTA as shared memory
+// and the launch allow.  Cluster classes run one worker per CTA of 128 or 256 threads.
+std::vector<std::pair<int, int>> tune_candidates(const BatchClass &c, int maxsm) {
+    std::vector<std::pair<int, int>> out;
+    for (int wt : {32, 64, 128, 256}) {
+        if (c.cl > 1 && wt < 128) continue;
+        if ((c.nmax + wt - 1) / wt > 4) continue;
+        if (c.cl > 1) {
+            out.emplace_back(wt, 1);
+            continue;
+        }
+        for (int w = 1; w * wt <= 256 && (size_t)w * c.slice <= (size_t)maxsm; ++w) out.emplace_back(wt, w);
+    }
+    return out;
+}
+
+// The grid of a shape: every SM filled with as many CTAs (clusters) as fit.
+int shape_grid(const BatchClass &c, int sms) {
+    int occ = 0;
+    if (pimqap::batch_occupancy(c.bits, c.cl, c.workers * c.worker_threads, c.workers * c.slice, &occ) !=
+            cudaSuccess || occ < 1) {
+        cudaGetLastError();
+        occ = 1;
+    }
+    return (c.cl == 1) ? sms * occ : occ * c.cl;
+}
+
+}  // namespace
+
+bool autotune_enabled() {
+    const char *v = std::getenv("PIMQAP_AUTOTUNE");
+    return !(v && v[0] == '0');
+}
+
+pimqap_status tune_classes(const pimqap_instance *insts, const pimqap_params *params, int32_t count,
+                           const std::vector<Plan> &plans, std::vector<BatchClass> &classes, int sms,
+                           int maxsm, std::vector<ClassTuning> *report) {
+    for (auto &c : classes) {
+        const TuneKey key = key_of(c, plans);
+        ClassTuning t{};
+        bool cached = false;
+        {
+            std::lock_guard<std::mutex> lk(g_tune_mu);
+            auto it = g_tune.find(key);
+            if (it != g_tune.end()) {
+                t = it->second;
+                cached = true;
+            }
+        }
+        const auto cands = tune_candidates(c, maxsm);
+        int64_t reps = 0;
+        for (int k : c.members) reps += (int64_t)plans[k].T * plans[k].R;
+        if (!cached && cands.size() > 1 && reps > 0) {
+            // one mega-iteration of every member, no goal: the same work under every shape
+            std::vector<pimqap_params> tp(params, params + count);
+            for (int k : c.members) {
+                tp[k].max_megaiters = 1;
+                tp[k].goal = std::numeric_limits<int64_t>::min();
+                tp[k].timeout_s = 0;
+            }
+            std::vector<pimqap_result> scratch(count);
+            for (auto &r : scratch) std::memset(&r, 0, sizeof(r));
+            double work = 0;
+            for (int k : c.members) work += instance_work(plans[k], 1);
+            t.fixed_threads = c.worker_threads;
+            t.fixed_workers = c.workers;
+            double best_ms = 0;
+            for (const auto &cand : cands) {
+                BatchClass cc = c;
+                cc.worker_threads = cand.first;
+                cc.workers = cand.second;
+                cc.grid = shape_grid(cc, sms);
+                ClassRun run;
+                pimqap_status st = run.prepare(insts, tp.data(), plans, cc);
+                if (st == PIMQAP_OK) st = run.launch();
+                if (st == PIMQAP_OK) st = run.finish(plans, scratch.data());
+                if (st != PIMQAP_OK) return st;
+                const double ms = run.device_ms;
+                ++t.tried;
+                if (cand.first == c.worker_threads && cand.second == c.workers) t.fixed_ms = ms;
+                if (best_ms == 0 || ms < best_ms) {
+                    best_ms = ms;
+                    t.threads = cand.first;
+                    t.workers = cand.second;
+                }
+            }
+            t.tuned_ms = best_ms;
+            t.work = work;
+            std::lock_guard<std::mutex> lk(g_tune_mu);
+            g_tune[key] = t;
+            cached = true;
+        }
+        if (cached && t.threads > 0) {
+            c.worker_threads = t.threads;
+            c.workers = t.workers;
+            c.grid = shape_grid(c, sms);
+        }
+        if (report) {
+            ClassTuning r = t;
+            r.bits = c.bits;
+            r.cl = c.cl;
+            r.band = c.band;
+            r.nmax = c.nmax;
+            r.members = (int)c.members.size();
+            r.threads = c.worker_threads;
+            r.workers = c.workers;
+            r.grid = c.grid;
+            report->push_back(r);
+        }
+        if (std::getenv("PIMQAP_TRACE"))
+            std::fprintf(stderr, "[pimqap] tuned class bits=%d cl=%d band=%d nmax=%d: %d x %d threads "
+                                 "(fixed rule %d x %d: %.3f ms, tuned %.3f ms, %d shapes timed)\n",
+                         c.bits, c.cl, c.band, c.nmax, c.workers, c.worker_threads, t.fixed_workers,
+                         t.fixed_threads, t.fixed_ms, t.tuned_ms, t.tried);
+    }
+    return PIMQAP_OK;
 }
 
 // One class: instance heads in one pinned image (one copy), tails cleared in one memset,
@@ -361,7 +507,11 @@ pimqap_status batch_solve(const pimqap_instance *insts, const pimqap_params *par
         megaiters[k] = params[k].max_megaiters;
     }
     trace("batch: plans");
-    const std::vector<BatchClass> classes = plan_classes(plans, megaiters, sms, maxsm, 0);
+    std::vector<BatchClass> classes = plan_classes(plans, megaiters, sms, maxsm, 0);
+    if (autotune_enabled()) {
+        st = tune_classes(insts, params, count, plans, classes, sms, maxsm, nullptr);
+        if (st != PIMQAP_OK) return st;
+    }
     if (std::getenv("PIMQAP_TRACE"))
         for (const auto &c : classes)
             std::fprintf(stderr, "[pimqap] class bits=%d cl=%d band=%d members=%zu work=%.3g grid=%d workers=%d x %d threads slice=%zu\n",
@@ -396,6 +546,58 @@ pimqap_status batch_solve(const pimqap_instance *insts, const pimqap_params *par
 
 }  // namespace detail
 }  // namespace pimqap
+
+extern "C" pimqap_status pimqap_batch_tune(const pimqap_instance *insts, const pimqap_params *params,
+                                           int32_t count, pimqap_class_tuning *out, int32_t capacity,
+                                           int32_t *class_count) {
+    if (count < 1 || !insts || !params || !class_count || capacity < 0 || (capacity > 0 && !out))
+        return fail(PIMQAP_ERR_ARG, "bad tuning arguments");
+    *class_count = 0;
+    for (int k = 0; k < count; ++k) {
+        pimqap_status st = check_params(&insts[k], &params[k]);
+        if (st != PIMQAP_OK) return st;
+        if (params[k].active_facilities > 0 || params[k].update_rule != PIMQAP_RULE_SEQUENTIAL ||
+            params[k].device != params[0].device)
+            return fail(PIMQAP_ERR_ARG, "batch entries: sequential rule, no active_facilities, one device");
+    }
+    int maxsm = 0;
+    pimqap_status st = open_device(params[0].device, &maxsm);
+    if (st != PIMQAP_OK) return st;
+    int sms = 0;
+    PQ_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, params[0].device));
+    std::vector<Plan> plans(count);
+    std::vector<int64_t> megaiters(count);
+    for (int k = 0; k < count; ++k) {
+        st = plan_instance(&insts[k], &params[k], (size_t)maxsm, params[k].cluster_size, &plans[k]);
+        if (st != PIMQAP_OK) return st;
+        megaiters[k] = params[k].max_megaiters;
+    }
+    std::vector<BatchClass> classes = plan_classes(plans, megaiters, sms, maxsm, 0);
+    std::vector<ClassTuning> report;
+    if (autotune_enabled()) {
+        st = tune_classes(insts, params, count, plans, classes, sms, maxsm, &report);
+        if (st != PIMQAP_OK) return st;
+    } else {
+        for (const auto &c : classes) {
+            ClassTuning r{};
+            r.bits = c.bits; r.cl = c.cl; r.band = c.band; r.nmax = c.nmax;
+            r.members = (int)c.members.size(); r.threads = c.worker_threads; r.workers = c.workers;
+            r.grid = c.grid; r.fixed_threads = c.worker_threads; r.fixed_workers = c.workers;
+            report.push_back(r);
+        }
+    }
+    *class_count = (int32_t)report.size();
+    for (int i = 0; i < (int)report.size() && i < capacity; ++i) {
+        const ClassTuning &r = report[i];
+        pimqap_class_tuning &o = out[i];
+        std::memset(&o, 0, sizeof(o));
+        o.force_bits = r.bits; o.cluster_size = r.cl; o.band = r.band; o.n_max = r.nmax;
+        o.members = r.members; o.threads = r.threads; o.workers = r.workers; o.grid = r.grid;
+        o.fixed_threads = r.fixed_threads; o.fixed_workers = r.fixed_workers; o.tried = r.tried;
+        o.fixed_ms = r.fixed_ms; o.tuned_ms = r.tuned_ms;
+    }
+    return PIMQAP_OK;
+}
 
 namespace {
 

@@ -18,6 +18,7 @@ namespace detail {
 // single-CTA replicas, one band of n), with the worker shape and grid picked for them.
 struct BatchClass {
     int bits = 32, cl = 1, band = 0;
+    int nmax = 0;                 // largest n among the members
     std::vector<int> members;     // indices into the batch
     double work = 0;              // estimated cost (relative)
     int worker_threads = 128;     // threads of one replica worker
@@ -29,10 +30,30 @@ struct BatchClass {
 // Relative cost of an instance: updates x (candidates + expected force-update share).
 double instance_work(const Plan &P, int64_t megaiters);
 
-// The autotuner: partitions plans into classes, picks worker shapes from the n range and the
-// occupancy of each shape, and splits the SMs between classes in proportion to work.
+// The fixed rules: partitions plans into classes and picks worker shapes from the n range and
+// the occupancy of each shape (tune_classes then measures the alternatives).
 std::vector<BatchClass> plan_classes(const std::vector<Plan> &plans, const std::vector<int64_t> &megaiters,
                                      int sms, int maxsm, int force_cluster);
+
+// What the autotuner measured for a class shape (device time of one mega-iteration of the
+// class's instances under the fixed rules' worker shape and under the fastest one).
+struct ClassTuning {
+    int bits = 0, cl = 0, band = 0, nmax = 0, members = 0;
+    int threads = 0, workers = 0, grid = 0;   // the shape in use
+    int fixed_threads = 0, fixed_workers = 0; // the fixed rules' shape
+    int tried = 0;                            // shapes timed (0: from the cache or nothing to choose)
+    double fixed_ms = 0, tuned_ms = 0, work = 0;
+};
+
+// PIMQAP_AUTOTUNE=0 in the environment turns the autotuner off (the fixed rules' shapes).
+bool autotune_enabled();
+
+// The autotuner: for every class whose shape is not cached yet, times one mega-iteration of its
+// members under each candidate worker shape and keeps the fastest (shapes never change results);
+// applies the cached choice to every class.  `report` (may be null) receives one entry per class.
+pimqap_status tune_classes(const pimqap_instance *insts, const pimqap_params *params, int32_t count,
+                           const std::vector<Plan> &plans, std::vector<BatchClass> &classes, int sms,
+                           int maxsm, std::vector<ClassTuning> *report);
 
 // Device state and stream of one class launch.
 struct ClassRun {

@@ -2335,7 +2335,7 @@ __global__ void __launch_bounds__(KIND == 2 ? 512 : 256, (CL == 4 && KIND != 2) 
             s.finish[g] = 0u;
             s.epoch[g] = e + 1;
             __threadfence();
-            if (atomicAdd(s.finish_all, 1u) == (unsigned)s.T - 1u) {
+            if (s.T == 1 || atomicAdd(s.finish_all, 1u) == (unsigned)s.T - 1u) {
                 *s.finish_all = 0u;
                 if (s.kill && *s.kill) atomicMin(s.stop_epoch, e + 1);
                 __threadfence();

@@ -38,6 +38,14 @@ class Instance(C.Structure):
     _fields_ = [("n", C.c_int32), ("flow", C.POINTER(C.c_int32)), ("dist", C.POINTER(C.c_int32))]
 
 
+class ClassTuning(C.Structure):
+    _fields_ = [("force_bits", C.c_int32), ("cluster_size", C.c_int32), ("band", C.c_int32),
+                ("n_max", C.c_int32), ("members", C.c_int32), ("threads", C.c_int32),
+                ("workers", C.c_int32), ("grid", C.c_int32), ("fixed_threads", C.c_int32),
+                ("fixed_workers", C.c_int32), ("tried", C.c_int32), ("pad", C.c_int32),
+                ("fixed_ms", C.c_double), ("tuned_ms", C.c_double)]
+
+
 class Params(C.Structure):
     _fields_ = [
         ("replicas", C.c_int32), ("groups", C.c_int32), ("sweeps_per_exchange", C.c_int32),
@@ -146,6 +154,9 @@ def lib() -> C.CDLL:
     L.pimqap_release_kept_memory.restype = st
     L.pimqap_batch_solve.argtypes = [C.POINTER(Instance), C.POINTER(Params), C.c_int32, C.POINTER(Result)]
     L.pimqap_batch_solve.restype = st
+    L.pimqap_batch_tune.argtypes = [C.POINTER(Instance), C.POINTER(Params), C.c_int32, C.POINTER(ClassTuning),
+                                    C.c_int32, C.POINTER(C.c_int32)]
+    L.pimqap_batch_tune.restype = st
     L.pimqap_server_create.argtypes = [C.POINTER(ServerConfig), C.POINTER(C.c_void_p)]
     L.pimqap_server_create.restype = st
     L.pimqap_server_submit.argtypes = [C.c_void_p, C.POINTER(Instance), C.POINTER(Params), C.POINTER(C.c_int64)]
@@ -384,6 +395,18 @@ def solve_static(F: np.ndarray, D: np.ndarray, params: Params) -> dict:
     r.best_perm = perm.ctypes.data_as(C.POINTER(C.c_int32))
     _check(lib().pimqap_solve_static(C.byref(inst.c), C.byref(params), C.byref(r)))
     return _result_dict(r, perm)
+
+
+def batch_tune(instances: Sequence, params: Sequence[Params]) -> List[dict]:
+    """pimqap_batch_tune: the autotuner's class shapes for this batch (timing them if new)."""
+    keep = [_Inst(F, D) for F, D in instances]
+    count = len(keep)
+    insts = (Instance * count)(*[k.c for k in keep])
+    ps = (Params * count)(*params)
+    out = (ClassTuning * 64)()
+    n = C.c_int32(0)
+    _check(lib().pimqap_batch_tune(insts, ps, count, out, 64, C.byref(n)))
+    return [{k: getattr(out[i], k) for k, _ in ClassTuning._fields_ if k != "pad"} for i in range(min(n.value, 64))]
 
 
 def batch_solve(instances: Sequence, params: Sequence[Params]) -> List[dict]:

@@ -119,3 +119,26 @@ def test_heavy_batch_matches_solo_and_oracle(gpu, oracle):
             s.run(2)
             bad = compare_solver_to_oracle(s, st, 10)
         assert not bad, (k, bad[:5])
+
+
+def test_autotuner_choice_is_no_slower_and_changes_no_result(gpu, monkeypatch):
+    """The autotuner times every candidate worker shape of a class, the fixed rules' shape among
+    them, and keeps the fastest; results are the same with its shapes and with the fixed rules'."""
+    batch = instances.uniform_batch(48, n_lo=20, n_hi=150, seed=11)
+    params = [gpu.default_params(replicas=8, groups=1, sweeps_per_exchange=2, beta_max=0.02, beta_ratio=1.3,
+                                 seed=70 + k, max_megaiters=3) for k in range(len(batch))]
+    pairs = [(b.F, b.D) for b in batch]
+    report = gpu.batch_tune(pairs, params)
+    assert report
+    for c in report:
+        assert c["members"] > 0 and c["threads"] >= 32 and c["workers"] >= 1 and c["grid"] >= 1
+        if c["tried"] > 1:
+            assert c["tuned_ms"] <= c["fixed_ms"], c
+    tuned = gpu.batch_solve(pairs, params)
+    monkeypatch.setenv("PIMQAP_AUTOTUNE", "0")
+    rules = gpu.batch_solve(pairs, params)
+    off = gpu.batch_tune(pairs, params)
+    assert all(c["tried"] == 0 and (c["threads"], c["workers"]) == (c["fixed_threads"], c["fixed_workers"])
+               for c in off)
+    for k, (a, b) in enumerate(zip(tuned, rules)):
+        assert same(a, b), k

@@ -17,10 +17,14 @@ def perm_energy(inst, perm):
     return int((inst.D.astype(np.int64) * inst.F[np.ix_(perm, perm)]).sum())
 
 
-def test_timeout_ends_an_unlimited_solve(gpu):
+# launch_mode 1: the host tests the time between graph launches; 2: the persistent launch stops
+# at the next mega-iteration boundary once the host sets its kill word
+@pytest.mark.parametrize("mode", [1, 2])
+def test_timeout_ends_an_unlimited_solve(gpu, mode):
     inst = instances.uniform(40, 401)
     p = gpu.default_params(replicas=8, groups=2, sweeps_per_exchange=4, beta_max=0.05, beta_ratio=1.3,
-                           seed=3, timeout_s=0.2, max_megaiters=2 ** 40, megaiters_per_launch=16)
+                           seed=3, timeout_s=0.2, max_megaiters=2 ** 40, megaiters_per_launch=16,
+                           launch_mode=mode)
     t0 = time.perf_counter()
     r = gpu.solve(inst.F, inst.D, p)
     wall = time.perf_counter() - t0
@@ -31,16 +35,21 @@ def test_timeout_ends_an_unlimited_solve(gpu):
     assert perm_energy(inst, r["best_perm"]) == r["best_energy"]
 
 
-def test_timeout_state_matches_the_oracle(gpu, oracle):
+@pytest.mark.parametrize("mode", [1, 2])
+def test_timeout_state_matches_the_oracle(gpu, oracle, mode):
     """The mega-iterations a timed-out run completed are ordinary ones: the full replica and
-    group state equals the oracle's after that many mega-iterations."""
+    group state equals the oracle's after that many mega-iterations, and a later run call
+    continues from there."""
     inst = instances.uniform(20, 402)
     kw = dict(replicas=4, groups=2, sweeps_per_exchange=2, beta_max=0.05, beta_ratio=1.4, seed=5)
-    p = gpu.default_params(timeout_s=0.05, max_megaiters=2 ** 40, megaiters_per_launch=4, **kw)
+    p = gpu.default_params(timeout_s=0.05, max_megaiters=2 ** 40, megaiters_per_launch=4, launch_mode=mode, **kw)
     with gpu.Solver(inst.F, inst.D, p) as s:
         s.run(2 ** 40)
+        first = s.result()["megaiters_done"]
+        assert 0 < first
+        s.run(2 ** 40)                       # a second call runs on after the first one's stop
         done = s.result()["megaiters_done"]
-        assert 0 < done
+        assert done > first and s.result()["stopped_by"] == 0
         st = oracle_after(oracle, inst.F, inst.D, T=2, R=4, spe=2, beta_max=0.05, beta_ratio=1.4,
                           seed=5, cap=10, megaiters=done)
         bad = compare_solver_to_oracle(s, st, 10)
