@@ -544,22 +544,23 @@ def run_heavy_suite(args):
     run_ttt_suite(args, "heavy", batch, 64, LADDER_HEAVY, args.heavy_sweeps, 8, args.xcheck)
 
 
-def run_serve_suite(args):
-    """Poisson arrivals (rate --rate, --duration s) of QAP solves, n ~ U[30, 256], half uniform,
-    half heavy-tailed instances, 32 replicas and 2000 sweeps each, into the continuous-batching
-    server; reports p50/p99 latency of completed requests, throughput and backlog."""
+def _serve_params(pimqap, inst, k):
+    b0, ratio = LADDER_UNIFORM if inst.name.startswith("uniform") else LADDER_HEAVY
+    return pimqap.default_params(replicas=32, groups=1, sweeps_per_exchange=4, beta_max=b0,
+                                 beta_ratio=ratio, beta_internal=1, seed=k + 1, max_megaiters=500)
+
+
+def serve_once(rate, duration, drain):
+    """One Poisson trace (`rate` arrivals/s for `duration` s) into a fresh server; results are
+    collected for up to `drain` s after the last arrival.  The request sequence (instances and
+    seeds) is the same at every rate; only the arrival times scale."""
     import pimqap
-    trace = list(instances.serving_trace(rate_hz=args.rate, duration_s=args.duration))
-
-    def params(inst, k):
-        b0, ratio = LADDER_UNIFORM if inst.name.startswith("uniform") else LADDER_HEAVY
-        return pimqap.default_params(replicas=32, groups=1, sweeps_per_exchange=4, beta_max=b0,
-                                     beta_ratio=ratio, beta_internal=1, seed=k + 1, max_megaiters=500)
-
+    trace = list(instances.serving_trace(rate_hz=rate, duration_s=duration))
     # the autotuner's sample: 64 requests spread over the trace (it picks classes and SM shares
     # from them; shapes it misses still get a launch of their own)
     step = max(1, len(trace) // 64)
-    sample = [(inst.F, inst.D, params(inst, k)) for k, (_, inst) in enumerate(trace) if k % step == 0][:64]
+    sample = [(inst.F, inst.D, _serve_params(pimqap, inst, k)) for k, (_, inst) in enumerate(trace)
+              if k % step == 0][:64]
     srv = pimqap.Server(sample=sample)
     t_start = time.perf_counter()
     tickets = []
@@ -567,34 +568,93 @@ def run_serve_suite(args):
         now = time.perf_counter() - t_start
         if t_arr > now:
             time.sleep(t_arr - now)
-        tickets.append((srv.submit(inst.F, inst.D, params(inst, k)), inst))
+        tickets.append((srv.submit(inst.F, inst.D, _serve_params(pimqap, inst, k)), k, inst))
     done = {}
-    deadline = t_start + args.duration + args.drain
+    deadline = t_start + duration + drain
     while len(done) < len(tickets) and time.perf_counter() < deadline:
-        for t, inst in tickets:
+        for t, k, inst in tickets:
             if t in done:
                 continue
             r = srv.poll(t)
             if r is not None:
-                done[t] = (r, inst, time.perf_counter() - t_start)
+                done[t] = (r, k, inst, time.perf_counter() - t_start)
         time.sleep(0.01)
     st = srv.stats()
     srv.close()
-    lat = sorted(r["latency_ms"] for r, _, _ in done.values())
-    t_last = max((t for _, _, t in done.values()), default=0.0)
-    props = sum(_sweeps_proposals(inst.n, 32, r["megaiters_done"] * 4) for r, inst, _ in done.values())
+    lat = sorted(r["latency_ms"] for r, _, _, _ in done.values())
+    t_last = max((t for _, _, _, t in done.values()), default=0.0)
+    props = sum(_sweeps_proposals(inst.n, 32, r["megaiters_done"] * 4) for r, _, inst, _ in done.values())
 
     def pct(q):
         return lat[min(len(lat) - 1, int(q * len(lat)))] if lat else None
 
-    line = {"suite": "serve", "metric": "serve p50/p99 latency and throughput",
-            "rate_hz": args.rate, "duration_s": args.duration, "submitted": len(tickets),
-            "completed": len(done), "backlog_at_end": len(tickets) - len(done),
-            "p50_ms": pct(0.50), "p99_ms": pct(0.99), "max_ms": lat[-1] if lat else None,
-            "throughput_req_per_s": len(done) / t_last if t_last else 0.0,
-            "proposals_per_s": props / t_last if t_last else 0.0,
-            "admitted": st["admitted"], "pending_at_end": st["pending"],
-            "classes": st["classes"], "error_word": st["error_word"]}
+    row = {"rate_hz": rate, "duration_s": duration, "submitted": len(tickets), "completed": len(done),
+           "backlog_at_end": len(tickets) - len(done), "p50_ms": pct(0.50), "p99_ms": pct(0.99),
+           "max_ms": lat[-1] if lat else None,
+           "throughput_req_per_s": len(done) / t_last if t_last else 0.0,
+           "proposals_per_s": props / t_last if t_last else 0.0,
+           "admitted": st["admitted"], "classes": st["classes"], "error_word": st["error_word"]}
+    return row, {k: (r, inst) for r, k, inst, _ in done.values()}
+
+
+def run_serve_suite(args):
+    """Serving at the published load: Poisson arrivals of QAP solves, n ~ U[30, 256], half
+    uniform, half heavy-tailed instances, 32 replicas and 2000 sweeps each, into the
+    continuous-batching server, for --duration s.  A search over --rates finds the highest rate
+    whose p99 latency stays within --p99-bound s with no backlog; that rate and --rate (the
+    published 200 req/s) are reported with p50 / p99 latency, throughput, backlog and each
+    completed request's gap to its best-known cost (the best of a batch run four times as long,
+    other seeds)."""
+    import pimqap
+    rows = []
+    results = {}
+    for rate in [float(r) for r in args.rates.split(",") if r]:
+        row, got = serve_once(rate, args.duration, args.drain)
+        rows.append(row)
+        results[rate] = got
+    ok = [r for r in rows if r["backlog_at_end"] == 0 and r["p99_ms"] is not None
+          and r["p99_ms"] <= 1e3 * args.p99_bound]
+    best = max(ok, key=lambda r: r["rate_hz"]) if ok else None
+    over, got_over = serve_once(args.rate, args.duration, args.drain)
+    # best-known costs of every request that completed in either run
+    ks = sorted(set(k for rate in ([best["rate_hz"]] if best else []) for k in results[rate]) | set(got_over))
+    trace = list(instances.serving_trace(rate_hz=args.rate, duration_s=args.duration))
+    if best:
+        trace_b = list(instances.serving_trace(rate_hz=best["rate_hz"], duration_s=args.duration))
+        trace = trace if len(trace) >= len(trace_b) else trace_b
+    insts = {k: trace[k][1] for k in ks if k < len(trace)}
+    t0 = time.perf_counter()
+    order = sorted(insts)
+    lparams = []
+    for k in order:                      # four times the sweeps, another seed
+        p = _serve_params(pimqap, insts[k], 10 ** 6 + k)
+        p.max_megaiters = 4 * p.max_megaiters
+        lparams.append(p)
+    long = pimqap.batch_solve([(insts[k].F, insts[k].D) for k in order], lparams) if order else []
+    targets = {k: r["best_energy"] for k, r in zip(order, long)}
+    long_wall = time.perf_counter() - t0
+
+    def gaps(got):
+        g = []
+        for k, (r, inst) in got.items():
+            t = min(targets.get(k, r["best_energy"]), r["best_energy"])
+            g.append((r["best_energy"] - t) / abs(t) if t else 0.0)
+        g.sort()
+        if not g:
+            return None
+        return {"requests": len(g), "median": g[len(g) // 2], "p90": g[int(0.9 * len(g))], "max": g[-1],
+                "within_0.1pct": sum(1 for x in g if x <= 1e-3) / len(g),
+                "within_1pct": sum(1 for x in g if x <= 1e-2) / len(g)}
+
+    if best:
+        best = dict(best, gap=gaps(results[best["rate_hz"]]))
+    over = dict(over, gap=gaps(got_over))
+    line = {"suite": "serve", "metric": "serve p50/p99 latency, throughput and gap to best-known",
+            "requests": "n ~ U[30, 256], half uniform [0, 99], half heavy-tailed; 32 replicas, 2000 sweeps",
+            "duration_s": args.duration, "drain_s": args.drain, "p99_bound_s": args.p99_bound,
+            "rate_search": rows, "sustainable": best, "published_rate": over,
+            "best_known": "best of a batch run of the same request with 4x the sweeps (other seed)",
+            "best_known_wall_s": long_wall}
     print(json.dumps(line))
 
 
@@ -691,9 +751,12 @@ def main():
                     help="batch / heavy suites: instances whose targets are checked against the reference's CPU code")
     ap.add_argument("--xcheck-sweeps", type=int, default=2000,
                     help="batch / heavy suites: sweeps of each reference group in that check (capped at 120 s)")
-    ap.add_argument("--rate", type=float, default=200.0, help="serve suite: arrivals per second")
-    ap.add_argument("--duration", type=float, default=5.0, help="serve suite: seconds of arrivals")
-    ap.add_argument("--drain", type=float, default=180.0, help="serve suite: seconds allowed after arrivals end")
+    ap.add_argument("--rate", type=float, default=200.0, help="serve suite: the published arrival rate (req/s)")
+    ap.add_argument("--rates", default="2,3,4,5", help="serve suite: arrival rates searched for the highest "
+                                                     "sustainable one (comma separated)")
+    ap.add_argument("--p99-bound", type=float, default=10.0, help="serve suite: p99 latency bound (s)")
+    ap.add_argument("--duration", type=float, default=60.0, help="serve suite: seconds of arrivals")
+    ap.add_argument("--drain", type=float, default=60.0, help="serve suite: seconds allowed after arrivals end")
     args = ap.parse_args()
     if args.warmup < 3:
         ap.error("--warmup must be >= 3")
