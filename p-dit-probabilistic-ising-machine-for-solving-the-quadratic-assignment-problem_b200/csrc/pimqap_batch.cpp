@@ -116,18 +116,19 @@ std::vector<BatchClass> plan_classes(const std::vector<Plan> &plans, const std::
 namespace {
 
 struct TuneKey {
-    int bits, cl, band, nmax16, spe;
+    int bits, cl, band, nmax16, spe, one_per_sm;
     bool operator<(const TuneKey &o) const {
-        return std::tie(bits, cl, band, nmax16, spe) < std::tie(o.bits, o.cl, o.band, o.nmax16, o.spe);
+        return std::tie(bits, cl, band, nmax16, spe, one_per_sm) <
+               std::tie(o.bits, o.cl, o.band, o.nmax16, o.spe, o.one_per_sm);
     }
 };
 std::mutex g_tune_mu;
 std::map<TuneKey, ClassTuning> g_tune;
 
-TuneKey key_of(const BatchClass &c, const std::vector<Plan> &plans) {
+TuneKey key_of(const BatchClass &c, const std::vector<Plan> &plans, bool one_per_sm) {
     int spe = 0;
     for (int k : c.members) spe = std::max(spe, plans[k].spe);
-    return TuneKey{c.bits, c.cl, c.band, (c.nmax + 15) / 16, spe};
+    return TuneKey{c.bits, c.cl, c.band, (c.nmax + 15) / 16, spe, one_per_sm ? 1 : 0};
 }
 
 // Worker shapes a class can run: threads per replica from 32 to 256 (every lane holds at most
@@ -147,8 +148,10 @@ std::vector<std::pair<int, int>> tune_candidates(const BatchClass &c, int maxsm)
     return out;
 }
 
-// The grid of a shape: every SM filled with as many CTAs (clusters) as fit.
-int shape_grid(const BatchClass &c, int sms) {
+// The grid of a shape: every SM filled with as many CTAs (clusters) as fit, or with one CTA
+// (cluster) per SM.
+int shape_grid(const BatchClass &c, int sms, bool one_per_sm) {
+    if (one_per_sm) return (c.cl == 1) ? sms : (sms / c.cl) * c.cl;
     int occ = 0;
     if (pimqap::batch_occupancy(c.bits, c.cl, c.workers * c.worker_threads, c.workers * c.slice, &occ) !=
             cudaSuccess || occ < 1) {
@@ -167,9 +170,9 @@ bool autotune_enabled() {
 
 pimqap_status tune_classes(const pimqap_instance *insts, const pimqap_params *params, int32_t count,
                            const std::vector<Plan> &plans, std::vector<BatchClass> &classes, int sms,
-                           int maxsm, std::vector<ClassTuning> *report) {
+                           int maxsm, std::vector<ClassTuning> *report, bool one_per_sm) {
     for (auto &c : classes) {
-        const TuneKey key = key_of(c, plans);
+        const TuneKey key = key_of(c, plans, one_per_sm);
         ClassTuning t{};
         bool cached = false;
         {
@@ -202,7 +205,7 @@ pimqap_status tune_classes(const pimqap_instance *insts, const pimqap_params *pa
                 BatchClass cc = c;
                 cc.worker_threads = cand.first;
                 cc.workers = cand.second;
-                cc.grid = shape_grid(cc, sms);
+                cc.grid = shape_grid(cc, sms, one_per_sm);
                 ClassRun run;
                 pimqap_status st = run.prepare(insts, tp.data(), plans, cc);
                 if (st == PIMQAP_OK) st = run.launch();
@@ -226,7 +229,7 @@ pimqap_status tune_classes(const pimqap_instance *insts, const pimqap_params *pa
         if (cached && t.threads > 0) {
             c.worker_threads = t.threads;
             c.workers = t.workers;
-            c.grid = shape_grid(c, sms);
+            c.grid = shape_grid(c, sms, false);
         }
         if (report) {
             ClassTuning r = t;

@@ -51,9 +51,10 @@ bool autotune_enabled();
 // The autotuner: for every class whose shape is not cached yet, times one mega-iteration of its
 // members under each candidate worker shape and keeps the fastest (shapes never change results);
 // applies the cached choice to every class.  `report` (may be null) receives one entry per class.
+// one_per_sm: shapes are timed with one CTA (cluster) per SM, as the serving launches run them.
 pimqap_status tune_classes(const pimqap_instance *insts, const pimqap_params *params, int32_t count,
                            const std::vector<Plan> &plans, std::vector<BatchClass> &classes, int sms,
-                           int maxsm, std::vector<ClassTuning> *report);
+                           int maxsm, std::vector<ClassTuning> *report, bool one_per_sm = false);
 
 // Device state and stream of one class launch.
 struct ClassRun {

@@ -204,6 +204,10 @@ template <class IT> __device__ __forceinline__ IT warp_max(IT v) {
     }
     return v;
 }
+// 32-bit values: one warp-wide reduction instruction (redux.sync) instead of five shuffles.
+template <> __device__ __forceinline__ int32_t warp_max<int32_t>(int32_t v) {
+    return __reduce_max_sync(0xffffffffu, v);
+}
 
 // ---- shared::cluster addressing, mbarriers, asynchronous remote stores, async copies
 

@@ -557,6 +557,11 @@ pimqap_status pimqap_server_create(const pimqap_server_config *config, pimqap_se
         megaiters[k] = sparams[k].max_megaiters;
     }
     std::vector<BatchClass> shapes = plan_classes(plans, megaiters, S.sms, S.maxsm, 0);
+    if (autotune_enabled()) {   // worker shapes measured on the sample (one mega-iteration each)
+        st = tune_classes(sample.data(), sparams.data(), (int32_t)sample.size(), plans, shapes, S.sms,
+                          S.maxsm, nullptr, true);
+        if (st != PIMQAP_OK) return st;
+    }
     if (config->sample && config->sample_count > 0) {
         // Every shape a request can have (n <= PIMQAP_MAX_N, int32 or int64 forces) must find a
         // resident launch: shapes of the built-in sample that no class from the caller's sample
