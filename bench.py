@@ -564,21 +564,25 @@ def serve_once(rate, duration, drain):
     srv = pimqap.Server(sample=sample)
     t_start = time.perf_counter()
     tickets = []
-    for k, (t_arr, inst) in enumerate(trace):
-        now = time.perf_counter() - t_start
-        if t_arr > now:
-            time.sleep(t_arr - now)
-        tickets.append((srv.submit(inst.F, inst.D, _serve_params(pimqap, inst, k)), k, inst))
     done = {}
-    deadline = t_start + duration + drain
-    while len(done) < len(tickets) and time.perf_counter() < deadline:
-        for t, k, inst in tickets:
-            if t in done:
-                continue
-            r = srv.poll(t)
-            if r is not None:
-                done[t] = (r, k, inst, time.perf_counter() - t_start)
-        time.sleep(0.01)
+    failure = None
+    try:
+        for k, (t_arr, inst) in enumerate(trace):
+            now = time.perf_counter() - t_start
+            if t_arr > now:
+                time.sleep(t_arr - now)
+            tickets.append((srv.submit(inst.F, inst.D, _serve_params(pimqap, inst, k)), k, inst))
+        deadline = t_start + duration + drain
+        while len(done) < len(tickets) and time.perf_counter() < deadline:
+            for t, k, inst in tickets:
+                if t in done:
+                    continue
+                r = srv.poll(t)
+                if r is not None:
+                    done[t] = (r, k, inst, time.perf_counter() - t_start)
+            time.sleep(0.01)
+    except pimqap.PimqapError as e:   # the run ends; its row says why
+        failure = f"{e} (after {time.perf_counter() - t_start:.1f} s, {len(tickets)} submitted)"
     st = srv.stats()
     srv.close()
     lat = sorted(r["latency_ms"] for r, _, _, _ in done.values())
@@ -593,7 +597,8 @@ def serve_once(rate, duration, drain):
            "max_ms": lat[-1] if lat else None,
            "throughput_req_per_s": len(done) / t_last if t_last else 0.0,
            "proposals_per_s": props / t_last if t_last else 0.0,
-           "admitted": st["admitted"], "classes": st["classes"], "error_word": st["error_word"]}
+           "admitted": st["admitted"], "classes": st["classes"], "error_word": st["error_word"],
+           "failure": failure}
     return row, {k: (r, inst) for r, k, inst, _ in done.values()}
 
 
@@ -612,7 +617,7 @@ def run_serve_suite(args):
         row, got = serve_once(rate, args.duration, args.drain)
         rows.append(row)
         results[rate] = got
-    ok = [r for r in rows if r["backlog_at_end"] == 0 and r["p99_ms"] is not None
+    ok = [r for r in rows if r["backlog_at_end"] == 0 and r["p99_ms"] is not None and not r["failure"]
           and r["p99_ms"] <= 1e3 * args.p99_bound]
     best = max(ok, key=lambda r: r["rate_hz"]) if ok else None
     over, got_over = serve_once(args.rate, args.duration, args.drain)
