@@ -226,7 +226,11 @@ pimqap_status tune_classes(const pimqap_instance *insts, const pimqap_params *pa
             g_tune[key] = t;
             cached = true;
         }
-        if (cached && t.threads > 0) {
+        // a shape cached for the same key may come from a class whose largest n (and so its
+        // slice) differs within the key's bucket: it applies only if it is a candidate here
+        bool fits = false;
+        for (const auto &cand : cands) fits = fits || (cand.first == t.threads && cand.second == t.workers);
+        if (cached && t.threads > 0 && fits) {
             c.worker_threads = t.threads;
             c.workers = t.workers;
             c.grid = shape_grid(c, sms, false);

@@ -305,6 +305,7 @@ bool class_fits(const BatchClass &sh, const pimqap_instance &inst, const pimqap_
     const size_t need = sh.cl == 1 ? pimqap::batch_slice_bytes(P.n, sh.bits)
                                     : 16 + std::max(P.smem, pimqap::exchange_scratch_bytes());
     if (need > sh.slice) return false;
+    if ((P.n + sh.worker_threads - 1) / sh.worker_threads > 4) return false;   // candidates per lane
     if (out) *out = P;
     return true;
 }

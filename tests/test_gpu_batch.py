@@ -142,3 +142,20 @@ def test_autotuner_choice_is_no_slower_and_changes_no_result(gpu, monkeypatch):
                for c in off)
     for k, (a, b) in enumerate(zip(tuned, rules)):
         assert same(a, b), k
+
+
+def test_cached_shape_is_not_applied_where_it_does_not_fit(gpu):
+    """The autotuner caches a class's shape by its largest n in buckets of 16; a batch whose
+    largest n is in the same bucket but needs a larger worker slice must not inherit a worker
+    count that overflows a CTA's shared memory (it keeps its own fixed-rule shape)."""
+    def batch(ns, seed):
+        insts = [instances.uniform(n, seed + k) for k, n in enumerate(ns)]
+        ps = [gpu.default_params(replicas=8, groups=1, sweeps_per_exchange=1, beta_max=0.02, beta_ratio=1.3,
+                                 seed=seed + k, max_megaiters=2) for k in range(len(ns))]
+        return insts, ps
+    small, ps = batch([150, 145, 153, 149] * 6, 700)
+    gpu.batch_tune([(i.F, i.D) for i in small], ps)
+    big, qs = batch([158, 157, 156, 155] * 6, 800)
+    got = gpu.batch_solve([(i.F, i.D) for i in big], qs)
+    for k, (inst, p) in enumerate(zip(big[:4], qs[:4])):
+        assert same(got[k], gpu.solve(inst.F, inst.D, p)), k
