@@ -23,7 +23,10 @@
 # absent the script does nothing and exits 0.
 set -euo pipefail
 
+# PIMQAP_REF_ROOT names the reference checkout; unset, the conventional read-only mount of the
+# build container is used, and the script says which source it builds from.
 REF_ROOT="${PIMQAP_REF_ROOT:-/root/reference}"
+[ -n "${PIMQAP_REF_ROOT:-}" ] || echo "build_ref.sh: PIMQAP_REF_ROOT unset, using $REF_ROOT"
 SRC="$REF_ROOT/CPU-PIM/CPU_PIM.cpp"
 HERE="$(cd "$(dirname "$0")" && pwd)"
 OUT="$HERE/_ref"
