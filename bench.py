@@ -283,7 +283,7 @@ def run_ours(args):
                   beta_ratio=W["ratio"], beta_internal=1, seed=1 + rank, device=local,
                   cluster_size=args.cluster_size, threads_per_block=args.threads,
                   active_facilities=W["act"], update_rule=rule, replica_pairing=args.pairing,
-                  launch_mode=args.launch_mode)
+                  launch_mode=args.launch_mode, sweep_pipeline=args.pipeline)
     params = pimqap.default_params(megaiters_per_launch=MPS, max_megaiters=2 ** 31 - 1, **common)
     flush = torch.empty(L2_FLUSH_BYTES, dtype=torch.uint8, device=f"cuda:{local}")
     solver = pimqap.Solver(inst.F, inst.D, params)
@@ -378,7 +378,7 @@ def run_ours(args):
             "data": f"synthetic (seeded {args.workload} instance per GPU)",
             "config": dict(workload_config(args.workload, args.update_rule, world, args.steps, args.groups),
                            cluster_size=r1["cluster_size"], force_bits=r1["force_bits"],
-                           replica_pairing=args.pairing,
+                           replica_pairing=args.pairing, sweep_pipeline=args.pipeline,
                            launch="one persistent launch per step" if persistent else
                                   "a CUDA graph of one launch per mega-iteration",
                            l2="flushed between steps (256 MiB write)"),
@@ -732,6 +732,8 @@ def main():
     ap.add_argument("--groups", type=int, default=1,
                     help="independent parallel-tempering groups of the workload's replicas per GPU (the "
                          "reference's -t; its CPU arm runs one group per host thread)")
+    ap.add_argument("--pipeline", type=int, default=0, choices=[0, 1, 2],
+                    help="binary-flow kernel: 2 = the pipelined epoch (next update's deltas during the pick)")
     ap.add_argument("--launch-mode", type=int, default=0, choices=[0, 1, 2],
                     help="0 = automatic (persistent when resident), 1 = a launch per mega-iteration, 2 = persistent")
     ap.add_argument("--update-rule", choices=["sequential", "one-shot"], default="sequential",

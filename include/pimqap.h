@@ -123,6 +123,12 @@ typedef struct pimqap_params {
                                     (every replica resident at once, no event log; rejected
                                     otherwise).  Same results either way.  pimqap_solve /
                                     solver handles only */
+    int32_t sweep_pipeline;      /* binary-flow instances: 0 = automatic (off), 1 = off,
+                                    2 = compute each update's deltas while the previous update
+                                    picks (half of a CTA's warps pick, half compute the next
+                                    deltas against the state before the pick's swap and then
+                                    correct them for it).  Same results either way; with
+                                    launch_mode 0 / 1, one replica per CTA set, no clique moves */
 } pimqap_params;
 
 #define PIMQAP_RULE_SEQUENTIAL 0

@@ -242,7 +242,7 @@ struct pimqap_solver {
     pimqap_params p{};
     int n = 0, T = 0, R = 0, cap = 0, spe = 0;
     int bits = 32, cl = 1, threads = 256;
-    bool sym = false, bin = false, pair = false;
+    bool sym = false, bin = false, pair = false, pipe = false;
     bool persistent = false;   // one persistent launch per run call (solve_kernel)
     size_t smem = 0;
     int device = 0;
@@ -322,6 +322,8 @@ pimqap_status check_params(const pimqap_instance *inst, const pimqap_params *p) 
         return fail(PIMQAP_ERR_ARG, "cluster_size must be 0, 1, 2 or 4");
     if (p->replica_pairing < 0 || p->replica_pairing > 2)
         return fail(PIMQAP_ERR_ARG, "replica_pairing must be 0 (automatic), 1 (off) or 2 (on)");
+    if (p->sweep_pipeline < 0 || p->sweep_pipeline > 2)
+        return fail(PIMQAP_ERR_ARG, "sweep_pipeline must be 0 (automatic), 1 (off) or 2 (on)");
     if (p->launch_mode < 0 || p->launch_mode > 2)
         return fail(PIMQAP_ERR_ARG, "launch_mode must be 0 (automatic), 1 (a launch per mega-iteration) or "
                                     "2 (one persistent launch)");
@@ -732,6 +734,16 @@ pimqap_status pimqap_solver_create(const pimqap_instance *inst, const pimqap_par
     if (st != PIMQAP_OK) return st;
     st = plan_pairing(inst, params, (size_t)maxsm, &plan);
     if (st != PIMQAP_OK) return st;
+    if (params->sweep_pipeline == 2) {   // the pipelined binary-flow epoch
+        const size_t sp = pimqap::epoch_smem_bytes_pipe(plan.n, plan.rpc, plan.lds);
+        if (!plan.bin || plan.act || plan.pair || params->launch_mode == 2 || sp > (size_t)maxsm)
+            return fail(PIMQAP_ERR_ARG, "sweep_pipeline = 2 needs the binary-flow kernel (symmetric 0/1 flows, "
+                                        "int16 distances, int32 forces), no clique moves, one replica per CTA "
+                                        "set, launch_mode 0 or 1, and a layout that fits the cluster size");
+        plan.pipe = true;
+        plan.smem_bin = sp;
+    }
+    s->pipe = plan.pipe;
     s->pair = plan.pair;
     s->n = plan.n;
     s->T = plan.T;
@@ -906,7 +918,7 @@ pimqap_status pimqap_solver_run(pimqap_solver *s, int64_t megaiters, double *dev
             PQ_CUDA(cudaStreamBeginCapture(s->stream, cudaStreamCaptureModeThreadLocal));
             for (int k = 0; k < g; ++k) {
                 cudaError_t e = pimqap::launch_epoch(s->dev, s->bits, s->cl, s->sym, s->bin, s->threads,
-                                                     s->smem, s->stream, s->pair);
+                                                     s->smem, s->stream, s->pair, s->pipe);
                 if (e != cudaSuccess) {
                     cudaStreamEndCapture(s->stream, &graph);
                     return fail(PIMQAP_ERR_CUDA, std::string("epoch launch: ") + cudaGetErrorString(e));

@@ -225,6 +225,9 @@ cudaError_t launch_setup(const SolveDev &s, int bits, cudaStream_t st);
 // One epoch: spe sweeps of every replica, then each group's tracking + exchange.  pair: the
 // binary-flow kernel with two replicas per CTA set (threads per replica; smem of the pair).
 cudaError_t launch_epoch(const SolveDev &s, int bits, int cluster, bool sym, bool bin, int threads,
-                         size_t smem, cudaStream_t st, bool pair = false);
+                         size_t smem, cudaStream_t st, bool pair = false, bool pipe = false);
+// Shared memory of the pipelined binary-flow epoch (deltas of the next update computed while
+// the current one picks; 256 threads).
+size_t epoch_smem_bytes_pipe(int n, int rpc, int lds);
 
 }  // namespace pimqap

@@ -1464,7 +1464,475 @@ __device__ bool replica_epoch_bin(const SolveDev &s, int rep, int rank, int e, c
     return true;
 }
 
-// ------------------------------------------------------------------ the one-shot epoch
+// ------------------------------------------------------------------ the pipelined binary-flow epoch
+
+// replica_epoch_bin with the deltas of update u + 1 computed while update u picks.  The CTA's
+// 256 threads are two groups: the pick group (threads 0-127, named barrier 1) forms the weights,
+// the prefix sums and the pick of update u; meanwhile the delta group (threads 128-255, named
+// barrier 2) computes the deltas of update u + 1 against the state before update u's swap
+// (Bpre / Apre).  Once the pick is known (CTA barrier 1), the delta group applies the swap,
+// adds the new log entry's term to every delta, recomputes the two rows whose facilities moved
+// (every delta when the next location is the swap partner, whose facility changed), and pushes
+// them (CTA barrier 2); the pick group writes the entry's column factors meanwhile.  Same integers,
+// weights, sums and picks as replica_epoch_bin; two CTA barriers per update instead of four.
+// The uniform r of update u + 1 is drawn by the delta group during update u.
+struct PipeLayout {
+    size_t I, phi, inv, bphi, Dd, A, B, Bpre, Apre, Ds, Fb, LU, V8, red, wsum, r, misc, bar, total;
+    __host__ __device__ PipeLayout(int n, int rpc, int lds) {
+        const size_t npad = (size_t)((n + 3) & ~3), rp = (size_t)rpc, nw = (size_t)((n + 31) / 32);
+        size_t o = 0;
+        I = o;     o = align16(o + rp * lds * 4);
+        phi = o;   o = align16(o + npad * 4);
+        inv = o;   o = align16(o + npad * 4);
+        bphi = o;  o = align16(o + npad * 4);
+        Dd = o;    o = align16(o + npad * 4);
+        A = o;     o = align16(o + 2 * npad * 4);           // [2][npad] by update parity
+        B = o;     o = align16(o + 2 * npad * 4);
+        Bpre = o;  o = align16(o + rp * 4);                 // next update's B of this CTA's rows
+        Apre = o;  o = align16(o + npad * 4);               // next update's A (owner of its row)
+        Ds = o;    o = align16(o + (size_t)n * rp * 2);
+        Fb = o;    o = align16(o + (size_t)n * nw * 4);
+        LU = o;    o = align16(o + (size_t)kBinLog * rp * 4);
+        V8 = o;    o = align16(o + (size_t)kBinLog * npad);
+        red = o;   o = align16(o + kMaxWarps * 8);
+        wsum = o;  o = align16(o + kMaxWarps * sizeof(double));
+        r = o;     o = align16(o + 2 * sizeof(double));      // r of the current / next update
+        misc = o;  o = align16(o + 4 * sizeof(int));
+        bar = o;   o = align16(o + 2 * sizeof(unsigned long long));
+        total = o;
+    }
+};
+
+size_t epoch_smem_bytes_pipe(int n, int rpc, int lds) { return PipeLayout(n, rpc, lds).total; }
+
+constexpr int kPipeGroup = 128;   // threads of each group of the pipelined epoch
+
+// The rewrite of the CTA's force rows with the m pending log entries, by every thread of the
+// CTA: I[k][c] += sum_p LU[p][k] V8[p][c], 8 rows x 4 columns of binary32 sums per thread (exact:
+// every partial sum stays below 2^24, as in replica_epoch_bin).
+__device__ void pipe_flush(int32_t *sI, const float *s_LU, const int8_t *s_V8, int rows, int rpc, int lds,
+                           int npad, int m) {
+    constexpr int VEC = 4, RT = 8;
+    const int tid = (int)threadIdx.x, BT = (int)blockDim.x;
+    const int nvec = npad / VEC;
+    const int ngroups = max(1, BT / nvec);                   // row-block groups in flight
+    for (int cv = tid % nvec, grp = tid / nvec; cv < nvec; cv += (BT >= nvec ? nvec : BT)) {
+        if (BT >= nvec && grp >= ngroups) break;
+        const int c0 = cv * VEC;
+        const int gfirst = (BT >= nvec) ? grp : 0, ginc = (BT >= nvec) ? ngroups : 1;
+        for (int kb = gfirst * RT; kb < rows; kb += ginc * RT) {
+            float acc[RT][VEC];
+#pragma unroll
+            for (int r = 0; r < RT; ++r)
+#pragma unroll
+                for (int q = 0; q < VEC; ++q) acc[r][q] = 0.0f;
+            for (int p = 0; p < m; ++p) {
+                const char4 v4 = *reinterpret_cast<const char4 *>(s_V8 + (size_t)p * npad + c0);
+                const float v[VEC] = {(float)v4.x, (float)v4.y, (float)v4.z, (float)v4.w};
+                // LU rows are rpc long (a multiple of 4): rows past `rows` hold zeros
+                const float4 l0 = *reinterpret_cast<const float4 *>(s_LU + (size_t)p * rpc + kb);
+                const float4 l1 = (kb + 4 < rpc) ? *reinterpret_cast<const float4 *>(s_LU + (size_t)p * rpc + kb + 4)
+                                                 : make_float4(0.f, 0.f, 0.f, 0.f);
+                const float u[RT] = {l0.x, l0.y, l0.z, l0.w, l1.x, l1.y, l1.z, l1.w};
+#pragma unroll
+                for (int r = 0; r < RT; ++r)
+#pragma unroll
+                    for (int q = 0; q < VEC; ++q) acc[r][q] = fmaf(u[r], v[q], acc[r][q]);
+            }
+#pragma unroll
+            for (int r = 0; r < RT; ++r) {
+                if (kb + r < rows) {
+                    Vec<int32_t> *dst = reinterpret_cast<Vec<int32_t> *>(sI + (size_t)(kb + r) * lds + c0);
+                    Vec<int32_t> xv = *dst;
+#pragma unroll
+                    for (int q = 0; q < VEC; ++q) xv.v[q] = (int32_t)((uint32_t)xv.v[q] + (uint32_t)(int)acc[r][q]);
+                    *dst = xv;
+                }
+            }
+        }
+    }
+}
+
+// One epoch of replica rep (blockDim.x == 2 * kPipeGroup; symmetric 0/1 flows, int16
+// distances, int32 forces, no clique moves).  Returns false when a bounded wait gave up.
+template <int CL>
+__device__ bool replica_epoch_pipe(const SolveDev &s, int rep, int rank, int e, unsigned char *smem) {
+    using IT = int32_t;
+    using U = uint32_t;
+    constexpr int VEC = 4;
+    const int n = s.n;
+    const int tid = (int)threadIdx.x, lane = tid & 31;
+    const bool pick_group = tid < kPipeGroup;
+    const int gt = pick_group ? tid : tid - kPipeGroup;         // thread within its group
+    const Grp P{gt, kPipeGroup, lane, gt >> 5, kPipeGroup / 32, 1};
+    const Grp Dg{gt, kPipeGroup, lane, gt >> 5, kPipeGroup / 32, 2};
+    const int g = rep / s.R, l = rep - g * s.R;
+    const int rpc = s.rpc, lds = s.lds;
+    const int row0 = rank * rpc;
+    const int rows = max(0, min(rpc, n - row0));
+    const int npad = (n + 3) & ~3, nvec = npad / VEC;
+    const int nw = (n + 31) / 32;
+    const PipeLayout L(n, rpc, lds);
+    IT *sI = reinterpret_cast<IT *>(smem + L.I);
+    int32_t *s_phi = reinterpret_cast<int32_t *>(smem + L.phi);
+    int32_t *s_inv = reinterpret_cast<int32_t *>(smem + L.inv);
+    int32_t *s_bphi = reinterpret_cast<int32_t *>(smem + L.bphi);
+    int32_t *s_Dd = reinterpret_cast<int32_t *>(smem + L.Dd);
+    IT *s_A = reinterpret_cast<IT *>(smem + L.A);
+    IT *s_B = reinterpret_cast<IT *>(smem + L.B);
+    IT *s_Bpre = reinterpret_cast<IT *>(smem + L.Bpre);
+    IT *s_Apre = reinterpret_cast<IT *>(smem + L.Apre);
+    int16_t *s_Ds = reinterpret_cast<int16_t *>(smem + L.Ds);
+    uint32_t *s_Fb = reinterpret_cast<uint32_t *>(smem + L.Fb);
+    float *s_LU = reinterpret_cast<float *>(smem + L.LU);
+    int8_t *s_V8 = reinterpret_cast<int8_t *>(smem + L.V8);
+    IT *s_red = reinterpret_cast<IT *>(smem + L.red);
+    double *s_wsum = reinterpret_cast<double *>(smem + L.wsum);
+    double *s_r = reinterpret_cast<double *>(smem + L.r);
+    int *s_misc = reinterpret_cast<int *>(smem + L.misc);   // [0] pick key, [1] improved at, [2] failed
+    unsigned long long *s_bar = reinterpret_cast<unsigned long long *>(smem + L.bar);
+    auto fbit = [&](int a, int b) -> int { return (int)((s_Fb[a * nw + (b >> 5)] >> (b & 31)) & 1u); };
+
+    // ---- load the replica and the instance (every thread)
+    {
+        const IT *gI = reinterpret_cast<const IT *>(s.I) + ((size_t)rep * n + row0) * s.ldg;
+        const int nvg = s.ldg / VEC;
+        for (int idx = tid; idx < rows * nvg; idx += blockDim.x) {
+            const int k = idx / nvg, v = idx - k * nvg;
+            const int4 w = __ldcg(reinterpret_cast<const int4 *>(gI + (size_t)k * s.ldg + v * VEC));
+            *reinterpret_cast<int4 *>(sI + (size_t)k * lds + v * VEC) = w;
+        }
+        const int32_t *gphi = s.phi + (size_t)rep * n;
+        for (int q = tid; q < npad; q += blockDim.x) {
+            int p = q < n ? __ldcg(gphi + q) : 0;
+            if ((unsigned)p >= (unsigned)n) {
+                atomicOr(s.error, kErrBadPerm);
+                p = 0;
+            }
+            s_phi[q] = p;
+            s_bphi[q] = p;
+            s_inv[q] = 0;
+            s_Dd[q] = q < n ? __ldcg(s.Ddiag + q) : 0;
+        }
+        load_bin_instance(s, rank, tid, (int)blockDim.x, lane, tid >> 5, (int)(blockDim.x >> 5), s_Ds, s_Fb);
+        if (tid == 0) {
+            s_misc[0] = 0x7fffffff;
+            s_misc[1] = -1;
+            s_misc[2] = 0;
+            if constexpr (CL > 1) {
+                mbar_init(smem_u32(&s_bar[0]), 1);
+                mbar_init(smem_u32(&s_bar[1]), 1);
+                mbar_fence_init();
+            }
+        }
+        __syncthreads();
+    }
+    for (int q = tid; q < n; q += blockDim.x) s_inv[s_phi[q]] = q;
+    cluster_sync<CL>(Grp{tid, (int)blockDim.x, lane, tid >> 5, (int)(blockDim.x >> 5), 0});
+
+    uint32_t A_at[CL], B_at[CL], bar_at[CL];
+    if constexpr (CL > 1) {
+#pragma unroll
+        for (int r = 0; r < CL; ++r) {
+            A_at[r] = cluster_addr(smem_u32(s_A), r);
+            B_at[r] = cluster_addr(smem_u32(s_B), r);
+            bar_at[r] = cluster_addr(smem_u32(s_bar), r);
+        }
+    }
+    const uint32_t tx_bytes = (uint32_t)((npad + n) * sizeof(IT));
+    uint32_t phase = 0;
+    const double beta = __ldcg(s.beta + rep);
+    const double cut_span = 20.0 / beta;                    // CPU_PIM.cpp:234
+    int64_t E = __ldcg((const long long *)s.E + rep), bestE = __ldcg((const long long *)s.bestE + rep);
+    unsigned long long accepts = 0;
+    const uint32_t k0 = (uint32_t)s.seed, k1 = (uint32_t)(s.seed >> 32);
+    const int K = (n + kPipeGroup - 1) / kPipeGroup;         // weights per pick thread (<= 4)
+    const int U_total = s.spe * n;                           // updates of this epoch
+    int m = 0;                                               // pending swaps (same in every thread)
+
+    // The uniform r of update u (:212): the caller's or the Philox stream's.
+    auto draw_r = [&](int u) -> double {
+        const int i = u % n;
+        const uint32_t sweep = (uint32_t)(e * s.spe + u / n);
+        if (s.replay_r) return __ldcg(s.replay_r + (size_t)sweep * n + i);
+        uint32_t w0, w1;
+        philox_2words((uint32_t)i, sweep, (uint32_t)l, (uint32_t)g, k0, k1, w0, w1);
+        return canonical53(w0, w1);
+    };
+    // The swap log's correction of a B-half entry (row jj, candidate b, facility a1 at the
+    // updating location) and of an A-half entry (row il of that location, column c), over the
+    // m pending entries (binary32 sums, exact as in replica_epoch_bin).
+    auto corr_B = [&](int jj, int a1, int b) -> int {
+        float cf = 0.0f;
+#pragma unroll 4
+        for (int q = 0; q < m; ++q) {
+            const int8_t *v8 = s_V8 + (size_t)q * npad;
+            cf = fmaf(s_LU[q * rpc + jj], (float)((int)v8[a1] - (int)v8[b]), cf);
+        }
+        return (int)cf;
+    };
+    // B-half of row jj for the update of location i1 (facility a1), candidate b = its facility:
+    // I[j][a1] - I[j][b] - dd ff with the log's corrections.
+    auto row_B = [&](int i1, int a1, int jj, int b) -> U {
+        const int j = row0 + jj;
+        const IT *Ij = sI + (size_t)jj * lds;
+        const U dd = (U)s_Dd[i1] + (U)s_Dd[j] - 2u * (U)(IT)s_Ds[(size_t)i1 * rpc + jj];
+        const U ff = (U)fbit(a1, a1) + (U)fbit(b, b) - 2u * (U)fbit(a1, b);
+        return (U)Ij[a1] - (U)Ij[b] - dd * ff + (U)corr_B(jj, a1, b);
+    };
+    // A-half of the update of location i1 (facility a1), columns 4 c4 .. 4 c4 + 3, by the owner
+    // of row i1: I[i1][c] - I[i1][a1] with the log's corrections.
+    auto chunk_A = [&](int i1, int a1, int c4) -> Vec<IT> {
+        const int il = i1 - row0;
+        const IT *Ii = sI + (size_t)il * lds;
+        const IT Iia = Ii[a1];
+        Vec<IT> v = *reinterpret_cast<const Vec<IT> *>(Ii + c4 * VEC);
+        const int c0 = c4 * VEC;
+        float cf[VEC] = {0.0f, 0.0f, 0.0f, 0.0f};
+#pragma unroll 4
+        for (int q = 0; q < m; ++q) {
+            const int8_t *v8 = s_V8 + (size_t)q * npad;
+            const char4 v4 = *reinterpret_cast<const char4 *>(v8 + c0);
+            const int va = (int)v8[a1];
+            const float lu = s_LU[q * rpc + il];
+            cf[0] = fmaf(lu, (float)((int)v4.x - va), cf[0]);
+            cf[1] = fmaf(lu, (float)((int)v4.y - va), cf[1]);
+            cf[2] = fmaf(lu, (float)((int)v4.z - va), cf[2]);
+            cf[3] = fmaf(lu, (float)((int)v4.w - va), cf[3]);
+        }
+#pragma unroll
+        for (int q = 0; q < VEC; ++q) v.v[q] = (IT)((U)v.v[q] - (U)Iia + (U)(int)cf[q]);
+        return v;
+    };
+    // Update u1's halves into the receive buffers of parity p1 of every CTA of the cluster.
+    auto push_B = [&](int p1, int b, IT v) {
+        if constexpr (CL == 1) {
+            s_B[p1 * npad + b] = v;
+        } else {
+#pragma unroll
+            for (int r = 0; r < CL; ++r)
+                st_async(B_at[r] + (uint32_t)((p1 * npad + b) * sizeof(IT)), v, bar_at[r] + p1 * 8);
+        }
+    };
+    auto push_A = [&](int p1, int c4, const Vec<IT> &v) {
+        if constexpr (CL == 1) {
+            *reinterpret_cast<Vec<IT> *>(s_A + p1 * npad + c4 * VEC) = v;
+        } else {
+#pragma unroll
+            for (int r = 0; r < CL; ++r)
+                st_async16(A_at[r] + (uint32_t)((p1 * npad + c4 * VEC) * sizeof(IT)), v, bar_at[r] + p1 * 8);
+        }
+    };
+
+    // ---- update 0's deltas (no swap before it) and r
+    if (!pick_group) {
+        const int a0 = s_phi[0];
+        for (int jj = gt; jj < rows; jj += kPipeGroup) push_B(0, s_phi[row0 + jj], (IT)row_B(0, a0, jj, s_phi[row0 + jj]));
+        if (0 / rpc == rank)
+            for (int c4 = gt; c4 < nvec; c4 += kPipeGroup) push_A(0, c4, chunk_A(0, a0, c4));
+        if (gt == kPipeGroup - 1) s_r[0] = draw_r(0);
+    } else if (CL > 1 && gt == 0) {
+        mbar_arrive_expect_tx(smem_u32(&s_bar[0]), tx_bytes);
+    }
+    __syncthreads();
+
+    bool failed = false;
+    for (int u = 0; u < U_total; ++u) {
+        const int i = u % n;
+        const int p = u & 1;
+        const int a = s_phi[i];
+        const bool has_next = u + 1 < U_total;
+        const int i1 = has_next ? (u + 1) % n : 0;
+        const int a1 = has_next ? s_phi[i1] : 0;            // before update u's swap
+        // ---- phase A: the pick of update u | the deltas of update u + 1
+        if (pick_group) {
+            bool timeout = false;
+            if constexpr (CL > 1) {
+                timeout = !mbar_wait_bounded(smem_u32(&s_bar[p]), (phase >> p) & 1u, kWaitLimitNs);
+                phase ^= 1u << p;
+            }
+            const int b0 = gt * K;
+            IT d[4];
+            double x[4];
+            IT lmax = 0;                                     // max starts at 0 (:208)
+#pragma unroll
+            for (int k = 0; k < 4; ++k) {
+                d[k] = 0;
+                x[k] = 0.0;
+                if (k < K && b0 + k < n) {
+                    const int b = b0 + k;
+                    d[k] = (IT)((U)s_A[p * npad + b] + (U)s_B[p * npad + b]);
+                    x[k] = exp2(__dmul_rn(beta, (double)d[k]));
+                    lmax = d[k] > lmax ? d[k] : lmax;
+                }
+            }
+            lmax = warp_max(lmax);
+            if (lane == 0) s_red[P.warp] = lmax;
+            if (P.sync_or(timeout)) {
+                if (gt == 0) {
+                    atomicOr(s.error, kErrTimeout);
+                    s_misc[2] = 1;
+                }
+            } else {
+                if (gt == 0) s_misc[0] = 0x7fffffff;
+                IT M = s_red[0];
+                for (int w = 1; w < P.nwarps; ++w) M = s_red[w] > M ? s_red[w] : M;
+                const long long cut = cutoff_trunc(__dsub_rn((double)M, cut_span));   // :234-235
+                double pre[4];
+                double local = 0.0;
+#pragma unroll
+                for (int k = 0; k < 4; ++k) {
+                    if (k < K && (long long)d[k] > cut && b0 + k < n) local = __dadd_rn(local, x[k]);
+                    pre[k] = local;
+                }
+                double incl = local;
+#pragma unroll
+                for (int o = 1; o < 32; o <<= 1) {
+                    const double y = __shfl_up_sync(0xffffffffu, incl, o);
+                    if (lane >= o) incl = __dadd_rn(incl, y);
+                }
+                double excl = __shfl_up_sync(0xffffffffu, incl, 1);
+                if (lane == 0) excl = 0.0;
+                if (lane == 31) s_wsum[P.warp] = incl;
+                P.sync();
+                double base = 0.0, total = 0.0;
+                for (int w = 0; w < P.nwarps; ++w) {
+                    if (w == P.warp) base = total;
+                    total = __dadd_rn(total, s_wsum[w]);
+                }
+                const double target = __dmul_rn(s_r[p], total);      // :247
+                const double X = __dadd_rn(base, excl);
+#pragma unroll
+                for (int k = 0; k < 4; ++k) {
+                    if (k < K && b0 + k < n) {
+                        if (__dadd_rn(X, pre[k]) >= target) {    // :251
+                            atomicMin(&s_misc[0], ((b0 + k) << 9) | s_inv[b0 + k]);
+                            break;
+                        }
+                    }
+                }
+            }
+        } else if (has_next) {
+            for (int jj = gt; jj < rows; jj += kPipeGroup) s_Bpre[jj] = (IT)row_B(i1, a1, jj, s_phi[row0 + jj]);
+            if (i1 / rpc == rank)
+                for (int c4 = gt; c4 < nvec; c4 += kPipeGroup)
+                    *reinterpret_cast<Vec<IT> *>(s_Apre + c4 * VEC) = chunk_A(i1, a1, c4);
+            if (gt == kPipeGroup - 1) s_r[p ^ 1] = draw_r(u + 1);
+        }
+        __syncthreads();                                     // 1: the pick is known
+        if (s_misc[2]) {
+            failed = true;
+            break;
+        }
+        const int key = s_misc[0];
+        const int bs = key >> 9, js = key & 511;
+        const bool accepted = bs < n && bs != a;             // no move / self move (:252)
+        if (accepted) {
+            E -= (int64_t)(IT)((U)s_A[p * npad + bs] + (U)s_B[p * npad + bs]);   // :256
+            ++accepts;
+            if (E < bestE) {                                 // :271-272
+                bestE = E;
+                if (tid == 0) s_misc[1] = u;
+            }
+        }
+        // ---- phase B: the log entry of the swap | update u + 1's deltas completed and pushed
+        if (pick_group) {
+            if (CL > 1 && has_next && gt == 0) mbar_arrive_expect_tx(smem_u32(&s_bar[p ^ 1]), tx_bytes);
+            if (accepted)
+                for (int c = gt; c < npad; c += kPipeGroup)
+                    s_V8[(size_t)m * npad + c] = (int8_t)(c < n ? fbit(bs, c) - fbit(a, c) : 0);
+        } else {
+            if (accepted) {
+                if (gt == 0) {                               // :257-261
+                    s_phi[i] = bs;
+                    s_inv[bs] = i;
+                    s_phi[js] = a;
+                    s_inv[a] = js;
+                }
+                for (int k = gt; k < rpc; k += kPipeGroup)
+                    s_LU[m * rpc + k] =
+                        k < rows ? (float)(2 * ((int)s_Ds[(size_t)js * rpc + k] - (int)s_Ds[(size_t)i * rpc + k])) : 0.0f;
+            }
+            if (has_next) {
+                const int p1 = p ^ 1;
+                // the new entry's row factor 2 (D[k][js] - D[k][i]) and column factor F[bs][c] - F[a][c]
+                auto lux = [&](int kk) -> int { return 2 * ((int)s_Ds[(size_t)js * rpc + kk] - (int)s_Ds[(size_t)i * rpc + kk]); };
+                auto vx = [&](int c) -> int { return fbit(bs, c) - fbit(a, c); };
+                const bool full = accepted && i1 == js;      // location i1 now holds facility a
+                const int a1n = full ? a : a1;
+                for (int jj = gt; jj < rows; jj += kPipeGroup) {
+                    const int j = row0 + jj;
+                    const bool moved = accepted && (j == i || j == js);
+                    const int b = moved ? (j == i ? bs : a) : s_phi[j];   // rows i / js: being rewritten
+                    U v = (full || moved) ? row_B(i1, a1n, jj, b) : (U)s_Bpre[jj];
+                    if (accepted) v += (U)(lux(jj) * (vx(a1n) - vx(b)));
+                    push_B(p1, b, (IT)v);
+                }
+                if (i1 / rpc == rank) {
+                    const int il = i1 - row0;
+                    for (int c4 = gt; c4 < nvec; c4 += kPipeGroup) {
+                        Vec<IT> v = full ? chunk_A(i1, a1n, c4) : *reinterpret_cast<const Vec<IT> *>(s_Apre + c4 * VEC);
+                        if (accepted) {
+                            const int lx = lux(il), va = vx(a1n);
+#pragma unroll
+                            for (int q = 0; q < VEC; ++q) {
+                                const int c = c4 * VEC + q;
+                                v.v[q] = (IT)((U)v.v[q] + (U)(lx * ((c < n ? vx(c) : 0) - va)));
+                            }
+                        }
+                        push_A(p1, c4, v);
+                    }
+                }
+            }
+        }
+        __syncthreads();                                     // 2: swap, log entry and pushes done
+        if (accepted) ++m;
+        if (s_misc[1] == u)
+            for (int q = tid; q < n; q += blockDim.x) s_bphi[q] = s_phi[q];
+        if (m == kBinLog) {
+            pipe_flush(sI, s_LU, s_V8, rows, rpc, lds, npad, m);
+            m = 0;
+            __syncthreads();
+        }
+    }
+    if (!failed && m > 0) {   // the swaps still pending (m is the same in every thread)
+        pipe_flush(sI, s_LU, s_V8, rows, rpc, lds, npad, m);
+        m = 0;
+        __syncthreads();
+    }
+    cluster_sync<CL>(Grp{tid, (int)blockDim.x, lane, tid >> 5, (int)(blockDim.x >> 5), 0});
+    if constexpr (CL > 1) {
+        if (tid == 0) {
+            mbar_inval(smem_u32(&s_bar[0]));
+            mbar_inval(smem_u32(&s_bar[1]));
+        }
+    }
+    if (failed) return false;
+    {
+        IT *gI = reinterpret_cast<IT *>(s.I) + ((size_t)rep * n + row0) * s.ldg;
+        const int nvg = s.ldg / VEC;
+        for (int idx = tid; idx < rows * nvg; idx += blockDim.x) {
+            const int k = idx / nvg, v = idx - k * nvg;
+            *reinterpret_cast<Vec<IT> *>(gI + (size_t)k * s.ldg + v * VEC) =
+                *reinterpret_cast<const Vec<IT> *>(sI + (size_t)k * lds + v * VEC);
+        }
+    }
+    if (rank == 0) {
+        int32_t *gphi = s.phi + (size_t)rep * n;
+        for (int q = tid; q < n; q += blockDim.x) gphi[q] = s_phi[q];
+        if (s_misc[1] >= 0) {
+            int32_t *gb = s.best_phi + (size_t)rep * n;
+            for (int q = tid; q < n; q += blockDim.x) gb[q] = s_bphi[q];
+        }
+        if (tid == 0) {
+            s.E[rep] = E;
+            s.bestE[rep] = bestE;
+            s.accepts[rep] = __ldcg(s.accepts + rep) + accepts;
+        }
+    }
+    __threadfence();
+    return true;
+}
 
 // The tensor-core force update of the one-shot epoch stages 64 factor columns at a time, as
 // fp16 rows of kMmaLd halves (144 bytes: the 8 rows and 4 column pairs one fragment load
@@ -2204,6 +2672,7 @@ __global__ void __launch_bounds__(KIND == 2 ? 512 : 256, (CL == 4 && KIND != 2) 
     bool ok;
     if constexpr (KIND == 1) ok = replica_epoch_bin<CL>(s, rep, rank, e, G, smem);
     else if constexpr (KIND == 2) ok = replica_epoch_os<IT, CL, SYM, GP>(s, rep, rank, e, G, smem);
+    else if constexpr (KIND == 3) ok = replica_epoch_pipe<CL>(s, rep, rank, e, smem);
     else ok = replica_epoch<IT, CL, SYM, GP>(s, rep, rank, e, G, smem);
     __syncthreads();
     if (ok && rank == 0 && threadIdx.x == 0) {
@@ -2836,6 +3305,16 @@ static void *solve_kernel_ptr(int bits, int cl, bool sym, bool gp, int kind) {
     return nullptr;
 }
 
+// The pipelined binary-flow epoch (2 x kPipeGroup threads).
+static void *epoch_pipe_ptr(int cl) {
+    switch (cl) {
+        case 1: return reinterpret_cast<void *>(&epoch_kernel<int32_t, 1, true, false, 3>);
+        case 2: return reinterpret_cast<void *>(&epoch_kernel<int32_t, 2, true, false, 3>);
+        case 4: return reinterpret_cast<void *>(&epoch_kernel<int32_t, 4, true, false, 3>);
+        default: return nullptr;
+    }
+}
+
 // The paired binary-flow epoch (two replicas per CTA set).
 static void *epoch_pair_ptr(int cl) {
     switch (cl) {
@@ -2996,6 +3475,8 @@ cudaError_t prepare_kernels() {
         if (err != cudaSuccess) return err;
         err = cudaFuncSetAttribute(epoch_pair_ptr(cl), cudaFuncAttributeMaxDynamicSharedMemorySize, maxsm);
         if (err != cudaSuccess) return err;
+        err = cudaFuncSetAttribute(epoch_pipe_ptr(cl), cudaFuncAttributeMaxDynamicSharedMemorySize, maxsm);
+        if (err != cudaSuccess) return err;
     }
     return cudaSuccess;
 }
@@ -3075,13 +3556,15 @@ cudaError_t launch_solve(const SolveDev &s, int bits, int cluster, bool sym, boo
 }
 
 cudaError_t launch_epoch(const SolveDev &s, int bits, int cluster, bool sym, bool bin, int threads,
-                         size_t smem, cudaStream_t st, bool pair) {
+                         size_t smem, cudaStream_t st, bool pair, bool pipe) {
     const bool gp = s.ev.log != nullptr && s.ev.goal_print != 0;
     const bool binary = bin && bits == 32 && sym && (!gp || s.act > 0);
     pair = pair && binary;
+    pipe = pipe && binary && !pair && s.act == 0;
     // clique-flow solves (s.act > 0) exist only in the binary-flow kernels
     void *fn = s.os_chunk > 0 ? epoch_os_ptr(bits, cluster, sym, gp)
                : pair         ? epoch_pair_ptr(cluster)
+               : pipe         ? epoch_pipe_ptr(cluster)
                : binary       ? epoch_bin_ptr(cluster)
                               : epoch_kernel_ptr(bits, cluster, sym, gp);
     if (!fn) return cudaErrorInvalidValue;
@@ -3089,7 +3572,7 @@ cudaError_t launch_epoch(const SolveDev &s, int bits, int cluster, bool sym, boo
     if (!pair) smem = std::max(smem, exchange_scratch_bytes());   // the pair's sections hold it
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3((unsigned)((pair ? (reps + 1) / 2 : reps) * cluster));
-    cfg.blockDim = dim3((unsigned)(pair ? 2 * threads : threads));
+    cfg.blockDim = dim3((unsigned)(pair ? 2 * threads : (pipe ? 2 * kPipeGroup : threads)));
     cfg.dynamicSmemBytes = smem;
     cfg.stream = st;
     cudaLaunchAttribute attr[1];

@@ -92,6 +92,7 @@ struct Plan {
     size_t smem = 0;       // epoch kernel shared memory per CTA (the generic kernel)
     size_t smem_bin = 0;   // the binary-flow kernel's (when bin; of the pair when pair)
     bool pair = false;     // the solve path runs two replicas per CTA set (binary-flow kernel)
+    bool pipe = false;     // the solve path runs the pipelined binary-flow epoch
     int act = 0;           // clique-flow moves with facilities 0..act-1 active (0 = off)
     int os_chunk = 0;      // > 0: the one-shot rule (swaps per force-update chunk)
     int os_xcol = 0;       // one-shot: peers push the force-matrix columns of the proposals

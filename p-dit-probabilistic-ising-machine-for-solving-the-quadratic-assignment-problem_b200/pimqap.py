@@ -60,6 +60,7 @@ class Params(C.Structure):
         ("update_rule", C.c_int32),
         ("replica_pairing", C.c_int32),
         ("launch_mode", C.c_int32),
+        ("sweep_pipeline", C.c_int32),
     ]
 
 

@@ -97,6 +97,18 @@ CASES = {
                             {"replica_pairing": 2, "threads_per_block": 64}),
     "clique92_n256_pair": (lambda: instances.clique_flow(35), 2, 3, 1, 0.002, 1.5, 3,
                            {"active_facilities": 92, "replica_pairing": 2}),
+    # the pipelined binary-flow epoch (sweep_pipeline = 2): an update's deltas computed while the
+    # previous update picks, then corrected for its swap; hot ladders put many swaps with the
+    # next location as partner (every delta recomputed) into a run
+    "grid_n256_pipe": (lambda: instances.grid256(17), 1, 4, 2, 0.0015, 1.5, 3, {"sweep_pipeline": 2}),
+    "grid_n256_pipe_cluster4": (lambda: instances.grid256(27), 1, 2, 1, 0.0015, 1.5, 2,
+                                {"sweep_pipeline": 2, "cluster_size": 4}),
+    "binary_n90_pipe_groups": (lambda: binary(90, 32), 2, 3, 2, 0.01, 1.4, 4, {"sweep_pipeline": 2}),
+    "binary_n37_pipe_hot": (lambda: binary(37, 33), 1, 4, 3, 0.0005, 1.3, 12, {"sweep_pipeline": 2}),
+    "binary_n200_pipe_cluster2": (lambda: binary(200, 34, 30000), 1, 2, 1, 0.0001, 1.5, 2,
+                                  {"sweep_pipeline": 2, "cluster_size": 2}),
+    "binary_n5_pipe": (lambda: binary(5, 45), 2, 3, 4, 0.05, 1.3, 10, {"sweep_pipeline": 2}),
+    "binary_n1_pipe": (lambda: binary(1, 46), 1, 2, 2, 0.05, 1.3, 3, {"sweep_pipeline": 2}),
     # the heavy-tailed workload unscaled (lognormal flows, 70 % zeros, Euclidean distances),
     # full 4-sweep epochs at n = 100, 180 and 256 on the heavy ladder (2^-13 internal), int32 and
     # int64 force matrices, clusters of 1, 2 and 4
@@ -245,14 +257,15 @@ HEADLINE_B0 = 2.0 ** -5
 HEADLINE_RATIO = 1.0671404006768237
 
 
-@pytest.mark.parametrize("pairing", [1, 2])
-def test_headline_configuration_matches_oracle(gpu, oracle, pairing):
-    """pairing 1: one replica per 2-CTA cluster; 2: two replicas per 4-CTA cluster."""
+@pytest.mark.parametrize("pairing,pipeline", [(1, 1), (2, 1), (1, 2)])
+def test_headline_configuration_matches_oracle(gpu, oracle, pairing, pipeline):
+    """pairing 1: one replica per 2-CTA cluster; 2: two replicas per 4-CTA cluster.
+    pipeline 2: the pipelined binary-flow epoch."""
     inst = instances.grid256(1000)
     M = 50
     p = gpu.default_params(replicas=64, groups=1, sweeps_per_exchange=4, beta_max=HEADLINE_B0,
                            beta_ratio=HEADLINE_RATIO, beta_internal=1, seed=1, max_megaiters=2 ** 31 - 1,
-                           megaiters_per_launch=25, replica_pairing=pairing)
+                           megaiters_per_launch=25, replica_pairing=pairing, sweep_pipeline=pipeline)
     with gpu.Solver(inst.F, inst.D, p) as s:
         s.run(25)
         s.run(25)
@@ -277,6 +290,18 @@ def test_pairing_takes_the_same_trajectory(gpu):
         r = gpu.solve(inst.F, inst.D, p)
         out.append((r["best_energy"], r["accepts"], r["best_perm"].tobytes()))
     assert out[0] == out[1] == out[2]
+
+
+def test_pipeline_is_rejected_where_it_cannot_run(gpu):
+    inst = instances.uniform(40, 80)                 # not 0/1 flows: no binary-flow kernel
+    p = gpu.default_params(replicas=4, groups=1, beta_max=0.02, max_megaiters=1, sweep_pipeline=2)
+    with pytest.raises(gpu.PimqapError) as e:
+        gpu.solve(inst.F, inst.D, p)
+    assert e.value.status == 1 and "sweep_pipeline" in str(e.value)
+    g = instances.grid256(81)
+    p = gpu.default_params(replicas=2, groups=1, beta_max=0.002, max_megaiters=1, sweep_pipeline=2, launch_mode=2)
+    with pytest.raises(gpu.PimqapError):
+        gpu.solve(g.F, g.D, p)
 
 
 def test_pairing_is_rejected_where_it_cannot_run(gpu):
