@@ -283,7 +283,8 @@ def run_ours(args):
                   beta_ratio=W["ratio"], beta_internal=1, seed=1 + rank, device=local,
                   cluster_size=args.cluster_size, threads_per_block=args.threads,
                   active_facilities=W["act"], update_rule=rule, replica_pairing=args.pairing,
-                  launch_mode=args.launch_mode, sweep_pipeline=args.pipeline)
+                  launch_mode=args.launch_mode, sweep_pipeline=args.pipeline,
+                  tensor_update=args.tensor_update)
     params = pimqap.default_params(megaiters_per_launch=MPS, max_megaiters=2 ** 31 - 1, **common)
     flush = torch.empty(L2_FLUSH_BYTES, dtype=torch.uint8, device=f"cuda:{local}")
     solver = pimqap.Solver(inst.F, inst.D, params)
@@ -379,6 +380,7 @@ def run_ours(args):
             "config": dict(workload_config(args.workload, args.update_rule, world, args.steps, args.groups),
                            cluster_size=r1["cluster_size"], force_bits=r1["force_bits"],
                            replica_pairing=args.pairing, sweep_pipeline=args.pipeline,
+                           tensor_update=args.tensor_update,
                            launch="one persistent launch per step" if persistent else
                                   "a CUDA graph of one launch per mega-iteration",
                            l2="flushed between steps (256 MiB write)"),
@@ -734,6 +736,9 @@ def main():
                          "reference's -t; its CPU arm runs one group per host thread)")
     ap.add_argument("--pipeline", type=int, default=0, choices=[0, 1, 2],
                     help="binary-flow kernel: 2 = the pipelined epoch (next update's deltas during the pick)")
+    ap.add_argument("--tensor-update", type=int, default=0, choices=[0, 1, 2, 3],
+                    help="one-shot rule's force update: 0 = automatic, 1 = integer CUDA cores, "
+                         "2 = mma.sync, 3 = tcgen05 (tensor memory)")
     ap.add_argument("--launch-mode", type=int, default=0, choices=[0, 1, 2],
                     help="0 = automatic (persistent when resident), 1 = a launch per mega-iteration, 2 = persistent")
     ap.add_argument("--update-rule", choices=["sequential", "one-shot"], default="sequential",

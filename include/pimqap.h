@@ -129,6 +129,15 @@ typedef struct pimqap_params {
                                     deltas against the state before the pick's swap and then
                                     correct them for it).  Same results either way; with
                                     launch_mode 0 / 1, one replica per CTA set, no clique moves */
+    int32_t tensor_update;       /* the one-shot rule's force update: 0 = automatic (tcgen05
+                                    where exact and it fits, else mma.sync where exact, else
+                                    the integer CUDA cores), 1 = integer CUDA cores, 2 = the
+                                    legacy tensor-core path (mma.sync m16n8k16), 3 = tcgen05
+                                    (fp16 factors in shared memory, the step's sums in tensor
+                                    memory; at most 128 rows per CTA and n <= 256).  2 and 3
+                                    need factors fp16 holds exactly (2 dD or dD, and dF, at
+                                    most 2048 in magnitude) and n |dD| |dF| < 2^24; the same
+                                    integer results in every form.  One-shot rule only */
 } pimqap_params;
 
 #define PIMQAP_RULE_SEQUENTIAL 0

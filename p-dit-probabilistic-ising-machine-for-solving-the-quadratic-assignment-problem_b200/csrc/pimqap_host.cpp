@@ -327,6 +327,11 @@ pimqap_status check_params(const pimqap_instance *inst, const pimqap_params *p) 
     if (p->launch_mode < 0 || p->launch_mode > 2)
         return fail(PIMQAP_ERR_ARG, "launch_mode must be 0 (automatic), 1 (a launch per mega-iteration) or "
                                     "2 (one persistent launch)");
+    if (p->tensor_update < 0 || p->tensor_update > 3)
+        return fail(PIMQAP_ERR_ARG, "tensor_update must be 0 (automatic), 1 (integer CUDA cores), 2 (mma.sync) "
+                                    "or 3 (tcgen05)");
+    if (p->tensor_update >= 2 && p->update_rule != PIMQAP_RULE_ONE_SHOT)
+        return fail(PIMQAP_ERR_ARG, "tensor_update 2 / 3 applies to the one-shot rule only");
     return PIMQAP_OK;
 }
 
@@ -378,29 +383,63 @@ pimqap_status plan_instance(const pimqap_instance *inst, const pimqap_params *pa
         // in magnitude: 2 dD for symmetric instances, dD otherwise, and dF) and no fp32 sum can
         // reach 2^24 (n / 2 swaps x 2 terms x |dD| |dF|)
         const int64_t dr = info.dmax - info.dmin, fr = info.fmax - info.fmin;
-        const bool mma = (info.symmetric ? 2 * dr : dr) <= 2048 && fr <= 2048 &&
-                         (int64_t)n * dr * fr < (int64_t)1 << 24 && params->compact_instance == 0;
-        P.os_mma = mma;
+        const bool exact = (info.symmetric ? 2 * dr : dr) <= 2048 && fr <= 2048 &&
+                           (int64_t)n * dr * fr < (int64_t)1 << 24 && params->compact_instance == 0;
+        const int want = params->tensor_update;              // 0 auto, 1 CUDA cores, 2 mma.sync, 3 tcgen05
+        if (want >= 2 && !exact)
+            return fail(PIMQAP_ERR_ARG, "tensor_update 2 / 3 needs an instance whose force-update factors fp16 "
+                                        "holds exactly (2 dD or dD, and dF, at most 2048 in magnitude) with "
+                                        "n |dD| |dF| below 2^24");
+        // tcgen05 (M = 128 rows per CTA, N <= 256 columns, four TMEM lane quarters read by
+        // warps 0-3 mod 4): at most 128 rows per CTA, n <= 256, a multiple of 128 threads
+        const int thr = params->threads_per_block;
+        auto os_mode = [&](int cl) {
+            if (!exact || want == 1) return 0;
+            const bool tc_ok = rows_per_cta(cl) <= 128 && n <= 256 && (thr == 0 || thr % 128 == 0);
+            if (want == 3) return tc_ok ? 2 : -1;
+            if (want == 2) return 1;
+            return tc_ok ? 2 : 1;
+        };
         for (int cl : {1, 2, 4}) {
             if (want_cluster && cl != want_cluster) continue;
+            const int mode = os_mode(cl);
+            if (mode < 0) continue;
             for (int xcol = (cl > 1 ? 1 : 0); xcol >= 0 && !P.cl; --xcol)
                 for (int pc : {32, 16, 8, 4}) {
                     const size_t sm = pimqap::epoch_smem_bytes_os(n, rows_per_cta(cl), P.lds, cl, P.bits, pc,
-                                                                  P.sym, xcol != 0, mma);
+                                                                  P.sym, xcol != 0, mode);
                     if (sm <= maxsm) {
                         P.cl = cl;
                         P.os_chunk = pc;
                         P.os_xcol = xcol;
+                        P.os_mma = mode;
                         P.smem = sm;
                         break;
                     }
                 }
             if (P.cl) break;
         }
+        if (!P.cl && want == 3)
+            return fail(PIMQAP_ERR_ARG, "tensor_update 3 (tcgen05) needs at most 128 rows per CTA, n <= 256 and a "
+                                        "multiple of 128 threads per block");
         if (!P.cl) return fail(PIMQAP_ERR_ARG, "force matrix does not fit the requested cluster size");
         P.rpc = rows_per_cta(P.cl);
         P.ldm = std::max(P.npad, P.cl * P.rpc);
         if (!params->threads_per_block) P.threads = P.rpc > 64 ? 512 : (P.rpc > 32 ? 256 : 128);
+        if (P.os_mma == 2) {
+            // Each CTA of the tcgen05 form holds `tcols` of its SM's 512 tensor-memory columns
+            // from start to end, and its allocation waits while they are taken; a CTA of a
+            // cluster waiting there for a CTA whose peer waits the same way elsewhere would wait
+            // for good.  So the shared-memory request is raised until at most 512 / tcols CTAs
+            // fit on one SM, and no allocation ever waits.
+            int dev = 0, smpm = 0, resv = 0;
+            PQ_CUDA(cudaGetDevice(&dev));
+            PQ_CUDA(cudaDeviceGetAttribute(&smpm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev));
+            PQ_CUDA(cudaDeviceGetAttribute(&resv, cudaDevAttrReservedSharedMemoryPerBlock, dev));
+            const int allowed = 512 / pimqap::os_tmem_columns(n);
+            if (smpm / ((int)P.smem + resv) > allowed)
+                P.smem = (size_t)round_up(smpm / (allowed + 1) - resv + 16, 16);   // allowed + 1 do not fit
+        }
     }
     if (!P.os_chunk) {
     P.cl = 0;

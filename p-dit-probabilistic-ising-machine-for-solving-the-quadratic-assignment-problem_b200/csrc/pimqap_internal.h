@@ -84,8 +84,10 @@ struct SolveDev {
                                //      many swaps (0: sequential sweeps)
     int32_t os_xcol;           // one-shot with a cluster: peers push the force-matrix columns
                                //      the proposals need (0: the proposals read them remotely)
-    int32_t os_mma;            // one-shot: the force update on the tensor cores (exact for this
-                               //      instance: small factors, sums below 2^24)
+    int32_t os_mma;            // one-shot: the force update on the integer CUDA cores (0), on the
+                               //      tensor cores by mma.sync (1) or by tcgen05 with the sums in
+                               //      tensor memory (2); 1 and 2 only where exact for this
+                               //      instance (small factors, sums below 2^24)
     const double *replay_r;    // [sweeps][n] the uniform r of every update, given by the caller
                                //      (pimqap_sweep_replay); nullptr: drawn from the Philox stream
     // The persistent solve (one launch runs many mega-iterations; solve_kernel):
@@ -199,9 +201,12 @@ size_t epoch_smem_bytes(int n, int rpc, int lds, int cluster, int bits);
 size_t epoch_smem_bytes_bin(int n, int rpc, int lds, int cluster);
 // Shared memory of the paired binary-flow epoch kernel (two replicas per CTA set).
 size_t epoch_smem_bytes_bin_pair(int n, int rpc, int lds, int cluster);
-// Shared memory of the one-shot epoch kernel (force update in chunks of `chunk` swaps).
+// Shared memory of the one-shot epoch kernel (force update in chunks of `chunk` swaps; mma:
+// 0 integer CUDA cores, 1 mma.sync, 2 tcgen05, as SolveDev::os_mma).
 size_t epoch_smem_bytes_os(int n, int rpc, int lds, int cluster, int bits, int chunk, bool sym, bool xcol,
-                           bool mma);
+                           int mma);
+// Tensor-memory columns one CTA of the tcgen05 one-shot epoch holds for its whole life.
+int os_tmem_columns(int n);
 
 // Resident clusters (CTAs for cl == 1) of the paired binary-flow epoch on the whole device.
 cudaError_t pair_occupancy(int cl, int threads, size_t smem, int *clusters);

@@ -1940,6 +1940,15 @@ __device__ bool replica_epoch_pipe(const SolveDev &s, int rep, int rank, int e, 
 constexpr int kMmaK = 64;
 constexpr int kMmaLd = 72;
 
+// The tcgen05 form stages the same 64 factor columns as fp16 core matrices (below): A holds
+// 128 rows (the MMA's M; rows past the CTA's are never read back), B the columns rounded up
+// to 16 (the MMA's N); one 8-row (8-column) group of 64 factor columns is 1024 bytes.
+constexpr int kTcGroupBytes = kMmaK / 8 * 128;
+constexpr int kTcABytes = 128 / 8 * kTcGroupBytes;
+
+// os_mma values of SolveDev (the one-shot force update)
+constexpr int kOsCudaCores = 0, kOsMmaSync = 1, kOsTcgen05 = 2;
+
 // Shared-memory layout of the one-shot epoch (replica_epoch_os).
 //   I       rpc rows of the force matrix; odd row stride lds, so 32 lanes reading one column
 //           of 32 rows hit 32 banks
@@ -1957,14 +1966,19 @@ constexpr int kMmaLd = 72;
 //           this CTA's rows (row stride rpc), V[p][c] = F[c][b] - F[c][a] (row stride 256, zero
 //           beyond n); asymmetric instances use U = D[k][j] - D[k][i] and add
 //           U2 = D[j][k] - D[i][k], V2 = F[b][c] - F[a][c].  They share T's space: they are
-//           live only between a step's proposals and its column exchange
+//           live only between a step's proposals and its column exchange.  The tensor-core
+//           forms stage their fp16 factors in the same space (mma.sync: rows of kMmaLd
+//           halves; tcgen05: core matrices, A then B)
 //   part    [CL] every CTA's share of sum_k I[k][phi(k)], then [kMaxWarpsOs] warp sums
 //   misc    [kMaxWarpsOs] warp counts of the pair compaction, [8] flags
+//   tc      (tcgen05) the mbarrier the MMAs complete on, the tensor-memory address
 struct OsLayout {
-    size_t I, phi, inv, bphi, Dd, Fd, diag, tgt, dlt, own, pair, uni, T, U, V, U2, V2, part, misc, total;
-    int tld;   // row stride of T (elements)
+    size_t I, phi, inv, bphi, Dd, Fd, diag, tgt, dlt, own, pair, uni, T, U, V, U2, V2, part, misc, tc, total;
+    int tld;    // row stride of T (elements)
+    int tcn;    // tcgen05: the MMA's N (columns rounded up to 16)
+    int tcols;  // tcgen05: tensor-memory columns allocated (a power of two, at least 32)
     __host__ __device__ OsLayout(int n, int rpc, int lds, int cluster, int isz, int pc, bool sym, bool xcol,
-                                 bool mma = false) {
+                                 int mma = kOsCudaCores) {
         const size_t npad = (size_t)((n + 3) & ~3), rp = (size_t)rpc, vld = 256;
         size_t o = 0;
         I = o;    o = align16(o + rp * lds * isz);
@@ -1987,19 +2001,28 @@ struct OsLayout {
         U2 = align16(V + (size_t)pc * vld * isz);
         V2 = align16(U2 + (sym ? 0 : (size_t)pc * rp * isz));
         size_t fend = align16(V2 + (sym ? 0 : (size_t)pc * vld * isz));
-        if (mma) {   // the tensor-core factors (fp16) share the same space
+        tcn = (n + 15) & ~15;
+        tcols = 32;
+        while (tcols < tcn) tcols *= 2;
+        if (mma == kOsMmaSync) {   // the tensor-core factors (fp16) share the same space
             const size_t mend = align16(U + (size_t)((rpc + 15) & ~15) * kMmaLd * 2 + (size_t)((n + 7) & ~7) * kMmaLd * 2);
+            fend = mend > fend ? mend : fend;
+        } else if (mma == kOsTcgen05) {
+            const size_t mend = align16(U + (size_t)kTcABytes + (size_t)(tcn / 8) * kTcGroupBytes);
             fend = mend > fend ? mend : fend;
         }
         o = align16(fend > o + tbytes ? fend : o + tbytes);
         part = o; o = align16(o + (size_t)(cluster + kMaxWarpsOs) * 8);
         misc = o; o = align16(o + (kMaxWarpsOs + 8) * sizeof(int));
+        tc = o;   o = align16(o + (mma == kOsTcgen05 ? 16 : 0));
         total = o;
     }
 };
 
+int os_tmem_columns(int n) { return OsLayout(n, 4, 5, 1, 4, 4, true, false, kOsTcgen05).tcols; }
+
 size_t epoch_smem_bytes_os(int n, int rpc, int lds, int cluster, int bits, int chunk, bool sym, bool xcol,
-                           bool mma) {
+                           int mma) {
     return OsLayout(n, rpc, lds, cluster, bits / 8, chunk, sym, xcol, mma).total;
 }
 
@@ -2010,6 +2033,86 @@ __device__ __forceinline__ void mma_16816(float d[4], const uint32_t a[4], const
         "{%8, %9}, {%0, %1, %2, %3};"
         : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
         : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b[0]), "r"(b[1]));
+}
+
+// ---- tcgen05: the 5th-generation tensor cores.  Operands in shared memory, named by matrix
+// descriptors; fp32 accumulators in tensor memory (TMEM: 128 lanes x 512 columns of 32 bits
+// per SM, lane m = row m of an M = 128 product); one thread issues, an mbarrier reports the
+// completion.
+
+// Shared-memory matrix descriptor of an fp16 operand stored MN-major without swizzle: core
+// matrices of 8 K-rows x 16 bytes (8 consecutive M or N entries), 128 contiguous bytes each;
+// kstride = bytes between core matrices adjacent in K (the leading byte offset), mnstride =
+// bytes between core matrices adjacent in M / N (the stride byte offset).  Bits: start
+// address >> 4 [0, 14), leading offset >> 4 [16, 30), stride offset >> 4 [32, 46), descriptor
+// version 1 [46, 48), base offset 0, layout type 0 (no swizzle) [61, 64).
+__device__ __forceinline__ uint64_t umma_desc_mn(uint32_t saddr, uint32_t kstride, uint32_t mnstride) {
+    return (uint64_t)((saddr >> 4) & 0x3FFFu) | ((uint64_t)((kstride >> 4) & 0x3FFFu) << 16) |
+           ((uint64_t)((mnstride >> 4) & 0x3FFFu) << 32) | ((uint64_t)1 << 46);
+}
+
+// Instruction descriptor of tcgen05.mma kind::f16 with fp16 A and B, both MN-major, and an
+// fp32 accumulator, M x N: D format [4, 6) = 1 (f32), A / B format [7, 10) / [10, 13) = 0
+// (f16), A / B major [15] / [16] = 1 (MN), N >> 3 [17, 23), M >> 4 [24, 29).
+__host__ __device__ constexpr uint32_t umma_idesc_f16_mn(int M, int N) {
+    return (1u << 4) | (1u << 15) | (1u << 16) | ((uint32_t)(N >> 3) << 17) | ((uint32_t)(M >> 4) << 24);
+}
+
+// Allocation of ncols tensor-memory columns (a power of two >= 32) by one whole warp; the
+// address is written to shared memory at dst.
+__device__ __forceinline__ void tmem_alloc(uint32_t dst, uint32_t ncols) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(dst), "r"(ncols)
+                 : "memory");
+}
+__device__ __forceinline__ void tmem_dealloc(uint32_t taddr, uint32_t ncols) {
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(taddr), "r"(ncols) : "memory");
+}
+// Orders this thread's tcgen05 operations before (after) a following (preceding) barrier.
+__device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+// Makes this thread's shared-memory stores visible to the tensor cores' (async-proxy) reads.
+__device__ __forceinline__ void fence_async_smem() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+
+// D (TMEM) = A B (+ D when accumulate), M x N x 16, one thread.
+__device__ __forceinline__ void umma_f16(uint32_t dtmem, uint64_t adesc, uint64_t bdesc, uint32_t idesc,
+                                         bool accumulate) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}"
+        ::"r"(dtmem), "l"(adesc), "l"(bdesc), "r"(idesc), "r"((uint32_t)accumulate)
+        : "memory");
+}
+// The mbarrier at bar gets one arrival when every tcgen05.mma this thread issued has completed.
+__device__ __forceinline__ void umma_commit(uint32_t bar) {
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar)
+                 : "memory");
+}
+// 16 consecutive 32-bit columns of the warp's 32 TMEM lanes (thread t: lane base + t); the
+// values are valid after tmem_wait_ld.
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, uint32_t (&v)[16]) {
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, "
+        "%13, %14, %15}, [%16];"
+        : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]),
+          "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15])
+        : "r"(taddr));
+}
+__device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
+
+// Eight int32 differences hi - lo (times `scale`) as eight fp16 in one 16-byte word (exact for
+// integers of at most 2048 in magnitude).
+__device__ __forceinline__ uint4 pack_half8(const int4 &h0, const int4 &l0, const int4 &h1, const int4 &l1,
+                                            int scale) {
+    const __half2 a = __halves2half2(__int2half_rn(scale * (h0.x - l0.x)), __int2half_rn(scale * (h0.y - l0.y)));
+    const __half2 b = __halves2half2(__int2half_rn(scale * (h0.z - l0.z)), __int2half_rn(scale * (h0.w - l0.w)));
+    const __half2 c = __halves2half2(__int2half_rn(scale * (h1.x - l1.x)), __int2half_rn(scale * (h1.y - l1.y)));
+    const __half2 d = __halves2half2(__int2half_rn(scale * (h1.z - l1.z)), __int2half_rn(scale * (h1.w - l1.w)));
+    uint4 r;
+    r.x = *reinterpret_cast<const uint32_t *>(&a);
+    r.y = *reinterpret_cast<const uint32_t *>(&b);
+    r.z = *reinterpret_cast<const uint32_t *>(&c);
+    r.w = *reinterpret_cast<const uint32_t *>(&d);
+    return r;
 }
 
 // Loads of this CTA's shared memory by 32-bit shared address.
@@ -2133,8 +2236,9 @@ __device__ bool replica_epoch_os(const SolveDev &s, int rep, int rank, int e, co
     const int npad = (n + 3) & ~3, vld = 256;           // V rows: every lane's 8 columns
     const int K = (n + 31) >> 5;                             // partners per lane (<= 8)
     const bool xcol = CL > 1 && s.os_xcol != 0;
-    const bool mma = s.os_mma != 0;
-    const OsLayout L(n, rpc, lds, CL, (int)sizeof(IT), pc, SYM, xcol, mma);
+    const bool tc = s.os_mma == kOsTcgen05;
+    const bool mma = s.os_mma == kOsMmaSync;
+    const OsLayout L(n, rpc, lds, CL, (int)sizeof(IT), pc, SYM, xcol, tc ? kOsTcgen05 : (mma ? kOsMmaSync : kOsCudaCores));
     const int tld = L.tld;
     IT *sI = reinterpret_cast<IT *>(smem + L.I);
     int32_t *s_phi = reinterpret_cast<int32_t *>(smem + L.phi);
@@ -2183,7 +2287,25 @@ __device__ bool replica_epoch_os(const SolveDev &s, int rep, int rank, int e, co
             s_Fd[q] = q < n ? __ldcg(s.Fdiag + q) : 0;
         }
     }
+    // tcgen05: the step's force-update sums live in L.tcols tensor-memory columns (warp 0
+    // allocates them; the CTA is alone on its SM, so the allocation does not wait), and the
+    // MMAs complete on one mbarrier
+    const uint32_t tc_bar = smem_u32(smem + L.tc);
+    uint32_t tmem = 0, tc_phase = 0;
+    bool tc_dead = false;                                    // a wait for the MMAs gave up
+    if (tc) {
+        if (warp == 0) tmem_alloc(smem_u32(smem + L.tc + 8), (uint32_t)L.tcols);
+        if (tid == 0) {
+            mbar_init(tc_bar, 1);
+            mbar_fence_init();
+        }
+        tc_fence_before();
+    }
     G.sync();
+    if (tc) {
+        tc_fence_after();
+        tmem = *reinterpret_cast<volatile uint32_t *>(smem + L.tc + 8);
+    }
     for (int q = tid; q < n; q += BT) s_inv[s_phi[q]] = q;
 
     // shared::cluster addresses of every CTA's rows and cluster-wide arrays
@@ -2397,7 +2519,92 @@ __device__ bool replica_epoch_os(const SolveDev &s, int rep, int rank, int e, co
             }
 
             // ---- 3. force update of this CTA's rows (qap.cu:1337-1412)
-            if (mma) {
+            if (tc) {
+                // dI = U V^T on the tcgen05 tensor cores: the factors of up to 64 factor columns
+                // (swaps, or two columns per swap for asymmetric instances) are staged as fp16
+                // MN-major core matrices, A = U over 128 rows (this CTA's, the rest unread), B = V
+                // over the columns rounded up to 16; thread 0 issues one M = 128, N = L.tcn,
+                // K = 16 MMA per 16 factor columns; the fp32 sums of the whole step accumulate in
+                // tensor memory and are added to the rows once.  Exact: every factor is an
+                // integer of at most 2048 in magnitude and every sum stays below 2^24 (the host
+                // checks both), so fp16 holds the factors and fp32 the sums.
+                const uint32_t aS = smem_u32(smem + L.U), bS = aS + (uint32_t)kTcABytes;
+                const int kpp = SYM ? 1 : 2, spc = kMmaK / kpp;
+                const int ga = (rows + 7) >> 3, gb = (n + 7) >> 3;   // 8-row / 8-column groups
+                const uint32_t idesc = umma_idesc_f16_mn(128, L.tcn);
+                for (int c0 = 0; c0 < np && !tc_dead; c0 += spc) {
+                    const int cn = min(spc, np - c0), kc = cn * kpp, kc16 = (kc + 15) & ~15;
+                    // factor column kk of group g: 16 bytes at g * kTcGroupBytes + (kk / 8) * 128 +
+                    // (kk % 8) * 16; consecutive threads take consecutive columns, so their
+                    // 16-byte stores fill whole core matrices (no bank conflicts).  Column 2p
+                    // (or p): D[k][j] - D[k][i] = DT[j][k] - DT[i][k] (doubled when symmetric) and
+                    // F[c][b] - F[c][a] = FT[b][c] - FT[a][c]; column 2p + 1: D[j][k] - D[i][k]
+                    // and F[b][c] - F[a][c].  Rows are read in 16-byte pieces up to rpc (D) and
+                    // npad (F), within the zero-padded ldm.
+                    for (int idx = tid; idx < (ga + gb) * kc; idx += BT) {
+                        const int grp = idx / kc, kk = idx - grp * kc;
+                        const int p = c0 + kk / kpp, part = SYM ? 0 : (kk & 1);
+                        const bool isA = grp < ga;
+                        const int gg = isA ? grp : grp - ga;
+                        const int x = isA ? s_pi[p] : s_pa[p], y = isA ? s_pj[p] : s_pb[p];
+                        const int32_t *M = isA ? (part ? s.D : s.DT) : (part ? s.F : s.FT);
+                        const int off = (isA ? row0 : 0) + 8 * gg, lim = isA ? rpc : npad;
+                        const int4 *hp = reinterpret_cast<const int4 *>(M + (size_t)y * ldm + off);
+                        const int4 *lp = reinterpret_cast<const int4 *>(M + (size_t)x * ldm + off);
+                        const int4 z = make_int4(0, 0, 0, 0);
+                        const int4 h0 = __ldg(hp), l0 = __ldg(lp);
+                        const bool two = 8 * gg + 4 < lim;
+                        const int4 h1 = two ? __ldg(hp + 1) : z, l1 = two ? __ldg(lp + 1) : z;
+                        const uint4 w = pack_half8(h0, l0, h1, l1, (SYM && isA) ? 2 : 1);
+                        *reinterpret_cast<uint4 *>(smem + L.U + (isA ? 0 : kTcABytes) + (size_t)gg * kTcGroupBytes +
+                                                   (kk >> 3) * 128 + (kk & 7) * 16) = w;
+                    }
+                    // zero factor columns kc..kc16-1, which the last K = 16 step reads
+                    for (int idx = tid; idx < (ga + gb) * (kc16 - kc); idx += BT) {
+                        const int grp = idx / (kc16 - kc), kk = kc + idx - grp * (kc16 - kc);
+                        const bool isA = grp < ga;
+                        const int gg = isA ? grp : grp - ga;
+                        *reinterpret_cast<uint4 *>(smem + L.U + (isA ? 0 : kTcABytes) + (size_t)gg * kTcGroupBytes +
+                                                   (kk >> 3) * 128 + (kk & 7) * 16) = make_uint4(0u, 0u, 0u, 0u);
+                    }
+                    fence_async_smem();
+                    G.sync();                                // the chunk's factors are staged
+                    if (tid == 0) {
+                        tc_fence_after();
+                        for (int ks = 0; ks < kc16 / 16; ++ks)
+                            umma_f16(tmem, umma_desc_mn(aS + 256u * ks, 128u, kTcGroupBytes),
+                                     umma_desc_mn(bS + 256u * ks, 128u, kTcGroupBytes), idesc, c0 > 0 || ks > 0);
+                        umma_commit(tc_bar);
+                    }
+                    // the MMAs have read the factors (the next chunk may restage them) and their
+                    // sums are in tensor memory
+                    const bool gave_up = !mbar_wait_bounded(tc_bar, tc_phase, kWaitLimitNs);
+                    tc_phase ^= 1u;
+                    if (G.sync_or(gave_up)) {
+                        if (tid == 0) atomicOr(s.error, kErrTimeout);
+                        tc_dead = true;
+                    }
+                }
+                if (!tc_dead) {
+                    // warp w reads TMEM lanes 32 (w % 4) .. + 31 (rows), 16 columns at a time, the
+                    // column blocks spread over the warps of each lane quarter
+                    tc_fence_after();
+                    const int quad = warp & 3, r = 32 * quad + lane;
+                    for (int cb = warp >> 2; 16 * cb < L.tcn; cb += nwarps >> 2) {
+                        uint32_t v[16];
+                        tmem_ld16(tmem + ((uint32_t)(32 * quad) << 16) + (uint32_t)(16 * cb), v);
+                        tmem_wait_ld();
+                        if (r < rows) {
+                            IT *dst = sI + (size_t)r * lds + 16 * cb;
+#pragma unroll
+                            for (int t = 0; t < 16; ++t)
+                                if (16 * cb + t < n) dst[t] = (IT)((U)dst[t] + (U)(IT)__float2int_rn(__uint_as_float(v[t])));
+                        }
+                    }
+                    tc_fence_before();                       // before the next step's MMAs overwrite
+                }
+                G.sync();
+            } else if (mma) {
                 // dI = U^T V on the tensor cores (m16n8k16, fp16 in, fp32 sums): the factors are
                 // integers of at most 2048 in magnitude and every sum stays below 2^24 (the host
                 // checks both), so the products and sums are exact; added to the rows once
@@ -2624,6 +2831,15 @@ __device__ bool replica_epoch_os(const SolveDev &s, int rep, int rank, int e, co
 
     // ---- store the replica
     cluster_sync<CL>(G);   // no CTA reads another's shared memory any more
+    if (tc) {   // every tensor-memory read has completed (tcgen05.wait::ld, fence, barrier)
+        if (warp == 0) {
+            // after a wait that gave up, one more bounded wait for the MMAs still in flight
+            if (tc_dead) mbar_wait_bounded(tc_bar, tc_phase ^ 1u, kWaitLimitNs);
+            tc_fence_after();
+            tmem_dealloc(tmem, (uint32_t)L.tcols);
+        }
+        if (tid == 0) mbar_inval(tc_bar);
+    }
     {
         IT *gI = reinterpret_cast<IT *>(s.I) + ((size_t)rep * n + row0) * s.ldg;
         const int nvg = s.ldg / VEC;

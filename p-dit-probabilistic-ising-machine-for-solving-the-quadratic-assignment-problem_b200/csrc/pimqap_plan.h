@@ -96,7 +96,7 @@ struct Plan {
     int act = 0;           // clique-flow moves with facilities 0..act-1 active (0 = off)
     int os_chunk = 0;      // > 0: the one-shot rule (swaps per force-update chunk)
     int os_xcol = 0;       // one-shot: peers push the force-matrix columns of the proposals
-    int os_mma = 0;        // one-shot: force update on the tensor cores
+    int os_mma = 0;        // one-shot: force update on CUDA cores (0), mma.sync (1), tcgen05 (2)
     size_t head = 0, tail = 0, total = 0;
     int64_t h2d_bytes = 0;
 };

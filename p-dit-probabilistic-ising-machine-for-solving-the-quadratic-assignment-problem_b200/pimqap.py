@@ -61,6 +61,7 @@ class Params(C.Structure):
         ("replica_pairing", C.c_int32),
         ("launch_mode", C.c_int32),
         ("sweep_pipeline", C.c_int32),
+        ("tensor_update", C.c_int32),
     ]
 
 

@@ -43,8 +43,9 @@ CASES = {
 }
 
 
-def run_case(gpu, oracle, name, seed=7):
+def run_case(gpu, oracle, name, seed=7, more=None):
     make, T, R, spe, bmax, ratio, M, extra = CASES[name]
+    extra = dict(extra, **(more or {}))
     inst = make()
     cap = max(R, 10)
     p = gpu.default_params(replicas=R, groups=T, sweeps_per_exchange=spe, beta_max=bmax,
@@ -72,6 +73,63 @@ def test_oneshot_trajectory_matches_oracle(gpu, oracle, name):
         assert st.accepts > 0
     if name == "goal_print_events":
         assert any(e["kind"] == gpu.EVENT_GOAL_PRINT for e in events)
+
+
+# the force update on the integer CUDA cores (1), by mma.sync (2) and by tcgen05 with the sums in
+# tensor memory (3): symmetric and asymmetric (two factor columns per swap), clusters of 1, 2
+# and 4 (rows per CTA 256 / 2, 250 / 4 ragged), N = 16 .. 256, steps of many swaps (hot ladders)
+FORM_CASES = ["plain_n32_R16", "groups_T3_R5_i4", "asym_signed_n18", "grid_n256_cluster2",
+              "n250_cluster4_ragged", "asym_n70_cluster2", "binary_n90", "n5_tiny", "hot_collisions",
+              "n1_trivial", "n200", "cold_forced_swaps"]
+
+
+@pytest.mark.parametrize("form", [1, 2, 3])
+@pytest.mark.parametrize("name", FORM_CASES)
+def test_force_update_forms_match_oracle(gpu, oracle, name, form):
+    inst, st, bad, res, _ = run_case(gpu, oracle, name, more={"tensor_update": form})
+    assert not bad, bad[:10]
+    assert res["accepts"] == st.accepts
+    assert res["best_energy"] == min(int(st.bestE.min()), st.single_best)
+
+
+def test_tcgen05_form_rejected_where_inexact_or_unshaped(gpu):
+    big = instances.uniform(30, 9)   # flows scaled past 2048: fp16 cannot hold every factor
+    F = np.ascontiguousarray(big.F * 40)
+    p = gpu.default_params(replicas=2, groups=1, beta_max=0.00001, max_megaiters=1,
+                           update_rule=gpu.RULE_ONE_SHOT, tensor_update=3)
+    with pytest.raises(gpu.PimqapError) as e:
+        gpu.solve(F, big.D, p)
+    assert "tensor_update" in str(e.value)
+    p.tensor_update = 2
+    with pytest.raises(gpu.PimqapError):
+        gpu.solve(F, big.D, p)
+    p.tensor_update = 0                # automatic: the integer CUDA cores
+    assert gpu.solve(F, big.D, p)["megaiters_done"] == 1
+    inst = instances.uniform(40, 23)
+    p = gpu.default_params(replicas=2, groups=1, beta_max=0.02, max_megaiters=1,
+                           update_rule=gpu.RULE_ONE_SHOT, tensor_update=3, threads_per_block=64)
+    with pytest.raises(gpu.PimqapError) as e:
+        gpu.solve(inst.F, inst.D, p)
+    assert "tcgen05" in str(e.value)
+    # automatic: the same instance and shape run (on mma.sync)
+    p.tensor_update = 0
+    assert gpu.solve(inst.F, inst.D, p)["megaiters_done"] == 1
+
+
+def test_tcgen05_many_small_ctas_per_sm(gpu, oracle):
+    """n = 24 (32 tensor-memory columns per CTA), 64 groups x 16 replicas: 1024 single-CTA
+    replicas of 128 threads, several per SM, each holding tensor memory for its whole epoch."""
+    inst = instances.uniform(24, 41)
+    T, R, spe, M = 64, 16, 1, 3
+    p = gpu.default_params(replicas=R, groups=T, sweeps_per_exchange=spe, beta_max=10.0,
+                           beta_ratio=1.5849, seed=3, max_megaiters=M, update_rule=gpu.RULE_ONE_SHOT,
+                           tensor_update=3)
+    with gpu.Solver(inst.F, inst.D, p) as s:
+        s.run(M)
+        st = oracle_after(oracle, inst.F, inst.D, T=T, R=R, spe=spe, beta_max=10.0, beta_ratio=1.5849,
+                          seed=3, cap=max(R, 10), megaiters=M, rule=1)
+        bad = compare_solver_to_oracle(s, st, max(R, 10))
+    assert not bad, bad[:10]
 
 
 def test_oneshot_shapes(gpu, oracle):
