@@ -721,6 +721,79 @@ def run_divergence_suite(args):
     print(json.dumps(out))
 
 
+def run_oneshot_divergence_suite(args):
+    """Decision divergence of the one-shot rule between the solver's kernel and GPU-CUPIM's own
+    kernels (perl-gpu/src/lib/qap/qap.cu:1462-1600, built from the reference source into
+    oracle/_ref/libref_cupim.so with its cuRANDDx generator replaced by one that copies the
+    solver's thresholds), for both of the solver's weight functions: CUDA's exp2f as the
+    reference writes it (oneshot_weights 0, the default) and the library's own 2^x
+    (oneshot_weights 1, the one the oracle restates).  Headline instance;
+    64 groups of one replica each (rank_slots 1: no exchange moves a beta), so the reference's
+    pool of 64 replicas takes exactly the solver's steps; a cold, a middle and a hot beta.  Every
+    --div-chunk mega-iterations (4 steps each) the permutation and energy of every replica are
+    compared; on a mismatch the divergence is counted and the reference's pool is reset to the
+    solver's permutations (its force matrices recomputed from them) and the run goes on.
+    Reports the proposals compared and the divergences seen."""
+    import tempfile
+    import pimqap
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    from oracle import CupimRef, Oracle
+    orc = Oracle()
+    ref = CupimRef()
+    inst = instances.grid256(1000)
+    G, spe = REPLICAS, SWEEPS_PER_EXCHANGE
+    betas = {"cold": BETA_MAX, "middle": BETA_MAX / 8, "hot": BETA_MAX / 64}
+    out = {"suite": "divergence", "update_rule": "one-shot",
+           "workload": "grid256 n=256, 64 groups of one replica (no exchange), 4 steps per mega-iteration",
+           "reference": "GPU-CUPIM os_* kernels built from the reference source (oracle/_ref/libref_cupim.so)",
+           "chunk_megaiters": args.div_chunk, "betas": {}}
+    t_start = time.perf_counter()
+    with tempfile.TemporaryDirectory() as tmp:
+        path = os.path.join(tmp, "grid256.dat")
+        instances.write_instance(path, inst)
+        for (wname, weights), (name, beta) in [(w, b) for w in (("cuda_exp2f", 0), ("own_exp2", 1))
+                                                for b in betas.items()]:
+            seed = 7
+            p = pimqap.default_params(replicas=1, groups=G, rank_slots=1, sweeps_per_exchange=spe,
+                                      beta_max=beta, beta_ratio=1.5, beta_internal=1, seed=seed,
+                                      max_megaiters=2 ** 31 - 1, megaiters_per_launch=args.div_chunk,
+                                      update_rule=pimqap.RULE_ONE_SHOT, goal=-(1 << 62),
+                                      oneshot_weights=weights)
+            bvec = np.full(G, np.float32(beta), np.float32)
+            done, divergences, first, swaps_seen = 0, 0, [], 0
+            ref.open(path, G)
+            try:
+                with pimqap.Solver(inst.F, inst.D, p) as s:
+                    phi = np.stack([s.replica(g, 0, force=False)["phi"] for g in range(G)]).astype(np.int32)
+                    ref.set(phi, bvec)
+                    step = 0
+                    while done < args.div_updates:
+                        s.run(args.div_chunk)
+                        for _ in range(args.div_chunk * spe):
+                            ref.step(orc.oneshot_uniforms(seed, G, 1, step, N))
+                            step += 1
+                        cphi, _, cscore, _ = ref.get(force=False)
+                        mine = [s.replica(g, 0, force=False) for g in range(G)]
+                        sphi = np.stack([r["phi"] for r in mine])
+                        swaps_seen += int(np.count_nonzero(sphi != phi))
+                        bad = [g for g in range(G) if not np.array_equal(mine[g]["phi"], cphi[g])
+                               or mine[g]["E"] != int(cscore[g])]
+                        done += G * args.div_chunk * spe * N
+                        if bad:
+                            divergences += 1
+                            first.append({"step_chunk_end": step, "groups": bad[:8]})
+                            ref.set(sphi, bvec)
+                        phi = sphi
+            finally:
+                ref.close()
+            out["betas"][f"{wname}/{name}"] = {"beta_internal": beta, "oneshot_weights": weights, "proposals_compared": done, "divergent_chunks": divergences,
+                                  "first": first[:10], "locations_moved_per_chunk":
+                                  swaps_seen / max(1, done // (G * args.div_chunk * spe * N)),
+                                  "rate_upper_95": 3.0 / done if divergences == 0 else None}
+    out["wall_s"] = time.perf_counter() - t_start
+    print(json.dumps(out))
+
+
 def main():
     ap = argparse.ArgumentParser(description=__doc__.split("\n")[0])
     ap.add_argument("--gpus", type=int, default=1)
@@ -749,7 +822,8 @@ def main():
                     help="replicas per CTA set of the binary-flow kernel: 0 = automatic, 1, 2")
     ap.add_argument("--suite", choices=["headline", "batch", "heavy", "serve", "divergence"], default="headline",
                     help="headline: the n=256 workload (the driver's line); batch / serve: the other "
-                         "workloads; divergence: GPU vs oracle decisions over a long stream")
+                         "workloads; divergence: GPU vs oracle decisions over a long stream (with "
+                         "--update-rule one-shot: GPU vs the reference's own one-shot kernels)")
     ap.add_argument("--div-updates", type=int, default=10_000_000,
                     help="divergence suite: updates compared per ladder")
     ap.add_argument("--div-chunk", type=int, default=10, help="divergence suite: mega-iterations per comparison")
@@ -782,7 +856,10 @@ def main():
         run_serve_suite(args)
         return
     if args.suite == "divergence":
-        run_divergence_suite(args)
+        if args.update_rule == "one-shot":
+            run_oneshot_divergence_suite(args)
+        else:
+            run_divergence_suite(args)
         return
     if args.impl == "reference":
         run_reference(args)

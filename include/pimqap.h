@@ -138,6 +138,13 @@ typedef struct pimqap_params {
                                     need factors fp16 holds exactly (2 dD or dD, and dF, at
                                     most 2048 in magnitude) and n |dD| |dF| < 2^24; the same
                                     integer results in every form.  One-shot rule only */
+    int32_t oneshot_weights;     /* the one-shot rule's binary32 2^x: 0 = CUDA's exp2f, the
+                                    function GPU-CUPIM's proposals call (qap.cu:1083-1086),
+                                    written as the reference writes it, so a step takes the
+                                    reference kernels' decisions; 1 = this library's own 2^x
+                                    (Cody-Waite reduction, degree-7 polynomial, under 1 ulp),
+                                    which the CPU oracle restates bit for bit.  One-shot rule
+                                    only */
 } pimqap_params;
 
 #define PIMQAP_RULE_SEQUENTIAL 0

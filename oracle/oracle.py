@@ -21,6 +21,7 @@ REF_DIR = os.path.join(HERE, "_ref")
 _i32p = np.ctypeslib.ndpointer(np.int32, flags="C_CONTIGUOUS")
 _i64p = np.ctypeslib.ndpointer(np.int64, flags="C_CONTIGUOUS")
 _f64p = np.ctypeslib.ndpointer(np.float64, flags="C_CONTIGUOUS")
+_f32p = np.ctypeslib.ndpointer(np.float32, flags="C_CONTIGUOUS")
 _u32p = np.ctypeslib.ndpointer(np.uint32, flags="C_CONTIGUOUS")
 
 NO_BEST = 2147483647
@@ -111,6 +112,7 @@ class Oracle:
         L.orc_exp2f_neg.restype = C.c_float
         L.orc_oneshot_uniform.argtypes = [C.c_uint32]
         L.orc_oneshot_uniform.restype = C.c_float
+        L.orc_oneshot_uniforms.argtypes = [C.c_uint64, C.c_int, C.c_int, C.c_uint32, C.c_int, _f32p]
         L.orc_oneshot_pick.argtypes = [C.c_int, _i64p, C.c_float, C.c_float, _i64p]
         L.orc_oneshot_pick.restype = C.c_int
         L.orc_oneshot_step.argtypes = [C.c_int, _i32p, _i32p, _i64p, _i32p, _i32p, _i64p, _i64p,
@@ -200,6 +202,12 @@ class Oracle:
 
     def oneshot_uniform(self, w0: int) -> float:
         return float(self.lib.orc_oneshot_uniform(w0))
+
+    def oneshot_uniforms(self, seed: int, count: int, R: int, step: int, n: int) -> np.ndarray:
+        """[count, n] thresholds of one step; replica k is replica k % R of group k // R."""
+        out = np.zeros((count, n), np.float32)
+        self.lib.orc_oneshot_uniforms(seed, count, R, step, n, out)
+        return out
 
     def oneshot_pick(self, d: np.ndarray, beta_f: float, u: float):
         """(target, delta) of one proposal from the deltas d of every partner location."""
@@ -312,3 +320,59 @@ class RefHarness:
 
     def single_best(self) -> int:
         return int(self.lib.ref_single_best())
+
+
+class CupimRef:
+    """GPU-CUPIM's own one-shot step (perl-gpu/src/lib/qap/qap.cu:1462-1600) built by
+    oracle/build_cupim.sh into _ref/libref_cupim.so and driven through oracle/cupim_harness.cu:
+    one pool of R replicas (float betas, int32 force matrices) whose step consumes the
+    thresholds the caller uploads.  Needs a GPU; one pool per process at a time."""
+
+    def __init__(self, path: Optional[str] = None):
+        path = path or os.path.join(REF_DIR, "libref_cupim.so")
+        if not os.path.exists(path):
+            raise FileNotFoundError(f"{path} not built (needs the reference source; run make -C oracle)")
+        L = self.lib = C.CDLL(path)
+        L.cupim_open.argtypes = [C.c_char_p, C.c_int]
+        L.cupim_set.argtypes = [_i32p, _f32p]
+        L.cupim_step.argtypes = [_f32p]
+        L.cupim_get.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
+        for f in (L.cupim_open, L.cupim_set, L.cupim_step, L.cupim_get, L.cupim_close):
+            f.restype = C.c_int
+        self.n = self.R = 0
+
+    @staticmethod
+    def _ok(rc: int, what: str) -> None:
+        if rc != 0:
+            raise RuntimeError(f"{what} failed: {rc}")
+
+    def open(self, path: str, R: int) -> None:
+        """A pool of R replicas on the instance file at path (n, then F, then D)."""
+        self._ok(self.lib.cupim_open(path.encode(), R), "cupim_open")
+        with open(path) as f:
+            self.n = int(f.readline().split()[0])
+        self.R = R
+
+    def set(self, phi: np.ndarray, betas: np.ndarray) -> None:
+        """Every replica's permutation [R, n] and beta (binary32); the reference recomputes the
+        force matrices and energies."""
+        self._ok(self.lib.cupim_set(np.ascontiguousarray(phi, np.int32), np.ascontiguousarray(betas, np.float32)),
+                 "cupim_set")
+
+    def step(self, u: np.ndarray) -> None:
+        """One step of every replica with the thresholds u [R, n]."""
+        self._ok(self.lib.cupim_step(np.ascontiguousarray(u, np.float32)), "cupim_step")
+
+    def get(self, force: bool = True):
+        """(phi [R, n], force [R, n, n] or None, energy [R], resolved proposals [R, n])."""
+        R, n = self.R, self.n
+        phi = np.zeros((R, n), np.int32)
+        frc = np.zeros((R, n, n), np.int32) if force else None
+        score = np.zeros(R, np.int32)
+        tg = np.zeros((R, n), np.int32)
+        self._ok(self.lib.cupim_get(phi.ctypes.data, frc.ctypes.data if force else None, score.ctypes.data,
+                                    tg.ctypes.data), "cupim_get")
+        return phi, frc, score, tg
+
+    def close(self) -> None:
+        self._ok(self.lib.cupim_close(), "cupim_close")

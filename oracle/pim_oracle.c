@@ -370,6 +370,13 @@ float orc_oneshot_uniform(uint32_t w0) {
     return (float)(((w0 >> 9) << 1) | 1u) * 0x1p-24f;
 }
 
+void orc_oneshot_uniforms(uint64_t seed, int count, int R, uint32_t step, int n, float *out) {
+    for (int k = 0; k < count; ++k)
+        for (int i = 0; i < n; ++i)
+            out[(size_t)k * n + i] = orc_oneshot_uniform(
+                orc_sweep_word(seed, (uint32_t)(k / R), (uint32_t)(k % R), step, (uint32_t)i, 0));
+}
+
 /* The proposal of one location (GPU-CUPIM qap.cu:1040-1146, os_pwc_d): deltas d[j] of every
    partner location j, weights 2^(beta (d[j] - max)) in binary32 with no cutoff, summed in the
    reference's warp order (lane t holds j = t, t+32, ...: a running sum per lane, then an

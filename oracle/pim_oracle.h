@@ -130,6 +130,9 @@ typedef struct orc_run_state {
    targets (optional, n entries) receives every location's proposal. */
 float orc_exp2f_neg(float x);
 float orc_oneshot_uniform(uint32_t w0);
+/* The thresholds of one step of `count` replicas, replica k being replica k % R of group k / R:
+   out[k][i] = orc_oneshot_uniform(word 0 of (group, replica, step, location i)). */
+void orc_oneshot_uniforms(uint64_t seed, int count, int R, uint32_t step, int n, float *out);
 int orc_oneshot_pick(int n, const int64_t *d, float beta_f, float u, int64_t *delta_out);
 int orc_oneshot_step(int n, const int32_t *D, const int32_t *F, int64_t *I, int32_t *phi,
                      int32_t *phiinv, int64_t *E, int64_t *bestE, double beta, uint64_t seed,

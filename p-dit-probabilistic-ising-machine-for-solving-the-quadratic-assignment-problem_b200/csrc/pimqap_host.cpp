@@ -332,6 +332,9 @@ pimqap_status check_params(const pimqap_instance *inst, const pimqap_params *p) 
                                     "or 3 (tcgen05)");
     if (p->tensor_update >= 2 && p->update_rule != PIMQAP_RULE_ONE_SHOT)
         return fail(PIMQAP_ERR_ARG, "tensor_update 2 / 3 applies to the one-shot rule only");
+    if (p->oneshot_weights < 0 || p->oneshot_weights > 1)
+        return fail(PIMQAP_ERR_ARG, "oneshot_weights must be 0 (CUDA's exp2f, as the reference) or 1 (this "
+                                    "library's own 2^x)");
     return PIMQAP_OK;
 }
 
@@ -374,6 +377,7 @@ pimqap_status plan_instance(const pimqap_instance *inst, const pimqap_params *pa
                                           : (n <= 64 ? 64 : (n <= 128 ? 128 : 256));
     auto rows_per_cta = [&](int cl) { return round_up((n + cl - 1) / cl, 4); };
     if (params->update_rule == PIMQAP_RULE_ONE_SHOT) {
+        P.os_own_exp2 = params->oneshot_weights == 1;
         // the one-shot epoch: odd row stride (column reads by 32 lanes hit 32 banks), the
         // smallest cluster that holds its rows with a force-update chunk of 32, 16, 8 or 4 swaps,
         // preferring the layout whose peers push the columns the proposals need
@@ -520,6 +524,7 @@ void carve_instance(const Plan &P, char *head, char *tail, SolveDev *out) {
     d.os_chunk = P.os_chunk;
     d.os_xcol = P.os_xcol;
     d.os_mma = P.os_mma;
+    d.os_own_exp2 = P.os_own_exp2;
     d.ldg = P.npad; d.lds = P.lds; d.ldm = P.ldm; d.rpc = P.rpc;
     char *cur = head;
     d.D = carve<int32_t>(cur, nn);

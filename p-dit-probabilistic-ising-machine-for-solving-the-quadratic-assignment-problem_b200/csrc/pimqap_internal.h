@@ -88,6 +88,8 @@ struct SolveDev {
                                //      tensor cores by mma.sync (1) or by tcgen05 with the sums in
                                //      tensor memory (2); 1 and 2 only where exact for this
                                //      instance (small factors, sums below 2^24)
+    int32_t os_own_exp2;       // one-shot: the weights by this library's own 2^x (exp2f_neg: the
+                               //      oracle's function) instead of CUDA's exp2f (the reference's)
     const double *replay_r;    // [sweeps][n] the uniform r of every update, given by the caller
                                //      (pimqap_sweep_replay); nullptr: drawn from the Philox stream
     // The persistent solve (one launch runs many mega-iterations; solve_kernel):

@@ -2212,7 +2212,8 @@ __device__ __forceinline__ void stage_factors(int tid, int BT, int cn, int nq, c
 // split by rows over the cluster as in the sequential epoch.  Per step:
 //   1. proposals: one warp per location i of this CTA; lane t evaluates partners j = t + 32k
 //      (the reference's lane layout), reading column phi(i) of the other CTAs' rows through
-//      distributed shared memory; binary32 weights 2^(beta (d - max)) with the exact exp2f_neg,
+//      distributed shared memory; binary32 weights 2^(beta (d - max)) by CUDA's exp2f as the
+//      reference computes them, or by this library's exp2f_neg (which the oracle restates),
 //      the reference's per-lane running sums and 32-lane scan, the threshold pick; the lane
 //      that owns location i stores the proposal into every CTA; cluster barrier;
 //   2. every CTA resolves all n proposals (shared-memory atomicMin on ballot words, same
@@ -2237,6 +2238,7 @@ __device__ bool replica_epoch_os(const SolveDev &s, int rep, int rank, int e, co
     const int K = (n + 31) >> 5;                             // partners per lane (<= 8)
     const bool xcol = CL > 1 && s.os_xcol != 0;
     const bool tc = s.os_mma == kOsTcgen05;
+    const bool own_exp2 = s.os_own_exp2 != 0;
     const bool mma = s.os_mma == kOsMmaSync;
     const OsLayout L(n, rpc, lds, CL, (int)sizeof(IT), pc, SYM, xcol, tc ? kOsTcgen05 : (mma ? kOsMmaSync : kOsCudaCores));
     const int tld = L.tld;
@@ -2419,7 +2421,12 @@ __device__ bool replica_epoch_os(const SolveDev &s, int rep, int rank, int e, co
                 if (k < K) {
                     const int j = lane + 32 * k;
                     float w = 0.0f;
-                    if (j < n) w = exp2f_neg(__fmul_rn(beta_f, __ll2float_rn((long long)d[k] - (long long)mx)));
+                    if (j < n) {
+                        const float x = __ll2float_rn((long long)d[k] - (long long)mx);
+                        // CUDA's exp2f as the reference writes it (exp2(beta * float(d - max)),
+                        // qap.cu:1083-1086), or this library's own 2^x, which the oracle restates
+                        w = own_exp2 ? exp2f_neg(__fmul_rn(beta_f, x)) : exp2f(beta_f * x);
+                    }
                     run = (k == 0) ? w : __fadd_rn(w, run);
                     sacc[k] = run;
                 }

@@ -62,6 +62,7 @@ class Params(C.Structure):
         ("launch_mode", C.c_int32),
         ("sweep_pipeline", C.c_int32),
         ("tensor_update", C.c_int32),
+        ("oneshot_weights", C.c_int32),
     ]
 
 

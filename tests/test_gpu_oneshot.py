@@ -2,9 +2,11 @@
 solver through its C ABI against the oracle restatement (orc_oneshot_step).
 
 Everything is bit-exact: permutations, force matrices, energies, bests, betas, rank slots,
-accept counts.  The proposals' binary32 weights come from the same exp2 on both sides (checked
-bit for bit below), and every other floating-point step is a single IEEE operation in the
-same order, so the proposals agree exactly (tolerance: zero mismatches).
+accept counts.  The solver runs with oneshot_weights = 1, the library's own binary32 2^x,
+which the oracle restates (checked bit for bit below); every other floating-point step is a
+single IEEE operation in the same order, so the proposals agree exactly (tolerance: zero
+mismatches).  The default weights (CUDA's exp2f, as the reference computes them) are compared
+with the reference's own kernels in tests/test_gpu_cupim_pin.py.
 """
 import numpy as np
 import pytest
@@ -50,7 +52,7 @@ def run_case(gpu, oracle, name, seed=7, more=None):
     cap = max(R, 10)
     p = gpu.default_params(replicas=R, groups=T, sweeps_per_exchange=spe, beta_max=bmax,
                            beta_ratio=ratio, seed=seed, max_megaiters=M, megaiters_per_launch=7,
-                           update_rule=gpu.RULE_ONE_SHOT, **extra)
+                           update_rule=gpu.RULE_ONE_SHOT, oneshot_weights=1, **extra)
     with gpu.Solver(inst.F, inst.D, p) as s:
         s.run(M)
         st = oracle_after(oracle, inst.F, inst.D, T=T, R=R, spe=spe, beta_max=bmax,
@@ -123,7 +125,7 @@ def test_tcgen05_many_small_ctas_per_sm(gpu, oracle):
     T, R, spe, M = 64, 16, 1, 3
     p = gpu.default_params(replicas=R, groups=T, sweeps_per_exchange=spe, beta_max=10.0,
                            beta_ratio=1.5849, seed=3, max_megaiters=M, update_rule=gpu.RULE_ONE_SHOT,
-                           tensor_update=3)
+                           tensor_update=3, oneshot_weights=1)
     with gpu.Solver(inst.F, inst.D, p) as s:
         s.run(M)
         st = oracle_after(oracle, inst.F, inst.D, T=T, R=R, spe=spe, beta_max=10.0, beta_ratio=1.5849,

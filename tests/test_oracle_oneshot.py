@@ -203,3 +203,24 @@ def test_run_rule_one_improves(oracle):
             I_ref, E_ref = oracle.force_init(np.ascontiguousarray(inst.D, np.int32),
                                              np.ascontiguousarray(inst.F, np.int32), st.phi[t, l])
             assert np.array_equal(st.I[t, l], I_ref) and st.E[t, l] == E_ref
+
+
+def test_oneshot_uniforms_match_the_per_word_draws(oracle):
+    u = oracle.oneshot_uniforms(123, 6, 3, 5, 7)
+    ref = [[oracle.oneshot_uniform(oracle.lib.orc_sweep_word(123, k // 3, k % 3, 5, i, 0)) for i in range(7)]
+           for k in range(6)]
+    assert np.array_equal(u, np.array(ref, np.float32))
+
+
+def test_reference_oneshot_harness_loads():
+    """GPU-CUPIM's one-shot step as built by oracle/build_cupim.sh (the pin of the one-shot
+    oracle, tests/test_gpu_cupim_pin.py, runs it on a GPU): it loads without a GPU and exports
+    the harness's entry points."""
+    import os
+    from oracle import REF_DIR, CupimRef
+    path = os.path.join(REF_DIR, "libref_cupim.so")
+    if not os.path.exists(path):
+        pytest.skip("libref_cupim.so not built (the reference source was absent at build time)")
+    ref = CupimRef(path)
+    for name in ("cupim_open", "cupim_set", "cupim_step", "cupim_get", "cupim_close"):
+        assert hasattr(ref.lib, name)
