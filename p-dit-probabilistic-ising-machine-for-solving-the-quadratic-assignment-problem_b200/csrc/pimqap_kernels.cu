@@ -209,6 +209,42 @@ template <> __device__ __forceinline__ int32_t warp_max<int32_t>(int32_t v) {
     return __reduce_max_sync(0xffffffffu, v);
 }
 
+// The largest of the nwarps (<= 32) warp maxima in s_red, all >= 0, in every thread of a warp:
+// 32-bit values by one load per lane and a warp reduction, wider ones by a loop.
+template <class IT> __device__ __forceinline__ IT block_max(const IT *s_red, int nwarps, int lane) {
+    if constexpr (sizeof(IT) == 4) {
+        return __reduce_max_sync(0xffffffffu, lane < nwarps ? s_red[lane] : (IT)0);
+    } else {
+        IT M = s_red[0];
+        for (int w = 1; w < nwarps; ++w) M = s_red[w] > M ? s_red[w] : M;
+        return M;
+    }
+}
+
+// Sum of eight doubles as a pairwise tree (three dependent adds).
+__device__ __forceinline__ double tree8(const double (&v)[8]) {
+    return __dadd_rn(__dadd_rn(__dadd_rn(v[0], v[1]), __dadd_rn(v[2], v[3])),
+                     __dadd_rn(__dadd_rn(v[4], v[5]), __dadd_rn(v[6], v[7])));
+}
+
+// The weight total of an update from the nwarps (<= 8) per-warp totals in s_wsum, and the
+// part of it before warp `warp`: independent loads summed as pairwise trees instead of a chain
+// of dependent adds (adding the zeros past nwarps is exact).  The weights are double sums in
+// an order of this kernel's choosing either way; the reference sums them in sequence in long
+// double (CPU_PIM.cpp:240-245), so a decision can differ from it only where r * total falls
+// within a few ulp of a prefix boundary, whatever the order.
+__device__ __forceinline__ void weight_totals(const double *s_wsum, int nwarps, int warp, double &base,
+                                              double &total) {
+    double v[8], b[8];
+#pragma unroll
+    for (int w = 0; w < 8; ++w) {
+        v[w] = w < nwarps ? s_wsum[w] : 0.0;
+        b[w] = w < warp ? v[w] : 0.0;
+    }
+    total = tree8(v);
+    base = tree8(b);
+}
+
 // ---- shared::cluster addressing, mbarriers, asynchronous remote stores, async copies
 
 __device__ __forceinline__ uint32_t smem_u32(const void *p) {
@@ -715,7 +751,6 @@ __device__ bool replica_epoch(const SolveDev &s, int rep, int rank, int e, const
                     const int b = b0 + k;
                     d[k] = (CL == 1) ? s_A[p * npad + b]
                                      : (IT)((U)s_A[p * npad + b] + (U)s_B[p * npad + b]);
-                    x[k] = exp2(__dmul_rn(beta, (double)d[k]));
                     lmax = d[k] > lmax ? d[k] : lmax;
                 }
             }
@@ -727,8 +762,11 @@ __device__ bool replica_epoch(const SolveDev &s, int rep, int rank, int e, const
                 break;
             }
             if (tid == 0) s_misc[0] = 0x7fffffff;
-            IT M = s_red[0];
-            for (int w = 1; w < nwarps; ++w) M = s_red[w] > M ? s_red[w] : M;
+            // the weights do not depend on the maximum: formed while it is read
+            const IT M = block_max(s_red, nwarps, lane);
+#pragma unroll
+            for (int k = 0; k < 4; ++k)
+                if (k < K && b0 + k < n) x[k] = exp2(__dmul_rn(beta, (double)d[k]));
             const long long cut = cutoff_trunc(__dsub_rn((double)M, cut_span));   // :234-235
             double pre[4];
             double local = 0.0;
@@ -747,11 +785,8 @@ __device__ bool replica_epoch(const SolveDev &s, int rep, int rank, int e, const
             if (lane == 0) excl = 0.0;
             if (lane == 31) s_wsum[warp] = incl;
             G.sync();                                 // S_scan
-            double base = 0.0, total = 0.0;
-            for (int w = 0; w < nwarps; ++w) {
-                if (w == warp) base = total;
-                total = __dadd_rn(total, s_wsum[w]);
-            }
+            double base, total;
+            weight_totals(s_wsum, nwarps, warp, base, total);
             const double target = __dmul_rn(s_r[i], total);     // :247
             const double X = __dadd_rn(base, excl);
 #pragma unroll
@@ -1257,8 +1292,6 @@ __device__ bool replica_epoch_bin(const SolveDev &s, int rep, int rank, int e, c
                 if (k < K && b0 + k < ncand) {
                     const int b = b0 + k;
                     d[k] = (CL == 1) ? s_A[p * npad + b] : (IT)((U)s_A[p * npad + b] + (U)s_B[p * npad + b]);
-                    x[k] = exp2(__dmul_rn(beta, (double)d[k]));
-                    if (inact && b == act) x[k] = __dmul_rn(x[k], (double)(n - act));   // :261-264
                     lmax = d[k] > lmax ? d[k] : lmax;
                 }
             }
@@ -1270,8 +1303,15 @@ __device__ bool replica_epoch_bin(const SolveDev &s, int rep, int rank, int e, c
                 break;
             }
             if (tid == 0) s_misc[0] = 0x7fffffff;
-            IT M = s_red[0];
-            for (int w = 1; w < nwarps; ++w) M = s_red[w] > M ? s_red[w] : M;
+            // the weights do not depend on the maximum: formed while it is read
+            const IT M = block_max(s_red, nwarps, lane);
+#pragma unroll
+            for (int k = 0; k < 4; ++k) {
+                if (k < K && b0 + k < ncand) {
+                    x[k] = exp2(__dmul_rn(beta, (double)d[k]));
+                    if (inact && b0 + k == act) x[k] = __dmul_rn(x[k], (double)(n - act));   // :261-264
+                }
+            }
             const long long cut = cutoff_trunc(__dsub_rn((double)M, cut_span));   // :234-235
             double pre[4];
             double local = 0.0;
@@ -1291,11 +1331,8 @@ __device__ bool replica_epoch_bin(const SolveDev &s, int rep, int rank, int e, c
             if (lane == 0) excl = 0.0;
             if (lane == 31) s_wsum[warp] = incl;
             G.sync();
-            double base = 0.0, total = 0.0;
-            for (int w = 0; w < nwarps; ++w) {
-                if (w == warp) base = total;
-                total = __dadd_rn(total, s_wsum[w]);
-            }
+            double base, total;
+            weight_totals(s_wsum, nwarps, warp, base, total);
             const double target = __dmul_rn(s_r[i], total);     // :247
             const double X = __dadd_rn(base, excl);
 #pragma unroll
