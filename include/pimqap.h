@@ -129,15 +129,22 @@ typedef struct pimqap_params {
                                     deltas against the state before the pick's swap and then
                                     correct them for it).  Same results either way; with
                                     launch_mode 0 / 1, one replica per CTA set, no clique moves */
-    int32_t tensor_update;       /* the one-shot rule's force update: 0 = automatic (tcgen05
-                                    where exact and it fits, else mma.sync where exact, else
-                                    the integer CUDA cores), 1 = integer CUDA cores, 2 = the
-                                    legacy tensor-core path (mma.sync m16n8k16), 3 = tcgen05
-                                    (fp16 factors in shared memory, the step's sums in tensor
-                                    memory; at most 128 rows per CTA and n <= 256).  2 and 3
-                                    need factors fp16 holds exactly (2 dD or dD, and dF, at
-                                    most 2048 in magnitude) and n |dD| |dF| < 2^24; the same
-                                    integer results in every form.  One-shot rule only */
+    int32_t tensor_update;       /* the force update on the tensor cores.  One-shot rule: 0 =
+                                    automatic (tcgen05 where exact and it fits, else mma.sync
+                                    where exact, else the integer CUDA cores), 1 = integer CUDA
+                                    cores, 2 = the legacy tensor-core path (mma.sync m16n8k16),
+                                    3 = tcgen05 (fp16 factors in shared memory, the step's sums
+                                    in tensor memory; at most 128 rows per CTA and n <= 256);
+                                    2 and 3 need factors fp16 holds exactly (2 dD or dD, and
+                                    dF, at most 2048 in magnitude) and n |dD| |dF| < 2^24.
+                                    Sequential rule (the binary-flow kernel's rewrite of its
+                                    rows every 16 accepted swaps): 0 = automatic (tcgen05 where
+                                    the distance range is at most 1024, n <= 256 and the
+                                    threads per block a multiple of 128, else binary32 FMAs on
+                                    the CUDA cores), 1 = the CUDA cores, 3 = tcgen05 (rejected
+                                    where it does not apply; the paired and pipelined epochs
+                                    keep the CUDA cores), 2 = rejected.  The same integer
+                                    results in every form */
     int32_t oneshot_weights;     /* the one-shot rule's binary32 2^x: 0 = CUDA's exp2f, the
                                     function GPU-CUPIM's proposals call (qap.cu:1083-1086),
                                     written as the reference writes it, so a step takes the

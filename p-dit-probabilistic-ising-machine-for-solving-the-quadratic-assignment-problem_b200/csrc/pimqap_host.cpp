@@ -330,8 +330,8 @@ pimqap_status check_params(const pimqap_instance *inst, const pimqap_params *p) 
     if (p->tensor_update < 0 || p->tensor_update > 3)
         return fail(PIMQAP_ERR_ARG, "tensor_update must be 0 (automatic), 1 (integer CUDA cores), 2 (mma.sync) "
                                     "or 3 (tcgen05)");
-    if (p->tensor_update >= 2 && p->update_rule != PIMQAP_RULE_ONE_SHOT)
-        return fail(PIMQAP_ERR_ARG, "tensor_update 2 / 3 applies to the one-shot rule only");
+    if (p->tensor_update == 2 && p->update_rule != PIMQAP_RULE_ONE_SHOT)
+        return fail(PIMQAP_ERR_ARG, "tensor_update 2 (mma.sync) applies to the one-shot rule only");
     if (p->oneshot_weights < 0 || p->oneshot_weights > 1)
         return fail(PIMQAP_ERR_ARG, "oneshot_weights must be 0 (CUDA's exp2f, as the reference) or 1 (this "
                                     "library's own 2^x)");
@@ -463,12 +463,44 @@ pimqap_status plan_instance(const pimqap_instance *inst, const pimqap_params *pa
     // binary flows and int16 distances: the instance itself fits next to the force rows
     if (info.symmetric && info.binary_flow && info.dist16 && P.bits == 32 && !P.os_chunk &&
         (params->compact_instance == 0 || params->active_facilities > 0)) {
-        const size_t sb = pimqap::epoch_smem_bytes_bin(n, P.rpc, P.lds, P.cl);
+        const size_t sb = pimqap::epoch_smem_bytes_bin(n, P.rpc, P.lds, P.cl, false);
         if (sb <= maxsm) {
             P.bin = true;
             P.smem_bin = sb;
         }
+        // its 16-swap rewrite of the rows on the tcgen05 tensor cores where fp16 holds every
+        // factor exactly (2 (D[k][j] - D[k][i]) at most 2048 in magnitude: a distance range of at
+        // most 1024; flow differences are -1, 0 or 1; 16 terms stay below 2^24), an M = 128 MMA
+        // covers a CTA's rows (n <= 256) and whole warp quarters read them back (a multiple of
+        // 128 threads); not with clique moves (no swap log)
+        const int want = params->tensor_update;
+        const bool tc_ok = P.bin && params->active_facilities == 0 && info.dmax - info.dmin <= 1024 &&
+                           P.rpc <= 128 && n <= 256 && P.threads % 128 == 0;
+        if (tc_ok && want != 1) {
+            size_t st = pimqap::epoch_smem_bytes_bin(n, P.rpc, P.lds, P.cl, true);
+            // each CTA holds `tcols` of its SM's 512 tensor-memory columns for its whole epoch and
+            // its allocation waits while they are taken; a CTA of a cluster waiting there for a
+            // CTA whose peer waits the same way elsewhere would wait for good.  So the shared-memory
+            // request is raised until at most 512 / tcols CTAs fit on an SM.
+            const int tcn = round_up(n, 16);
+            const int tcols = tcn <= 32 ? 32 : (tcn <= 64 ? 64 : (tcn <= 128 ? 128 : 256));
+            const int allowed = 512 / tcols;
+            int dev = 0, smpm = 0, resv = 0;
+            PQ_CUDA(cudaGetDevice(&dev));
+            PQ_CUDA(cudaDeviceGetAttribute(&smpm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev));
+            PQ_CUDA(cudaDeviceGetAttribute(&resv, cudaDevAttrReservedSharedMemoryPerBlock, dev));
+            if (smpm / ((int)st + resv) > allowed) st = (size_t)round_up(smpm / (allowed + 1) - resv + 16, 16);
+            if (st <= maxsm) {
+                P.bin_tc = true;
+                P.smem_bin = st;
+            }
+        }
     }
+    if (params->tensor_update == 3 && params->update_rule != PIMQAP_RULE_ONE_SHOT && !P.bin_tc)
+        return fail(PIMQAP_ERR_ARG, "tensor_update 3 (tcgen05) with the sequential rule needs the binary-flow "
+                                    "kernel (symmetric 0/1 flows, int16 distances, int32 forces), a distance "
+                                    "range of at most 1024, no clique moves, n <= 256, a multiple of 128 "
+                                    "threads per block and a layout that fits");
     if (params->active_facilities > 0) {   // the tai256c program's moves (CPU_PIM_tai256c.cpp)
         if (!P.bin || !info.symmetric || info.clique != params->active_facilities)
             return fail(PIMQAP_ERR_ARG, "active_facilities needs a symmetric instance whose flows are a clique of "
@@ -525,6 +557,7 @@ void carve_instance(const Plan &P, char *head, char *tail, SolveDev *out) {
     d.os_xcol = P.os_xcol;
     d.os_mma = P.os_mma;
     d.os_own_exp2 = P.os_own_exp2;
+    d.bin_tc = (P.bin_tc && !P.pair && !P.pipe) ? 1 : 0;
     d.ldg = P.npad; d.lds = P.lds; d.ldm = P.ldm; d.rpc = P.rpc;
     char *cur = head;
     d.D = carve<int32_t>(cur, nn);

@@ -88,6 +88,8 @@ struct SolveDev {
                                //      tensor cores by mma.sync (1) or by tcgen05 with the sums in
                                //      tensor memory (2); 1 and 2 only where exact for this
                                //      instance (small factors, sums below 2^24)
+    int32_t bin_tc;            // binary-flow epoch: the 16-swap rewrite of the rows on the tcgen05
+                               //      tensor cores (exact for this instance: small distance range)
     int32_t os_own_exp2;       // one-shot: the weights by this library's own 2^x (exp2f_neg: the
                                //      oracle's function) instead of CUDA's exp2f (the reference's)
     const double *replay_r;    // [sweeps][n] the uniform r of every update, given by the caller
@@ -200,7 +202,7 @@ size_t exchange_scratch_bytes();
 // Shared memory of one CTA of the epoch kernel.
 size_t epoch_smem_bytes(int n, int rpc, int lds, int cluster, int bits);
 // Shared memory of the binary-flow epoch kernel (0 / 1 flows and int16 distances resident).
-size_t epoch_smem_bytes_bin(int n, int rpc, int lds, int cluster);
+size_t epoch_smem_bytes_bin(int n, int rpc, int lds, int cluster, bool tc_rewrite);
 // Shared memory of the paired binary-flow epoch kernel (two replicas per CTA set).
 size_t epoch_smem_bytes_bin_pair(int n, int rpc, int lds, int cluster);
 // Shared memory of the one-shot epoch kernel (force update in chunks of `chunk` swaps; mma:

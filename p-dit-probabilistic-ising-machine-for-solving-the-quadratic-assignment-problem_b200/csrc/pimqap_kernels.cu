@@ -954,16 +954,100 @@ __device__ bool replica_epoch(const SolveDev &s, int rep, int rank, int e, const
     return true;
 }
 
+// ---- tcgen05: the 5th-generation tensor cores.  Operands in shared memory, named by matrix
+// descriptors; fp32 accumulators in tensor memory (TMEM: 128 lanes x 512 columns of 32 bits
+// per SM, lane m = row m of an M = 128 product); one thread issues, an mbarrier reports the
+// completion.
+
+// Shared-memory matrix descriptor of an fp16 operand stored MN-major without swizzle: core
+// matrices of 8 K-rows x 16 bytes (8 consecutive M or N entries), 128 contiguous bytes each;
+// kstride = bytes between core matrices adjacent in K (the leading byte offset), mnstride =
+// bytes between core matrices adjacent in M / N (the stride byte offset).  Bits: start
+// address >> 4 [0, 14), leading offset >> 4 [16, 30), stride offset >> 4 [32, 46), descriptor
+// version 1 [46, 48), base offset 0, layout type 0 (no swizzle) [61, 64).
+__device__ __forceinline__ uint64_t umma_desc_mn(uint32_t saddr, uint32_t kstride, uint32_t mnstride) {
+    return (uint64_t)((saddr >> 4) & 0x3FFFu) | ((uint64_t)((kstride >> 4) & 0x3FFFu) << 16) |
+           ((uint64_t)((mnstride >> 4) & 0x3FFFu) << 32) | ((uint64_t)1 << 46);
+}
+
+// Instruction descriptor of tcgen05.mma kind::f16 with fp16 A and B, both MN-major, and an
+// fp32 accumulator, M x N: D format [4, 6) = 1 (f32), A / B format [7, 10) / [10, 13) = 0
+// (f16), A / B major [15] / [16] = 1 (MN), N >> 3 [17, 23), M >> 4 [24, 29).
+__host__ __device__ constexpr uint32_t umma_idesc_f16_mn(int M, int N) {
+    return (1u << 4) | (1u << 15) | (1u << 16) | ((uint32_t)(N >> 3) << 17) | ((uint32_t)(M >> 4) << 24);
+}
+
+// Allocation of ncols tensor-memory columns (a power of two >= 32) by one whole warp; the
+// address is written to shared memory at dst.
+__device__ __forceinline__ void tmem_alloc(uint32_t dst, uint32_t ncols) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(dst), "r"(ncols)
+                 : "memory");
+}
+__device__ __forceinline__ void tmem_dealloc(uint32_t taddr, uint32_t ncols) {
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(taddr), "r"(ncols) : "memory");
+}
+// Orders this thread's tcgen05 operations before (after) a following (preceding) barrier.
+__device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+// Makes this thread's shared-memory stores visible to the tensor cores' (async-proxy) reads.
+__device__ __forceinline__ void fence_async_smem() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+
+// D (TMEM) = A B (+ D when accumulate), M x N x 16, one thread.
+__device__ __forceinline__ void umma_f16(uint32_t dtmem, uint64_t adesc, uint64_t bdesc, uint32_t idesc,
+                                         bool accumulate) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}"
+        ::"r"(dtmem), "l"(adesc), "l"(bdesc), "r"(idesc), "r"((uint32_t)accumulate)
+        : "memory");
+}
+// The mbarrier at bar gets one arrival when every tcgen05.mma this thread issued has completed.
+__device__ __forceinline__ void umma_commit(uint32_t bar) {
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar)
+                 : "memory");
+}
+// 16 consecutive 32-bit columns of the warp's 32 TMEM lanes (thread t: lane base + t); the
+// values are valid after tmem_wait_ld.
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, uint32_t (&v)[16]) {
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, "
+        "%13, %14, %15}, [%16];"
+        : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]),
+          "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15])
+        : "r"(taddr));
+}
+__device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
+
+// Eight small integers (exact in fp16) as eight fp16 in one 16-byte word, element 0 first.
+template <class T>
+__device__ __forceinline__ uint4 pack_f16x8(T a, T b, T c, T d, T e, T f, T g, T h) {
+    const __half2 h0 = __floats2half2_rn((float)a, (float)b), h1 = __floats2half2_rn((float)c, (float)d);
+    const __half2 h2 = __floats2half2_rn((float)e, (float)f), h3 = __floats2half2_rn((float)g, (float)h);
+    uint4 r;
+    memcpy(&r.x, &h0, 4);
+    memcpy(&r.y, &h1, 4);
+    memcpy(&r.z, &h2, 4);
+    memcpy(&r.w, &h3, 4);
+    return r;
+}
+
 // Shared-memory layout of the binary-flow epoch (replica_epoch_bin): the instance itself is
 // resident next to the force-matrix rows, D as int16 columns of this CTA's rows and F as bit
 // rows, so no update waits for a row from L2.
 constexpr int kBinLog = 16;   // accepted swaps the binary-flow epoch keeps before rewriting its rows
+// The staged A operand of the tensor-core rewrite: 16 groups of 8 rows x 2 core matrices of
+// 8 log entries x 8 rows x 2 bytes.
+constexpr int kBinTcA = 16 * 256;
 
 //   inst = false: the replica's own section only (no Ds / Fb), for two replicas of one
 //   instance that share one copy of the instance tables (BinPairLayout).
+//   tcr = true: the rows are rewritten on the tcgen05 tensor cores (replica_epoch_bin): the log
+//   region [LU, V8 end) also holds, once the log is full, its entries restaged as fp16 MN-major
+//   core matrices (A: 128 rows x 16 entries, 4 KB; B: columns rounded up to 16 x 16 entries,
+//   32 B per column), and `tc` holds the MMA's mbarrier and the tensor-memory address.
 struct BinLayout {
-    size_t I, phi, inv, bphi, Dd, A, B, Ds, Fb, LU, V8, red, wsum, r, misc, bar, total;
-    __host__ __device__ BinLayout(int n, int rpc, int lds, int cluster, bool inst = true) {
+    size_t I, phi, inv, bphi, Dd, A, B, Ds, Fb, LU, V8, red, wsum, r, misc, bar, tc, total;
+    __host__ __device__ BinLayout(int n, int rpc, int lds, int cluster, bool inst = true, bool tcr = false) {
         const size_t npad = (size_t)((n + 3) & ~3), rp = (size_t)rpc, nw = (size_t)((n + 31) / 32);
         const size_t ni = inst ? (size_t)n : 0;
         size_t o = 0;
@@ -978,11 +1062,16 @@ struct BinLayout {
         Fb = o;    o = align16(o + ni * nw * 4);   // bit b % 32 of Fb[a][b / 32] = F[a][b]
         LU = o;    o = align16(o + (size_t)kBinLog * rp * 4);   // LU[p][k] = 2 (D[k][j_p] - D[k][i_p])
         V8 = o;    o = align16(o + (size_t)kBinLog * npad);     // V8[p][c] = F[b_p][c] - F[a_p][c]
+        if (tcr) {   // room for the staged operands
+            const size_t staged = (size_t)kBinTcA + (size_t)((n + 15) & ~15) * 32;
+            if (o - LU < staged) o = LU + staged;
+        }
         red = o;   o = align16(o + kMaxWarps * 8);
         wsum = o;  o = align16(o + kMaxWarps * sizeof(double));
         r = o;     o = align16(o + npad * sizeof(double));   // r of each update of a sweep
         misc = o;  o = align16(o + 4 * sizeof(int));
         bar = o;   o = align16(o + 2 * sizeof(unsigned long long));
+        tc = o;    o = align16(o + (tcr ? 16 : 0));
         total = o;
     }
 };
@@ -1006,8 +1095,8 @@ struct BinPairLayout {
     }
 };
 
-size_t epoch_smem_bytes_bin(int n, int rpc, int lds, int cluster) {
-    return BinLayout(n, rpc, lds, cluster).total;
+size_t epoch_smem_bytes_bin(int n, int rpc, int lds, int cluster, bool tcr) {
+    return BinLayout(n, rpc, lds, cluster, true, tcr).total;
 }
 
 size_t epoch_smem_bytes_bin_pair(int n, int rpc, int lds, int cluster) {
@@ -1057,7 +1146,8 @@ __device__ bool replica_epoch_bin(const SolveDev &s, int rep, int rank, int e, c
     const int npad = (n + 3) & ~3;
     const int nw = (n + 31) / 32;
     const bool own_inst = Ds_shared == nullptr;
-    const BinLayout L(n, rpc, lds, CL, own_inst);
+    const bool tcr = own_inst && s.bin_tc != 0;             // rows rewritten on the tensor cores
+    const BinLayout L(n, rpc, lds, CL, own_inst, tcr);
     IT *sI = reinterpret_cast<IT *>(smem + L.I);
     int32_t *s_phi = reinterpret_cast<int32_t *>(smem + L.phi);
     int32_t *s_inv = reinterpret_cast<int32_t *>(smem + L.inv);
@@ -1075,6 +1165,12 @@ __device__ bool replica_epoch_bin(const SolveDev &s, int rep, int rank, int e, c
     int *s_misc = reinterpret_cast<int *>(smem + L.misc);   // [0] pick key, [1] improved-at
     unsigned long long *s_bar = reinterpret_cast<unsigned long long *>(smem + L.bar);
     auto fbit = [&](int a, int b) -> int { return (int)((s_Fb[a * nw + (b >> 5)] >> (b & 31)) & 1u); };
+
+    const int tcn = (n + 15) & ~15;                          // the rewrite MMA's N
+    const uint32_t tcols = tcn <= 32 ? 32u : (tcn <= 64 ? 64u : (tcn <= 128 ? 128u : 256u));
+    const uint32_t tc_bar = smem_u32(smem + L.tc);
+    uint32_t tmem = 0, tc_phase = 0;
+    bool tc_dead = false;                                    // a wait for the rewrite MMA gave up
 
     // ---- load the replica and the instance
     {
@@ -1107,7 +1203,23 @@ __device__ bool replica_epoch_bin(const SolveDev &s, int rep, int rank, int e, c
                 mbar_fence_init();
             }
         }
+        if (tcr) {
+            // the rewrite's sums live in tcols tensor-memory columns (warp 0 allocates them; the
+            // host caps the CTAs per SM at 512 / tcols, so the allocation does not wait), and
+            // its MMA completes on one mbarrier
+            __syncwarp();
+            if (warp == 0) tmem_alloc(smem_u32(smem + L.tc + 8), tcols);
+            if (tid == 0) {
+                mbar_init(tc_bar, 1);
+                mbar_fence_init();
+            }
+            tc_fence_before();
+        }
         G.sync();
+        if (tcr) {
+            tc_fence_after();
+            tmem = *reinterpret_cast<volatile uint32_t *>(smem + L.tc + 8);
+        }
     }
     for (int q = tid; q < n; q += BT) s_inv[s_phi[q]] = q;
     cluster_sync<CL>(G);
@@ -1144,7 +1256,107 @@ __device__ bool replica_epoch_bin(const SolveDev &s, int rep, int rank, int e, c
     // the rows are rewritten once for all of them.  Integer sums in any order: exact.
     const bool lazy = act == 0;
     int m = 0;                                               // pending swaps (same in all CTAs)
+    // The rewrite on the tcgen05 tensor cores (tcr): I[k][c] += sum_p LU[p][k] V8[p][c] as one
+    // M = 128, N = tcn, K = 16 MMA with fp16 operands and fp32 sums in tensor memory.  Exact:
+    // the host enables it only where |LU| <= 2048 (twice the instance's distance range at
+    // most 1024), |V8| <= 1, and 16 terms keep every sum below 2^24.  The log entries are
+    // restaged in place (every thread reads its chunks, a barrier, then writes them) as fp16
+    // MN-major core matrices without swizzle: 8 rows (or columns) x 8 entries, 16 bytes per
+    // entry, 128 bytes each; 128 bytes between the two core matrices of a group along the
+    // entries (LBO), 256 bytes between groups of 8 rows or columns (SBO).  Entries past m are
+    // zero, rows past rpc and columns past npad too.  Warp w reads back tensor-memory lanes
+    // 32 (w % 4) .. + 31 (its rows), 16 columns at a time, and adds the sums to the rows.
+    auto flush_tc = [&]() {
+        constexpr int kChunks = 6;                            // (256 + 512) chunks / 128 threads
+        const int nA = 16 * kBinLog, nB = (tcn / 8) * kBinLog;
+        uint4 v[kChunks];
+#pragma unroll
+        for (int t = 0; t < kChunks; ++t) {
+            const int c = tid + t * BT;
+            uint4 w = make_uint4(0u, 0u, 0u, 0u);
+            if (c < nA) {
+                const int p = c >> 4, g = c & 15;             // log entry, group of 8 rows
+                if (p < m && 8 * g < rpc) {
+                    const float *lu = s_LU + (size_t)p * rpc + 8 * g;
+                    const float4 f0 = *reinterpret_cast<const float4 *>(lu);
+                    const float4 f1 = (8 * g + 4 < rpc) ? *reinterpret_cast<const float4 *>(lu + 4)
+                                                        : make_float4(0.f, 0.f, 0.f, 0.f);
+                    w = pack_f16x8(f0.x, f0.y, f0.z, f0.w, f1.x, f1.y, f1.z, f1.w);
+                }
+            } else if (c < nA + nB) {
+                const int c2 = c - nA, p = c2 & 15, cg = c2 >> 4;   // log entry, group of 8 columns
+                if (p < m && 8 * cg < npad) {
+                    const int8_t *v8 = s_V8 + (size_t)p * npad + 8 * cg;
+                    const char4 b0 = *reinterpret_cast<const char4 *>(v8);
+                    const char4 b1 = (8 * cg + 4 < npad) ? *reinterpret_cast<const char4 *>(v8 + 4)
+                                                         : make_char4(0, 0, 0, 0);
+                    w = pack_f16x8(b0.x, b0.y, b0.z, b0.w, b1.x, b1.y, b1.z, b1.w);
+                }
+            }
+            v[t] = w;
+        }
+        G.sync();                                             // every log entry read
+#pragma unroll
+        for (int t = 0; t < kChunks; ++t) {
+            const int c = tid + t * BT;
+            if (c < nA) {
+                const int p = c >> 4, g = c & 15;
+                *reinterpret_cast<uint4 *>(smem + L.LU + (size_t)g * 256 + (p >> 3) * 128 + (p & 7) * 16) = v[t];
+            } else if (c < nA + nB) {
+                const int c2 = c - nA, p = c2 & 15, cg = c2 >> 4;
+                *reinterpret_cast<uint4 *>(smem + L.LU + kBinTcA + (size_t)cg * 256 + (p >> 3) * 128 + (p & 7) * 16) =
+                    v[t];
+            }
+        }
+        fence_async_smem();
+        G.sync();                                             // the operands are staged
+        if (tid == 0) {
+            tc_fence_after();
+            const uint32_t a = smem_u32(smem + L.LU);
+            umma_f16(tmem, umma_desc_mn(a, 128u, 256u), umma_desc_mn(a + kBinTcA, 128u, 256u),
+                     umma_idesc_f16_mn(128, tcn), false);
+            umma_commit(tc_bar);
+        }
+        const bool gave_up = !mbar_wait_bounded(tc_bar, tc_phase, kWaitLimitNs);
+        tc_phase ^= 1u;
+        if (G.sync_or(gave_up)) {
+            if (tid == 0) atomicOr(s.error, kErrTimeout);
+            tc_dead = true;
+            failed = true;
+            return;
+        }
+        tc_fence_after();
+        const int quad = warp & 3, r = 32 * quad + lane;
+        for (int cb = warp >> 2; 16 * cb < tcn; cb += nwarps >> 2) {
+            uint32_t acc[16];
+            tmem_ld16(tmem + ((uint32_t)(32 * quad) << 16) + (uint32_t)(16 * cb), acc);
+            tmem_wait_ld();
+            if (r < rows) {
+                IT *dst = sI + (size_t)r * lds + 16 * cb;
+                if (16 * cb + 16 <= npad) {
+#pragma unroll
+                    for (int q4 = 0; q4 < 4; ++q4) {
+                        int4 x = *reinterpret_cast<const int4 *>(dst + 4 * q4);
+                        x.x = (int)((U)x.x + (U)__float2int_rn(__uint_as_float(acc[4 * q4 + 0])));
+                        x.y = (int)((U)x.y + (U)__float2int_rn(__uint_as_float(acc[4 * q4 + 1])));
+                        x.z = (int)((U)x.z + (U)__float2int_rn(__uint_as_float(acc[4 * q4 + 2])));
+                        x.w = (int)((U)x.w + (U)__float2int_rn(__uint_as_float(acc[4 * q4 + 3])));
+                        *reinterpret_cast<int4 *>(dst + 4 * q4) = x;
+                    }
+                } else {
+#pragma unroll
+                    for (int t = 0; t < 16; ++t)
+                        if (16 * cb + t < npad) dst[t] = (IT)((U)dst[t] + (U)__float2int_rn(__uint_as_float(acc[t])));
+                }
+            }
+        }
+        tc_fence_before();                                    // before the next rewrite's MMA
+    };
     auto flush = [&]() {
+        if (tcr) {
+            flush_tc();
+            return;
+        }
         // rows in blocks of 8 consecutive rows x 4 columns per thread
         constexpr int RT = 8;
         const int ngroups = max(1, BT / nvec);               // row-block groups in flight
@@ -1392,6 +1604,7 @@ __device__ bool replica_epoch_bin(const SolveDev &s, int rep, int rank, int e, c
                     G.sync();
                     flush();
                     m = 0;
+                    if (failed) break;                       // the rewrite's MMA did not complete
                 }
                 G.sync();                                    // log, rows and phi visible
                 if (s_misc[1] == upd) {
@@ -1461,13 +1674,22 @@ __device__ bool replica_epoch_bin(const SolveDev &s, int rep, int rank, int e, c
         }
     }
 
-    if (m > 0) {   // the swaps still pending (m is the same in every thread)
+    if (m > 0 && !tc_dead) {   // the swaps still pending (m is the same in every thread)
         G.sync();
         flush();
         m = 0;
         G.sync();
     }
     cluster_sync<CL>(G);
+    if (tcr) {   // every tensor-memory read has completed (tcgen05.wait::ld, fence, barrier)
+        if (warp == 0) {
+            // after a wait that gave up, one more bounded wait for the MMA still in flight
+            if (tc_dead) mbar_wait_bounded(tc_bar, tc_phase ^ 1u, kWaitLimitNs);
+            tc_fence_after();
+            tmem_dealloc(tmem, tcols);
+        }
+        if (tid == 0) mbar_inval(tc_bar);
+    }
     if constexpr (CL > 1) {
         if (tid == 0) {
             mbar_inval(smem_u32(&s_bar[0]));
@@ -2071,70 +2293,6 @@ __device__ __forceinline__ void mma_16816(float d[4], const uint32_t a[4], const
         : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
         : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b[0]), "r"(b[1]));
 }
-
-// ---- tcgen05: the 5th-generation tensor cores.  Operands in shared memory, named by matrix
-// descriptors; fp32 accumulators in tensor memory (TMEM: 128 lanes x 512 columns of 32 bits
-// per SM, lane m = row m of an M = 128 product); one thread issues, an mbarrier reports the
-// completion.
-
-// Shared-memory matrix descriptor of an fp16 operand stored MN-major without swizzle: core
-// matrices of 8 K-rows x 16 bytes (8 consecutive M or N entries), 128 contiguous bytes each;
-// kstride = bytes between core matrices adjacent in K (the leading byte offset), mnstride =
-// bytes between core matrices adjacent in M / N (the stride byte offset).  Bits: start
-// address >> 4 [0, 14), leading offset >> 4 [16, 30), stride offset >> 4 [32, 46), descriptor
-// version 1 [46, 48), base offset 0, layout type 0 (no swizzle) [61, 64).
-__device__ __forceinline__ uint64_t umma_desc_mn(uint32_t saddr, uint32_t kstride, uint32_t mnstride) {
-    return (uint64_t)((saddr >> 4) & 0x3FFFu) | ((uint64_t)((kstride >> 4) & 0x3FFFu) << 16) |
-           ((uint64_t)((mnstride >> 4) & 0x3FFFu) << 32) | ((uint64_t)1 << 46);
-}
-
-// Instruction descriptor of tcgen05.mma kind::f16 with fp16 A and B, both MN-major, and an
-// fp32 accumulator, M x N: D format [4, 6) = 1 (f32), A / B format [7, 10) / [10, 13) = 0
-// (f16), A / B major [15] / [16] = 1 (MN), N >> 3 [17, 23), M >> 4 [24, 29).
-__host__ __device__ constexpr uint32_t umma_idesc_f16_mn(int M, int N) {
-    return (1u << 4) | (1u << 15) | (1u << 16) | ((uint32_t)(N >> 3) << 17) | ((uint32_t)(M >> 4) << 24);
-}
-
-// Allocation of ncols tensor-memory columns (a power of two >= 32) by one whole warp; the
-// address is written to shared memory at dst.
-__device__ __forceinline__ void tmem_alloc(uint32_t dst, uint32_t ncols) {
-    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(dst), "r"(ncols)
-                 : "memory");
-}
-__device__ __forceinline__ void tmem_dealloc(uint32_t taddr, uint32_t ncols) {
-    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(taddr), "r"(ncols) : "memory");
-}
-// Orders this thread's tcgen05 operations before (after) a following (preceding) barrier.
-__device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
-__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
-// Makes this thread's shared-memory stores visible to the tensor cores' (async-proxy) reads.
-__device__ __forceinline__ void fence_async_smem() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
-
-// D (TMEM) = A B (+ D when accumulate), M x N x 16, one thread.
-__device__ __forceinline__ void umma_f16(uint32_t dtmem, uint64_t adesc, uint64_t bdesc, uint32_t idesc,
-                                         bool accumulate) {
-    asm volatile(
-        "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
-        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}"
-        ::"r"(dtmem), "l"(adesc), "l"(bdesc), "r"(idesc), "r"((uint32_t)accumulate)
-        : "memory");
-}
-// The mbarrier at bar gets one arrival when every tcgen05.mma this thread issued has completed.
-__device__ __forceinline__ void umma_commit(uint32_t bar) {
-    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar)
-                 : "memory");
-}
-// 16 consecutive 32-bit columns of the warp's 32 TMEM lanes (thread t: lane base + t); the
-// values are valid after tmem_wait_ld.
-__device__ __forceinline__ void tmem_ld16(uint32_t taddr, uint32_t (&v)[16]) {
-    asm volatile(
-        "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, "
-        "%13, %14, %15}, [%16];"
-        : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]),
-          "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15])
-        : "r"(taddr));
-}
-__device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
 
 // Eight int32 differences hi - lo (times `scale`) as eight fp16 in one 16-byte word (exact for
 // integers of at most 2048 in magnitude).

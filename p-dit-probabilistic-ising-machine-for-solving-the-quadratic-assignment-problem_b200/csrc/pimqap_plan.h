@@ -98,6 +98,7 @@ struct Plan {
     int os_xcol = 0;       // one-shot: peers push the force-matrix columns of the proposals
     int os_mma = 0;        // one-shot: force update on CUDA cores (0), mma.sync (1), tcgen05 (2)
     int os_own_exp2 = 0;   // one-shot: weights by this library's 2^x (1) or CUDA's exp2f (0)
+    bool bin_tc = false;   // binary-flow epoch: the row rewrite on the tcgen05 tensor cores
     size_t head = 0, tail = 0, total = 0;
     int64_t h2d_bytes = 0;
 };

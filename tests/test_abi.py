@@ -133,7 +133,7 @@ def test_invalid_params_rejected_before_device(entry, field, value):
                                     {"threads_per_block": 32, "update_rule": 1},
                                     {"sweep_pipeline": 3}, {"sweep_pipeline": -1},
                                     {"tensor_update": 4}, {"tensor_update": -1},
-                                    {"tensor_update": 2}, {"tensor_update": 3},
+                                    {"tensor_update": 2},
                                     {"oneshot_weights": 2}, {"oneshot_weights": -1}])
 def test_invalid_combinations_rejected_before_device(entry, fields):
     inst = instances.uniform(8, 1)

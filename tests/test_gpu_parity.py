@@ -257,15 +257,17 @@ HEADLINE_B0 = 2.0 ** -5
 HEADLINE_RATIO = 1.0671404006768237
 
 
-@pytest.mark.parametrize("pairing,pipeline", [(1, 1), (2, 1), (1, 2)])
-def test_headline_configuration_matches_oracle(gpu, oracle, pairing, pipeline):
+@pytest.mark.parametrize("pairing,pipeline,tensor", [(1, 1, 0), (1, 1, 1), (2, 1, 0), (1, 2, 0)])
+def test_headline_configuration_matches_oracle(gpu, oracle, pairing, pipeline, tensor):
     """pairing 1: one replica per 2-CTA cluster; 2: two replicas per 4-CTA cluster.
-    pipeline 2: the pipelined binary-flow epoch."""
+    pipeline 2: the pipelined binary-flow epoch.  tensor 0: the rows rewritten every 16 swaps
+    on the tcgen05 tensor cores (automatic for this instance); 1: on the CUDA cores."""
     inst = instances.grid256(1000)
     M = 50
     p = gpu.default_params(replicas=64, groups=1, sweeps_per_exchange=4, beta_max=HEADLINE_B0,
                            beta_ratio=HEADLINE_RATIO, beta_internal=1, seed=1, max_megaiters=2 ** 31 - 1,
-                           megaiters_per_launch=25, replica_pairing=pairing, sweep_pipeline=pipeline)
+                           megaiters_per_launch=25, replica_pairing=pairing, sweep_pipeline=pipeline,
+                           tensor_update=tensor)
     with gpu.Solver(inst.F, inst.D, p) as s:
         s.run(25)
         s.run(25)
@@ -278,6 +280,40 @@ def test_headline_configuration_matches_oracle(gpu, oracle, pairing, pipeline):
     assert not bad, bad[:10]
     assert res["accepts"] == st.accepts
     assert res["accepts"] > 0.9 * 64 * 4 * M * 256
+
+
+# The binary-flow kernel's rewrite of its rows every 16 accepted swaps (and at the end of an
+# epoch) on the CUDA cores (1) and on the tcgen05 tensor cores (3): one CTA with 128 threads and
+# 90 ragged rows, 2- and 4-CTA clusters (128 and 64 rows per CTA), both launch modes.
+REWRITE_CASES = ["binary_n90_single_cta", "grid_n256_cluster", "grid_n256_cluster4"]
+
+
+@pytest.mark.parametrize("mode", [1, 2])
+@pytest.mark.parametrize("form", [1, 3])
+@pytest.mark.parametrize("name", REWRITE_CASES)
+def test_rewrite_forms_match_oracle(gpu, oracle, name, form, mode):
+    inst, st, bad, res = run_case(gpu, oracle, name, tensor_update=form, launch_mode=mode)
+    assert not bad, bad[:10]
+    assert res["accepts"] == st.accepts
+
+
+def test_tcgen05_rewrite_rejected_where_it_does_not_apply(gpu):
+    wide_d = binary(60, 47, 3000)                  # distance range 3000: fp16 cannot hold 2 dD
+    p = gpu.default_params(replicas=2, groups=1, beta_max=0.01, max_megaiters=1, tensor_update=3)
+    with pytest.raises(gpu.PimqapError) as e:
+        gpu.solve(wide_d.F, wide_d.D, p)
+    assert e.value.status == 1 and "tensor_update 3" in str(e.value)
+    p.tensor_update = 0                            # automatic: the CUDA cores
+    assert gpu.solve(wide_d.F, wide_d.D, p)["megaiters_done"] == 1
+    inst = instances.uniform(40, 48)               # not 0/1 flows: no binary-flow kernel
+    p.tensor_update = 3
+    with pytest.raises(gpu.PimqapError):
+        gpu.solve(inst.F, inst.D, p)
+    g = binary(64, 49)
+    p = gpu.default_params(replicas=2, groups=1, beta_max=0.01, max_megaiters=1, tensor_update=3,
+                           threads_per_block=64)   # 64 threads: not every tensor-memory lane quarter
+    with pytest.raises(gpu.PimqapError):
+        gpu.solve(g.F, g.D, p)
 
 
 def test_pairing_takes_the_same_trajectory(gpu):
