@@ -75,8 +75,6 @@ std::vector<BatchClass> plan_classes(const std::vector<Plan> &plans, const std::
         c.members.push_back(k);
         c.work += instance_work(P, megaiters[k]);
     }
-    double total = 0;
-    for (auto &c : classes) total += c.work;
     for (auto &c : classes) {
         c.nmax = 0;
         for (int k : c.members) c.nmax = std::max(c.nmax, plans[k].n);
@@ -105,7 +103,6 @@ std::vector<BatchClass> plan_classes(const std::vector<Plan> &plans, const std::
         // release when their work runs out.
         c.grid = (c.cl == 1) ? sms * occ : occ * c.cl;   // occ: resident clusters for cl > 1
     }
-    (void)total;
     std::stable_sort(classes.begin(), classes.end(),
                      [](const BatchClass &a, const BatchClass &b) { return a.work > b.work; });
     return classes;
