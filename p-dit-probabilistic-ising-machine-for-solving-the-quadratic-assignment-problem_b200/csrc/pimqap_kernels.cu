@@ -1398,6 +1398,13 @@ __device__ bool replica_epoch_bin(const SolveDev &s, int rep, int rank, int e, c
         }
     };
 
+    // Facilities kept in registers across updates, so an update's first shared-memory loads
+    // need no earlier one: a_nx = phi of the next update's location (read during an update,
+    // set for its swap; -1: read it), and, when every thread holds at most one row of the CTA
+    // (rows <= BT), bj = phi of the thread's own row, kept through every swap.
+    const bool one_row = rows <= BT;
+    int a_nx = -1;
+    int bj = (one_row && tid < rows) ? s_phi[row0 + tid] : 0;
     for (int sw = 0; sw < s.spe && !failed; ++sw) {
         const uint32_t sweep = (uint32_t)(e * s.spe + sw);
         // r of every update of this sweep (:212), one Philox block each, drawn by all threads up
@@ -1417,20 +1424,23 @@ __device__ bool replica_epoch_bin(const SolveDev &s, int rep, int rank, int e, c
             if constexpr (CL > 1) {
                 if (tid == 0) mbar_arrive_expect_tx(smem_u32(&s_bar[p]), tx_bytes);
             }
-            const int a = s_phi[i];
+            const int a = a_nx >= 0 ? a_nx : s_phi[i];
+            const int inext = i + 1 == n ? 0 : i + 1;
             // clique flows (act > 0): an inactive facility weighs the actives and one lumped
             // candidate b = act for all inactives (CPU_PIM_tai256c.cpp:236, :253-266)
             const bool inact = act > 0 && a >= act;
             const int ncand = inact ? act + 1 : n, npick = inact ? act : n;
             const int16_t *Di = s_Ds + (size_t)i * rpc;      // D[i][own rows]
-            const int owner = i / rpc;
+            int owner = 0;                                   // i / rpc without a division
+#pragma unroll
+            for (int r = 1; r < CL; ++r) owner += i >= r * rpc;
             const int Dii = s_Dd[i], Faa = fbit(a, a);
             IT Iia = 0;
             const IT *Ii = sI + (size_t)(i - owner * rpc) * lds;
             if (owner == rank) Iia = Ii[a];
             for (int jj = tid; jj < rows; jj += BT) {
                 const int j = row0 + jj;
-                const int b = s_phi[j];
+                const int b = one_row ? bj : s_phi[j];
                 const IT *Ij = sI + (size_t)jj * lds;
                 const U dd = (U)Dii + (U)s_Dd[j] - 2u * (U)(IT)Di[jj];
                 const U ff = (U)Faa + (U)fbit(b, b) - 2u * (U)fbit(a, b);
@@ -1486,6 +1496,8 @@ __device__ bool replica_epoch_bin(const SolveDev &s, int rep, int rank, int e, c
                 }
             }
 
+            // the next location's facility, unchanged unless this update's swap moves it
+            const int a_pref = s_phi[inext];
             bool timeout = false;
             if constexpr (CL == 1) {
                 G.sync();
@@ -1574,12 +1586,22 @@ __device__ bool replica_epoch_bin(const SolveDev &s, int rep, int rank, int e, c
                     if (b != a) ++accepts;                   // tid 0's count is the one stored
                 }
                 G.sync();
+                a_nx = -1;                                   // only thread 0 knows the partner
+                if (one_row && tid < rows) bj = s_phi[row0 + tid];
                 continue;
             }
-            if (bs >= n || bs == a) continue;                // no move / self move (:252)
+            if (bs >= n || bs == a) {                        // no move / self move (:252)
+                a_nx = a_pref;
+                continue;
+            }
 
             // ---- accepted swap: every row and bit row it needs is already in shared memory
             const int j = key & 511;
+            a_nx = inext == j ? a : (inext == i ? bs : a_pref);
+            if (one_row && tid < rows) {
+                if (row0 + tid == i) bj = bs;
+                else if (row0 + tid == j) bj = a;
+            }
             const IT dEsel = (CL == 1) ? s_A[p * npad + bs] : (IT)((U)s_A[p * npad + bs] + (U)s_B[p * npad + bs]);
             if (tid == 0) {                                  // :257-261
                 s_phi[i] = bs;
