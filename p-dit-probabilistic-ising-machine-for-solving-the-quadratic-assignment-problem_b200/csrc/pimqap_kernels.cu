@@ -697,7 +697,9 @@ __device__ bool replica_epoch(const SolveDev &s, int rep, int rank, int e, const
             }
 
             // ---- 1. delta halves: B from the rows this CTA owns, A from row i's owner
-            const int owner = i / rpc;
+            int owner = 0;                                   // i / rpc without a division
+#pragma unroll
+            for (int r = 1; r < CL; ++r) owner += i >= r * rpc;
             const int32_t Dii = s_Dd[i], Faa = s_Fd[a];
             IT Iia = 0;
             const IT *Ii = sI + (size_t)(i - owner * rpc) * lds;
