@@ -35,7 +35,10 @@ extern "C" int cupim_open(const char *path, int R) {
     g_host = Pool::from_file(path, (uint32_t)R, 1, 1.0f, 1.0f);
     g_n = g_host.invariants.problem_size;
     g_R = (uint32_t)R;
-    if (g_n < 1 || g_n > 256) return -2;
+    if (g_n < 1 || g_n > 256) {
+        g_host.cu_free();
+        return -2;
+    }
     // from_file leaves the layout's own permutation arrays zero-length, while cu_copy copies n
     // entries of them: give them n entries first
     delete[] g_host.invariants.facility_at_position;
@@ -47,13 +50,18 @@ extern "C" int cupim_open(const char *path, int R) {
     g_dev = g_host.cu_copy(cudaMemcpyHostToDevice);
     const size_t nq = ((size_t)g_R * g_n + 3) / 4;
     int rc = cuda_ok(cudaMalloc(&g_uni, nq * sizeof(float4)));
-    if (rc) return rc;
-    rc = cuda_ok(cudaMemset(g_uni, 0, nq * sizeof(float4)));
-    if (rc) return rc;
-    rc = cuda_ok(cudaMemcpyToSymbol(g_pin_uniforms, &g_uni, sizeof(g_uni)));
-    if (rc) return rc;
+    if (!rc) rc = cuda_ok(cudaMemset(g_uni, 0, nq * sizeof(float4)));
+    if (!rc) rc = cuda_ok(cudaMemcpyToSymbol(g_pin_uniforms, &g_uni, sizeof(g_uni)));
+    if (!rc) rc = cuda_ok(cudaDeviceSynchronize());
+    if (rc) {   // leave nothing behind: a later open starts clean
+        g_dev.cu_free();
+        g_host.cu_free();
+        cudaFree(g_uni);
+        g_uni = nullptr;
+        return rc;
+    }
     g_open = true;
-    return cuda_ok(cudaDeviceSynchronize());
+    return 0;
 }
 
 // Sets every replica's permutation (phi[r][i] = facility at location i) and beta, then lets the
